@@ -1,0 +1,100 @@
+/*
+ * pdhcg_b200.h -- additive entry points of libpdhcg_b200.so beyond the
+ * reference interface in pdhcg.h.  None of them changes a struct of
+ * pdhcg_types.h; callers that only use pdhcg.h never see them.
+ *
+ * All functions return 0 on success and a negative code on error, unless
+ * stated otherwise; a CUDA error is reported on stderr and returned, never
+ * turned into exit().
+ */
+#pragma once
+
+#include "pdhcg_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Arithmetic of the iteration. */
+typedef enum {
+    PDHCG_B200_FP64 = 0,       /* every vector and matrix value in double */
+    PDHCG_B200_MIXED = 1       /* FP32 matrix values and iterates with FP64 accumulation and FP64
+                                  residuals/restarts, then an FP64 polish phase */
+} pdhcg_b200_precision_t;
+
+typedef struct {
+    int precision;                 /* pdhcg_b200_precision_t */
+    double polish_threshold;       /* MIXED: relative KKT error at which FP64 takes over (default 1e-5) */
+    int has_initial_primal_weight; /* warm start of the primal weight (no counterpart in the reference,
+                                      which recomputes it, reference src/pdhg_core_op.cu:962-970) */
+    double initial_primal_weight;
+    int use_graphs;                /* capture the iterations between two evaluations in a CUDA graph */
+    int time_steps;                /* bracket every fused step with CUDA events (fills step_kernel_ms) */
+    int reserved[6];
+} pdhcg_b200_options_t;
+
+void pdhcg_b200_default_options(pdhcg_b200_options_t *opts);
+
+/* solve_qp_problem with options.  Same ownership and error rules. */
+pdhcg_result_t *pdhcg_b200_solve(const qp_problem_t *prob, const pdhg_parameters_t *params,
+                                 const pdhcg_b200_options_t *opts);
+
+/* Device-side statistics of the last solve on the calling thread. */
+typedef struct {
+    double setup_ms;             /* upload, transpose, rescaling, power method (CUDA events) */
+    double loop_ms;              /* main loop on the device, first to last iteration (CUDA events) */
+    double step_kernel_ms;       /* summed duration of the fused primal/dual step kernels */
+    long long step_kernel_launches;
+    long long kernel_launches;   /* all kernels launched by the solve */
+    int iterations;
+    int fp32_iterations;
+    int restarts;
+    int evaluations;
+    double step_bytes;           /* algorithmic HBM bytes of one primal + dual step */
+    double spmv_bytes;           /* algorithmic bytes of the two SpMVs inside one step */
+    double reserved[6];
+} pdhcg_b200_stats_t;
+
+int pdhcg_b200_last_stats(pdhcg_b200_stats_t *out);
+
+/* ---- kernel-level entry points on device pointers ------------------------
+ * For parity tests and embedding.  Pointers are device memory of the current
+ * device; stream may be NULL (legacy default stream).  They allocate nothing
+ * and return after enqueueing (call cudaStreamSynchronize to wait). */
+
+/* y = M x for a CSR matrix (int32 indices, FP64 values). */
+int pdhcg_b200_csr_spmv(int rows, const int *row_ptr, const int *col_ind, const double *val, const double *x,
+                        double *y, void *stream);
+
+/* Project each cone block of x (scaled space) onto {x : x_i / d_i in K} in the
+ * metric sum_i (1 + tau q_i)(x_i - r_i)^2; q may be NULL.  cone_type holds
+ * cone_type_t values. */
+int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *cone_vdim, const int *cone_type,
+                             const double *cone_alpha, double *x, const double *d, const double *q, double tau,
+                             void *stream);
+
+/* One restarted-Halpern PDHG step (primal prox with diagonal Q or none, cone
+ * projection, dual prox, reflection, Halpern averaging) on device arrays;
+ * the layout mirrors oracle_step_t of the oracle.  Sizes: n variables, m rows. */
+typedef struct {
+    int n, m;
+    const int *A_row_ptr, *A_col_ind;
+    const double *A_val;
+    const int *At_row_ptr, *At_col_ind;
+    const double *At_val;
+    const double *c, *var_lb, *var_ub, *q_diag;
+    const double *con_lb, *con_ub, *affine_offset;
+    const double *var_rescale;
+    int num_cones;
+    const int *cone_start, *cone_vdim, *cone_type;
+    const double *cone_alpha;
+    double tau, sigma, halpern_weight, reflection;
+    double *x_init, *x_cur, *y_init, *y_cur;
+    double *x_pdhg, *x_refl, *y_pdhg, *y_refl, *Aty, *Ax;
+} pdhcg_b200_step_t;
+
+int pdhcg_b200_pdhg_step(const pdhcg_b200_step_t *s, void *stream);
+
+#ifdef __cplusplus
+}
+#endif

@@ -36,7 +36,7 @@ class CsrComponent(C.Structure):
 
 class ConeBlocks(C.Structure):
     _fields_ = [("num_cones", C.c_int), ("start_idx", _ip), ("v_dim", _ip), ("type", _ip),
-                ("power_alpha", _dp), ("fixed_mask_size", C.c_int), ("is_fixed", C.c_char_p)]
+                ("power_alpha", _dp), ("fixed_mask_size", C.c_int), ("is_fixed", C.POINTER(C.c_byte))]
 
 
 class ConeSpec(C.Structure):

@@ -1,0 +1,17 @@
+// internal.h -- declarations shared by the host files of libpdhcg_b200.
+#pragma once
+
+#include "../../include/pdhcg.h"
+#include "../../include/pdhcg_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+int pdhcg_b200_cone_length(cone_type_t type, int v_dim);
+qp_problem_t *pdhcg_b200_problem_clone(const qp_problem_t *p);
+int pdhcg_b200_cancel_requested(void);
+
+#ifdef __cplusplus
+}
+#endif

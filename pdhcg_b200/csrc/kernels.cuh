@@ -1,0 +1,256 @@
+// kernels.cuh -- the CUDA kernels of one PDHCG-B200 solve.
+//
+// Layout in HBM (one solve, n variables, m rows):
+//   A  : CSR, int32 row_ptr[m+1], int32 col[nnz], values MT[nnz]
+//   At : CSR of A^T (n rows), built on the device by a stable sort so each
+//        row lists its entries in increasing row index (what the
+//        reference's csr2csc produces, src/solver_state.cu:739-770)
+//   vectors: FP64 problem data (c, bounds, diag Q, rescaling) and iterates
+//        (x_init, x_cur, x_pdhg, x_refl; y_init, y_cur, y_pdhg).
+// Hot kernels of one iteration (reference pdhg_update + halpern_update,
+// src/pdhg_core_op.cu:705-845), two launches:
+//   primal_step : row-group SpMV on At (A^T y), diagonal-Q prox, box
+//                 projection, cone projection (warp per cone block), the
+//                 reflection and the Halpern average of x, all in registers
+//   dual_step   : row-group SpMV on A (A x_refl), dual prox, reflection and
+//                 Halpern average of y
+// Both are HBM-bandwidth bound: every matrix byte and every vector byte is
+// read once per iteration; the gathered vectors (y, x_refl) stay in L2.
+#pragma once
+
+#include "device.cuh"
+
+namespace pdhcg {
+
+constexpr int TPB = 256;
+constexpr int WARPS = TPB / 32;
+
+// ---------------------------------------------------------------------------
+// Per-iteration parameters of the step kernels (passed by value).
+// ---------------------------------------------------------------------------
+struct StepParams {
+    double tau, sigma;   // primal / dual step sizes
+    double w;            // Halpern weight (k+1)/(k+2)
+    double rho;          // reflection coefficient
+    int store_primal;    // write x_pdhg (and LP dual slack)
+    int store_dual;      // write y_pdhg
+    int want_fpe;        // write x_refl - x_cur into dx, y_refl - y_cur into dy
+    int lp_slack;        // NON_Q: store (p - t)/tau in dual_slack
+};
+
+template <typename MT>
+struct StepData {
+    int n, m;
+    const int *A_rp, *A_ci;
+    const MT *A_v;
+    const int *At_rp, *At_ci;
+    const MT *At_v;
+    const double *c, *l, *u, *q;
+    const double *lc, *uc, *g;
+    const double *vr; // variable rescaling (cone metric)
+    const int *free_idx; int n_free; // variables outside cones (NULL: all)
+    const int *cone_start, *cone_len, *cone_type; int n_cones;
+    double *x0, *x, *xp, *xr, *dx, *dual_slack;
+    double *y0, *y, *yp, *dy;
+};
+
+// x-side element update shared by the free and the cone path
+struct PrimalOut {
+    double p;  // pdhg candidate (before cone projection)
+};
+
+template <int G, typename MT, bool HAS_Q, bool HAS_BOX>
+__global__ void __launch_bounds__(TPB) primal_free_kernel(StepData<MT> D, StepParams P)
+{
+    const int groups_per_block = TPB / G;
+    const int lane = threadIdx.x % G;
+    const int nrows = D.free_idx ? D.n_free : D.n;
+    for (int r = blockIdx.x * groups_per_block + threadIdx.x / G; r < nrows; r += gridDim.x * groups_per_block) {
+        const int j = D.free_idx ? D.free_idx[r] : r;
+        double aty = row_dot<G>(D.At_rp, D.At_ci, D.At_v, D.y, j, lane);
+        if (lane == 0) {
+            double xi = D.x[j];
+            double t = xi - P.tau * (D.c[j] - aty);
+            if (HAS_Q)
+                t /= (1.0 + P.tau * D.q[j]);
+            double p = HAS_BOX ? clampd(D.l[j], t, D.u[j]) : t;
+            double xr = 2.0 * p - xi;
+            D.xr[j] = xr;
+            if (P.store_primal) {
+                D.xp[j] = p;
+                if (P.lp_slack)
+                    D.dual_slack[j] = (p - t) / P.tau;
+            }
+            if (P.want_fpe)
+                D.dx[j] = xr - xi;
+            double refl = P.rho * xr + (1.0 - P.rho) * xi;
+            D.x[j] = P.w * refl + (1.0 - P.w) * D.x0[j];
+        }
+    }
+}
+
+// One warp per cone block.  The prox candidate of every slot is projected
+// onto the cone in the (1 + tau q) d^2 metric (diagonal Q) or d^2 metric (LP).
+template <int S, typename MT, bool HAS_Q>
+__global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<MT> D, StepParams P)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = blockIdx.x * WARPS + (threadIdx.x >> 5);
+    const int nwarps = gridDim.x * WARPS;
+    for (int cb = warp; cb < D.n_cones; cb += nwarps) {
+        const int st = D.cone_start[cb], L = D.cone_len[cb], type = D.cone_type[cb];
+        WarpSlots<S> sl;
+        double xi[S], tt[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            int i = lane + 32 * s;
+            sl.x[s] = 0.0;
+            sl.d[s] = 1.0;
+            sl.w[s] = 1.0;
+            xi[s] = 0.0;
+            tt[s] = 0.0;
+            if (i < L) {
+                int j = st + i;
+                double aty = row_dot<1>(D.At_rp, D.At_ci, D.At_v, D.y, j, 0);
+                xi[s] = D.x[j];
+                double t = xi[s] - P.tau * (D.c[j] - aty);
+                if (HAS_Q)
+                    t /= (1.0 + P.tau * D.q[j]);
+                tt[s] = t;
+                sl.x[s] = clampd(D.l[j], t, D.u[j]);
+                sl.d[s] = D.vr[j];
+                sl.w[s] = HAS_Q ? 1.0 + P.tau * D.q[j] : 1.0;
+            }
+        }
+        // LP dual slack of the box step is recorded before the cone
+        // projection (reference compute_lp_next_pdhg_primal_solution_major_kernel
+        // then project_cone_runtime, src/pdhg_core_op.cu:426-455, 729-735)
+        if (P.lp_slack) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                int i = lane + 32 * s;
+                if (i < L)
+                    D.dual_slack[st + i] = (sl.x[s] - tt[s]) / P.tau;
+            }
+        }
+        bool uni = warp_uniform_unit<S>(sl, L, lane);
+        warp_project<S>(type, sl, L, lane, uni);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            int i = lane + 32 * s;
+            if (i < L) {
+                int j = st + i;
+                double p = sl.x[s];
+                double xr = 2.0 * p - xi[s];
+                D.xr[j] = xr;
+                D.xp[j] = p; // cones force the pdhg store (reference :428, :460)
+                if (P.want_fpe)
+                    D.dx[j] = xr - xi[s];
+                double refl = P.rho * xr + (1.0 - P.rho) * xi[s];
+                D.x[j] = P.w * refl + (1.0 - P.w) * D.x0[j];
+            }
+        }
+    }
+}
+
+template <int G, typename MT, bool EQ_ROWS, bool HAS_G>
+__global__ void __launch_bounds__(TPB) dual_kernel(StepData<MT> D, StepParams P)
+{
+    const int groups_per_block = TPB / G;
+    const int lane = threadIdx.x % G;
+    for (int i = blockIdx.x * groups_per_block + threadIdx.x / G; i < D.m; i += gridDim.x * groups_per_block) {
+        double ax = row_dot<G>(D.A_rp, D.A_ci, D.A_v, D.xr, i, lane);
+        if (lane == 0) {
+            double v = HAS_G ? ax + D.g[i] : ax;
+            double yi = D.y[i];
+            double pr;
+            if (EQ_ROWS)
+                pr = D.lc[i];
+            else
+                pr = clampd(D.lc[i], v - yi / P.sigma, D.uc[i]);
+            double yn = yi - P.sigma * v + P.sigma * pr;
+            if (P.store_dual)
+                D.yp[i] = yn;
+            double yr = 2.0 * yn - yi;
+            if (P.want_fpe)
+                D.dy[i] = yr - yi;
+            double refl = P.rho * yr + (1.0 - P.rho) * yi;
+            D.y[i] = P.w * refl + (1.0 - P.w) * D.y0[i];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic reductions: each block writes NS partial values; a one-block
+// kernel folds them in a fixed order.
+// ---------------------------------------------------------------------------
+enum ReduceOp { RSUM = 0, RMAX = 1 };
+
+template <int NS>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NS], const int (&op)[NS], double *partials)
+{
+    __shared__ double sh[WARPS][NS];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        double t = op[s] == RMAX ? warp_max(v[s]) : warp_sum(v[s]);
+        if (lane == 0)
+            sh[wid][s] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < NS) {
+        int s = threadIdx.x;
+        double acc = sh[0][s];
+        for (int w = 1; w < WARPS; ++w)
+            acc = op[s] == RMAX ? fmax(acc, sh[w][s]) : acc + sh[w][s];
+        partials[(size_t)blockIdx.x * NS + s] = acc;
+    }
+    __syncthreads();
+}
+
+// out[s] = fold over blocks of partials[b*NS+s]; one block of TPB threads.
+__global__ void fold_partials_kernel(const double *partials, int nblocks, int ns, const int *ops, double *out)
+{
+    __shared__ double sh[TPB];
+    for (int s = 0; s < ns; ++s) {
+        int op = ops[s];
+        double acc = op == RMAX ? 0.0 : 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += TPB) {
+            double v = partials[(size_t)b * ns + s];
+            acc = op == RMAX ? fmax(acc, v) : acc + v;
+        }
+        sh[threadIdx.x] = acc;
+        __syncthreads();
+        for (int o = TPB / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o)
+                sh[threadIdx.x] = op == RMAX ? fmax(sh[threadIdx.x], sh[threadIdx.x + o])
+                                             : sh[threadIdx.x] + sh[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+            out[s] = sh[0];
+        __syncthreads();
+    }
+}
+
+template <int G>
+__global__ void __launch_bounds__(TPB) spmv_kernel(int rows, const int *rp, const int *ci, const double *v,
+                                                   const double *x, double *y)
+{
+    const int gpb = TPB / G, lane = threadIdx.x % G;
+    for (int r = blockIdx.x * gpb + threadIdx.x / G; r < rows; r += gridDim.x * gpb) {
+        double a = row_dot<G>(rp, ci, v, x, r, lane);
+        if (lane == 0)
+            y[r] = a;
+    }
+}
+
+__global__ void cone_len_kernel(int nc, const int *vdim, const int *type, int *len)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nc; b += gridDim.x * blockDim.x) {
+        int t = type[b], v = vdim[b];
+        len[b] = (t == 2 || t == 3) ? 3 : (t == 4 ? v * (v + 1) / 2 : v + 2);
+    }
+}
+
+} // namespace pdhcg

@@ -1,0 +1,229 @@
+// residual.cuh -- KKT residual, objectives and restart distances in one
+// launch (reference compute_residual, src/pdhg_core_op.cu:1037-1294, with
+// compute_qp_residual_kernel / compute_lp_residual_kernel,
+// src/kernels/pdhcg_kernels.cu:628-738, the cone dual residual and the
+// projected-gradient augmentation, src/cone_dispatch.cu:88-116 and
+// src/pdhg_core_op.cu:67-90, and the distances of perform_restart,
+// src/pdhg_core_op.cu:859-880).  Three block ranges: constraint rows, free
+// variables, cone blocks (a warp each).  Every block leaves NS partial
+// scalars; fold_partials_kernel folds them in a fixed order, so the result
+// is deterministic.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace pdhcg {
+
+enum ResidualScalar {
+    RS_PRIMAL_RES = 0, // max |r_p| or sum r_p^2 (scaled by D_con)
+    RS_PRIMAL_SLACK,   // sum of bound * y terms of the dual objective
+    RS_DUAL_RES,       // max |r_d| or sum r_d^2
+    RS_CX,             // c . x
+    RS_XQX,            // x . Qx
+    RS_SLACKX,         // dual_slack . x
+    RS_QX_NORM,        // |Qx * D_var|
+    RS_ATY_NORM,       // |A^T y * D_var|
+    RS_DIST_X,         // |x_pdhg - x_init|^2
+    RS_DIST_Y,         // |y_pdhg - y_init|^2
+    RS_COUNT
+};
+
+struct ResidualParams {
+    int l2;           // 1: Euclidean norms, 0: infinity norms
+    int is_lp;        // NON_Q problem type (dual slack comes from the primal step)
+    int qmode;        // 0 none, 1 diagonal q, 2 precomputed qx vector
+    int has_cones;
+    int want_dist;    // restart distances
+    double tau;       // step / primal weight (QP dual slack)
+    double s_aug;     // step of the projected-gradient augmentation
+};
+
+template <typename MT>
+struct ResidualData {
+    int n, m;
+    const int *A_rp, *A_ci;
+    const MT *A_v;
+    const int *At_rp, *At_ci;
+    const MT *At_v;
+    const double *c, *l, *u, *q, *qx;
+    const double *lc, *uc, *g, *cr, *vr;
+    const double *xp, *yp, *x0, *y0;
+    const double *dual_slack;
+    const int *free_idx; int n_free;
+    const int *cone_start, *cone_len, *cone_type; int n_cones;
+    double *partials;
+    int rows_blocks, free_blocks, cone_blocks;
+};
+
+__device__ __forceinline__ double norm_term(double v, int l2) { return l2 ? v * v : abs_or_inf(v); }
+
+template <int G, int S, typename MT>
+__global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<MT> D, ResidualParams P)
+{
+    const int NOP = P.l2 ? RSUM : RMAX;
+    const int ops[RS_COUNT] = {NOP, RSUM, NOP, RSUM, RSUM, RSUM, NOP, NOP, RSUM, RSUM};
+    double acc[RS_COUNT];
+#pragma unroll
+    for (int s = 0; s < RS_COUNT; ++s)
+        acc[s] = 0.0;
+    auto fold = [&](int s, double v) { acc[s] = ops[s] == RMAX ? fmax(acc[s], v) : acc[s] + v; };
+
+    int b = blockIdx.x;
+    if (b < D.rows_blocks) {
+        const int gpb = TPB / G, lane = threadIdx.x % G;
+        for (int i = b * gpb + threadIdx.x / G; i < D.m; i += D.rows_blocks * gpb) {
+            double ax = row_dot<G>(D.A_rp, D.A_ci, D.A_v, D.xp, i, lane);
+            if (lane == 0) {
+                double v = ax + D.g[i];
+                double proj = clampd(D.lc[i], v, D.uc[i]);
+                fold(RS_PRIMAL_RES, norm_term((v - proj) * D.cr[i], P.l2));
+                double y = D.yp[i];
+                double lcf = isfinite(D.lc[i]) ? D.lc[i] : 0.0, ucf = isfinite(D.uc[i]) ? D.uc[i] : 0.0;
+                fold(RS_PRIMAL_SLACK, fmax(y, 0.0) * lcf + fmin(y, 0.0) * ucf - D.g[i] * y);
+                if (P.want_dist) {
+                    double d = y - D.y0[i];
+                    fold(RS_DIST_Y, d * d);
+                }
+            }
+        }
+    } else if (b < D.rows_blocks + D.free_blocks) {
+        b -= D.rows_blocks;
+        const int gpb = TPB / G, lane = threadIdx.x % G;
+        const int nrows = D.free_idx ? D.n_free : D.n;
+        for (int r = b * gpb + threadIdx.x / G; r < nrows; r += D.free_blocks * gpb) {
+            const int j = D.free_idx ? D.free_idx[r] : r;
+            double aty = row_dot<G>(D.At_rp, D.At_ci, D.At_v, D.yp, j, lane);
+            if (lane == 0) {
+                double x = D.xp[j];
+                double qx = P.qmode == 1 ? D.q[j] * x : (P.qmode == 2 ? D.qx[j] : 0.0);
+                double dr, ds;
+                if (P.is_lp) {
+                    ds = D.dual_slack[j];
+                    dr = (D.c[j] - aty - ds) * D.vr[j];
+                } else {
+                    double gr = qx + D.c[j] - aty;
+                    double t = x - P.tau * gr;
+                    double p = fmax(D.l[j], fmin(D.u[j], t));
+                    ds = (p - t) / P.tau;
+                    dr = (gr - ds) * D.vr[j];
+                }
+                if (P.has_cones) {
+                    double eff = P.qmode ? D.c[j] + qx : D.c[j];
+                    double pt = clampd(D.l[j], x - P.s_aug * (eff - aty), D.u[j]);
+                    double rr = (x - pt) / P.s_aug * D.vr[j];
+                    if (!isfinite(rr))
+                        rr = copysign(INFINITY, rr);
+                    if (fabs(rr) > fabs(dr))
+                        dr = rr;
+                }
+                fold(RS_DUAL_RES, norm_term(dr, P.l2));
+                fold(RS_CX, D.c[j] * x);
+                fold(RS_XQX, x * qx);
+                fold(RS_SLACKX, ds * x);
+                fold(RS_QX_NORM, norm_term(qx * D.vr[j], P.l2));
+                fold(RS_ATY_NORM, norm_term(aty * D.vr[j], P.l2));
+                if (P.want_dist) {
+                    double d = x - D.x0[j];
+                    fold(RS_DIST_X, d * d);
+                }
+            }
+        }
+    } else {
+        b -= D.rows_blocks + D.free_blocks;
+        const int lane = threadIdx.x & 31;
+        const int nwarps = D.cone_blocks * WARPS;
+        for (int cb = b * WARPS + (threadIdx.x >> 5); cb < D.n_cones; cb += nwarps) {
+            const int st = D.cone_start[cb], L = D.cone_len[cb], type = D.cone_type[cb];
+            WarpSlots<S> dual, aug;
+            double xv[S], rc[S], qxv[S], atyv[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                int i = lane + 32 * s;
+                dual.x[s] = aug.x[s] = 0.0;
+                dual.d[s] = aug.d[s] = 1.0;
+                dual.w[s] = aug.w[s] = 1.0;
+                xv[s] = rc[s] = qxv[s] = atyv[s] = 0.0;
+                if (i < L) {
+                    int j = st + i;
+                    double aty = row_dot<1>(D.At_rp, D.At_ci, D.At_v, D.yp, j, 0);
+                    double x = D.xp[j];
+                    double qx = P.qmode == 1 ? D.q[j] * x : (P.qmode == 2 ? D.qx[j] : 0.0);
+                    double eff = P.qmode ? D.c[j] + qx : D.c[j];
+                    xv[s] = x;
+                    atyv[s] = aty;
+                    qxv[s] = qx;
+                    rc[s] = eff - aty;
+                    // dual cone of {x : x/d in K} is {s : s*d in K}: metric 1/d
+                    dual.x[s] = rc[s];
+                    dual.d[s] = 1.0 / D.vr[j];
+                    aug.x[s] = clampd(D.l[j], x - P.s_aug * rc[s], D.u[j]);
+                    aug.d[s] = D.vr[j];
+                }
+            }
+            bool uni = warp_uniform_unit<S>(aug, L, lane); // d uniform <=> 1/d uniform
+            warp_project<S>(type, dual, L, lane, uni);
+            warp_project<S>(type, aug, L, lane, uni);
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                int i = lane + 32 * s;
+                if (i < L) {
+                    int j = st + i;
+                    double vr = D.vr[j];
+                    double dr = (rc[s] - dual.x[s]) * vr;
+                    double rr = (xv[s] - aug.x[s]) / P.s_aug * vr;
+                    if (!isfinite(rr))
+                        rr = copysign(INFINITY, rr);
+                    if (fabs(rr) > fabs(dr))
+                        dr = rr;
+                    fold(RS_DUAL_RES, norm_term(dr, P.l2));
+                    fold(RS_CX, D.c[j] * xv[s]);
+                    fold(RS_XQX, xv[s] * qxv[s]);
+                    fold(RS_SLACKX, rc[s] * xv[s]);
+                    fold(RS_QX_NORM, norm_term(qxv[s] * vr, P.l2));
+                    fold(RS_ATY_NORM, norm_term(atyv[s] * vr, P.l2));
+                    if (P.want_dist) {
+                        double d = xv[s] - D.x0[j];
+                        fold(RS_DIST_X, d * d);
+                    }
+                }
+            }
+        }
+    }
+    block_reduce_store<RS_COUNT>(acc, ops, D.partials);
+}
+
+// Fixed-point error pieces (reference compute_fixed_point_error,
+// src/pdhg_core_op.cu:973-1035): |dx|^2, |dy|^2 and (A^T dy) . dx, with
+// dx = x_refl - x_cur and dy = y_refl - y_cur written by the step kernels.
+enum FpeScalar { FP_DX2 = 0, FP_DY2, FP_CROSS, FP_COUNT };
+
+template <int G, typename MT>
+__global__ void __launch_bounds__(TPB) fpe_kernel(int n, int m, const int *At_rp, const int *At_ci, const MT *At_v,
+                                                  const double *dx, const double *dy, double *partials,
+                                                  int col_blocks)
+{
+    const int ops[FP_COUNT] = {RSUM, RSUM, RSUM};
+    double acc[FP_COUNT] = {0.0, 0.0, 0.0};
+    int b = blockIdx.x;
+    if (b < col_blocks) {
+        const int gpb = TPB / G, lane = threadIdx.x % G;
+        for (int j = b * gpb + threadIdx.x / G; j < n; j += col_blocks * gpb) {
+            double a = row_dot<G>(At_rp, At_ci, At_v, dy, j, lane);
+            if (lane == 0) {
+                double d = dx[j];
+                acc[FP_DX2] += d * d;
+                acc[FP_CROSS] += a * d;
+            }
+        }
+    } else {
+        b -= col_blocks;
+        int nb = gridDim.x - col_blocks;
+        for (int i = b * TPB + threadIdx.x; i < m; i += nb * TPB) {
+            double d = dy[i];
+            acc[FP_DY2] += d * d;
+        }
+    }
+    block_reduce_store<FP_COUNT>(acc, ops, partials);
+}
+
+} // namespace pdhcg

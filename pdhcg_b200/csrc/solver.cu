@@ -1,0 +1,1240 @@
+// solver.cu -- host driver of one PDHCG-B200 solve, plus the kernel-level
+// C entry points.
+//
+// The control flow mirrors the reference's optimize() (src/solver.cu:35-210)
+// decision for decision -- evaluation cadence, the (k+2) store rule for
+// PDHG iterates, restart tests, PID primal weight -- because those
+// decisions shape the iterate trajectory.  What differs is where the work
+// runs: preprocessing (transpose, rescaling, power method) runs on the
+// device, each iteration is two fused kernels, and the host synchronises
+// only at evaluation points, reading one small block of scalars.
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <csignal>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "residual.cuh"
+#include "setup.cuh"
+
+using namespace pdhcg;
+
+namespace {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define CK(call)                                                                                                       \
+    do {                                                                                                               \
+        cudaError_t e_ = (call);                                                                                       \
+        if (e_ != cudaSuccess)                                                                                         \
+            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_) + " at " + __FILE__ + ":" +            \
+                            std::to_string(__LINE__));                                                                 \
+    } while (0)
+
+thread_local pdhcg_b200_stats_t g_last_stats;
+
+// device allocations owned by one solve
+struct Arena {
+    std::vector<void *> ptrs;
+    template <typename T>
+    T *alloc(size_t count)
+    {
+        void *p = nullptr;
+        CK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+        ptrs.push_back(p);
+        return (T *)p;
+    }
+    template <typename T>
+    T *upload(const T *h, size_t count, cudaStream_t s)
+    {
+        T *d = alloc<T>(count);
+        if (count)
+            CK(cudaMemcpyAsync(d, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+        return d;
+    }
+    ~Arena()
+    {
+        for (void *p : ptrs)
+            cudaFree(p);
+    }
+};
+
+int grid_for(long long work, int per_block, int cap = 148 * 16)
+{
+    long long g = (work + per_block - 1) / per_block;
+    if (g < 1)
+        g = 1;
+    if (g > cap)
+        g = cap;
+    return (int)g;
+}
+
+int print_frequency(int iter)
+{
+    int step = 10;
+    long long threshold = 1000;
+    while (iter >= threshold) {
+        step *= 10;
+        threshold *= 10;
+    }
+    return step;
+}
+
+// lanes per row from the mean row length
+int pick_group(long long nnz, int rows)
+{
+    double mean = rows > 0 ? (double)nnz / rows : 0.0;
+    if (mean <= 12)
+        return 1;
+    if (mean <= 24)
+        return 2;
+    if (mean <= 48)
+        return 4;
+    if (mean <= 96)
+        return 8;
+    if (mean <= 192)
+        return 16;
+    return 32;
+}
+
+// slots per lane of the warp-per-cone kernels (cone blocks up to 256 slots)
+int slots_class(int maxlen)
+{
+    int s = (maxlen + 31) / 32;
+    if (s <= 1)
+        return 1;
+    if (s <= 2)
+        return 2;
+    if (s <= 4)
+        return 4;
+    if (s <= 8)
+        return 8;
+    return -1;
+}
+
+// lanes per row of the residual kernel (one kernel serves A and A^T rows)
+int residual_group(int g)
+{
+    return g <= 2 ? 1 : (g <= 8 ? 4 : 32);
+}
+
+struct DevCsr {
+    int rows = 0, cols = 0, nnz = 0;
+    int *rp = nullptr, *ci = nullptr;
+    double *v = nullptr;
+};
+
+// stable transpose on the device (entries of each output row in increasing
+// input-row order)
+DevCsr transpose(const DevCsr &M, Arena &ar, cudaStream_t s)
+{
+    DevCsr T;
+    T.rows = M.cols;
+    T.cols = M.rows;
+    T.nnz = M.nnz;
+    T.rp = ar.alloc<int>((size_t)T.rows + 1);
+    T.ci = ar.alloc<int>(M.nnz);
+    T.v = ar.alloc<double>(M.nnz);
+    if (M.nnz == 0) {
+        CK(cudaMemsetAsync(T.rp, 0, ((size_t)T.rows + 1) * sizeof(int), s));
+        return T;
+    }
+    int *row_of = ar.alloc<int>(M.nnz), *idx = ar.alloc<int>(M.nnz), *keys_out = ar.alloc<int>(M.nnz),
+        *perm = ar.alloc<int>(M.nnz);
+    expand_rows_kernel<<<grid_for(M.rows, TPB), TPB, 0, s>>>(M.rp, M.rows, row_of);
+    iota_kernel<<<grid_for(M.nnz, TPB), TPB, 0, s>>>(idx, M.nnz);
+    size_t tmp_bytes = 0;
+    int bits = 1;
+    while ((1LL << bits) <= (long long)M.cols)
+        ++bits;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, M.ci, keys_out, idx, perm, M.nnz, 0, bits, s);
+    void *tmp = ar.alloc<char>(tmp_bytes);
+    CK(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, M.ci, keys_out, idx, perm, M.nnz, 0, bits, s));
+    col_ptr_kernel<<<grid_for((long long)T.rows + 1, TPB), TPB, 0, s>>>(keys_out, M.nnz, T.rows, T.rp);
+    gather_transpose_kernel<<<grid_for(M.nnz, TPB), TPB, 0, s>>>(perm, row_of, M.v, M.nnz, T.ci, T.v);
+    return T;
+}
+
+struct HostScalars {
+    double v[RS_COUNT + 2 * FP_COUNT];
+};
+
+class Solve {
+public:
+    Solve(const qp_problem_t *prob, const pdhg_parameters_t &prm, const pdhcg_b200_options_t &opt)
+        : P_(prob), prm_(prm), opt_(opt)
+    {
+    }
+    ~Solve()
+    {
+        for (cudaEvent_t e : ev_pool_)
+            cudaEventDestroy(e);
+        if (h_scal_)
+            cudaFreeHost(h_scal_);
+        if (st_)
+            cudaStreamDestroy(st_);
+    }
+    pdhcg_result_t *run();
+
+private:
+    void build_host();
+    void upload_and_preprocess();
+    void rescale();
+    void init_state();
+    void step_size();
+    void loop();
+    void enqueue_step(bool store_primal, bool store_dual, bool want_fpe, double w);
+    void enqueue_residual(bool want_dist);
+    void read_residual();
+    void enqueue_fpe(int slot);
+    pdhcg_result_t *make_result();
+    template <typename F>
+    void dispatch_g(int G, F &&f);
+
+    const qp_problem_t *P_;
+    pdhg_parameters_t prm_;
+    pdhcg_b200_options_t opt_;
+    cudaStream_t st_ = nullptr;
+    Arena ar_;
+
+    // host copy of the working problem (dummy row added when m == 0)
+    int n_ = 0, m_ = 0;
+    std::vector<int> A_rp_, A_ci_;
+    std::vector<double> A_v_, c_, l_, u_, lc_, uc_, g_;
+    int qtype_ = PDHCG_NON_Q;
+    bool has_g_ = false, box_free_ = true, eq_rows_ = true;
+    std::vector<int> cone_start_, cone_len_, cone_type_, cone_vdim_, free_idx_;
+    int S_ = 1;
+
+    // device
+    DevCsr A_, At_, Q_;
+    double *c_d_ = nullptr, *l_d_ = nullptr, *u_d_ = nullptr, *q_d_ = nullptr, *lc_d_ = nullptr, *uc_d_ = nullptr,
+           *g_d_ = nullptr, *cr_d_ = nullptr, *vr_d_ = nullptr;
+    int *free_d_ = nullptr, *cst_d_ = nullptr, *clen_d_ = nullptr, *ctype_d_ = nullptr, *cvdim_d_ = nullptr;
+    double *x0_, *x_, *xp_, *xr_, *dx_, *dslack_, *y0_, *y_, *yp_, *dy_;
+    double *partials_ = nullptr, *scal_d_ = nullptr, *h_scal_ = nullptr;
+    int *res_ops_d_ = nullptr, *fpe_ops_d_ = nullptr, *norm_ops_d_ = nullptr;
+    int res_rows_blocks_ = 0, res_free_blocks_ = 0, res_cone_blocks_ = 0;
+    int fpe_col_blocks_ = 0, fpe_row_blocks_ = 0;
+    int GA_ = 1, GAt_ = 1;
+
+    // scaling
+    double sb_ = 1.0, sc_ = 1.0, cnorm_ = 0.0, bnorm_ = 0.0;
+
+    // iteration state (host scalars, reference pdhg_solver_state_t)
+    double step_ = 0.0, omega_ = 1.0, best_omega_ = 1.0, best_gap_ = INFINITY;
+    double pw_err_sum_ = 0.0, pw_last_err_ = 0.0;
+    int k_ = 0, inner_count_ = 0;
+    long long inner_total_ = 0;
+    bool is_major_ = false;
+    double fpe_ = 0.0, fpe0_ = 0.0, fpe_last_ = INFINITY;
+    double abs_p_ = 0, rel_p_ = 0, abs_d_ = 0, rel_d_ = 0, pobj_ = 0, dobj_ = 0, gap_ = 0, rel_gap_ = 0;
+    double dist_x_ = 0, dist_y_ = 0;
+    bool pending_fpe0_ = false;
+    int pending_fpe_slot_ = -1;
+    termination_reason_t reason_ = TERMINATION_REASON_UNSPECIFIED;
+    double cum_time_ = 0.0;
+    pdhcg_b200_stats_t stats_{};
+    double nonconvexity_ = 0.0;
+
+    // optional CUDA-event timing of the fused step kernels: pairs of events
+    // recorded around each step, harvested at every host synchronisation
+    std::vector<cudaEvent_t> ev_pool_;
+    size_t ev_used_ = 0;
+    void harvest_step_events();
+};
+
+template <typename F>
+void Solve::dispatch_g(int G, F &&f)
+{
+    switch (G) {
+    case 1: f(std::integral_constant<int, 1>{}); break;
+    case 2: f(std::integral_constant<int, 2>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 16: f(std::integral_constant<int, 16>{}); break;
+    default: f(std::integral_constant<int, 32>{}); break;
+    }
+}
+
+template <typename F>
+void dispatch_s(int S, F &&f)
+{
+    switch (S) {
+    case 1: f(std::integral_constant<int, 1>{}); break;
+    case 2: f(std::integral_constant<int, 2>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    default: f(std::integral_constant<int, 8>{}); break;
+    }
+}
+
+template <typename F>
+void dispatch_rg(int G, F &&f)
+{
+    switch (G) {
+    case 1: f(std::integral_constant<int, 1>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    default: f(std::integral_constant<int, 32>{}); break;
+    }
+}
+
+// ---- host-side classification (reference preprocess_qp_problem and
+// detect_q_type, src/preconditioner.c:715-830, src/utils.cu:834-885) ------
+void Solve::build_host()
+{
+    const qp_problem_t *p = P_;
+    n_ = p->num_variables;
+    bool dummy = p->num_constraints == 0 || p->constraint_matrix == nullptr;
+    if (dummy) { // reference create_problem_with_dummy_constraint, src/utils.cu:80-135
+        m_ = 1;
+        A_rp_ = {0, 1};
+        A_ci_ = {0};
+        A_v_ = {1.0};
+        lc_ = {-INFINITY};
+        uc_ = {INFINITY};
+        g_ = {0.0};
+    } else {
+        m_ = p->num_constraints;
+        int nnz = p->constraint_matrix_num_nonzeros;
+        A_rp_.assign(p->constraint_matrix->row_ptr, p->constraint_matrix->row_ptr + m_ + 1);
+        A_ci_.assign(p->constraint_matrix->col_ind, p->constraint_matrix->col_ind + nnz);
+        A_v_.assign(p->constraint_matrix->val, p->constraint_matrix->val + nnz);
+        lc_.assign(p->constraint_lower_bound, p->constraint_lower_bound + m_);
+        uc_.assign(p->constraint_upper_bound, p->constraint_upper_bound + m_);
+        g_.assign(p->affine_cone_offset, p->affine_cone_offset + m_);
+    }
+    c_.assign(p->objective_vector, p->objective_vector + n_);
+    l_.assign(p->variable_lower_bound, p->variable_lower_bound + n_);
+    u_.assign(p->variable_upper_bound, p->variable_upper_bound + n_);
+    for (double v : g_)
+        has_g_ |= v != 0.0;
+    for (int i = 0; i < n_; ++i)
+        box_free_ &= !std::isfinite(l_[i]) && !std::isfinite(u_[i]);
+    for (int i = 0; i < m_; ++i)
+        eq_rows_ &= lc_[i] == uc_[i] && std::isfinite(lc_[i]);
+
+    // objective structure
+    int nnzq = (p->objective_sparse_matrix && p->objective_sparse_matrix->row_ptr)
+                   ? p->objective_sparse_matrix_num_nonzeros
+                   : 0;
+    int nnzr = (p->objective_lowrank_matrix && p->objective_lowrank_matrix->row_ptr && p->num_rank_lowrank_obj > 0)
+                   ? p->objective_lowrank_matrix_num_nonzeros
+                   : 0;
+    if (nnzq == 0 && nnzr == 0)
+        qtype_ = PDHCG_NON_Q;
+    else if (nnzr > 0)
+        qtype_ = nnzq > 0 ? PDHCG_LOW_RANK_PLUS_SPARSE_Q : PDHCG_LOW_RANK_Q;
+    else {
+        qtype_ = PDHCG_DIAG_Q;
+        const CsrComponent *Q = p->objective_sparse_matrix;
+        for (int i = 0; i < n_ && qtype_ == PDHCG_DIAG_Q; ++i)
+            for (int k = Q->row_ptr[i]; k < Q->row_ptr[i + 1]; ++k)
+                if (Q->col_ind[k] != i) {
+                    qtype_ = PDHCG_SPARSE_Q;
+                    break;
+                }
+    }
+
+    // cones
+    int maxlen = 0;
+    std::vector<char> in_cone(n_, 0);
+    for (int b = 0; b < p->cones.num_cones; ++b) {
+        int len = pdhcg_b200_cone_length(p->cones.type[b], p->cones.v_dim[b]);
+        cone_start_.push_back(p->cones.start_idx[b]);
+        cone_len_.push_back(len);
+        cone_type_.push_back((int)p->cones.type[b]);
+        cone_vdim_.push_back(p->cones.v_dim[b]);
+        maxlen = std::max(maxlen, len);
+        for (int i = 0; i < len; ++i)
+            in_cone[p->cones.start_idx[b] + i] = 1;
+    }
+    if (!cone_start_.empty()) {
+        for (int i = 0; i < n_; ++i)
+            if (!in_cone[i])
+                free_idx_.push_back(i);
+        S_ = slots_class(maxlen);
+    }
+}
+
+void Solve::upload_and_preprocess()
+{
+    cudaStream_t s = st_;
+    A_.rows = m_;
+    A_.cols = n_;
+    A_.nnz = (int)A_v_.size();
+    A_.rp = ar_.upload(A_rp_.data(), A_rp_.size(), s);
+    A_.ci = ar_.upload(A_ci_.data(), A_ci_.size(), s);
+    A_.v = ar_.upload(A_v_.data(), A_v_.size(), s);
+    At_ = transpose(A_, ar_, s);
+    c_d_ = ar_.upload(c_.data(), n_, s);
+    l_d_ = ar_.upload(l_.data(), n_, s);
+    u_d_ = ar_.upload(u_.data(), n_, s);
+    lc_d_ = ar_.upload(lc_.data(), m_, s);
+    uc_d_ = ar_.upload(uc_.data(), m_, s);
+    g_d_ = ar_.upload(g_.data(), m_, s);
+    if (qtype_ != PDHCG_NON_Q) {
+        const CsrComponent *Q = P_->objective_sparse_matrix;
+        Q_.rows = n_;
+        Q_.cols = n_;
+        Q_.nnz = P_->objective_sparse_matrix_num_nonzeros;
+        Q_.rp = ar_.upload(Q->row_ptr, (size_t)n_ + 1, s);
+        Q_.ci = ar_.upload(Q->col_ind, Q_.nnz, s);
+        Q_.v = ar_.upload(Q->val, Q_.nnz, s);
+    }
+    int nc = (int)cone_start_.size();
+    if (nc > 0) {
+        cst_d_ = ar_.upload(cone_start_.data(), nc, s);
+        clen_d_ = ar_.upload(cone_len_.data(), nc, s);
+        ctype_d_ = ar_.upload(cone_type_.data(), nc, s);
+        cvdim_d_ = ar_.upload(cone_vdim_.data(), nc, s);
+        if (!free_idx_.empty())
+            free_d_ = ar_.upload(free_idx_.data(), free_idx_.size(), s);
+    }
+    GA_ = pick_group(A_.nnz, m_);
+    GAt_ = pick_group(At_.nnz, n_);
+}
+
+// ---- rescaling (reference rescale_problem, src/preconditioner.c:654-713) --
+void Solve::rescale()
+{
+    cudaStream_t s = st_;
+    int n = n_, m = m_, nc = (int)cone_start_.size();
+    cr_d_ = ar_.alloc<double>(m);
+    vr_d_ = ar_.alloc<double>(n);
+    double *fcr = ar_.alloc<double>(m), *fvr = ar_.alloc<double>(n);
+    std::vector<double> ones_n(n, 1.0), ones_m(m, 1.0);
+    CK(cudaMemcpyAsync(cr_d_, ones_m.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(vr_d_, ones_n.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+    bool pres = prm_.use_cone_preserving_scaling;
+    auto apply = [&](int ruiz_phase) {
+        CK(cudaGetLastError());
+        sqrt_or_one_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(fvr, n);
+        sqrt_or_one_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(fcr, m);
+        if (nc > 0) {
+            if (pres)
+                cone_scaling_adjust_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(fvr, nc, cst_d_, clen_d_, ruiz_phase);
+            else
+                psd_scaling_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(fvr, nc, cst_d_, cvdim_d_, ctype_d_);
+        }
+        scale_csr_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.ci, A_.v, m, fcr, fvr, 0);
+        scale_csr_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.ci, At_.v, n, fvr, fcr, 1);
+        if (Q_.nnz > 0)
+            scale_csr_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(Q_.rp, Q_.ci, Q_.v, n, fvr, fvr, 0);
+        scale_vectors_kernel<<<grid_for((long long)n + m, TPB), TPB, 0, s>>>(n, m, c_d_, l_d_, u_d_, fvr, lc_d_,
+                                                                             uc_d_, g_d_, fcr, vr_d_, cr_d_);
+        CK(cudaGetLastError());
+    };
+    if (prm_.curtis_reid_iterations > 0)
+        throw CudaError("Curtis-Reid scaling is not available on the device path yet");
+    for (int it = 0; it < prm_.l_inf_ruiz_iterations; ++it) {
+        row_absmax_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.v, m, fcr);
+        row_absmax_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.v, n, fvr);
+        apply(1);
+    }
+    if (prm_.has_pock_chambolle_alpha) {
+        double a = prm_.pock_chambolle_alpha;
+        row_powsum_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.v, m, a, fcr);
+        row_powsum_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.v, n, 2.0 - a, fvr);
+        apply(0);
+    }
+    if (prm_.bound_objective_rescaling) {
+        int nb = grid_for((long long)n + m, TPB, 148 * 4);
+        norms_kernel<<<nb, TPB, 0, s>>>(n, m, c_d_, lc_d_, uc_d_, g_d_, partials_);
+        fold_partials_kernel<<<1, TPB, 0, s>>>(partials_, nb, NS_COUNT, norm_ops_d_, scal_d_);
+        double h[NS_COUNT];
+        CK(cudaMemcpyAsync(h, scal_d_, sizeof(h), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        sb_ = 1.0 / (std::sqrt(h[NS_B2]) + 1.0);
+        sc_ = 1.0 / (std::sqrt(h[NS_C2]) + 1.0);
+        bound_obj_scale_kernel<<<grid_for((long long)n + m, TPB), TPB, 0, s>>>(n, m, sb_, sc_, c_d_, l_d_, u_d_,
+                                                                               lc_d_, uc_d_, g_d_);
+        if (Q_.nnz > 0)
+            mul_scalar_kernel<<<grid_for(Q_.nnz, TPB), TPB, 0, s>>>(Q_.v, Q_.nnz, sc_ / sb_);
+    }
+    CK(cudaGetLastError());
+}
+
+void Solve::init_state()
+{
+    cudaStream_t s = st_;
+    int n = n_, m = m_, nc = (int)cone_start_.size();
+    x0_ = ar_.alloc<double>(n);
+    x_ = ar_.alloc<double>(n);
+    xp_ = ar_.alloc<double>(n);
+    xr_ = ar_.alloc<double>(n);
+    dx_ = ar_.alloc<double>(n);
+    dslack_ = ar_.alloc<double>(n);
+    y0_ = ar_.alloc<double>(m);
+    y_ = ar_.alloc<double>(m);
+    yp_ = ar_.alloc<double>(m);
+    dy_ = ar_.alloc<double>(m);
+    CK(cudaMemsetAsync(x0_, 0, n * sizeof(double), s));
+    CK(cudaMemsetAsync(dslack_, 0, n * sizeof(double), s));
+    if (P_->primal_start) {
+        double *ps = ar_.upload(P_->primal_start, n, s);
+        scale_start_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(n, ps, vr_d_, sb_, x0_);
+    }
+    const double *ds = nullptr;
+    if (P_->dual_start && !(P_->num_constraints == 0 || P_->constraint_matrix == nullptr))
+        ds = ar_.upload(P_->dual_start, m, s);
+    dual_start_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(m, ds, cr_d_, sc_, y0_, y_, yp_);
+    if (nc > 0) {
+        cone_aux_init_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(nc, cst_d_, cvdim_d_, ctype_d_, vr_d_, sb_, x0_);
+        dispatch_s(S_, [&](auto SC) {
+            project_cones_kernel<SC.value><<<grid_for(nc, WARPS), TPB, 0, s>>>(nc, cst_d_, clen_d_, ctype_d_, x0_,
+                                                                             vr_d_, nullptr, 0.0);
+        });
+    }
+    box_clamp_copy_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(n, l_d_, u_d_, x0_, x_, xp_, xr_);
+    if (qtype_ == PDHCG_DIAG_Q) {
+        q_d_ = ar_.alloc<double>(n);
+        CK(cudaMemsetAsync(q_d_, 0, n * sizeof(double), s));
+        q_diag_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(Q_.rp, Q_.ci, Q_.v, n, q_d_);
+        std::vector<double> qh(n);
+        CK(cudaMemcpyAsync(qh.data(), q_d_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        double mn = 0.0;
+        for (double v : qh)
+            mn = std::fmin(mn, v);
+        nonconvexity_ = mn; // reference initialize_quadratic_term_information, src/solver_state.cu:400-418
+    }
+    CK(cudaGetLastError());
+}
+
+// ---- step size (reference initialize_step_size_and_primal_weight,
+// src/pdhg_core_op.cu:933-971) -------------------------------------------
+void Solve::step_size()
+{
+    cudaStream_t s = st_;
+    if (A_.nnz == 0) {
+        step_ = 1.0;
+    } else {
+        int m = m_, n = n_;
+        std::vector<double> v0(m);
+        unsigned int seed = 1234;
+        for (int i = 0; i < m; ++i)
+            v0[i] = ((double)rand_r(&seed) / (double)RAND_MAX) * 2.0 - 1.0;
+        double *v = ar_.upload(v0.data(), m, s), *nv = ar_.alloc<double>(m), *dp = ar_.alloc<double>(n);
+        double *out = ar_.alloc<double>(2);
+        int dev = 0, nsm = 0, per_sm = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, power_sigma_kernel<double>, TPB, 0));
+        int grid = std::max(1, std::min(nsm * std::max(per_sm, 1), nsm * 4));
+        double *part = ar_.alloc<double>((size_t)4 * grid);
+        int max_iter = prm_.sv_max_iter;
+        double tol = prm_.sv_tol;
+        void *args[] = {&m, &n, &A_.rp, &A_.ci, &A_.v, &At_.rp, &At_.ci, &At_.v, &v, &nv, &dp, &part, &max_iter,
+                        &tol, &out};
+        CK(cudaLaunchCooperativeKernel((void *)power_sigma_kernel<double>, grid, TPB, args, 0, s));
+        double h[2];
+        CK(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        double sv = h[0];
+        step_ = sv < 1e-12 ? 1.0 : 0.998 / sv;
+    }
+    omega_ = prm_.bound_objective_rescaling ? 1.0 : (cnorm_ + 1.0) / (bnorm_ + 1.0);
+    if (opt_.has_initial_primal_weight && opt_.initial_primal_weight > 0.0)
+        omega_ = opt_.initial_primal_weight;
+    best_omega_ = omega_;
+}
+
+void Solve::harvest_step_events()
+{
+    for (size_t i = 0; i + 1 < ev_used_; i += 2) {
+        float ms = 0.0f;
+        CK(cudaEventSynchronize(ev_pool_[i + 1]));
+        CK(cudaEventElapsedTime(&ms, ev_pool_[i], ev_pool_[i + 1]));
+        stats_.step_kernel_ms += ms;
+    }
+    ev_used_ = 0;
+}
+
+void Solve::enqueue_step(bool store_primal, bool store_dual, bool want_fpe, double w)
+{
+    cudaStream_t s = st_;
+    if (opt_.time_steps) {
+        if (ev_used_ + 2 > ev_pool_.size()) {
+            for (int i = 0; i < 64; ++i) {
+                cudaEvent_t e;
+                CK(cudaEventCreate(&e));
+                ev_pool_.push_back(e);
+            }
+        }
+        CK(cudaEventRecord(ev_pool_[ev_used_++], s));
+    }
+    StepParams P;
+    P.tau = step_ / omega_;
+    if (nonconvexity_ < 0) {
+        P.tau = std::fmax(P.tau, -1.01 * std::fmin(0.0, nonconvexity_));
+        P.tau /= 100;
+    }
+    P.sigma = step_ * omega_;
+    P.w = w;
+    P.rho = prm_.reflection_coefficient;
+    P.store_primal = store_primal;
+    P.store_dual = store_dual;
+    P.want_fpe = want_fpe;
+    P.lp_slack = qtype_ == PDHCG_NON_Q;
+    StepData<double> D;
+    D.n = n_;
+    D.m = m_;
+    D.A_rp = A_.rp;
+    D.A_ci = A_.ci;
+    D.A_v = A_.v;
+    D.At_rp = At_.rp;
+    D.At_ci = At_.ci;
+    D.At_v = At_.v;
+    D.c = c_d_;
+    D.l = l_d_;
+    D.u = u_d_;
+    D.q = q_d_;
+    D.lc = lc_d_;
+    D.uc = uc_d_;
+    D.g = g_d_;
+    D.vr = vr_d_;
+    D.free_idx = free_d_;
+    D.n_free = (int)free_idx_.size();
+    D.cone_start = cst_d_;
+    D.cone_len = clen_d_;
+    D.cone_type = ctype_d_;
+    D.n_cones = (int)cone_start_.size();
+    D.x0 = x0_;
+    D.x = x_;
+    D.xp = xp_;
+    D.xr = xr_;
+    D.dx = dx_;
+    D.dual_slack = dslack_;
+    D.y0 = y0_;
+    D.y = y_;
+    D.yp = yp_;
+    D.dy = dy_;
+    bool hasq = qtype_ == PDHCG_DIAG_Q;
+    int nfree = D.n_cones > 0 ? D.n_free : n_;
+    if (nfree > 0) {
+        dispatch_g(GAt_, [&](auto GC) {
+            constexpr int G = GC.value;
+            int grid = grid_for((long long)nfree, TPB / G);
+            if (hasq) {
+                if (box_free_)
+                    primal_free_kernel<G, double, true, false><<<grid, TPB, 0, s>>>(D, P);
+                else
+                    primal_free_kernel<G, double, true, true><<<grid, TPB, 0, s>>>(D, P);
+            } else {
+                if (box_free_)
+                    primal_free_kernel<G, double, false, false><<<grid, TPB, 0, s>>>(D, P);
+                else
+                    primal_free_kernel<G, double, false, true><<<grid, TPB, 0, s>>>(D, P);
+            }
+        });
+        stats_.kernel_launches++;
+    }
+    if (D.n_cones > 0) {
+        dispatch_s(S_, [&](auto SC) {
+            int grid = grid_for(D.n_cones, WARPS);
+            if (hasq)
+                primal_cone_kernel<SC.value, double, true><<<grid, TPB, 0, s>>>(D, P);
+            else
+                primal_cone_kernel<SC.value, double, false><<<grid, TPB, 0, s>>>(D, P);
+        });
+        stats_.kernel_launches++;
+    }
+    dispatch_g(GA_, [&](auto GC) {
+        constexpr int G = GC.value;
+        int grid = grid_for((long long)m_, TPB / G);
+        if (eq_rows_) {
+            if (has_g_)
+                dual_kernel<G, double, true, true><<<grid, TPB, 0, s>>>(D, P);
+            else
+                dual_kernel<G, double, true, false><<<grid, TPB, 0, s>>>(D, P);
+        } else {
+            if (has_g_)
+                dual_kernel<G, double, false, true><<<grid, TPB, 0, s>>>(D, P);
+            else
+                dual_kernel<G, double, false, false><<<grid, TPB, 0, s>>>(D, P);
+        }
+    });
+    stats_.kernel_launches++;
+    stats_.step_kernel_launches++;
+    if (opt_.time_steps)
+        CK(cudaEventRecord(ev_pool_[ev_used_++], s));
+}
+
+void Solve::enqueue_residual(bool want_dist)
+{
+    cudaStream_t s = st_;
+    ResidualData<double> D;
+    D.n = n_;
+    D.m = m_;
+    D.A_rp = A_.rp;
+    D.A_ci = A_.ci;
+    D.A_v = A_.v;
+    D.At_rp = At_.rp;
+    D.At_ci = At_.ci;
+    D.At_v = At_.v;
+    D.c = c_d_;
+    D.l = l_d_;
+    D.u = u_d_;
+    D.q = q_d_;
+    D.qx = nullptr;
+    D.lc = lc_d_;
+    D.uc = uc_d_;
+    D.g = g_d_;
+    D.cr = cr_d_;
+    D.vr = vr_d_;
+    D.xp = xp_;
+    D.yp = yp_;
+    D.x0 = x0_;
+    D.y0 = y0_;
+    D.dual_slack = dslack_;
+    D.free_idx = free_d_;
+    D.n_free = (int)free_idx_.size();
+    D.cone_start = cst_d_;
+    D.cone_len = clen_d_;
+    D.cone_type = ctype_d_;
+    D.n_cones = (int)cone_start_.size();
+    D.partials = partials_;
+    D.rows_blocks = res_rows_blocks_;
+    D.free_blocks = res_free_blocks_;
+    D.cone_blocks = res_cone_blocks_;
+    ResidualParams P;
+    P.l2 = prm_.optimality_norm == NORM_TYPE_L2;
+    P.is_lp = qtype_ == PDHCG_NON_Q;
+    P.qmode = qtype_ == PDHCG_DIAG_Q ? 1 : 0;
+    P.has_cones = D.n_cones > 0;
+    P.want_dist = want_dist;
+    P.tau = step_ / omega_;
+    double sa = step_ / omega_;
+    if (!(sa > 0.0) || !std::isfinite(sa))
+        sa = 1.0;
+    P.s_aug = sa;
+    int nb = D.rows_blocks + D.free_blocks + D.cone_blocks;
+    // G for the rows range: A; the free range uses A^T with the same G
+    // template, so both row-group widths must agree -> use the smaller.
+    int G = residual_group(std::min(GA_, GAt_));
+    dispatch_rg(G, [&](auto GC) {
+        dispatch_s(S_, [&](auto SC) { residual_kernel<GC.value, SC.value, double><<<nb, TPB, 0, s>>>(D, P); });
+    });
+    fold_partials_kernel<<<1, TPB, 0, s>>>(partials_, nb, RS_COUNT, res_ops_d_, scal_d_);
+    stats_.kernel_launches += 2;
+    stats_.evaluations++;
+}
+
+void Solve::enqueue_fpe(int slot)
+{
+    cudaStream_t s = st_;
+    int nb = fpe_col_blocks_ + fpe_row_blocks_;
+    double *part = partials_; // stream order serialises every user of the partials buffer
+    dispatch_rg(residual_group(GAt_), [&](auto GC) {
+        fpe_kernel<GC.value, double><<<nb, TPB, 0, s>>>(n_, m_, At_.rp, At_.ci, At_.v, dx_, dy_, part,
+                                                          fpe_col_blocks_);
+    });
+    fold_partials_kernel<<<1, TPB, 0, s>>>(part, nb, FP_COUNT, fpe_ops_d_, scal_d_ + RS_COUNT + slot * FP_COUNT);
+    stats_.kernel_launches += 2;
+}
+
+
+// ---- main loop (reference optimize, src/solver.cu:121-170) ---------------
+void Solve::read_residual()
+{
+    cudaStream_t s = st_;
+    CK(cudaMemcpyAsync(h_scal_, scal_d_, (RS_COUNT + 2 * FP_COUNT) * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    harvest_step_events();
+    const double *r = h_scal_;
+    bool l2 = prm_.optimality_norm == NORM_TYPE_L2;
+    auto nrm = [&](double v) { return l2 ? std::sqrt(v) : v; };
+    // pending fixed-point errors computed since the previous read
+    auto fpe_of = [&](const double *f) {
+        double pn2 = f[FP_DX2], dn2 = f[FP_DY2], cross = f[FP_CROSS];
+        double movement = pn2 * omega_ + dn2 / omega_;
+        return std::sqrt(movement + 2 * step_ * cross);
+    };
+    if (pending_fpe0_) {
+        fpe0_ = fpe_of(r + RS_COUNT);
+        pending_fpe0_ = false;
+    }
+    if (pending_fpe_slot_ >= 0) {
+        fpe_ = fpe_of(r + RS_COUNT + pending_fpe_slot_ * FP_COUNT);
+        pending_fpe_slot_ = -1;
+    }
+    // compute_residual scalars (reference src/pdhg_core_op.cu:1169-1293)
+    abs_p_ = nrm(r[RS_PRIMAL_RES]) / sb_;
+    double lin_abs_p = abs_p_;
+    abs_d_ = nrm(r[RS_DUAL_RES]) / sc_;
+    double half_xqx = qtype_ == PDHCG_NON_Q ? 0.0 : 0.5 * r[RS_XQX];
+    pobj_ = (r[RS_CX] + half_xqx) / (sb_ * sc_) + P_->objective_constant;
+    dobj_ = (r[RS_SLACKX] + r[RS_PRIMAL_SLACK] - half_xqx) / (sb_ * sc_) + P_->objective_constant;
+    rel_p_ = lin_abs_p / (1.0 + bnorm_);
+    double den;
+    if (qtype_ == PDHCG_NON_Q)
+        den = 1.0 + cnorm_;
+    else
+        den = 1.0 + std::fmax(cnorm_, std::fmax(nrm(r[RS_QX_NORM]) / sc_, nrm(r[RS_ATY_NORM]) / sc_));
+    rel_d_ = abs_d_ / den;
+    gap_ = std::fabs(pobj_ - dobj_);
+    rel_gap_ = gap_ / (1.0 + std::fabs(pobj_) + std::fabs(dobj_));
+    dist_x_ = std::sqrt(r[RS_DIST_X]);
+    dist_y_ = std::sqrt(r[RS_DIST_Y]);
+}
+
+void Solve::loop()
+{
+    const termination_criteria_t &tc = prm_.termination_criteria;
+    const restart_parameters_t &rp = prm_.restart_params;
+    int freq = prm_.termination_evaluation_frequency;
+    bool do_restart = false;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, st_));
+    auto t0 = std::chrono::steady_clock::now();
+    while (k_ < tc.iteration_limit) {
+        if (is_major_ || k_ == 0 || (k_ % print_frequency(k_)) == 0) {
+            bool restart_check = is_major_ || k_ == 0;
+            enqueue_residual(restart_check);
+            read_residual();
+            cum_time_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            // check_termination_criteria (reference src/utils.cu:250-289); the
+            // infeasibility certificates stay zero, which never fires
+            if (rel_d_ < tc.eps_feasible_relative && rel_p_ < tc.eps_feasible_relative &&
+                rel_gap_ < tc.eps_optimal_relative)
+                reason_ = TERMINATION_REASON_OPTIMAL;
+            else if (k_ >= tc.iteration_limit)
+                reason_ = TERMINATION_REASON_ITERATION_LIMIT;
+            else if (cum_time_ >= tc.time_sec_limit)
+                reason_ = TERMINATION_REASON_TIME_LIMIT;
+            if (pdhcg_b200_cancel_requested())
+                reason_ = TERMINATION_REASON_USER_INTERRUPT;
+            if (reason_ != TERMINATION_REASON_UNSPECIFIED)
+                break;
+        }
+        if (is_major_ || k_ == 0) {
+            // should_do_adaptive_restart (reference src/utils.cu:291-322)
+            do_restart = false;
+            if (k_ == freq)
+                do_restart = true;
+            else if (k_ > freq) {
+                if (fpe_ <= rp.sufficient_reduction_for_restart * fpe0_)
+                    do_restart = true;
+                if (fpe_ <= rp.necessary_reduction_for_restart * fpe0_ && fpe_ > fpe_last_)
+                    do_restart = true;
+                if (inner_count_ >= rp.artificial_restart_threshold * k_)
+                    do_restart = true;
+            }
+            fpe_last_ = fpe_;
+            if (do_restart) {
+                // perform_restart (reference src/pdhg_core_op.cu:859-931)
+                double pd = dist_x_, dd = dist_y_, ratio = rel_d_ / rel_p_;
+                if (pd > 1e-16 && dd > 1e-16 && pd < 1e12 && dd < 1e12 && ratio > 1e-8 && ratio < 1e8) {
+                    double err = std::log(dd) - std::log(pd) - std::log(omega_);
+                    pw_err_sum_ *= rp.i_smooth;
+                    pw_err_sum_ += err;
+                    double derr = err - pw_last_err_;
+                    omega_ *= std::exp(rp.k_p * err + rp.k_i * pw_err_sum_ + rp.k_d * derr);
+                    pw_last_err_ = err;
+                } else {
+                    omega_ = best_omega_;
+                    pw_err_sum_ = 0.0;
+                    pw_last_err_ = 0.0;
+                }
+                double g = std::fabs(std::log10(rel_d_ / rel_p_));
+                if (g < best_gap_) {
+                    best_gap_ = g;
+                    best_omega_ = omega_;
+                }
+                restart_copy_kernel<<<grid_for((long long)n_ + m_, TPB), TPB, 0, st_>>>(n_, m_, xp_, x0_, x_, yp_,
+                                                                                        y0_, y_);
+                stats_.kernel_launches++;
+                stats_.restarts++;
+                inner_count_ = 0;
+                fpe_last_ = INFINITY;
+            }
+        }
+        is_major_ = ((k_ + 1) % freq) == 0;
+        bool store_rule = ((k_ + 2) % print_frequency(k_ + 2)) == 0;
+        bool store_primal = is_major_ || store_rule || !cone_start_.empty();
+        bool store_dual = is_major_ || store_rule;
+        bool want_fpe = is_major_ || do_restart;
+        double w = (double)(inner_count_ + 1) / (inner_count_ + 2);
+        enqueue_step(store_primal, store_dual, want_fpe, w);
+        inner_total_++;
+        if (want_fpe) {
+            // The error of this iteration becomes fixed_point_error, and on a
+            // restart also initial_fixed_point_error.  Slot 0 holds a
+            // restart's error, slot 1 a later major iteration's, so both
+            // survive until the next read.
+            int slot = do_restart ? 0 : 1;
+            enqueue_fpe(slot);
+            if (do_restart)
+                pending_fpe0_ = true;
+            pending_fpe_slot_ = slot;
+            do_restart = false;
+        }
+        inner_count_++;
+        k_++;
+        CK(cudaGetLastError());
+    }
+    if (reason_ == TERMINATION_REASON_UNSPECIFIED) {
+        reason_ = TERMINATION_REASON_ITERATION_LIMIT;
+        enqueue_residual(false);
+        read_residual();
+    }
+    CK(cudaEventRecord(e1, st_));
+    CK(cudaEventSynchronize(e1));
+    harvest_step_events();
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    stats_.loop_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    stats_.iterations = k_;
+}
+
+pdhcg_result_t *Solve::make_result()
+{
+    cudaStream_t s = st_;
+    int n = n_, m = m_;
+    double *xo = ar_.alloc<double>(n), *yo = ar_.alloc<double>(m), *rco = ar_.alloc<double>(n);
+    result_kernel<double><<<grid_for((long long)n + m, TPB), TPB, 0, s>>>(
+        n, m, At_.rp, At_.ci, At_.v, c_d_, q_d_, nullptr, qtype_ == PDHCG_DIAG_Q ? 1 : 0, l_d_, u_d_, vr_d_, cr_d_,
+        sb_, sc_, xp_, yp_, xo, yo, rco);
+    pdhcg_result_t *r = (pdhcg_result_t *)std::calloc(1, sizeof(pdhcg_result_t));
+    r->primal_solution = (double *)std::malloc(std::max(n, 1) * sizeof(double));
+    r->dual_solution = (double *)std::malloc(std::max(m, 1) * sizeof(double));
+    r->reduced_cost = (double *)std::malloc(std::max(n, 1) * sizeof(double));
+    CK(cudaMemcpyAsync(r->primal_solution, xo, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(r->dual_solution, yo, m * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(r->reduced_cost, rco, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    r->num_variables = P_->num_variables;
+    r->num_constraints = P_->num_constraints;
+    r->num_nonzeros = P_->constraint_matrix_num_nonzeros;
+    r->total_count = k_;
+    r->total_inner_count = (int)inner_total_;
+    r->cumulative_time_sec = cum_time_;
+    r->relative_primal_residual = rel_p_;
+    r->relative_dual_residual = rel_d_;
+    r->absolute_primal_residual = abs_p_;
+    r->absolute_dual_residual = abs_d_;
+    r->primal_objective_value = pobj_;
+    r->dual_objective_value = dobj_;
+    r->objective_gap = gap_;
+    r->relative_objective_gap = rel_gap_;
+    r->termination_reason = reason_;
+    return r;
+}
+
+pdhcg_result_t *Solve::run()
+{
+    auto t_setup = std::chrono::steady_clock::now();
+    CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    build_host();
+    if (qtype_ != PDHCG_NON_Q && qtype_ != PDHCG_DIAG_Q)
+        throw CudaError("non-diagonal Q (inner BB solve) is not available yet");
+    if (S_ < 0)
+        throw CudaError("cone blocks longer than 256 slots are not supported yet");
+    for (int t : cone_type_)
+        if (t != CONE_STANDARD_SOC && t != CONE_ROTATED_SOC)
+            throw CudaError("only SOC and rotated SOC cones are available on the device path yet");
+    if (P_->cones.is_fixed)
+        throw CudaError("fixed cone slots are not available on the device path yet");
+    if (P_->affine_cones.num_cones > 0)
+        throw CudaError("affine cones are not available on the device path yet");
+    upload_and_preprocess();
+    // reduction scratch sized for the widest user
+    int rg = residual_group(std::min(GA_, GAt_));
+    res_rows_blocks_ = grid_for(m_, TPB / rg, 148 * 8);
+    res_free_blocks_ = grid_for(cone_start_.empty() ? n_ : (long long)free_idx_.size(), TPB / rg, 148 * 8);
+    if (!cone_start_.empty() && free_idx_.empty())
+        res_free_blocks_ = 0;
+    res_cone_blocks_ = cone_start_.empty() ? 0 : grid_for((long long)cone_start_.size(), WARPS, 148 * 8);
+    fpe_col_blocks_ = grid_for(n_, TPB / residual_group(GAt_), 148 * 8);
+    fpe_row_blocks_ = grid_for(m_, TPB, 148 * 4);
+    int maxb = std::max({res_rows_blocks_ + res_free_blocks_ + res_cone_blocks_, fpe_col_blocks_ + fpe_row_blocks_,
+                         148 * 4});
+    partials_ = ar_.alloc<double>((size_t)maxb * RS_COUNT);
+    scal_d_ = ar_.alloc<double>(RS_COUNT + 2 * FP_COUNT);
+    CK(cudaMemsetAsync(scal_d_, 0, (RS_COUNT + 2 * FP_COUNT) * sizeof(double), st_));
+    CK(cudaMallocHost(&h_scal_, (RS_COUNT + 2 * FP_COUNT) * sizeof(double)));
+    {
+        int nop = prm_.optimality_norm == NORM_TYPE_L2 ? RSUM : RMAX;
+        int res_ops[RS_COUNT] = {nop, RSUM, nop, RSUM, RSUM, RSUM, nop, nop, RSUM, RSUM};
+        int fpe_ops[FP_COUNT] = {RSUM, RSUM, RSUM};
+        int norm_ops[NS_COUNT] = {RSUM, RSUM, RMAX, RMAX};
+        res_ops_d_ = ar_.upload(res_ops, RS_COUNT, st_);
+        fpe_ops_d_ = ar_.upload(fpe_ops, FP_COUNT, st_);
+        norm_ops_d_ = ar_.upload(norm_ops, NS_COUNT, st_);
+        CK(cudaStreamSynchronize(st_)); // the uploads above read stack arrays
+    }
+    // unscaled norms for the relative errors (reference src/solver_state.cu:854-934)
+    {
+        int nb = grid_for((long long)n_ + m_, TPB, 148 * 4);
+        norms_kernel<<<nb, TPB, 0, st_>>>(n_, m_, c_d_, lc_d_, uc_d_, g_d_, partials_);
+        fold_partials_kernel<<<1, TPB, 0, st_>>>(partials_, nb, NS_COUNT, norm_ops_d_, scal_d_);
+        double h[NS_COUNT];
+        CK(cudaMemcpyAsync(h, scal_d_, sizeof(h), cudaMemcpyDeviceToHost, st_));
+        CK(cudaStreamSynchronize(st_));
+        if (prm_.optimality_norm == NORM_TYPE_L_INF) {
+            cnorm_ = h[NS_CMAX];
+            bnorm_ = h[NS_BMAX];
+        } else {
+            cnorm_ = std::sqrt(h[NS_C2]);
+            bnorm_ = std::sqrt(h[NS_B2]);
+        }
+        if (P_->num_constraints == 0 || P_->constraint_matrix == nullptr)
+            bnorm_ = 0.0; // the dummy row has infinite bounds and no offset
+    }
+    rescale();
+    init_state();
+    step_size();
+    CK(cudaStreamSynchronize(st_));
+    stats_.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_setup).count();
+    loop();
+    pdhcg_result_t *r = make_result();
+    r->rescaling_time_sec = stats_.setup_ms * 1e-3;
+    double nnz = (double)A_.nnz;
+    stats_.spmv_bytes = 2.0 * nnz * (8 + 4) + 4.0 * ((double)n_ + m_ + 2) + 8.0 * ((double)n_ + m_);
+    stats_.step_bytes = stats_.spmv_bytes + 8.0 * (8.0 * n_ + 5.0 * m_);
+    g_last_stats = stats_;
+    return r;
+}
+
+// Kernel-level step: the solver's fused kernels on caller-owned arrays.
+int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cudaStream_t s)
+{
+    int n = t->n, nc = t->num_cones;
+    int *len_d = nullptr, *free_d = nullptr;
+    int S = 1;
+    if (nc > 0) {
+        std::vector<int> st(nc), vd(nc), tp(nc), len(nc);
+        CK(cudaMemcpyAsync(st.data(), t->cone_start, nc * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(vd.data(), t->cone_vdim, nc * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(tp.data(), t->cone_type, nc * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        std::vector<char> in(n, 0);
+        int maxlen = 0;
+        for (int b = 0; b < nc; ++b) {
+            len[b] = pdhcg_b200_cone_length((cone_type_t)tp[b], vd[b]);
+            maxlen = std::max(maxlen, len[b]);
+            for (int i = 0; i < len[b]; ++i)
+                in[st[b] + i] = 1;
+        }
+        std::vector<int> fr;
+        for (int i = 0; i < n; ++i)
+            if (!in[i])
+                fr.push_back(i);
+        S = slots_class(maxlen);
+        if (S < 0)
+            return -2;
+        CK(cudaMallocAsync((void **)&len_d, nc * sizeof(int), s));
+        CK(cudaMallocAsync((void **)&free_d, std::max<size_t>(fr.size(), 1) * sizeof(int), s));
+        CK(cudaMemcpyAsync(len_d, len.data(), nc * sizeof(int), cudaMemcpyHostToDevice, s));
+        if (!fr.empty())
+            CK(cudaMemcpyAsync(free_d, fr.data(), fr.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s)); // host vectors go out of scope
+        D.free_idx = free_d;
+        D.n_free = (int)fr.size();
+        D.cone_start = t->cone_start;
+        D.cone_len = len_d;
+        D.cone_type = t->cone_type;
+        D.n_cones = nc;
+    }
+    bool hasq = t->q_diag != nullptr;
+    int nfree = nc > 0 ? D.n_free : n;
+    if (nfree > 0) {
+        int grid = grid_for(nfree, TPB);
+        if (hasq)
+            primal_free_kernel<1, double, true, true><<<grid, TPB, 0, s>>>(D, P);
+        else
+            primal_free_kernel<1, double, false, true><<<grid, TPB, 0, s>>>(D, P);
+    }
+    if (nc > 0)
+        dispatch_s(S, [&](auto SC) {
+            if (hasq)
+                primal_cone_kernel<SC.value, double, true><<<grid_for(nc, WARPS), TPB, 0, s>>>(D, P);
+            else
+                primal_cone_kernel<SC.value, double, false><<<grid_for(nc, WARPS), TPB, 0, s>>>(D, P);
+        });
+    if (t->affine_offset)
+        dual_kernel<1, double, false, true><<<grid_for(t->m, TPB), TPB, 0, s>>>(D, P);
+    else
+        dual_kernel<1, double, false, false><<<grid_for(t->m, TPB), TPB, 0, s>>>(D, P);
+    CK(cudaGetLastError());
+    if (len_d)
+        CK(cudaFreeAsync(len_d, s));
+    if (free_d)
+        CK(cudaFreeAsync(free_d, s));
+    return 0;
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// C entry points
+// ---------------------------------------------------------------------------
+
+static volatile std::sig_atomic_t g_cancel = 0;
+
+extern "C" {
+
+int pdhcg_b200_cancel_requested(void) { return g_cancel != 0; }
+
+void pdhcg_b200_request_cancel(int on) { g_cancel = on ? 1 : 0; }
+
+void pdhcg_b200_default_options(pdhcg_b200_options_t *o)
+{
+    std::memset(o, 0, sizeof(*o));
+    o->precision = PDHCG_B200_FP64;
+    o->polish_threshold = 1e-5;
+}
+
+pdhcg_result_t *pdhcg_b200_solve(const qp_problem_t *prob, const pdhg_parameters_t *params,
+                                 const pdhcg_b200_options_t *opts)
+{
+    if (!prob) {
+        std::fprintf(stderr, "[interface] solve_qp_problem: invalid arguments.\n");
+        return nullptr;
+    }
+    pdhg_parameters_t prm;
+    if (params)
+        prm = *params;
+    else
+        set_default_parameters(&prm);
+    pdhcg_b200_options_t opt;
+    if (opts)
+        opt = *opts;
+    else
+        pdhcg_b200_default_options(&opt);
+    try {
+        Solve s(prob, prm, opt);
+        pdhcg_result_t *r = s.run();
+        if (r && prm.verbose >= 1) {
+            std::printf("Solution Summary\n");
+            std::printf("  Status             : %d\n", (int)r->termination_reason);
+            std::printf("  Solve time         : %.3g sec\n", r->cumulative_time_sec);
+            std::printf("  Iterations         : %d\n", r->total_count);
+            std::printf("  Primal objective   : %.10g\n", r->primal_objective_value);
+            std::printf("  Dual objective     : %.10g\n", r->dual_objective_value);
+            std::printf("  Objective gap      : %.3e\n", r->relative_objective_gap);
+            std::printf("  Primal infeas      : %.3e\n", r->relative_primal_residual);
+            std::printf("  Dual infeas        : %.3e\n", r->relative_dual_residual);
+        }
+        return r;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "[pdhcg_b200] solve failed: %s\n", e.what());
+        return nullptr;
+    }
+}
+
+pdhcg_result_t *solve_qp_problem(const qp_problem_t *prob, const pdhg_parameters_t *params)
+{
+    return pdhcg_b200_solve(prob, params, nullptr);
+}
+
+int pdhcg_b200_last_stats(pdhcg_b200_stats_t *out)
+{
+    if (!out)
+        return -1;
+    *out = g_last_stats;
+    return 0;
+}
+
+int pdhcg_b200_csr_spmv(int rows, const int *row_ptr, const int *col_ind, const double *val, const double *x,
+                        double *y, void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    spmv_kernel<1><<<grid_for(rows, TPB), TPB, 0, s>>>(rows, row_ptr, col_ind, val, x, y);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *cone_vdim, const int *cone_type,
+                             const double *cone_alpha, double *x, const double *d, const double *q, double tau,
+                             void *stream)
+{
+    (void)cone_alpha;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (num_cones <= 0)
+        return 0;
+    // cone lengths from v_dim (SOC / RSOC: v_dim + 2) on the device
+    int *len = nullptr;
+    if (cudaMallocAsync((void **)&len, num_cones * sizeof(int), s) != cudaSuccess)
+        return -1;
+    cone_len_kernel<<<grid_for(num_cones, TPB), TPB, 0, s>>>(num_cones, cone_vdim, cone_type, len);
+    int maxlen = 0;
+    {
+        std::vector<int> h(num_cones);
+        cudaMemcpyAsync(h.data(), len, num_cones * sizeof(int), cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        for (int v : h)
+            maxlen = std::max(maxlen, v);
+    }
+    int S = slots_class(maxlen);
+    if (S < 0) {
+        cudaFreeAsync(len, s);
+        return -2;
+    }
+    dispatch_s(S, [&](auto SC) {
+        project_cones_kernel<SC.value><<<grid_for(num_cones, WARPS), TPB, 0, s>>>(num_cones, cone_start, len,
+                                                                                 cone_type, x, d, q, tau);
+    });
+    cudaFreeAsync(len, s);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int pdhcg_b200_pdhg_step(const pdhcg_b200_step_t *t, void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    StepData<double> D{};
+    D.n = t->n;
+    D.m = t->m;
+    D.A_rp = t->A_row_ptr;
+    D.A_ci = t->A_col_ind;
+    D.A_v = t->A_val;
+    D.At_rp = t->At_row_ptr;
+    D.At_ci = t->At_col_ind;
+    D.At_v = t->At_val;
+    D.c = t->c;
+    D.l = t->var_lb;
+    D.u = t->var_ub;
+    D.q = t->q_diag;
+    D.lc = t->con_lb;
+    D.uc = t->con_ub;
+    D.g = t->affine_offset;
+    D.vr = t->var_rescale;
+    D.free_idx = nullptr;
+    D.n_free = 0;
+    D.n_cones = 0;
+    D.x0 = t->x_init;
+    D.x = t->x_cur;
+    D.xp = t->x_pdhg;
+    D.xr = t->x_refl;
+    D.dx = t->x_refl; // unused (want_fpe = 0)
+    D.dual_slack = nullptr;
+    D.y0 = t->y_init;
+    D.y = t->y_cur;
+    D.yp = t->y_pdhg;
+    D.dy = nullptr;
+    StepParams P{t->tau, t->sigma, t->halpern_weight, t->reflection, 1, 1, 0, 0};
+    // the kernel-level step keeps cone handling separate: free kernel over all
+    // variables, then project + re-reflect cone blocks, then the dual kernel.
+    // Halpern is applied at the end so the cone correction sees x_cur.
+    try {
+        return step_impl(D, P, t, s);
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "[pdhcg_b200] step failed: %s\n", e.what());
+        return -1;
+    }
+}
+
+} // extern "C"

@@ -1,0 +1,152 @@
+"""Seeded synthetic instances of the benchmark workloads.
+
+The reference publishes no benchmark data, so every workload is generated
+from a seed with the shapes and value distributions of its description:
+
+- ``sparse_qp``      random sparse convex QP, n=10000, m=5000, 8 nnz/row,
+                     Q = B'B + 0.1 I with B 2000 x n, 4 nnz/row (BB inner solve)
+- ``soc_qp``         SOC-constrained QP, n=1e6, m=5e5, 10 nnz/row, diagonal Q,
+                     20000 SOC blocks of 50 slots, equality rows b = A x0 with
+                     x0 strictly inside the cones
+- ``portfolio``      low-rank portfolio QP with a rotated-SOC tracking-error block
+- ``mpc_batch``      batched uneven MPC-style QPs
+- ``parametric_qp``  parametric family for the learned warm start
+
+Every generator takes a ``scale`` in (0, 1] that shrinks the sizes for
+parity tests while keeping the structure.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+
+from .capi import CONE_ROTATED_SOC, CONE_STANDARD_SOC, Cone, CsrMatrix, Problem
+
+
+def random_csr(rng: np.random.Generator, m: int, n: int, per_row: int, values: str = "normal") -> CsrMatrix:
+    """m x n CSR with exactly ``per_row`` distinct uniform columns per row."""
+    k = min(per_row, n)
+    cols = rng.integers(0, n, size=(m, k), dtype=np.int64)
+    cols.sort(axis=1)
+    for _ in range(64):
+        dup = np.zeros_like(cols, dtype=bool)
+        dup[:, 1:] = cols[:, 1:] == cols[:, :-1]
+        nd = int(dup.sum())
+        if nd == 0:
+            break
+        cols[dup] = rng.integers(0, n, size=nd)
+        cols.sort(axis=1)
+    vals = rng.standard_normal((m, k)) if values == "normal" else rng.uniform(-1, 1, (m, k))
+    row_ptr = np.arange(0, (m + 1) * k, k, dtype=np.int32)
+    return CsrMatrix(m, n, row_ptr, cols.reshape(-1).astype(np.int32), vals.reshape(-1).astype(np.float64))
+
+
+def sparse_qp(seed: int = 1, scale: float = 1.0) -> Problem:
+    """Random sparse convex QP (sparse Q, inner BB solve)."""
+    rng = np.random.default_rng(seed)
+    n = max(20, int(10000 * scale))
+    m = max(10, int(5000 * scale))
+    nb = max(4, int(2000 * scale))
+    A = random_csr(rng, m, n, 8)
+    B = random_csr(rng, nb, n, 4).to_scipy()
+    Q = (B.T @ B + 0.1 * sp.identity(n, format="csr")).tocsr()
+    Q.sort_indices()
+    c = rng.standard_normal(n)
+    x0 = rng.uniform(-1, 1, n)
+    ax = A.to_scipy() @ x0
+    lo = ax - rng.uniform(0, 1, m)
+    up = ax + rng.uniform(0, 1, m)
+    return Problem(c=c, A=A, con_lb=lo, con_ub=up, var_lb=np.full(n, -10.0), var_ub=np.full(n, 10.0),
+                   Q=CsrMatrix.from_scipy(Q))
+
+
+def soc_qp(seed: int = 2, scale: float = 1.0, block: int = 50) -> Problem:
+    """SOC-constrained QP with a diagonal Q; all variables in SOC blocks."""
+    rng = np.random.default_rng(seed)
+    nblocks = max(2, int(20000 * scale))
+    n = nblocks * block
+    m = n // 2
+    A = random_csr(rng, m, n, 10)
+    q = rng.uniform(0.01, 1.0, n)
+    c = rng.standard_normal(n)
+    # x0 strictly inside every block: z = |(v, w)| + 1
+    x0 = rng.standard_normal(n)
+    xb = x0.reshape(nblocks, block)
+    xb[:, -1] = np.linalg.norm(xb[:, :-1], axis=1) + 1.0
+    x0 = xb.reshape(-1)
+    b = A.to_scipy() @ x0
+    cones = [Cone(CONE_STANDARD_SOC, i * block, block - 2) for i in range(nblocks)]
+    Q = CsrMatrix(n, n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), q)
+    return Problem(c=c, A=A, con_lb=b, con_ub=b.copy(), var_lb=np.full(n, -np.inf), var_ub=np.full(n, np.inf),
+                   Q=Q, cones=cones)
+
+
+def box_lp(seed: int = 3, n: int = 300, m: int = 150) -> Problem:
+    """Feasible random LP with row ranges and a box."""
+    rng = np.random.default_rng(seed)
+    A = random_csr(rng, m, n, 6)
+    x0 = rng.uniform(-1, 1, n)
+    ax = A.to_scipy() @ x0
+    lo = ax - rng.uniform(0, 1, m)
+    up = ax + rng.uniform(0, 1, m)
+    eq = rng.random(m) < 0.3
+    up[eq] = lo[eq] = ax[eq]
+    return Problem(c=rng.standard_normal(n), A=A, con_lb=lo, con_ub=up, var_lb=np.full(n, -2.0),
+                   var_ub=np.full(n, 2.0))
+
+
+def diag_qp(seed: int = 4, n: int = 300, m: int = 150) -> Problem:
+    p = box_lp(seed, n, m)
+    rng = np.random.default_rng(seed + 100)
+    q = rng.uniform(0.05, 1.0, n)
+    p.Q = CsrMatrix(n, n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), q)
+    return p
+
+
+def conic_lp(seed: int = 5, nfree: int = 60, nsoc: int = 10, soc_len: int = 12, nrsoc: int = 4,
+             rsoc_len: int = 8, with_q: bool = False) -> Problem:
+    """Free box variables plus SOC and rotated-SOC blocks, equality rows
+    through a strictly feasible point (so the problem is feasible)."""
+    rng = np.random.default_rng(seed)
+    n = nfree + nsoc * soc_len + nrsoc * rsoc_len
+    m = n // 3
+    A = random_csr(rng, m, n, 5)
+    x0 = np.zeros(n)
+    x0[:nfree] = rng.uniform(-0.5, 0.5, nfree)
+    cones = []
+    st = nfree
+    for _ in range(nsoc):
+        v = rng.standard_normal(soc_len - 1)
+        x0[st:st + soc_len - 1] = v
+        x0[st + soc_len - 1] = np.linalg.norm(v) + 1.0
+        cones.append(Cone(CONE_STANDARD_SOC, st, soc_len - 2))
+        st += soc_len
+    for _ in range(nrsoc):
+        v = rng.standard_normal(rsoc_len - 2)
+        s_ = 1.0 + rng.random()
+        x0[st:st + rsoc_len - 2] = v
+        x0[st + rsoc_len - 2] = s_
+        x0[st + rsoc_len - 1] = (v @ v) / (2 * s_) + 1.0
+        cones.append(Cone(CONE_ROTATED_SOC, st, rsoc_len - 2))
+        st += rsoc_len
+    b = A.to_scipy() @ x0
+    lb = np.full(n, -np.inf)
+    ub = np.full(n, np.inf)
+    lb[:nfree] = -1.0
+    ub[:nfree] = 1.0
+    # a bounded objective: c in the interior of the dual cone on cone slots
+    c = rng.standard_normal(n) * 0.5
+    st = nfree
+    for k in cones:
+        L = k.v_dim + 2
+        if k.type == CONE_STANDARD_SOC:
+            c[st + L - 1] = np.linalg.norm(c[st:st + L - 1]) + 1.0
+        else:
+            c[st + L - 2] = abs(c[st + L - 2]) + 1.0
+            c[st + L - 1] = (c[st:st + L - 2] @ c[st:st + L - 2]) / (2 * c[st + L - 2]) + 1.0
+        st += L
+    p = Problem(c=c, A=A, con_lb=b, con_ub=b.copy(), var_lb=lb, var_ub=ub, cones=cones)
+    if with_q:
+        q = rng.uniform(0.1, 1.0, n)
+        p.Q = CsrMatrix(n, n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), q)
+    return p

@@ -1,0 +1,164 @@
+"""Kernel-level parity through the C ABI (device pointers from torch):
+SpMV against scipy, cone projections and one fused PDHG step against the
+oracle.  FP64 throughout; tolerance 1e-12 relative (different summation
+order only) except projections found by root finding (1e-9)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from pdhcg_b200 import capi, instances, native
+
+pytestmark = pytest.mark.gpu
+_dp = C.POINTER(C.c_double)
+
+
+def _dev(a, dtype=None):
+    import torch
+    t = torch.as_tensor(np.ascontiguousarray(a, dtype=dtype)).cuda()
+    return t
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def test_csr_spmv_matches_scipy(lib):
+    import torch
+    rng = np.random.default_rng(0)
+    for rows, cols, per in [(1000, 700, 8), (37, 5000, 300), (5000, 10, 3)]:
+        M = instances.random_csr(rng, rows, cols, per)
+        x = rng.standard_normal(cols)
+        rp, ci, v, xd = _dev(M.row_ptr, np.int32), _dev(M.col_ind, np.int32), _dev(M.val), _dev(x)
+        y = torch.zeros(rows, dtype=torch.float64, device="cuda")
+        assert lib.pdhcg_b200_csr_spmv(rows, _ptr(rp), _ptr(ci), _ptr(v), _ptr(xd), _ptr(y), None) == 0
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(y.cpu().numpy(), M.to_scipy() @ x, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+@pytest.mark.parametrize("uniform_d", [False, True])
+def test_cone_projection_matches_oracle(lib, oracle, weighted, uniform_d):
+    import torch
+    rng = np.random.default_rng(1 + 2 * weighted + uniform_d)
+    blocks = []
+    st = 0
+    for L, t in [(3, 1), (5, 0), (50, 1), (33, 1), (102, 0), (4, 0), (250, 1), (64, 0)] * 3:
+        blocks.append((st, L, t))
+        st += L
+    n = st
+    x = rng.standard_normal(n) * 2
+    d = np.ones(n) * 1.7 if uniform_d else rng.uniform(0.5, 2.0, n)
+    if uniform_d:
+        for s0, L, t in blocks:  # uniform within each block, varying across
+            d[s0:s0 + L] = rng.uniform(0.5, 2.0)
+    q = rng.uniform(0.0, 2.0, n) if weighted else None
+    tau = 0.37
+    expect = x.copy()
+    for s0, L, t in blocks:
+        blk = expect[s0:s0 + L].copy()
+        dd = d[s0:s0 + L].copy()
+        qq = q[s0:s0 + L].copy() if weighted else None
+        oracle.oracle_project_cone_block(t, L - 2, 0.0, blk.ctypes.data_as(_dp), dd.ctypes.data_as(_dp),
+                                         qq.ctypes.data_as(_dp) if weighted else None, tau)
+        expect[s0:s0 + L] = blk
+    starts = _dev([b[0] for b in blocks], np.int32)
+    vdims = _dev([b[1] - 2 for b in blocks], np.int32)
+    types = _dev([b[2] for b in blocks], np.int32)
+    xd, dd_, qd = _dev(x), _dev(d), (_dev(q) if weighted else None)
+    rc = lib.pdhcg_b200_project_cones(len(blocks), _ptr(starts), _ptr(vdims), _ptr(types), None, _ptr(xd),
+                                      _ptr(dd_), _ptr(qd), tau, None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    got = xd.cpu().numpy()
+    tol = 1e-12 if (uniform_d and not weighted) else 1e-9
+    np.testing.assert_allclose(got, expect, rtol=tol, atol=tol * np.abs(expect).max())
+
+
+@pytest.mark.parametrize("with_q,with_cones", [(False, False), (True, False), (False, True), (True, True)])
+def test_fused_step_matches_oracle(lib, oracle, with_q, with_cones):
+    import torch
+    p = instances.conic_lp(seed=21, with_q=with_q) if with_cones else (
+        instances.diag_qp(seed=22) if with_q else instances.box_lp(seed=23))
+    rng = np.random.default_rng(5)
+    n, m = p.n, p.A.m
+    A = p.A.to_scipy().tocsr()
+    At = A.T.tocsr()
+    At.sort_indices()
+    q = p.Q.val.copy() if with_q else None
+    vr = rng.uniform(0.5, 2.0, n)
+    for k in p.cones:
+        vr[k.start:k.start + k.v_dim + 2] = vr[k.start]
+    x0, x, y0, y = (rng.standard_normal(n), rng.standard_normal(n), rng.standard_normal(m), rng.standard_normal(m))
+    tau, sigma, w, rho = 0.3, 0.7, 5.0 / 6.0, 1.0
+    lb = np.where(np.isfinite(p.var_lb), p.var_lb, -np.inf)
+    ub = np.where(np.isfinite(p.var_ub), p.var_ub, np.inf)
+
+    # oracle
+    class OStep(C.Structure):
+        _fields_ = [("n", C.c_int), ("m", C.c_int)] + [(f, C.c_void_p) for f in (
+            "A_row_ptr", "A_col_ind", "A_val", "At_row_ptr", "At_col_ind", "At_val", "c", "var_lb", "var_ub",
+            "q_diag", "con_lb", "con_ub", "affine_offset", "var_rescale")] + [
+            ("num_cones", C.c_int)] + [(f, C.c_void_p) for f in ("cone_start", "cone_vdim", "cone_type", "cone_alpha")] + [
+            (f, C.c_double) for f in ("tau", "sigma", "halpern_weight", "reflection")] + [
+            (f, C.c_void_p) for f in ("x_init", "x_cur", "y_init", "y_cur", "x_pdhg", "x_refl", "y_pdhg", "y_refl",
+                                      "Aty", "Ax")]
+
+    host = {}
+
+    def h(name, a, dt=np.float64):
+        host[name] = np.ascontiguousarray(a, dtype=dt)
+        return host[name].ctypes.data
+
+    cst = [k.start for k in p.cones]
+    cvd = [k.v_dim for k in p.cones]
+    cty = [k.type for k in p.cones]
+    o = OStep()
+    o.n, o.m = n, m
+    o.A_row_ptr, o.A_col_ind, o.A_val = h("arp", A.indptr, np.int32), h("aci", A.indices, np.int32), h("av", A.data)
+    o.At_row_ptr, o.At_col_ind, o.At_val = (h("trp", At.indptr, np.int32), h("tci", At.indices, np.int32),
+                                            h("tv", At.data))
+    o.c, o.var_lb, o.var_ub = h("c", p.c), h("lb", lb), h("ub", ub)
+    o.q_diag = h("q", q) if with_q else None
+    o.con_lb, o.con_ub, o.affine_offset = h("lc", p.con_lb), h("uc", p.con_ub), None
+    o.var_rescale = h("vr", vr)
+    o.num_cones = len(cst)
+    o.cone_start, o.cone_vdim, o.cone_type = (h("cs", cst, np.int32), h("cv", cvd, np.int32),
+                                              h("ct", cty, np.int32))
+    o.cone_alpha = None
+    o.tau, o.sigma, o.halpern_weight, o.reflection = tau, sigma, w, rho
+    o.x_init, o.x_cur, o.y_init, o.y_cur = h("x0", x0), h("x", x), h("y0", y0), h("y", y)
+    for f, k in (("x_pdhg", n), ("x_refl", n), ("y_pdhg", m), ("y_refl", m), ("Aty", n), ("Ax", m)):
+        setattr(o, f, h(f, np.zeros(k)))
+    oracle.oracle_pdhg_step.argtypes = [C.POINTER(OStep)]
+    oracle.oracle_pdhg_step(C.byref(o))
+
+    # device
+    dev = {}
+
+    def d(name, a, dt=np.float64):
+        dev[name] = _dev(a, dt)
+        return dev[name].data_ptr()
+
+    s = native.StepArgs()
+    s.n, s.m = n, m
+    s.A_row_ptr, s.A_col_ind, s.A_val = d("arp", A.indptr, np.int32), d("aci", A.indices, np.int32), d("av", A.data)
+    s.At_row_ptr, s.At_col_ind, s.At_val = (d("trp", At.indptr, np.int32), d("tci", At.indices, np.int32),
+                                            d("tv", At.data))
+    s.c, s.var_lb, s.var_ub = d("c", p.c), d("lb", lb), d("ub", ub)
+    s.q_diag = d("q", q) if with_q else None
+    s.con_lb, s.con_ub, s.affine_offset = d("lc", p.con_lb), d("uc", p.con_ub), None
+    s.var_rescale = d("vr", vr)
+    s.num_cones = len(cst)
+    if cst:
+        s.cone_start, s.cone_vdim, s.cone_type = d("cs", cst, np.int32), d("cv", cvd, np.int32), d("ct", cty, np.int32)
+    s.tau, s.sigma, s.halpern_weight, s.reflection = tau, sigma, w, rho
+    s.x_init, s.x_cur, s.y_init, s.y_cur = d("x0", x0), d("x", x), d("y0", y0), d("y", y)
+    for f, k in (("x_pdhg", n), ("x_refl", n), ("y_pdhg", m), ("y_refl", m), ("Aty", n), ("Ax", m)):
+        setattr(s, f, d(f, np.zeros(k)))
+    assert lib.pdhcg_b200_pdhg_step(C.byref(s), None) == 0
+    torch.cuda.synchronize()
+    tol = 1e-9 if with_cones else 1e-12
+    for key in ("x_pdhg", "x_refl", "x", "y_pdhg", "y"):
+        np.testing.assert_allclose(dev[key].cpu().numpy(), host[key], rtol=tol, atol=tol, err_msg=key)

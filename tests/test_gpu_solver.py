@@ -1,0 +1,86 @@
+"""Whole solves on the GPU through the C ABI, checked against the oracle and
+against the answers of the reference's own end-to-end tests.
+
+Tolerances: both sides run the same FP64 iteration, but the device sums
+in a different order, so trajectories agree to rounding and drift apart
+slowly.  The termination status must be identical; objectives must agree to
+within the termination tolerance; iteration counts within 25 %.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from pdhcg_b200 import capi, instances, native
+from problems import KNOWN_ANSWERS, check_known_answer
+
+pytestmark = pytest.mark.gpu
+
+
+def _solve_gpu(lib, p, params):
+    prob, keep = capi.build(lib, p)
+    assert prob
+    prm = capi.default_params(lib, **params)
+    r = lib.solve_qp_problem(prob, C.byref(prm))
+    assert r, "solve_qp_problem returned NULL"
+    m = p.A.m if p.A is not None else 0
+    d = capi.result_dict(r, p.n, max(m, 1))
+    lib.pdhcg_result_free(r)
+    lib.qp_problem_free(prob)
+    return d
+
+
+def _solve_oracle(oracle, lib, p, params):
+    prob, keep = capi.build(lib, p)
+    prm = capi.default_params(lib, **params)
+    r = oracle.oracle_solve(prob, C.byref(prm))
+    assert r
+    m = p.A.m if p.A is not None else 0
+    d = capi.result_dict(r, p.n, max(m, 1))
+    oracle.oracle_result_free(r)
+    lib.qp_problem_free(prob)
+    return d
+
+
+@pytest.mark.parametrize("name", sorted(n for n in KNOWN_ANSWERS if n != "sparse_q_soc"))
+def test_known_answers_on_gpu(lib, name):
+    p, prm, expect = KNOWN_ANSWERS[name]()
+    res = _solve_gpu(lib, p, prm)
+    check_known_answer(res, expect)
+
+
+CASES = {
+    "box_lp": (lambda: instances.box_lp(), {}),
+    "diag_qp": (lambda: instances.diag_qp(), {}),
+    "conic_lp": (lambda: instances.conic_lp(), {}),
+    "conic_qp": (lambda: instances.conic_lp(with_q=True), {}),
+    "soc_qp_small": (lambda: instances.soc_qp(scale=0.001),
+                     {"termination_criteria.eps_optimal_relative": 1e-6,
+                      "termination_criteria.eps_feasible_relative": 1e-6}),
+    "diag_qp_l2": (lambda: instances.diag_qp(seed=9), {"optimality_norm": capi.NORM_L2}),
+    "box_lp_no_bound_obj": (lambda: instances.box_lp(seed=8), {"bound_objective_rescaling": False}),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_gpu_matches_oracle(lib, oracle, name):
+    make, prm = CASES[name]
+    p = make()
+    prm = {"termination_criteria.iteration_limit": 100000, **prm}
+    g = _solve_gpu(lib, p, prm)
+    o = _solve_oracle(oracle, lib, p, prm)
+    assert g["status"] == o["status"] == "OPTIMAL"
+    eps = prm.get("termination_criteria.eps_optimal_relative", 1e-4)
+    assert abs(g["primal_objective_value"] - o["primal_objective_value"]) <= 10 * eps * (
+        1 + abs(o["primal_objective_value"]))
+    assert abs(g["total_count"] - o["total_count"]) <= max(40, 0.25 * o["total_count"]), (
+        g["total_count"], o["total_count"])
+    assert g["rel_kkt"] < eps
+
+
+def test_gpu_iteration_limit_and_result_fields(lib):
+    p = instances.box_lp(seed=11)
+    g = _solve_gpu(lib, p, {"termination_criteria.iteration_limit": 37})
+    assert g["status"] == "ITERATION_LIMIT"
+    assert g["total_count"] == 37
+    assert np.all(np.isfinite(g["x"])) and np.all(np.isfinite(g["y"]))
