@@ -204,7 +204,8 @@ def run_ours(args):
                 "d2h_bytes_per_step": int(8 * (2 * problem.n + problem.A.m))},
         "gpu_launches": int(stats["kernel_launches"]) * args.steps,
         "clocks": clocks,
-        "setup_ms": stats["setup_ms"], "loop_ms": stats["loop_ms"],
+        "breakdown_ms": {k: stats[k] for k in ("host_copy_ms", "upload_ms", "setup_ms", "loop_ms", "result_ms",
+                                               "total_ms")},
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(problem, res["total_count"])

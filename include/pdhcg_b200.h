@@ -52,7 +52,11 @@ typedef struct {
     int evaluations;
     double step_bytes;           /* algorithmic HBM bytes of one primal + dual step */
     double spmv_bytes;           /* algorithmic bytes of the two SpMVs inside one step */
-    double reserved[6];
+    double host_copy_ms;         /* host-side copy / classification of the problem */
+    double upload_ms;            /* allocation and host->device copies */
+    double result_ms;            /* result kernel and device->host copies */
+    double total_ms;             /* the whole call, wall clock */
+    double reserved[2];
 } pdhcg_b200_stats_t;
 
 int pdhcg_b200_last_stats(pdhcg_b200_stats_t *out);

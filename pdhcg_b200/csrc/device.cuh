@@ -97,11 +97,13 @@ struct WarpSlots {
 };
 
 // Standard SOC [v(k), w, z]: L = k + 2, apex slot index L-1.
+// warm: this cone's multiplier from the previous call (NULL: none); on a
+// root-finding exit the new multiplier is stored there (the reference keeps
+// the same per-cone warm start, internal/internal_types.h:250).
 template <int S>
-__device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform_unit)
+__device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform_unit, double *warm)
 {
     const int apex = L - 1;
-    // apex values broadcast from the owning lane
     const int apex_lane = apex & 31, apex_s = apex >> 5;
     double xz = 0.0, dz = 1.0, wz = 1.0;
 #pragma unroll
@@ -145,19 +147,20 @@ __device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform
         return;
     }
 
-    // u-space data
-    double a[S], om[S];
+    // u-space data: a = x / d, omega = w d^2; b = omega * a
+    double b[S], om[S];
     double n2 = 0.0, p2 = 0.0;
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         int i = lane + 32 * s;
-        a[s] = 0.0;
+        b[s] = 0.0;
         om[s] = 1.0;
         if (i < apex) {
-            a[s] = sl.x[s] / sl.d[s];
+            double a = sl.x[s] / sl.d[s];
             om[s] = fmax(sl.w[s] * sl.d[s] * sl.d[s], DBL_MIN);
-            n2 += a[s] * a[s];
-            p2 += (om[s] * a[s]) * (om[s] * a[s]);
+            b[s] = om[s] * a;
+            n2 += a * a;
+            p2 += b[s] * b[s];
         }
     }
     n2 = warp_sum(n2);
@@ -173,76 +176,62 @@ __device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform
                 sl.x[s] = 0.0;
         return;
     }
-    double lam;
-    double uz;
+    double lam, uz;
     if (az == 0.0) {
         lam = omz;
         double t2 = 0.0;
 #pragma unroll
         for (int s = 0; s < S; ++s)
             if (lane + 32 * s < apex) {
-                double t = om[s] * a[s] / (om[s] + lam);
+                double t = b[s] / (om[s] + lam);
                 t2 += t * t;
             }
         uz = sqrt(warp_sum(t2));
     } else {
+        // f(lam) = |U|^2 - Z^2 with U_i = b_i/(om_i+lam), Z = omz az/(omz-lam);
+        // root in (0, omz) when az > 0, in (omz, inf) when az < 0.
         const bool lower = az > 0.0;
-        double lo, hi;
-        if (lower) {
-            lo = 0.0;
-            hi = omz * (1.0 - 1e-14);
-        } else {
-            lo = omz * (1.0 + 1e-14);
-            hi = 2.0 * omz;
-            for (int e = 0; e < 200; ++e) {
-                double t2 = 0.0;
-#pragma unroll
-                for (int s = 0; s < S; ++s)
-                    if (lane + 32 * s < apex) {
-                        double t = om[s] * a[s] / (om[s] + hi);
-                        t2 += t * t;
-                    }
-                t2 = warp_sum(t2);
-                double z = omz * az / (omz - hi);
-                if (t2 - z * z >= 0.0)
-                    break;
-                lo = hi;
-                hi *= 2.0;
-            }
-        }
-        lam = 0.5 * (lo + hi);
+        const double bz = omz * az;
+        double lo = lower ? 0.0 : omz * (1.0 + 1e-14);
+        double hi = lower ? omz * (1.0 - 1e-14) : INFINITY;
+        double w0 = warm ? *warm : -1.0;
+        lam = (w0 > lo && w0 < hi && isfinite(w0)) ? w0 : (lower ? 0.5 * (lo + hi) : 2.0 * omz);
         for (int it = 0; it < ROOT_ITERS; ++it) {
             double t2 = 0.0, dt2 = 0.0;
 #pragma unroll
             for (int s = 0; s < S; ++s)
                 if (lane + 32 * s < apex) {
-                    double t = om[s] * a[s] / (om[s] + lam);
+                    double inv = 1.0 / (om[s] + lam);
+                    double t = b[s] * inv;
                     t2 += t * t;
-                    dt2 -= 2.0 * t * t / (om[s] + lam);
+                    dt2 += t * t * inv;
                 }
             t2 = warp_sum(t2);
             dt2 = warp_sum(dt2);
-            double z = omz * az / (omz - lam);
+            double izl = 1.0 / (omz - lam);
+            double z = bz * izl;
             double f = t2 - z * z;
-            double df = dt2 - 2.0 * z * z / (omz - lam);
+            double df = -2.0 * dt2 - 2.0 * z * z * izl;
             if ((lower && f > 0.0) || (!lower && f < 0.0))
                 lo = lam;
             else
                 hi = lam;
-            if (fabs(f) <= 1e-13 * (1.0 + t2 + z * z) || hi - lo <= 1e-13 * (1.0 + hi + lo))
+            if (fabs(f) <= 1e-13 * (1.0 + t2 + z * z) || (isfinite(hi) && hi - lo <= 1e-13 * (1.0 + hi + lo)))
                 break;
             double nx = lam - f / df;
             if (!isfinite(nx) || !(nx > lo && nx < hi))
-                nx = 0.5 * (lo + hi);
+                nx = isfinite(hi) ? 0.5 * (lo + hi) : 2.0 * lam;
             lam = nx;
         }
-        uz = omz * az / (omz - lam);
+        uz = bz / (omz - lam);
+        if (warm && lane == 0)
+            *warm = lam;
     }
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         int i = lane + 32 * s;
         if (i < apex)
-            sl.x[s] = (om[s] * a[s] / (om[s] + lam)) * sl.d[s];
+            sl.x[s] = (b[s] / (om[s] + lam)) * sl.d[s];
         else if (i == apex)
             sl.x[s] = uz * dz;
     }
@@ -250,7 +239,7 @@ __device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform
 
 // Rotated SOC [v(k), s, t]: 2 s t >= |v|^2, s, t >= 0.  L = k + 2.
 template <int S>
-__device__ void warp_project_rsoc(WarpSlots<S> &sl, int L, int lane, bool uniform_unit)
+__device__ void warp_project_rsoc(WarpSlots<S> &sl, int L, int lane, bool uniform_unit, double *warm)
 {
     const int is = L - 2, it_ = L - 1;
     double xs = 0.0, xt = 0.0, ds = 1.0, dt = 1.0, ws = 1.0, wt = 1.0;
@@ -284,8 +273,6 @@ __device__ void warp_project_rsoc(WarpSlots<S> &sl, int L, int lane, bool unifor
             if (lane + 32 * s < is)
                 ss += sl.x[s] * sl.x[s];
         double r = sqrt(wv * wv + warp_sum(ss));
-        // reference order: sumsq starts at w*w then adds v's; summation
-        // order differs only by rounding
         if (r <= zv)
             return;
         if (r <= -zv) {
@@ -359,61 +346,42 @@ __device__ void warp_project_rsoc(WarpSlots<S> &sl, int L, int lane, bool unifor
         ps = (st + delta) / sqs;
         pt = st / sqt;
     } else {
+        // f(lam) = |U|^2 - 2 s t; root in (0, rm) when balance > 0, else (rm, inf)
         const bool lower = balance > 0.0;
-        double lo, hi;
-        if (lower) {
-            lo = 0.0;
-            hi = rm * (1.0 - 1e-14);
-        } else {
-            lo = rm * (1.0 + 1e-14);
-            hi = 2.0 * rm;
-            for (int e = 0; e < 200; ++e) {
-                double t2 = 0.0;
-#pragma unroll
-                for (int s = 0; s < S; ++s)
-                    if (lane + 32 * s < is) {
-                        double t = om[s] * a[s] / (om[s] + hi);
-                        t2 += t * t;
-                    }
-                t2 = warp_sum(t2);
-                double det = oms * omt - hi * hi;
-                double sv = omt * (oms * as + hi * at) / det, tv = oms * (omt * at + hi * as) / det;
-                double f = (sv >= 0.0 && tv >= 0.0) ? t2 - 2.0 * sv * tv : INFINITY;
-                if (f >= 0.0)
-                    break;
-                lo = hi;
-                hi *= 2.0;
-            }
-        }
-        lam = 0.5 * (lo + hi);
+        double lo = lower ? 0.0 : rm * (1.0 + 1e-14);
+        double hi = lower ? rm * (1.0 - 1e-14) : INFINITY;
+        double w0 = warm ? *warm : -1.0;
+        lam = (w0 > lo && w0 < hi && isfinite(w0)) ? w0 : (lower ? 0.5 * (lo + hi) : 2.0 * rm);
         for (int itn = 0; itn < ROOT_ITERS; ++itn) {
             double t2 = 0.0, dt2 = 0.0;
 #pragma unroll
             for (int s = 0; s < S; ++s)
                 if (lane + 32 * s < is) {
-                    double t = om[s] * a[s] / (om[s] + lam);
+                    double inv = 1.0 / (om[s] + lam);
+                    double t = om[s] * a[s] * inv;
                     t2 += t * t;
-                    dt2 -= 2.0 * t * t / (om[s] + lam);
+                    dt2 += t * t * inv;
                 }
             t2 = warp_sum(t2);
             dt2 = warp_sum(dt2);
-            double det = oms * omt - lam * lam;
-            double sv = omt * (oms * as + lam * at) / det, tv = oms * (omt * at + lam * as) / det;
-            double f = INFINITY, df = dt2;
+            double idet = 1.0 / (oms * omt - lam * lam);
+            double sv = omt * (oms * as + lam * at) * idet, tv = oms * (omt * at + lam * as) * idet;
+            double f = INFINITY, df = -2.0 * dt2;
             if (sv >= 0.0 && tv >= 0.0) {
                 f = t2 - 2.0 * sv * tv;
-                double dsl = (omt * tv + lam * sv) / det, dtl = (lam * tv + oms * sv) / det;
+                double dsl = (omt * tv + lam * sv) * idet, dtl = (lam * tv + oms * sv) * idet;
                 df -= 2.0 * (dsl * tv + sv * dtl);
             }
             if ((lower && f > 0.0) || (!lower && f < 0.0))
                 lo = lam;
             else
                 hi = lam;
-            if (isfinite(f) && (fabs(f) <= 1e-13 * (1.0 + t2 + 2.0 * sv * tv) || hi - lo <= 1e-13 * (1.0 + hi + lo)))
+            if (isfinite(f) && (fabs(f) <= 1e-13 * (1.0 + t2 + 2.0 * sv * tv) ||
+                                (isfinite(hi) && hi - lo <= 1e-13 * (1.0 + hi + lo))))
                 break;
             double nx = lam - f / df;
             if (!isfinite(nx) || !(nx > lo && nx < hi))
-                nx = 0.5 * (lo + hi);
+                nx = isfinite(hi) ? 0.5 * (lo + hi) : 2.0 * lam;
             lam = nx;
         }
         double det = oms * omt - lam * lam;
@@ -442,6 +410,8 @@ __device__ void warp_project_rsoc(WarpSlots<S> &sl, int L, int lane, bool unifor
         ps = 0.0;
         pt = t_axis;
     }
+    if (warm && lane == 0 && !axis)
+        *warm = lam;
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         int i = lane + 32 * s;
@@ -455,12 +425,13 @@ __device__ void warp_project_rsoc(WarpSlots<S> &sl, int L, int lane, bool unifor
 }
 
 template <int S>
-__device__ __forceinline__ void warp_project(int type, WarpSlots<S> &sl, int L, int lane, bool uniform_unit)
+__device__ __forceinline__ void warp_project(int type, WarpSlots<S> &sl, int L, int lane, bool uniform_unit,
+                                             double *warm)
 {
     if (type == 1) // CONE_STANDARD_SOC
-        warp_project_soc<S>(sl, L, lane, uniform_unit);
+        warp_project_soc<S>(sl, L, lane, uniform_unit, warm);
     else if (type == 0) // CONE_ROTATED_SOC
-        warp_project_rsoc<S>(sl, L, lane, uniform_unit);
+        warp_project_rsoc<S>(sl, L, lane, uniform_unit, warm);
 }
 
 // Is d uniform over the block and w == 1 everywhere?  (warp vote)

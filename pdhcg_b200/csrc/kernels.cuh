@@ -50,6 +50,7 @@ struct StepData {
     const double *vr; // variable rescaling (cone metric)
     const int *free_idx; int n_free; // variables outside cones (NULL: all)
     const int *cone_start, *cone_len, *cone_type; int n_cones;
+    double *cone_warm; // per-cone multiplier warm start (may be NULL)
     double *x0, *x, *xp, *xr, *dx, *dual_slack;
     double *y0, *y, *yp, *dy;
 };
@@ -134,7 +135,7 @@ __global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<MT> D, StepPa
             }
         }
         bool uni = warp_uniform_unit<S>(sl, L, lane);
-        warp_project<S>(type, sl, L, lane, uni);
+        warp_project<S>(type, sl, L, lane, uni, D.cone_warm ? D.cone_warm + cb : nullptr);
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             int i = lane + 32 * s;

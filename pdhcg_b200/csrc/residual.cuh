@@ -51,6 +51,7 @@ struct ResidualData {
     const double *dual_slack;
     const int *free_idx; int n_free;
     const int *cone_start, *cone_len, *cone_type; int n_cones;
+    double *warm_dual, *warm_aug; // per-cone warm starts of the two projections
     double *partials;
     int rows_blocks, free_blocks, cone_blocks;
 };
@@ -161,8 +162,8 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<MT> D, Resid
                 }
             }
             bool uni = warp_uniform_unit<S>(aug, L, lane); // d uniform <=> 1/d uniform
-            warp_project<S>(type, dual, L, lane, uni);
-            warp_project<S>(type, aug, L, lane, uni);
+            warp_project<S>(type, dual, L, lane, uni, D.warm_dual ? D.warm_dual + cb : nullptr);
+            warp_project<S>(type, aug, L, lane, uni, D.warm_aug ? D.warm_aug + cb : nullptr);
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 int i = lane + 32 * s;

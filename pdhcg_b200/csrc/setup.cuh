@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(TPB) project_cones_kernel(int ncones, const in
             sl.w[s] = (i < L && q) ? 1.0 + tau * q[st + i] : 1.0;
         }
         bool uni = warp_uniform_unit<S>(sl, L, lane);
-        warp_project<S>(tp, sl, L, lane, uni);
+        warp_project<S>(tp, sl, L, lane, uni, nullptr);
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             int i = lane + 32 * s;

@@ -221,6 +221,7 @@ private:
     double *c_d_ = nullptr, *l_d_ = nullptr, *u_d_ = nullptr, *q_d_ = nullptr, *lc_d_ = nullptr, *uc_d_ = nullptr,
            *g_d_ = nullptr, *cr_d_ = nullptr, *vr_d_ = nullptr;
     int *free_d_ = nullptr, *cst_d_ = nullptr, *clen_d_ = nullptr, *ctype_d_ = nullptr, *cvdim_d_ = nullptr;
+    double *cone_warm_ = nullptr, *warm_dual_ = nullptr, *warm_aug_ = nullptr; // per-cone multipliers
     double *x0_, *x_, *xp_, *xr_, *dx_, *dslack_, *y0_, *y_, *yp_, *dy_;
     double *partials_ = nullptr, *scal_d_ = nullptr, *h_scal_ = nullptr;
     int *res_ops_d_ = nullptr, *fpe_ops_d_ = nullptr, *norm_ops_d_ = nullptr;
@@ -489,6 +490,10 @@ void Solve::init_state()
         ds = ar_.upload(P_->dual_start, m, s);
     dual_start_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(m, ds, cr_d_, sc_, y0_, y_, yp_);
     if (nc > 0) {
+        cone_warm_ = ar_.alloc<double>(3 * (size_t)nc);
+        warm_dual_ = cone_warm_ + nc;
+        warm_aug_ = cone_warm_ + 2 * (size_t)nc;
+        CK(cudaMemsetAsync(cone_warm_, 0, 3 * (size_t)nc * sizeof(double), s)); // 0 = no warm start
         cone_aux_init_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(nc, cst_d_, cvdim_d_, ctype_d_, vr_d_, sb_, x0_);
         dispatch_s(S_, [&](auto SC) {
             project_cones_kernel<SC.value><<<grid_for(nc, WARPS), TPB, 0, s>>>(nc, cst_d_, clen_d_, ctype_d_, x0_,
@@ -586,7 +591,8 @@ void Solve::enqueue_step(bool store_primal, bool store_dual, bool want_fpe, doub
     P.store_dual = store_dual;
     P.want_fpe = want_fpe;
     P.lp_slack = qtype_ == PDHCG_NON_Q;
-    StepData<double> D;
+    StepData<double> D{};
+    D.cone_warm = cone_warm_;
     D.n = n_;
     D.m = m_;
     D.A_rp = A_.rp;
@@ -673,7 +679,9 @@ void Solve::enqueue_step(bool store_primal, bool store_dual, bool want_fpe, doub
 void Solve::enqueue_residual(bool want_dist)
 {
     cudaStream_t s = st_;
-    ResidualData<double> D;
+    ResidualData<double> D{};
+    D.warm_dual = warm_dual_;
+    D.warm_aug = warm_aug_;
     D.n = n_;
     D.m = m_;
     D.A_rp = A_.rp;
@@ -940,6 +948,8 @@ pdhcg_result_t *Solve::run()
     auto t_setup = std::chrono::steady_clock::now();
     CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     build_host();
+    auto t_host = std::chrono::steady_clock::now();
+    stats_.host_copy_ms = std::chrono::duration<double, std::milli>(t_host - t_setup).count();
     if (qtype_ != PDHCG_NON_Q && qtype_ != PDHCG_DIAG_Q)
         throw CudaError("non-diagonal Q (inner BB solve) is not available yet");
     if (S_ < 0)
@@ -952,6 +962,8 @@ pdhcg_result_t *Solve::run()
     if (P_->affine_cones.num_cones > 0)
         throw CudaError("affine cones are not available on the device path yet");
     upload_and_preprocess();
+    CK(cudaStreamSynchronize(st_));
+    stats_.upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host).count();
     // reduction scratch sized for the widest user
     int rg = residual_group(std::min(GA_, GAt_));
     res_rows_blocks_ = grid_for(m_, TPB / rg, 148 * 8);
@@ -1001,7 +1013,9 @@ pdhcg_result_t *Solve::run()
     CK(cudaStreamSynchronize(st_));
     stats_.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_setup).count();
     loop();
+    auto t_res = std::chrono::steady_clock::now();
     pdhcg_result_t *r = make_result();
+    stats_.result_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_res).count();
     r->rescaling_time_sec = stats_.setup_ms * 1e-3;
     double nnz = (double)A_.nnz;
     stats_.spmv_bytes = 2.0 * nnz * (8 + 4) + 4.0 * ((double)n_ + m_ + 2) + 8.0 * ((double)n_ + m_);
@@ -1117,8 +1131,13 @@ pdhcg_result_t *pdhcg_b200_solve(const qp_problem_t *prob, const pdhg_parameters
     else
         pdhcg_b200_default_options(&opt);
     try {
-        Solve s(prob, prm, opt);
-        pdhcg_result_t *r = s.run();
+        auto t0 = std::chrono::steady_clock::now();
+        pdhcg_result_t *r = nullptr;
+        {
+            Solve s(prob, prm, opt);
+            r = s.run();
+        }
+        g_last_stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         if (r && prm.verbose >= 1) {
             std::printf("Solution Summary\n");
             std::printf("  Status             : %d\n", (int)r->termination_reason);

@@ -29,7 +29,8 @@ class Stats(C.Structure):
                 ("step_kernel_launches", C.c_longlong), ("kernel_launches", C.c_longlong),
                 ("iterations", C.c_int), ("fp32_iterations", C.c_int), ("restarts", C.c_int),
                 ("evaluations", C.c_int), ("step_bytes", C.c_double), ("spmv_bytes", C.c_double),
-                ("reserved", C.c_double * 6)]
+                ("host_copy_ms", C.c_double), ("upload_ms", C.c_double), ("result_ms", C.c_double),
+                ("total_ms", C.c_double), ("reserved", C.c_double * 2)]
 
 
 class StepArgs(C.Structure):

@@ -108,7 +108,7 @@ def test_fused_step_matches_oracle(lib, oracle, with_q, with_cones):
     host = {}
 
     def h(name, a, dt=np.float64):
-        host[name] = np.ascontiguousarray(a, dtype=dt)
+        host[name] = np.array(a, dtype=dt, copy=True)  # the oracle updates x, y in place
         return host[name].ctypes.data
 
     cst = [k.start for k in p.cones]
