@@ -66,6 +66,18 @@ __device__ __forceinline__ double row_dot(const int *__restrict__ rp, const int 
     return group_sum<G>(s);
 }
 
+// Entries [b, e) of one row, G lanes cooperating; every lane of the warp
+// must call it (the group reduction shuffles over the full warp).
+template <int G, typename V, typename X>
+__device__ __forceinline__ double range_dot(const int *__restrict__ ci, const V *__restrict__ val,
+                                            const X *__restrict__ x, int b, int e, int lane)
+{
+    double s = 0.0;
+    for (int k = b + lane; k < e; k += G)
+        s += (double)__ldg(val + k) * (double)__ldg(x + __ldg(ci + k));
+    return group_sum<G>(s);
+}
+
 __device__ __forceinline__ double clampd(double lo, double x, double hi) { return fmax(lo, fmin(x, hi)); }
 
 // ---------------------------------------------------------------------------

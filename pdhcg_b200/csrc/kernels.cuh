@@ -1,21 +1,27 @@
-// kernels.cuh -- the CUDA kernels of one PDHCG-B200 solve.
+// kernels.cuh -- the hot kernels of one PDHCG-B200 iteration.
 //
 // Layout in HBM (one solve, n variables, m rows):
-//   A  : CSR, int32 row_ptr[m+1], int32 col[nnz], values MT[nnz]
+//   A  : CSR, int32 row_ptr[m+1], int32 col[nnz], values T[nnz]
 //   At : CSR of A^T (n rows), built on the device by a stable sort so each
 //        row lists its entries in increasing row index (what the
 //        reference's csr2csc produces, src/solver_state.cu:739-770)
-//   vectors: FP64 problem data (c, bounds, diag Q, rescaling) and iterates
-//        (x_init, x_cur, x_pdhg, x_refl; y_init, y_cur, y_pdhg).
-// Hot kernels of one iteration (reference pdhg_update + halpern_update,
-// src/pdhg_core_op.cu:705-845), two launches:
-//   primal_step : row-group SpMV on At (A^T y), diagonal-Q prox, box
-//                 projection, cone projection (warp per cone block), the
-//                 reflection and the Halpern average of x, all in registers
-//   dual_step   : row-group SpMV on A (A x_refl), dual prox, reflection and
-//                 Halpern average of y
-// Both are HBM-bandwidth bound: every matrix byte and every vector byte is
-// read once per iteration; the gathered vectors (y, x_refl) stay in L2.
+//   vectors: problem data (c, bounds, diagonal Q, rescaling) and iterates
+//        (x_init, x_cur, x_pdhg, x_refl; y_init, y_cur, y_pdhg), all of
+//        storage type T.
+// T = double is the plain FP64 iteration; T = float is the mixed-precision
+// bulk phase: every load is widened to double, products are accumulated and
+// the prox / projection arithmetic is done in double, and only the stores
+// are rounded to FP32.
+//
+// One iteration (reference pdhg_update + halpern_update,
+// src/pdhg_core_op.cu:705-845) is two launches:
+//   primal_free_kernel / primal_cone_kernel : A^T y by row groups, diagonal-Q
+//        prox, box clamp, cone projection (one warp per cone block), the
+//        reflection and the Halpern average of x, all in registers
+//   dual_kernel : A x_refl, dual prox, reflection and Halpern average of y
+// Both are HBM-bandwidth bound: every matrix byte and every streamed vector
+// byte is read once per iteration; the gathered vectors (y, x_refl) stay in
+// L2.
 #pragma once
 
 #include "device.cuh"
@@ -25,43 +31,39 @@ namespace pdhcg {
 constexpr int TPB = 256;
 constexpr int WARPS = TPB / 32;
 
-// ---------------------------------------------------------------------------
 // Per-iteration parameters of the step kernels (passed by value).
-// ---------------------------------------------------------------------------
 struct StepParams {
-    double tau, sigma;   // primal / dual step sizes
-    double w;            // Halpern weight (k+1)/(k+2)
-    double rho;          // reflection coefficient
-    int store_primal;    // write x_pdhg (and LP dual slack)
-    int store_dual;      // write y_pdhg
-    int want_fpe;        // write x_refl - x_cur into dx, y_refl - y_cur into dy
-    int lp_slack;        // NON_Q: store (p - t)/tau in dual_slack
+    double tau, sigma; // primal / dual step sizes
+    double w;          // Halpern weight (k+1)/(k+2)
+    double rho;        // reflection coefficient
+    int store_primal;  // write x_pdhg (and LP dual slack)
+    int store_dual;    // write y_pdhg
+    int want_fpe;      // write x_refl - x_cur into dx, y_refl - y_cur into dy
+    int lp_slack;      // NON_Q: store (p - t)/tau in dual_slack
+    int cone_box;      // some cone slot has a finite box bound (|bound| >= 1e30 passes validation)
 };
 
-template <typename MT>
+template <typename T>
 struct StepData {
     int n, m;
     const int *A_rp, *A_ci;
-    const MT *A_v;
+    const T *A_v;
     const int *At_rp, *At_ci;
-    const MT *At_v;
-    const double *c, *l, *u, *q;
-    const double *lc, *uc, *g;
-    const double *vr; // variable rescaling (cone metric)
-    const int *free_idx; int n_free; // variables outside cones (NULL: all)
-    const int *cone_start, *cone_len, *cone_type; int n_cones;
+    const T *At_v;
+    const T *c, *l, *u, *q;
+    const T *lc, *uc, *g;
+    const T *vr; // variable rescaling (cone metric)
+    const int *free_idx;
+    int n_free; // variables outside cones (NULL: all)
+    const int *cone_start, *cone_len, *cone_type;
+    int n_cones;
     double *cone_warm; // per-cone multiplier warm start (may be NULL)
-    double *x0, *x, *xp, *xr, *dx, *dual_slack;
-    double *y0, *y, *yp, *dy;
+    T *x0, *x, *xp, *xr, *dx, *dual_slack;
+    T *y0, *y, *yp, *dy;
 };
 
-// x-side element update shared by the free and the cone path
-struct PrimalOut {
-    double p;  // pdhg candidate (before cone projection)
-};
-
-template <int G, typename MT, bool HAS_Q, bool HAS_BOX>
-__global__ void __launch_bounds__(TPB) primal_free_kernel(StepData<MT> D, StepParams P)
+template <int G, typename T, bool HAS_Q, bool HAS_BOX>
+__global__ void __launch_bounds__(TPB) primal_free_kernel(StepData<T> D, StepParams P)
 {
     const int groups_per_block = TPB / G;
     const int lane = threadIdx.x % G;
@@ -71,35 +73,61 @@ __global__ void __launch_bounds__(TPB) primal_free_kernel(StepData<MT> D, StepPa
         double aty = row_dot<G>(D.At_rp, D.At_ci, D.At_v, D.y, j, lane);
         if (lane == 0) {
             double xi = D.x[j];
-            double t = xi - P.tau * (D.c[j] - aty);
+            double t = xi - P.tau * ((double)D.c[j] - aty);
             if (HAS_Q)
-                t /= (1.0 + P.tau * D.q[j]);
+                t /= (1.0 + P.tau * (double)D.q[j]);
             double p = HAS_BOX ? clampd(D.l[j], t, D.u[j]) : t;
             double xr = 2.0 * p - xi;
-            D.xr[j] = xr;
+            D.xr[j] = (T)xr;
             if (P.store_primal) {
-                D.xp[j] = p;
+                D.xp[j] = (T)p;
                 if (P.lp_slack)
-                    D.dual_slack[j] = (p - t) / P.tau;
+                    D.dual_slack[j] = (T)((p - t) / P.tau);
             }
             if (P.want_fpe)
-                D.dx[j] = xr - xi;
+                D.dx[j] = (T)(xr - xi);
             double refl = P.rho * xr + (1.0 - P.rho) * xi;
-            D.x[j] = P.w * refl + (1.0 - P.w) * D.x0[j];
+            D.x[j] = (T)(P.w * refl + (1.0 - P.w) * (double)D.x0[j]);
         }
     }
 }
 
 // One warp per cone block.  The prox candidate of every slot is projected
 // onto the cone in the (1 + tau q) d^2 metric (diagonal Q) or d^2 metric (LP).
-template <int S, typename MT, bool HAS_Q>
-__global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<MT> D, StepParams P)
+// A^T y for the L consecutive rows [st, st+L) of one cone block into a
+// per-warp staging buffer, G lanes per row so each load instruction reads
+// G consecutive entries of 32/G rows.
+template <int G, typename V, typename X>
+__device__ __forceinline__ void warp_rows_dot(const int *__restrict__ rp, const int *__restrict__ ci,
+                                              const V *__restrict__ val, const X *__restrict__ x, int st, int L,
+                                              int lane, double *out_sm)
 {
+    const int sub = lane % G;
+    for (int base = 0; base < L; base += 32 / G) {
+        int slot = base + lane / G;
+        int b = 0, e = 0;
+        if (slot < L) {
+            b = __ldg(rp + st + slot);
+            e = __ldg(rp + st + slot + 1);
+        }
+        double a = range_dot<G>(ci, val, x, b, e, sub);
+        if (sub == 0 && slot < L)
+            out_sm[slot] = a;
+    }
+    __syncwarp();
+}
+
+template <int S, int G, typename T, bool HAS_Q>
+__global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<T> D, StepParams P)
+{
+    __shared__ double aty_all[WARPS][32 * S];
     const int lane = threadIdx.x & 31;
     const int warp = blockIdx.x * WARPS + (threadIdx.x >> 5);
     const int nwarps = gridDim.x * WARPS;
+    double *aty_sm = aty_all[threadIdx.x >> 5];
     for (int cb = warp; cb < D.n_cones; cb += nwarps) {
         const int st = D.cone_start[cb], L = D.cone_len[cb], type = D.cone_type[cb];
+        warp_rows_dot<G>(D.At_rp, D.At_ci, D.At_v, D.y, st, L, lane, aty_sm);
         WarpSlots<S> sl;
         double xi[S], tt[S];
 #pragma unroll
@@ -112,17 +140,18 @@ __global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<MT> D, StepPa
             tt[s] = 0.0;
             if (i < L) {
                 int j = st + i;
-                double aty = row_dot<1>(D.At_rp, D.At_ci, D.At_v, D.y, j, 0);
+                double aty = aty_sm[i];
                 xi[s] = D.x[j];
-                double t = xi[s] - P.tau * (D.c[j] - aty);
+                double t = xi[s] - P.tau * ((double)D.c[j] - aty);
                 if (HAS_Q)
-                    t /= (1.0 + P.tau * D.q[j]);
+                    t /= (1.0 + P.tau * (double)D.q[j]);
                 tt[s] = t;
-                sl.x[s] = clampd(D.l[j], t, D.u[j]);
+                sl.x[s] = P.cone_box ? clampd(D.l[j], t, D.u[j]) : t;
                 sl.d[s] = D.vr[j];
-                sl.w[s] = HAS_Q ? 1.0 + P.tau * D.q[j] : 1.0;
+                sl.w[s] = HAS_Q ? 1.0 + P.tau * (double)D.q[j] : 1.0;
             }
         }
+        __syncwarp(); // the staging buffer is reused by the next block
         // LP dual slack of the box step is recorded before the cone
         // projection (reference compute_lp_next_pdhg_primal_solution_major_kernel
         // then project_cone_runtime, src/pdhg_core_op.cu:426-455, 729-735)
@@ -131,7 +160,7 @@ __global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<MT> D, StepPa
             for (int s = 0; s < S; ++s) {
                 int i = lane + 32 * s;
                 if (i < L)
-                    D.dual_slack[st + i] = (sl.x[s] - tt[s]) / P.tau;
+                    D.dual_slack[st + i] = (T)((sl.x[s] - tt[s]) / P.tau);
             }
         }
         bool uni = warp_uniform_unit<S>(sl, L, lane);
@@ -143,26 +172,26 @@ __global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<MT> D, StepPa
                 int j = st + i;
                 double p = sl.x[s];
                 double xr = 2.0 * p - xi[s];
-                D.xr[j] = xr;
-                D.xp[j] = p; // cones force the pdhg store (reference :428, :460)
+                D.xr[j] = (T)xr;
+                D.xp[j] = (T)p; // cones force the pdhg store (reference :428, :460)
                 if (P.want_fpe)
-                    D.dx[j] = xr - xi[s];
+                    D.dx[j] = (T)(xr - xi[s]);
                 double refl = P.rho * xr + (1.0 - P.rho) * xi[s];
-                D.x[j] = P.w * refl + (1.0 - P.w) * D.x0[j];
+                D.x[j] = (T)(P.w * refl + (1.0 - P.w) * (double)D.x0[j]);
             }
         }
     }
 }
 
-template <int G, typename MT, bool EQ_ROWS, bool HAS_G>
-__global__ void __launch_bounds__(TPB) dual_kernel(StepData<MT> D, StepParams P)
+template <int G, typename T, bool EQ_ROWS, bool HAS_G>
+__global__ void __launch_bounds__(TPB) dual_kernel(StepData<T> D, StepParams P)
 {
     const int groups_per_block = TPB / G;
     const int lane = threadIdx.x % G;
     for (int i = blockIdx.x * groups_per_block + threadIdx.x / G; i < D.m; i += gridDim.x * groups_per_block) {
         double ax = row_dot<G>(D.A_rp, D.A_ci, D.A_v, D.xr, i, lane);
         if (lane == 0) {
-            double v = HAS_G ? ax + D.g[i] : ax;
+            double v = HAS_G ? ax + (double)D.g[i] : ax;
             double yi = D.y[i];
             double pr;
             if (EQ_ROWS)
@@ -171,12 +200,12 @@ __global__ void __launch_bounds__(TPB) dual_kernel(StepData<MT> D, StepParams P)
                 pr = clampd(D.lc[i], v - yi / P.sigma, D.uc[i]);
             double yn = yi - P.sigma * v + P.sigma * pr;
             if (P.store_dual)
-                D.yp[i] = yn;
+                D.yp[i] = (T)yn;
             double yr = 2.0 * yn - yi;
             if (P.want_fpe)
-                D.dy[i] = yr - yi;
+                D.dy[i] = (T)(yr - yi);
             double refl = P.rho * yr + (1.0 - P.rho) * yi;
-            D.y[i] = P.w * refl + (1.0 - P.w) * D.y0[i];
+            D.y[i] = (T)(P.w * refl + (1.0 - P.w) * (double)D.y0[i]);
         }
     }
 }
@@ -215,7 +244,7 @@ __global__ void fold_partials_kernel(const double *partials, int nblocks, int ns
     __shared__ double sh[TPB];
     for (int s = 0; s < ns; ++s) {
         int op = ops[s];
-        double acc = op == RMAX ? 0.0 : 0.0;
+        double acc = 0.0;
         for (int b = threadIdx.x; b < nblocks; b += TPB) {
             double v = partials[(size_t)b * ns + s];
             acc = op == RMAX ? fmax(acc, v) : acc + v;
@@ -252,6 +281,14 @@ __global__ void cone_len_kernel(int nc, const int *vdim, const int *type, int *l
         int t = type[b], v = vdim[b];
         len[b] = (t == 2 || t == 3) ? 3 : (t == 4 ? v * (v + 1) / 2 : v + 2);
     }
+}
+
+// element-wise precision conversion (phase switch of the mixed solve)
+template <typename A, typename B>
+__global__ void convert_kernel(const A *src, B *dst, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (B)src[i];
 }
 
 } // namespace pdhcg

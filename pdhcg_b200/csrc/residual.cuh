@@ -38,17 +38,20 @@ struct ResidualParams {
     double s_aug;     // step of the projected-gradient augmentation
 };
 
-template <typename MT>
+// VT: storage type of the iterates (FP32 during the mixed bulk phase); the
+// matrices and problem data are read in FP64 so residuals are exact FP64
+// evaluations of the stored iterates.
+template <typename VT>
 struct ResidualData {
     int n, m;
     const int *A_rp, *A_ci;
-    const MT *A_v;
+    const double *A_v;
     const int *At_rp, *At_ci;
-    const MT *At_v;
+    const double *At_v;
     const double *c, *l, *u, *q, *qx;
     const double *lc, *uc, *g, *cr, *vr;
-    const double *xp, *yp, *x0, *y0;
-    const double *dual_slack;
+    const VT *xp, *yp, *x0, *y0;
+    const VT *dual_slack;
     const int *free_idx; int n_free;
     const int *cone_start, *cone_len, *cone_type; int n_cones;
     double *warm_dual, *warm_aug; // per-cone warm starts of the two projections
@@ -58,9 +61,10 @@ struct ResidualData {
 
 __device__ __forceinline__ double norm_term(double v, int l2) { return l2 ? v * v : abs_or_inf(v); }
 
-template <int G, int S, typename MT>
-__global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<MT> D, ResidualParams P)
+template <int G, int S, typename VT>
+__global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, ResidualParams P)
 {
+    __shared__ double aty_all[WARPS][32 * S];
     const int NOP = P.l2 ? RSUM : RMAX;
     const int ops[RS_COUNT] = {NOP, RSUM, NOP, RSUM, RSUM, RSUM, NOP, NOP, RSUM, RSUM};
     double acc[RS_COUNT];
@@ -133,8 +137,10 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<MT> D, Resid
         b -= D.rows_blocks + D.free_blocks;
         const int lane = threadIdx.x & 31;
         const int nwarps = D.cone_blocks * WARPS;
+        double *aty_sm = aty_all[threadIdx.x >> 5];
         for (int cb = b * WARPS + (threadIdx.x >> 5); cb < D.n_cones; cb += nwarps) {
             const int st = D.cone_start[cb], L = D.cone_len[cb], type = D.cone_type[cb];
+            warp_rows_dot<4>(D.At_rp, D.At_ci, D.At_v, D.yp, st, L, lane, aty_sm);
             WarpSlots<S> dual, aug;
             double xv[S], rc[S], qxv[S], atyv[S];
 #pragma unroll
@@ -146,7 +152,7 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<MT> D, Resid
                 xv[s] = rc[s] = qxv[s] = atyv[s] = 0.0;
                 if (i < L) {
                     int j = st + i;
-                    double aty = row_dot<1>(D.At_rp, D.At_ci, D.At_v, D.yp, j, 0);
+                    double aty = aty_sm[i];
                     double x = D.xp[j];
                     double qx = P.qmode == 1 ? D.q[j] * x : (P.qmode == 2 ? D.qx[j] : 0.0);
                     double eff = P.qmode ? D.c[j] + qx : D.c[j];
@@ -161,6 +167,7 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<MT> D, Resid
                     aug.d[s] = D.vr[j];
                 }
             }
+            __syncwarp(); // staging buffer reused by the next block
             bool uni = warp_uniform_unit<S>(aug, L, lane); // d uniform <=> 1/d uniform
             warp_project<S>(type, dual, L, lane, uni, D.warm_dual ? D.warm_dual + cb : nullptr);
             warp_project<S>(type, aug, L, lane, uni, D.warm_aug ? D.warm_aug + cb : nullptr);
@@ -198,9 +205,9 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<MT> D, Resid
 // dx = x_refl - x_cur and dy = y_refl - y_cur written by the step kernels.
 enum FpeScalar { FP_DX2 = 0, FP_DY2, FP_CROSS, FP_COUNT };
 
-template <int G, typename MT>
-__global__ void __launch_bounds__(TPB) fpe_kernel(int n, int m, const int *At_rp, const int *At_ci, const MT *At_v,
-                                                  const double *dx, const double *dy, double *partials,
+template <int G, typename VT>
+__global__ void __launch_bounds__(TPB) fpe_kernel(int n, int m, const int *At_rp, const int *At_ci, const double *At_v,
+                                                  const VT *dx, const VT *dy, double *partials,
                                                   int col_blocks)
 {
     const int ops[FP_COUNT] = {RSUM, RSUM, RSUM};

@@ -332,17 +332,17 @@ __global__ void __launch_bounds__(TPB) project_cones_kernel(int ncones, const in
 }
 
 // restart: x_init = x_cur = x_pdhg, y_init = y_cur = y_pdhg
-__global__ void restart_copy_kernel(int n, int m, const double *xp, double *x0, double *x, const double *yp,
-                                    double *y0, double *y)
+template <typename VT>
+__global__ void restart_copy_kernel(int n, int m, const VT *xp, VT *x0, VT *x, const VT *yp, VT *y0, VT *y)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x) {
         if (i < n) {
-            double v = xp[i];
+            VT v = xp[i];
             x0[i] = v;
             x[i] = v;
         } else {
             int r = i - n;
-            double v = yp[r];
+            VT v = yp[r];
             y0[r] = v;
             y[r] = v;
         }
@@ -352,18 +352,18 @@ __global__ void restart_copy_kernel(int n, int m, const double *xp, double *x0, 
 // Final answer: reduced cost and unscaling (reference create_result_from_state
 // and compute_and_rescale_reduced_cost_qp_kernel, src/pdhg_core_op.cu:1431-1471,
 // src/kernels/pdhcg_kernels.cu:866-894, rescale_solution_kernel :308-327).
-template <typename MT>
-__global__ void result_kernel(int n, int m, const int *At_rp, const int *At_ci, const MT *At_v, const double *c,
+template <typename VT>
+__global__ void result_kernel(int n, int m, const int *At_rp, const int *At_ci, const double *At_v, const double *c,
                               const double *q, const double *qx, int qmode, const double *l, const double *u,
-                              const double *vr, const double *cr, double sb, double sc, const double *xp,
-                              const double *yp, double *x_out, double *y_out, double *rc_out)
+                              const double *vr, const double *cr, double sb, double sc, const VT *xp,
+                              const VT *yp, double *x_out, double *y_out, double *rc_out)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x) {
         if (i < n) {
             double aty = row_dot<1>(At_rp, At_ci, At_v, yp, i, 0);
             double g = c[i];
             if (qmode == 1)
-                g += q[i] * xp[i];
+                g += q[i] * (double)xp[i];
             else if (qmode == 2)
                 g += qx[i];
             double rc = (g - aty) * vr[i] / sc;
@@ -372,10 +372,10 @@ __global__ void result_kernel(int n, int m, const int *At_rp, const int *At_ci, 
             if (!isfinite(u[i]))
                 rc = fmax(rc, 0.0);
             rc_out[i] = rc;
-            x_out[i] = xp[i] / vr[i] / sb;
+            x_out[i] = (double)xp[i] / vr[i] / sb;
         } else {
             int r = i - n;
-            y_out[r] = yp[r] / cr[r] / sc;
+            y_out[r] = (double)yp[r] / cr[r] / sc;
         }
     }
 }

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "internal.h"
@@ -94,15 +95,15 @@ int print_frequency(int iter)
 int pick_group(long long nnz, int rows)
 {
     double mean = rows > 0 ? (double)nnz / rows : 0.0;
-    if (mean <= 12)
+    if (mean <= 1.5)
         return 1;
-    if (mean <= 24)
+    if (mean <= 3)
         return 2;
-    if (mean <= 48)
+    if (mean <= 6)
         return 4;
-    if (mean <= 96)
+    if (mean <= 12)
         return 8;
-    if (mean <= 192)
+    if (mean <= 24)
         return 16;
     return 32;
 }
@@ -120,6 +121,22 @@ int slots_class(int maxlen)
     if (s <= 8)
         return 8;
     return -1;
+}
+
+// lanes per row of the cone kernels' staging SpMV
+int cone_group(int g)
+{
+    return g <= 2 ? 2 : (g <= 4 ? 4 : 8);
+}
+
+template <typename F>
+void dispatch_cg(int G, F &&f)
+{
+    switch (G) {
+    case 2: f(std::integral_constant<int, 2>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    default: f(std::integral_constant<int, 8>{}); break;
+    }
 }
 
 // lanes per row of the residual kernel (one kernel serves A and A^T rows)
@@ -194,7 +211,16 @@ private:
     void step_size();
     void loop();
     void enqueue_step(bool store_primal, bool store_dual, bool want_fpe, double w);
+    template <typename T>
+    void enqueue_step_t(bool store_primal, bool store_dual, bool want_fpe, double w);
+    template <typename T>
+    StepData<T> step_data();
+    double step_bytes(size_t s, bool store_primal, bool store_dual) const;
     void enqueue_residual(bool want_dist);
+    template <typename VT>
+    void enqueue_residual_t(bool want_dist);
+    void enter_fp32();
+    void leave_fp32();
     void read_residual();
     void enqueue_fpe(int slot);
     pdhcg_result_t *make_result();
@@ -212,7 +238,7 @@ private:
     std::vector<int> A_rp_, A_ci_;
     std::vector<double> A_v_, c_, l_, u_, lc_, uc_, g_;
     int qtype_ = PDHCG_NON_Q;
-    bool has_g_ = false, box_free_ = true, eq_rows_ = true;
+    bool has_g_ = false, box_free_ = true, eq_rows_ = true, cone_box_ = false;
     std::vector<int> cone_start_, cone_len_, cone_type_, cone_vdim_, free_idx_;
     int S_ = 1;
 
@@ -223,6 +249,17 @@ private:
     int *free_d_ = nullptr, *cst_d_ = nullptr, *clen_d_ = nullptr, *ctype_d_ = nullptr, *cvdim_d_ = nullptr;
     double *cone_warm_ = nullptr, *warm_dual_ = nullptr, *warm_aug_ = nullptr; // per-cone multipliers
     double *x0_, *x_, *xp_, *xr_, *dx_, *dslack_, *y0_, *y_, *yp_, *dy_;
+    // FP32 mirrors of the matrices, problem vectors and iterates (mixed precision)
+    struct {
+        float *Av = nullptr, *Atv = nullptr, *c = nullptr, *l = nullptr, *u = nullptr, *q = nullptr, *lc = nullptr,
+              *uc = nullptr, *g = nullptr, *vr = nullptr;
+        float *x0 = nullptr, *x = nullptr, *xp = nullptr, *xr = nullptr, *dx = nullptr, *dslack = nullptr;
+        float *y0 = nullptr, *y = nullptr, *yp = nullptr, *dy = nullptr;
+    } f_;
+    bool fp32_ = false;
+    double step_bytes_sum_ = 0.0;
+    double best_fp32_kkt_ = INFINITY;
+    int fp32_stall_ = 0;
     double *partials_ = nullptr, *scal_d_ = nullptr, *h_scal_ = nullptr;
     int *res_ops_d_ = nullptr, *fpe_ops_d_ = nullptr, *norm_ops_d_ = nullptr;
     int res_rows_blocks_ = 0, res_free_blocks_ = 0, res_cone_blocks_ = 0;
@@ -356,8 +393,11 @@ void Solve::build_host()
         cone_type_.push_back((int)p->cones.type[b]);
         cone_vdim_.push_back(p->cones.v_dim[b]);
         maxlen = std::max(maxlen, len);
-        for (int i = 0; i < len; ++i)
-            in_cone[p->cones.start_idx[b] + i] = 1;
+        for (int i = 0; i < len; ++i) {
+            int j = p->cones.start_idx[b] + i;
+            in_cone[j] = 1;
+            cone_box_ |= std::isfinite(l_[j]) || std::isfinite(u_[j]);
+        }
     }
     if (!cone_start_.empty()) {
         for (int i = 0; i < n_; ++i)
@@ -565,7 +605,79 @@ void Solve::harvest_step_events()
     ev_used_ = 0;
 }
 
+template <typename T>
+StepData<T> Solve::step_data()
+{
+    StepData<T> D{};
+    D.cone_warm = cone_warm_;
+    D.n = n_;
+    D.m = m_;
+    D.A_rp = A_.rp;
+    D.A_ci = A_.ci;
+    D.At_rp = At_.rp;
+    D.At_ci = At_.ci;
+    D.free_idx = free_d_;
+    D.n_free = (int)free_idx_.size();
+    D.cone_start = cst_d_;
+    D.cone_len = clen_d_;
+    D.cone_type = ctype_d_;
+    D.n_cones = (int)cone_start_.size();
+    if constexpr (std::is_same<T, double>::value) {
+        D.A_v = A_.v;
+        D.At_v = At_.v;
+        D.c = c_d_;
+        D.l = l_d_;
+        D.u = u_d_;
+        D.q = q_d_;
+        D.lc = lc_d_;
+        D.uc = uc_d_;
+        D.g = g_d_;
+        D.vr = vr_d_;
+        D.x0 = x0_;
+        D.x = x_;
+        D.xp = xp_;
+        D.xr = xr_;
+        D.dx = dx_;
+        D.dual_slack = dslack_;
+        D.y0 = y0_;
+        D.y = y_;
+        D.yp = yp_;
+        D.dy = dy_;
+    } else {
+        D.A_v = f_.Av;
+        D.At_v = f_.Atv;
+        D.c = f_.c;
+        D.l = f_.l;
+        D.u = f_.u;
+        D.q = f_.q;
+        D.lc = f_.lc;
+        D.uc = f_.uc;
+        D.g = f_.g;
+        D.vr = f_.vr;
+        D.x0 = f_.x0;
+        D.x = f_.x;
+        D.xp = f_.xp;
+        D.xr = f_.xr;
+        D.dx = f_.dx;
+        D.dual_slack = f_.dslack;
+        D.y0 = f_.y0;
+        D.y = f_.y;
+        D.yp = f_.yp;
+        D.dy = f_.dy;
+    }
+    return D;
+}
+
 void Solve::enqueue_step(bool store_primal, bool store_dual, bool want_fpe, double w)
+{
+    if (fp32_)
+        enqueue_step_t<float>(store_primal, store_dual, want_fpe, w);
+    else
+        enqueue_step_t<double>(store_primal, store_dual, want_fpe, w);
+}
+
+template <typename T>
+void Solve::enqueue_step_t(bool store_primal, bool store_dual, bool want_fpe, double w)
 {
     cudaStream_t s = st_;
     if (opt_.time_steps) {
@@ -591,40 +703,8 @@ void Solve::enqueue_step(bool store_primal, bool store_dual, bool want_fpe, doub
     P.store_dual = store_dual;
     P.want_fpe = want_fpe;
     P.lp_slack = qtype_ == PDHCG_NON_Q;
-    StepData<double> D{};
-    D.cone_warm = cone_warm_;
-    D.n = n_;
-    D.m = m_;
-    D.A_rp = A_.rp;
-    D.A_ci = A_.ci;
-    D.A_v = A_.v;
-    D.At_rp = At_.rp;
-    D.At_ci = At_.ci;
-    D.At_v = At_.v;
-    D.c = c_d_;
-    D.l = l_d_;
-    D.u = u_d_;
-    D.q = q_d_;
-    D.lc = lc_d_;
-    D.uc = uc_d_;
-    D.g = g_d_;
-    D.vr = vr_d_;
-    D.free_idx = free_d_;
-    D.n_free = (int)free_idx_.size();
-    D.cone_start = cst_d_;
-    D.cone_len = clen_d_;
-    D.cone_type = ctype_d_;
-    D.n_cones = (int)cone_start_.size();
-    D.x0 = x0_;
-    D.x = x_;
-    D.xp = xp_;
-    D.xr = xr_;
-    D.dx = dx_;
-    D.dual_slack = dslack_;
-    D.y0 = y0_;
-    D.y = y_;
-    D.yp = yp_;
-    D.dy = dy_;
+    P.cone_box = cone_box_;
+    StepData<T> D = step_data<T>();
     bool hasq = qtype_ == PDHCG_DIAG_Q;
     int nfree = D.n_cones > 0 ? D.n_free : n_;
     if (nfree > 0) {
@@ -633,14 +713,14 @@ void Solve::enqueue_step(bool store_primal, bool store_dual, bool want_fpe, doub
             int grid = grid_for((long long)nfree, TPB / G);
             if (hasq) {
                 if (box_free_)
-                    primal_free_kernel<G, double, true, false><<<grid, TPB, 0, s>>>(D, P);
+                    primal_free_kernel<G, T, true, false><<<grid, TPB, 0, s>>>(D, P);
                 else
-                    primal_free_kernel<G, double, true, true><<<grid, TPB, 0, s>>>(D, P);
+                    primal_free_kernel<G, T, true, true><<<grid, TPB, 0, s>>>(D, P);
             } else {
                 if (box_free_)
-                    primal_free_kernel<G, double, false, false><<<grid, TPB, 0, s>>>(D, P);
+                    primal_free_kernel<G, T, false, false><<<grid, TPB, 0, s>>>(D, P);
                 else
-                    primal_free_kernel<G, double, false, true><<<grid, TPB, 0, s>>>(D, P);
+                    primal_free_kernel<G, T, false, true><<<grid, TPB, 0, s>>>(D, P);
             }
         });
         stats_.kernel_launches++;
@@ -649,9 +729,13 @@ void Solve::enqueue_step(bool store_primal, bool store_dual, bool want_fpe, doub
         dispatch_s(S_, [&](auto SC) {
             int grid = grid_for(D.n_cones, WARPS);
             if (hasq)
-                primal_cone_kernel<SC.value, double, true><<<grid, TPB, 0, s>>>(D, P);
+                dispatch_cg(cone_group(GAt_), [&](auto GC) {
+                    primal_cone_kernel<SC.value, GC.value, T, true><<<grid, TPB, 0, s>>>(D, P);
+                });
             else
-                primal_cone_kernel<SC.value, double, false><<<grid, TPB, 0, s>>>(D, P);
+                dispatch_cg(cone_group(GAt_), [&](auto GC) {
+                    primal_cone_kernel<SC.value, GC.value, T, false><<<grid, TPB, 0, s>>>(D, P);
+                });
         });
         stats_.kernel_launches++;
     }
@@ -660,26 +744,60 @@ void Solve::enqueue_step(bool store_primal, bool store_dual, bool want_fpe, doub
         int grid = grid_for((long long)m_, TPB / G);
         if (eq_rows_) {
             if (has_g_)
-                dual_kernel<G, double, true, true><<<grid, TPB, 0, s>>>(D, P);
+                dual_kernel<G, T, true, true><<<grid, TPB, 0, s>>>(D, P);
             else
-                dual_kernel<G, double, true, false><<<grid, TPB, 0, s>>>(D, P);
+                dual_kernel<G, T, true, false><<<grid, TPB, 0, s>>>(D, P);
         } else {
             if (has_g_)
-                dual_kernel<G, double, false, true><<<grid, TPB, 0, s>>>(D, P);
+                dual_kernel<G, T, false, true><<<grid, TPB, 0, s>>>(D, P);
             else
-                dual_kernel<G, double, false, false><<<grid, TPB, 0, s>>>(D, P);
+                dual_kernel<G, T, false, false><<<grid, TPB, 0, s>>>(D, P);
         }
     });
     stats_.kernel_launches++;
     stats_.step_kernel_launches++;
+    step_bytes_sum_ += step_bytes(sizeof(T), store_primal || !cone_start_.empty(), store_dual);
+    if (fp32_)
+        stats_.fp32_iterations++;
     if (opt_.time_steps)
         CK(cudaEventRecord(ev_pool_[ev_used_++], s));
 }
 
+// Algorithmic HBM bytes of one step as the kernels above move them: each
+// matrix byte and each streamed vector once, each gathered vector once.
+double Solve::step_bytes(size_t s, bool store_primal, bool store_dual) const
+{
+    double n = n_, m = m_, nnz = A_.nnz, nc = (double)cone_start_.size();
+    double ncs = 0.0; // slots in cones
+    for (int L : cone_len_)
+        ncs += L;
+    double nf = n - ncs;
+    bool hasq = qtype_ == PDHCG_DIAG_Q;
+    // primal: A^T (values + indices + row pointers), y gathered once,
+    // x_cur, x_init, c (+ q) (+ box) read; x_refl, x_cur (+ x_pdhg) written
+    double primal = nnz * (s + 4) + (n + 1) * 4 + m * s + n * s * (3 + (hasq ? 1 : 0)) +
+                    (box_free_ ? 0.0 : 2 * nf * s) + (cone_box_ ? 2 * ncs * s : 0.0) /* box on cone slots */ + ncs * s /* d */ +
+                    (nc > 0 ? nf * 4 + nc * (3 * 4 + 2 * 8) : 0.0) + n * s * (2 + (store_primal ? 1 : 0));
+    // dual: A, x_refl gathered once, y_cur, y_init, bounds (+ offset) read;
+    // y_cur (+ y_pdhg) written
+    double dual = nnz * (s + 4) + (m + 1) * 4 + n * s + m * s * (2 + (eq_rows_ ? 1 : 2) + (has_g_ ? 1 : 0)) +
+                  m * s * (1 + (store_dual ? 1 : 0));
+    return primal + dual;
+}
+
 void Solve::enqueue_residual(bool want_dist)
 {
+    if (fp32_)
+        enqueue_residual_t<float>(want_dist);
+    else
+        enqueue_residual_t<double>(want_dist);
+}
+
+template <typename VT>
+void Solve::enqueue_residual_t(bool want_dist)
+{
     cudaStream_t s = st_;
-    ResidualData<double> D{};
+    ResidualData<VT> D{};
     D.warm_dual = warm_dual_;
     D.warm_aug = warm_aug_;
     D.n = n_;
@@ -700,11 +818,19 @@ void Solve::enqueue_residual(bool want_dist)
     D.g = g_d_;
     D.cr = cr_d_;
     D.vr = vr_d_;
-    D.xp = xp_;
-    D.yp = yp_;
-    D.x0 = x0_;
-    D.y0 = y0_;
-    D.dual_slack = dslack_;
+    if constexpr (std::is_same<VT, double>::value) {
+        D.xp = xp_;
+        D.yp = yp_;
+        D.x0 = x0_;
+        D.y0 = y0_;
+        D.dual_slack = dslack_;
+    } else {
+        D.xp = f_.xp;
+        D.yp = f_.yp;
+        D.x0 = f_.x0;
+        D.y0 = f_.y0;
+        D.dual_slack = f_.dslack;
+    }
     D.free_idx = free_d_;
     D.n_free = (int)free_idx_.size();
     D.cone_start = cst_d_;
@@ -727,11 +853,10 @@ void Solve::enqueue_residual(bool want_dist)
         sa = 1.0;
     P.s_aug = sa;
     int nb = D.rows_blocks + D.free_blocks + D.cone_blocks;
-    // G for the rows range: A; the free range uses A^T with the same G
-    // template, so both row-group widths must agree -> use the smaller.
+    // one row-group width serves both the A rows and the A^T rows
     int G = residual_group(std::min(GA_, GAt_));
     dispatch_rg(G, [&](auto GC) {
-        dispatch_s(S_, [&](auto SC) { residual_kernel<GC.value, SC.value, double><<<nb, TPB, 0, s>>>(D, P); });
+        dispatch_s(S_, [&](auto SC) { residual_kernel<GC.value, SC.value, VT><<<nb, TPB, 0, s>>>(D, P); });
     });
     fold_partials_kernel<<<1, TPB, 0, s>>>(partials_, nb, RS_COUNT, res_ops_d_, scal_d_);
     stats_.kernel_launches += 2;
@@ -744,13 +869,79 @@ void Solve::enqueue_fpe(int slot)
     int nb = fpe_col_blocks_ + fpe_row_blocks_;
     double *part = partials_; // stream order serialises every user of the partials buffer
     dispatch_rg(residual_group(GAt_), [&](auto GC) {
-        fpe_kernel<GC.value, double><<<nb, TPB, 0, s>>>(n_, m_, At_.rp, At_.ci, At_.v, dx_, dy_, part,
-                                                          fpe_col_blocks_);
+        if (fp32_)
+            fpe_kernel<GC.value, float><<<nb, TPB, 0, s>>>(n_, m_, At_.rp, At_.ci, At_.v, f_.dx, f_.dy, part,
+                                                             fpe_col_blocks_);
+        else
+            fpe_kernel<GC.value, double><<<nb, TPB, 0, s>>>(n_, m_, At_.rp, At_.ci, At_.v, dx_, dy_, part,
+                                                              fpe_col_blocks_);
     });
     fold_partials_kernel<<<1, TPB, 0, s>>>(part, nb, FP_COUNT, fpe_ops_d_, scal_d_ + RS_COUNT + slot * FP_COUNT);
     stats_.kernel_launches += 2;
 }
 
+// ---- mixed precision (FP32 bulk phase, then FP64 polish) ----------------
+void Solve::enter_fp32()
+{
+    cudaStream_t s = st_;
+    long long n = n_, m = m_, nnz = A_.nnz;
+    auto mk = [&](long long k) { return ar_.alloc<float>((size_t)std::max(k, 1LL)); };
+    auto cv = [&](const double *src, float *dst, long long k) {
+        if (k > 0 && src)
+            convert_kernel<double, float><<<grid_for(k, TPB), TPB, 0, s>>>(src, dst, k);
+    };
+    f_.Av = mk(nnz);
+    f_.Atv = mk(nnz);
+    cv(A_.v, f_.Av, nnz);
+    cv(At_.v, f_.Atv, nnz);
+    float **vecs_n[] = {&f_.c, &f_.l, &f_.u, &f_.vr, &f_.x0, &f_.x, &f_.xp, &f_.xr, &f_.dx, &f_.dslack};
+    for (float **p : vecs_n)
+        *p = mk(n);
+    float **vecs_m[] = {&f_.lc, &f_.uc, &f_.g, &f_.y0, &f_.y, &f_.yp, &f_.dy};
+    for (float **p : vecs_m)
+        *p = mk(m);
+    cv(c_d_, f_.c, n);
+    cv(l_d_, f_.l, n);
+    cv(u_d_, f_.u, n);
+    cv(vr_d_, f_.vr, n);
+    cv(lc_d_, f_.lc, m);
+    cv(uc_d_, f_.uc, m);
+    cv(g_d_, f_.g, m);
+    if (q_d_) {
+        f_.q = mk(n);
+        cv(q_d_, f_.q, n);
+    }
+    cv(x0_, f_.x0, n);
+    cv(x_, f_.x, n);
+    cv(xp_, f_.xp, n);
+    cv(xr_, f_.xr, n);
+    cv(dslack_, f_.dslack, n);
+    cv(y0_, f_.y0, m);
+    cv(y_, f_.y, m);
+    cv(yp_, f_.yp, m);
+    CK(cudaGetLastError());
+    fp32_ = true;
+}
+
+void Solve::leave_fp32()
+{
+    cudaStream_t s = st_;
+    long long n = n_, m = m_;
+    auto cv = [&](const float *src, double *dst, long long k) {
+        if (k > 0)
+            convert_kernel<float, double><<<grid_for(k, TPB), TPB, 0, s>>>(src, dst, k);
+    };
+    cv(f_.x0, x0_, n);
+    cv(f_.x, x_, n);
+    cv(f_.xp, xp_, n);
+    cv(f_.xr, xr_, n);
+    cv(f_.dslack, dslack_, n);
+    cv(f_.y0, y0_, m);
+    cv(f_.y, y_, m);
+    cv(f_.yp, yp_, m);
+    CK(cudaGetLastError());
+    fp32_ = false;
+}
 
 // ---- main loop (reference optimize, src/solver.cu:121-170) ---------------
 void Solve::read_residual()
@@ -826,6 +1017,19 @@ void Solve::loop()
                 reason_ = TERMINATION_REASON_USER_INTERRUPT;
             if (reason_ != TERMINATION_REASON_UNSPECIFIED)
                 break;
+            if (fp32_) {
+                // FP32 bulk phase hands over to FP64 once the relative KKT error
+                // is below the polish threshold, or when it stops improving
+                double kkt = std::fmax(rel_p_, std::fmax(rel_d_, rel_gap_));
+                if (kkt < best_fp32_kkt_ * 0.9) {
+                    best_fp32_kkt_ = kkt;
+                    fp32_stall_ = 0;
+                } else {
+                    ++fp32_stall_;
+                }
+                if (kkt < opt_.polish_threshold || fp32_stall_ >= 30)
+                    leave_fp32();
+            }
         }
         if (is_major_ || k_ == 0) {
             // should_do_adaptive_restart (reference src/utils.cu:291-322)
@@ -861,8 +1065,12 @@ void Solve::loop()
                     best_gap_ = g;
                     best_omega_ = omega_;
                 }
-                restart_copy_kernel<<<grid_for((long long)n_ + m_, TPB), TPB, 0, st_>>>(n_, m_, xp_, x0_, x_, yp_,
-                                                                                        y0_, y_);
+                if (fp32_)
+                    restart_copy_kernel<float><<<grid_for((long long)n_ + m_, TPB), TPB, 0, st_>>>(
+                        n_, m_, f_.xp, f_.x0, f_.x, f_.yp, f_.y0, f_.y);
+                else
+                    restart_copy_kernel<double><<<grid_for((long long)n_ + m_, TPB), TPB, 0, st_>>>(
+                        n_, m_, xp_, x0_, x_, yp_, y0_, y_);
                 stats_.kernel_launches++;
                 stats_.restarts++;
                 inner_count_ = 0;
@@ -914,9 +1122,14 @@ pdhcg_result_t *Solve::make_result()
     cudaStream_t s = st_;
     int n = n_, m = m_;
     double *xo = ar_.alloc<double>(n), *yo = ar_.alloc<double>(m), *rco = ar_.alloc<double>(n);
-    result_kernel<double><<<grid_for((long long)n + m, TPB), TPB, 0, s>>>(
-        n, m, At_.rp, At_.ci, At_.v, c_d_, q_d_, nullptr, qtype_ == PDHCG_DIAG_Q ? 1 : 0, l_d_, u_d_, vr_d_, cr_d_,
-        sb_, sc_, xp_, yp_, xo, yo, rco);
+    if (fp32_)
+        result_kernel<float><<<grid_for((long long)n + m, TPB), TPB, 0, s>>>(
+            n, m, At_.rp, At_.ci, At_.v, c_d_, q_d_, nullptr, qtype_ == PDHCG_DIAG_Q ? 1 : 0, l_d_, u_d_, vr_d_,
+            cr_d_, sb_, sc_, f_.xp, f_.yp, xo, yo, rco);
+    else
+        result_kernel<double><<<grid_for((long long)n + m, TPB), TPB, 0, s>>>(
+            n, m, At_.rp, At_.ci, At_.v, c_d_, q_d_, nullptr, qtype_ == PDHCG_DIAG_Q ? 1 : 0, l_d_, u_d_, vr_d_,
+            cr_d_, sb_, sc_, xp_, yp_, xo, yo, rco);
     pdhcg_result_t *r = (pdhcg_result_t *)std::calloc(1, sizeof(pdhcg_result_t));
     r->primal_solution = (double *)std::malloc(std::max(n, 1) * sizeof(double));
     r->dual_solution = (double *)std::malloc(std::max(m, 1) * sizeof(double));
@@ -1011,6 +1224,8 @@ pdhcg_result_t *Solve::run()
     init_state();
     step_size();
     CK(cudaStreamSynchronize(st_));
+    if (opt_.precision == PDHCG_B200_MIXED)
+        enter_fp32();
     stats_.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_setup).count();
     loop();
     auto t_res = std::chrono::steady_clock::now();
@@ -1019,7 +1234,7 @@ pdhcg_result_t *Solve::run()
     r->rescaling_time_sec = stats_.setup_ms * 1e-3;
     double nnz = (double)A_.nnz;
     stats_.spmv_bytes = 2.0 * nnz * (8 + 4) + 4.0 * ((double)n_ + m_ + 2) + 8.0 * ((double)n_ + m_);
-    stats_.step_bytes = stats_.spmv_bytes + 8.0 * (8.0 * n_ + 5.0 * m_);
+    stats_.step_bytes = stats_.step_kernel_launches > 0 ? step_bytes_sum_ / stats_.step_kernel_launches : 0.0;
     g_last_stats = stats_;
     return r;
 }
@@ -1076,9 +1291,9 @@ int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cuda
     if (nc > 0)
         dispatch_s(S, [&](auto SC) {
             if (hasq)
-                primal_cone_kernel<SC.value, double, true><<<grid_for(nc, WARPS), TPB, 0, s>>>(D, P);
+                primal_cone_kernel<SC.value, 4, double, true><<<grid_for(nc, WARPS), TPB, 0, s>>>(D, P);
             else
-                primal_cone_kernel<SC.value, double, false><<<grid_for(nc, WARPS), TPB, 0, s>>>(D, P);
+                primal_cone_kernel<SC.value, 4, double, false><<<grid_for(nc, WARPS), TPB, 0, s>>>(D, P);
         });
     if (t->affine_offset)
         dual_kernel<1, double, false, true><<<grid_for(t->m, TPB), TPB, 0, s>>>(D, P);
@@ -1244,7 +1459,7 @@ int pdhcg_b200_pdhg_step(const pdhcg_b200_step_t *t, void *stream)
     D.y = t->y_cur;
     D.yp = t->y_pdhg;
     D.dy = nullptr;
-    StepParams P{t->tau, t->sigma, t->halpern_weight, t->reflection, 1, 1, 0, 0};
+    StepParams P{t->tau, t->sigma, t->halpern_weight, t->reflection, 1, 1, 0, 0, 1};
     // the kernel-level step keeps cone handling separate: free kernel over all
     // variables, then project + re-reflect cone blocks, then the dual kernel.
     // Halpern is applied at the end so the cone correction sees x_cur.

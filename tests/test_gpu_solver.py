@@ -84,3 +84,35 @@ def test_gpu_iteration_limit_and_result_fields(lib):
     assert g["status"] == "ITERATION_LIMIT"
     assert g["total_count"] == 37
     assert np.all(np.isfinite(g["x"])) and np.all(np.isfinite(g["y"]))
+
+
+def _solve_gpu_opts(lib, p, params, **opts):
+    prob, keep = capi.build(lib, p)
+    prm = capi.default_params(lib, **params)
+    o = native.default_options(**opts)
+    r = lib.pdhcg_b200_solve(prob, C.byref(prm), C.byref(o))
+    assert r
+    m = p.A.m if p.A is not None else 0
+    d = capi.result_dict(r, p.n, max(m, 1))
+    lib.pdhcg_result_free(r)
+    lib.qp_problem_free(prob)
+    return d, native.last_stats()
+
+
+@pytest.mark.parametrize("name", ["diag_qp", "conic_qp", "soc_qp_small", "box_lp"])
+def test_mixed_precision_reaches_fp64_answer(lib, name):
+    """FP32 bulk phase + FP64 polish: same status as plain FP64, objective
+    within the termination tolerance of the FP64 answer, and the FP32 phase
+    actually ran (fp32_iterations > 0)."""
+    make, prm = CASES[name]
+    p = make()
+    prm = {"termination_criteria.iteration_limit": 100000,
+           "termination_criteria.eps_optimal_relative": 1e-6,
+           "termination_criteria.eps_feasible_relative": 1e-6}
+    ref, _ = _solve_gpu_opts(lib, p, prm, precision=0)
+    mix, st = _solve_gpu_opts(lib, p, prm, precision=1)
+    assert ref["status"] == mix["status"] == "OPTIMAL"
+    assert st["fp32_iterations"] > 0
+    assert mix["rel_kkt"] < 1e-6
+    assert abs(mix["primal_objective_value"] - ref["primal_objective_value"]) <= 1e-5 * (
+        1 + abs(ref["primal_objective_value"]))
