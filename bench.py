@@ -138,46 +138,62 @@ def run_ours(args):
     problem = instances.soc_qp(seed=2 + rank, scale=args.scale)
     prob, keep = capi.build(lib, problem)
     prm = _params(lib, args.iters)
-    forms = {"fp64": native.default_options(precision=0), "mixed": native.default_options(precision=1)}
+    forms = {"fp64": 0, "mixed": 1}
+    handle = lib.pdhcg_b200_upload(prob)
+    if not handle:
+        raise RuntimeError("pdhcg_b200_upload failed")
 
-    def solve(opts):
+    def solve(precision, device, time_steps=0):
+        opts = native.default_options(precision=precision, time_steps=time_steps, solution_on_device=int(device))
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        r = lib.pdhcg_b200_solve(prob, C.byref(prm), C.byref(opts))
+        if device:
+            r = lib.pdhcg_b200_solve_device(handle, C.byref(prm), C.byref(opts))
+        else:
+            r = lib.pdhcg_b200_solve(prob, C.byref(prm), C.byref(opts))
         e1.record()
         torch.cuda.synchronize()
         if not r:
             raise RuntimeError("solve failed")
-        d = capi.result_dict(r, problem.n, problem.A.m)
+        if device:
+            rr = r.contents
+            d = {"status": capi.TERMINATION_REASONS[rr.termination_reason], "total_count": rr.total_count,
+                 "rel_kkt": max(rr.relative_primal_residual, rr.relative_dual_residual, rr.relative_objective_gap),
+                 "primal_objective_value": rr.primal_objective_value}
+        else:
+            d = capi.result_dict(r, problem.n, problem.A.m)
         lib.pdhcg_result_free(r)
         return e0.elapsed_time(e1) / 1e3, d, native.last_stats()
 
-    def time_form(opts):
-        for _ in range(args.warmup):
-            solve(opts)
-        sampler = ClockSampler(local)
-        sampler.start()
-        times, res, stats = [], None, None
-        for _ in range(args.steps):
+    def time_form(precision):
+        res = {}
+        for device in (True, False):
+            for _ in range(args.warmup):
+                solve(precision, device)
+            sampler = ClockSampler(local)
+            sampler.start()
+            times, r1, st = [], None, None
+            for _ in range(args.steps):
+                if world > 1:
+                    torch.distributed.barrier()
+                t, r1, st = solve(precision, device)
+                times.append(t)
+            clocks = sampler.stop()
             if world > 1:
-                torch.distributed.barrier()
-            t, res, stats = solve(opts)
-            times.append(t)
-        clocks = sampler.stop()
-        if world > 1:
-            tt = torch.tensor([sum(times)], device="cuda")
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-            total = tt.item()
-        else:
-            total = sum(times)
+                tt = torch.tensor([max(times)], device="cuda")
+                torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+                worst = tt.item()
+            else:
+                worst = max(times)
+            res["device" if device else "host"] = (sum(times) / len(times), worst, r1, st, clocks)
         # kernel-level timing in a separate run (events around each fused step)
-        opts.time_steps = 1
-        _, _, tstats = solve(opts)
-        opts.time_steps = 0
-        return total / args.steps, res, stats, tstats, clocks
+        _, _, tstats = solve(precision, True, time_steps=1)
+        res["tstats"] = tstats
+        return res
 
-    out = {name: time_form(o) for name, o in forms.items()}
+    out = {name: time_form(pr) for name, pr in forms.items()}
+    lib.pdhcg_b200_device_problem_free(handle)
     if world > 1:
         torch.distributed.barrier()
     if rank != 0:
@@ -193,9 +209,10 @@ def run_ours(args):
                 "frac": (ach / peak) if ach else None, "traffic": None, "peak_kind": peak_kind,
                 "bytes_per_step": tstats["step_bytes"], "step_kernel_ms": step_ms}
 
-    per_solve, res, stats, tstats, clocks = out["mixed"]
-    fp64 = out["fp64"]
-    rl = roof(tstats)
+    mixed, fp64 = out["mixed"], out["fp64"]
+    per_solve, _, res, stats, clocks = mixed["device"]
+    e2e_solve, _, e2e_res, e2e_stats, _ = mixed["host"]
+    rl = roof(mixed["tstats"])
     line = {
         "metric": METRIC, "value": per_solve, "unit": "s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_solve * 1e3,
@@ -203,22 +220,27 @@ def run_ours(args):
         "config": {"workload": WORKLOAD, "parallelism": "replicas" if world > 1 else "single",
                    "eps": EPS, "form": "mixed: FP32 bulk, FP64 polish below 1e-5",
                    "l2_flush": "working set (>=134 MB) larger than L2",
-                   "inputs": "host (solve_qp_problem path; device-resident handle not yet split out)"},
+                   "inputs": "value: problem resident in HBM (pdhcg_b200_upload once), solution left on device; "
+                             "e2e: host buffers through pdhcg_b200_solve"},
         "status": res["status"], "iterations": res["total_count"], "rel_kkt": res["rel_kkt"],
         "objective": res["primal_objective_value"], "fp32_iterations": stats["fp32_iterations"],
-        "fp64_form": {"value": fp64[0], "status": fp64[1]["status"], "iterations": fp64[1]["total_count"],
-                      "rel_kkt": fp64[1]["rel_kkt"], "objective": fp64[1]["primal_objective_value"],
-                      "roofline": roof(fp64[3]), "loop_ms": fp64[2]["loop_ms"]},
-        "speedup_mixed_vs_fp64": fp64[0] / per_solve,
+        "fp64_form": {"value": fp64["device"][0], "e2e": fp64["host"][0], "status": fp64["device"][2]["status"],
+                      "iterations": fp64["device"][2]["total_count"], "rel_kkt": fp64["device"][2]["rel_kkt"],
+                      "objective": fp64["device"][2]["primal_objective_value"], "roofline": roof(fp64["tstats"])},
+        "speedup_mixed_vs_fp64": fp64["device"][0] / per_solve,
         "spmv_gbs": rl["achieved"],
         "roofline": rl,
-        "e2e": {"value": per_solve, "unit": "s",
-                "h2d_bytes_per_step": int(8 * (problem.A.nnz * 1.5 + 4 * problem.n + 2 * problem.A.m)),
-                "d2h_bytes_per_step": int(8 * (2 * problem.n + problem.A.m))},
+        "e2e": {"value": e2e_solve, "unit": "s",
+                "h2d_bytes_per_step": int(problem.A.nnz * 12 + (problem.A.m + 1) * 4 + problem.n * 8 * 4 +
+                                          problem.A.m * 8 * 3 + problem.n * 12),
+                "d2h_bytes_per_step": int(8 * (2 * problem.n + problem.A.m)),
+                "status": e2e_res["status"], "iterations": e2e_res["total_count"]},
         "gpu_launches": int(stats["kernel_launches"]) * args.steps,
         "clocks": clocks,
         "breakdown_ms": {k: stats[k] for k in ("host_copy_ms", "upload_ms", "setup_ms", "loop_ms", "result_ms",
                                                "total_ms")},
+        "e2e_breakdown_ms": {k: e2e_stats[k] for k in ("host_copy_ms", "upload_ms", "setup_ms", "loop_ms",
+                                                       "result_ms", "total_ms")},
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(problem, res["total_count"])

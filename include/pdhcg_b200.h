@@ -30,7 +30,9 @@ typedef struct {
     double initial_primal_weight;
     int use_graphs;                /* capture the iterations between two evaluations in a CUDA graph */
     int time_steps;                /* bracket every fused step with CUDA events (fills step_kernel_ms) */
-    int reserved[6];
+    int solution_on_device;        /* pdhcg_b200_solve_device only: leave x, y, reduced cost in device
+                                      memory (result arrays are NULL); see pdhcg_b200_device_solution */
+    int reserved[5];
 } pdhcg_b200_options_t;
 
 void pdhcg_b200_default_options(pdhcg_b200_options_t *opts);
@@ -38,6 +40,24 @@ void pdhcg_b200_default_options(pdhcg_b200_options_t *opts);
 /* solve_qp_problem with options.  Same ownership and error rules. */
 pdhcg_result_t *pdhcg_b200_solve(const qp_problem_t *prob, const pdhg_parameters_t *params,
                                  const pdhcg_b200_options_t *opts);
+
+/* ---- problems resident in device memory -----------------------------------
+ * pdhcg_b200_upload copies a problem's raw arrays to the current device
+ * once; pdhcg_b200_solve_device then solves from that copy without any
+ * host->device traffic for the problem data (each solve rescales a private
+ * device copy, so the handle can be solved many times, e.g. with different
+ * parameters).  No counterpart in the reference, which uploads inside
+ * every solve (reference src/solver_state.cu:688-851). */
+typedef struct pdhcg_b200_device_problem_s pdhcg_b200_device_problem_t;
+
+pdhcg_b200_device_problem_t *pdhcg_b200_upload(const qp_problem_t *prob);
+pdhcg_result_t *pdhcg_b200_solve_device(pdhcg_b200_device_problem_t *handle, const pdhg_parameters_t *params,
+                                        const pdhcg_b200_options_t *opts);
+/* Device pointers of the last solution kept with solution_on_device; valid
+ * until the next solve on the handle or its release.  Returns 0 or -1. */
+int pdhcg_b200_device_solution(const pdhcg_b200_device_problem_t *handle, const double **x, const double **y,
+                               const double **reduced_cost);
+void pdhcg_b200_device_problem_free(pdhcg_b200_device_problem_t *handle);
 
 /* Device-side statistics of the last solve on the calling thread. */
 typedef struct {

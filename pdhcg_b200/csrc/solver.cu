@@ -186,10 +186,154 @@ struct HostScalars {
     double v[RS_COUNT + 2 * FP_COUNT];
 };
 
+// A problem resident in HBM: the raw (unscaled) arrays of a qp_problem_t
+// plus the host-side metadata a solve needs.  solve_qp_problem builds a
+// temporary one and lets the solve scale it in place; the handle API
+// (pdhcg_b200_upload) keeps one and every solve works on copies.
+struct DeviceProblem {
+    int n = 0, m = 0, nnzA = 0, nnzQ = 0, qtype = PDHCG_NON_Q, S = 1;
+    bool dummy = false, has_g = false, box_free = true, eq_rows = true, cone_box = false;
+    std::vector<int> cone_start, cone_len, cone_type, cone_vdim, free_idx;
+    double obj_const = 0.0;
+    int orig_vars = 0, orig_cons = 0, orig_nnz = 0;
+    std::string unsupported; // non-empty: reason the device path cannot solve it
+    Arena ar;
+    int *A_rp = nullptr, *A_ci = nullptr, *Q_rp = nullptr, *Q_ci = nullptr;
+    double *A_v = nullptr, *Q_v = nullptr;
+    double *c = nullptr, *l = nullptr, *u = nullptr, *lc = nullptr, *uc = nullptr, *g = nullptr;
+    int *cst = nullptr, *clen = nullptr, *ctype = nullptr, *cvdim = nullptr, *free_d = nullptr;
+    double *pstart = nullptr, *dstart = nullptr;
+    // solution kept on the device when a solve is asked to leave it there
+    double *x_out = nullptr, *y_out = nullptr, *rc_out = nullptr;
+};
+
+// Classification (reference preprocess_qp_problem and detect_q_type,
+// src/preconditioner.c:715-830, src/utils.cu:834-885) and upload.
+std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaStream_t s)
+{
+    auto dp = std::make_unique<DeviceProblem>();
+    DeviceProblem &d = *dp;
+    d.n = p->num_variables;
+    d.orig_vars = p->num_variables;
+    d.orig_cons = p->num_constraints;
+    d.orig_nnz = p->constraint_matrix_num_nonzeros;
+    d.obj_const = p->objective_constant;
+    d.dummy = p->num_constraints == 0 || p->constraint_matrix == nullptr;
+    Arena &ar = d.ar;
+    if (d.dummy) { // reference create_problem_with_dummy_constraint, src/utils.cu:80-135
+        d.m = 1;
+        d.nnzA = 1;
+        const int rp[2] = {0, 1}, ci[1] = {0};
+        const double v[1] = {1.0}, lo[1] = {-INFINITY}, up[1] = {INFINITY}, g0[1] = {0.0};
+        d.A_rp = ar.upload(rp, 2, s);
+        d.A_ci = ar.upload(ci, 1, s);
+        d.A_v = ar.upload(v, 1, s);
+        d.lc = ar.upload(lo, 1, s);
+        d.uc = ar.upload(up, 1, s);
+        d.g = ar.upload(g0, 1, s);
+        CK(cudaStreamSynchronize(s)); // stack sources
+        d.box_free = true;
+        d.eq_rows = false;
+    } else {
+        d.m = p->num_constraints;
+        d.nnzA = p->constraint_matrix_num_nonzeros;
+        d.A_rp = ar.upload(p->constraint_matrix->row_ptr, (size_t)d.m + 1, s);
+        d.A_ci = ar.upload(p->constraint_matrix->col_ind, d.nnzA, s);
+        d.A_v = ar.upload(p->constraint_matrix->val, d.nnzA, s);
+        d.lc = ar.upload(p->constraint_lower_bound, d.m, s);
+        d.uc = ar.upload(p->constraint_upper_bound, d.m, s);
+        d.g = ar.upload(p->affine_cone_offset, d.m, s);
+        for (int i = 0; i < d.m; ++i) {
+            d.has_g |= p->affine_cone_offset[i] != 0.0;
+            d.eq_rows &= p->constraint_lower_bound[i] == p->constraint_upper_bound[i] &&
+                         std::isfinite(p->constraint_lower_bound[i]);
+        }
+        if (p->dual_start)
+            d.dstart = ar.upload(p->dual_start, d.m, s);
+    }
+    d.c = ar.upload(p->objective_vector, d.n, s);
+    d.l = ar.upload(p->variable_lower_bound, d.n, s);
+    d.u = ar.upload(p->variable_upper_bound, d.n, s);
+    if (p->primal_start)
+        d.pstart = ar.upload(p->primal_start, d.n, s);
+    for (int i = 0; i < d.n; ++i)
+        d.box_free &= !std::isfinite(p->variable_lower_bound[i]) && !std::isfinite(p->variable_upper_bound[i]);
+
+    int nnzq = (p->objective_sparse_matrix && p->objective_sparse_matrix->row_ptr)
+                   ? p->objective_sparse_matrix_num_nonzeros
+                   : 0;
+    int nnzr = (p->objective_lowrank_matrix && p->objective_lowrank_matrix->row_ptr && p->num_rank_lowrank_obj > 0)
+                   ? p->objective_lowrank_matrix_num_nonzeros
+                   : 0;
+    if (nnzq == 0 && nnzr == 0)
+        d.qtype = PDHCG_NON_Q;
+    else if (nnzr > 0)
+        d.qtype = nnzq > 0 ? PDHCG_LOW_RANK_PLUS_SPARSE_Q : PDHCG_LOW_RANK_Q;
+    else {
+        d.qtype = PDHCG_DIAG_Q;
+        const CsrComponent *Q = p->objective_sparse_matrix;
+        for (int i = 0; i < d.n && d.qtype == PDHCG_DIAG_Q; ++i)
+            for (int k = Q->row_ptr[i]; k < Q->row_ptr[i + 1]; ++k)
+                if (Q->col_ind[k] != i) {
+                    d.qtype = PDHCG_SPARSE_Q;
+                    break;
+                }
+    }
+    if (d.qtype != PDHCG_NON_Q) {
+        const CsrComponent *Q = p->objective_sparse_matrix;
+        d.nnzQ = p->objective_sparse_matrix_num_nonzeros;
+        d.Q_rp = ar.upload(Q->row_ptr, (size_t)d.n + 1, s);
+        d.Q_ci = ar.upload(Q->col_ind, d.nnzQ, s);
+        d.Q_v = ar.upload(Q->val, d.nnzQ, s);
+    }
+
+    int maxlen = 0;
+    std::vector<char> in_cone(d.n, 0);
+    for (int b = 0; b < p->cones.num_cones; ++b) {
+        int len = pdhcg_b200_cone_length(p->cones.type[b], p->cones.v_dim[b]);
+        d.cone_start.push_back(p->cones.start_idx[b]);
+        d.cone_len.push_back(len);
+        d.cone_type.push_back((int)p->cones.type[b]);
+        d.cone_vdim.push_back(p->cones.v_dim[b]);
+        maxlen = std::max(maxlen, len);
+        for (int i = 0; i < len; ++i) {
+            int j = p->cones.start_idx[b] + i;
+            in_cone[j] = 1;
+            d.cone_box |= std::isfinite(p->variable_lower_bound[j]) || std::isfinite(p->variable_upper_bound[j]);
+        }
+        if (p->cones.type[b] != CONE_STANDARD_SOC && p->cones.type[b] != CONE_ROTATED_SOC)
+            d.unsupported = "only SOC and rotated SOC cones are available on the device path yet";
+    }
+    int nc = (int)d.cone_start.size();
+    if (nc > 0) {
+        for (int i = 0; i < d.n; ++i)
+            if (!in_cone[i])
+                d.free_idx.push_back(i);
+        d.S = slots_class(maxlen);
+        d.cst = ar.upload(d.cone_start.data(), nc, s);
+        d.clen = ar.upload(d.cone_len.data(), nc, s);
+        d.ctype = ar.upload(d.cone_type.data(), nc, s);
+        d.cvdim = ar.upload(d.cone_vdim.data(), nc, s);
+        if (!d.free_idx.empty())
+            d.free_d = ar.upload(d.free_idx.data(), d.free_idx.size(), s);
+    }
+    if (d.qtype != PDHCG_NON_Q && d.qtype != PDHCG_DIAG_Q)
+        d.unsupported = "non-diagonal Q (inner BB solve) is not available yet";
+    if (d.S < 0)
+        d.unsupported = "cone blocks longer than 256 slots are not supported yet";
+    if (p->cones.is_fixed)
+        d.unsupported = "fixed cone slots are not available on the device path yet";
+    if (p->affine_cones.num_cones > 0)
+        d.unsupported = "affine cones are not available on the device path yet";
+    CK(cudaStreamSynchronize(s)); // host sources of the uploads may go away
+    return dp;
+}
+
 class Solve {
 public:
-    Solve(const qp_problem_t *prob, const pdhg_parameters_t &prm, const pdhcg_b200_options_t &opt)
-        : P_(prob), prm_(prm), opt_(opt)
+    // own_inputs: the solve may scale dp's arrays in place (dp is temporary)
+    Solve(DeviceProblem &dp, bool own_inputs, const pdhg_parameters_t &prm, const pdhcg_b200_options_t &opt)
+        : dp_(dp), own_(own_inputs), prm_(prm), opt_(opt)
     {
     }
     ~Solve()
@@ -227,16 +371,15 @@ private:
     template <typename F>
     void dispatch_g(int G, F &&f);
 
-    const qp_problem_t *P_;
+    DeviceProblem &dp_;
+    bool own_;
     pdhg_parameters_t prm_;
     pdhcg_b200_options_t opt_;
     cudaStream_t st_ = nullptr;
     Arena ar_;
 
-    // host copy of the working problem (dummy row added when m == 0)
+    // working problem (dummy row added when m == 0)
     int n_ = 0, m_ = 0;
-    std::vector<int> A_rp_, A_ci_;
-    std::vector<double> A_v_, c_, l_, u_, lc_, uc_, g_;
     int qtype_ = PDHCG_NON_Q;
     bool has_g_ = false, box_free_ = true, eq_rows_ = true, cone_box_ = false;
     std::vector<int> cone_start_, cone_len_, cone_type_, cone_vdim_, free_idx_;
@@ -326,121 +469,61 @@ void dispatch_rg(int G, F &&f)
     }
 }
 
-// ---- host-side classification (reference preprocess_qp_problem and
-// detect_q_type, src/preconditioner.c:715-830, src/utils.cu:834-885) ------
+// ---- working copy on the device --------------------------------------------
 void Solve::build_host()
 {
-    const qp_problem_t *p = P_;
-    n_ = p->num_variables;
-    bool dummy = p->num_constraints == 0 || p->constraint_matrix == nullptr;
-    if (dummy) { // reference create_problem_with_dummy_constraint, src/utils.cu:80-135
-        m_ = 1;
-        A_rp_ = {0, 1};
-        A_ci_ = {0};
-        A_v_ = {1.0};
-        lc_ = {-INFINITY};
-        uc_ = {INFINITY};
-        g_ = {0.0};
-    } else {
-        m_ = p->num_constraints;
-        int nnz = p->constraint_matrix_num_nonzeros;
-        A_rp_.assign(p->constraint_matrix->row_ptr, p->constraint_matrix->row_ptr + m_ + 1);
-        A_ci_.assign(p->constraint_matrix->col_ind, p->constraint_matrix->col_ind + nnz);
-        A_v_.assign(p->constraint_matrix->val, p->constraint_matrix->val + nnz);
-        lc_.assign(p->constraint_lower_bound, p->constraint_lower_bound + m_);
-        uc_.assign(p->constraint_upper_bound, p->constraint_upper_bound + m_);
-        g_.assign(p->affine_cone_offset, p->affine_cone_offset + m_);
-    }
-    c_.assign(p->objective_vector, p->objective_vector + n_);
-    l_.assign(p->variable_lower_bound, p->variable_lower_bound + n_);
-    u_.assign(p->variable_upper_bound, p->variable_upper_bound + n_);
-    for (double v : g_)
-        has_g_ |= v != 0.0;
-    for (int i = 0; i < n_; ++i)
-        box_free_ &= !std::isfinite(l_[i]) && !std::isfinite(u_[i]);
-    for (int i = 0; i < m_; ++i)
-        eq_rows_ &= lc_[i] == uc_[i] && std::isfinite(lc_[i]);
-
-    // objective structure
-    int nnzq = (p->objective_sparse_matrix && p->objective_sparse_matrix->row_ptr)
-                   ? p->objective_sparse_matrix_num_nonzeros
-                   : 0;
-    int nnzr = (p->objective_lowrank_matrix && p->objective_lowrank_matrix->row_ptr && p->num_rank_lowrank_obj > 0)
-                   ? p->objective_lowrank_matrix_num_nonzeros
-                   : 0;
-    if (nnzq == 0 && nnzr == 0)
-        qtype_ = PDHCG_NON_Q;
-    else if (nnzr > 0)
-        qtype_ = nnzq > 0 ? PDHCG_LOW_RANK_PLUS_SPARSE_Q : PDHCG_LOW_RANK_Q;
-    else {
-        qtype_ = PDHCG_DIAG_Q;
-        const CsrComponent *Q = p->objective_sparse_matrix;
-        for (int i = 0; i < n_ && qtype_ == PDHCG_DIAG_Q; ++i)
-            for (int k = Q->row_ptr[i]; k < Q->row_ptr[i + 1]; ++k)
-                if (Q->col_ind[k] != i) {
-                    qtype_ = PDHCG_SPARSE_Q;
-                    break;
-                }
-    }
-
-    // cones
-    int maxlen = 0;
-    std::vector<char> in_cone(n_, 0);
-    for (int b = 0; b < p->cones.num_cones; ++b) {
-        int len = pdhcg_b200_cone_length(p->cones.type[b], p->cones.v_dim[b]);
-        cone_start_.push_back(p->cones.start_idx[b]);
-        cone_len_.push_back(len);
-        cone_type_.push_back((int)p->cones.type[b]);
-        cone_vdim_.push_back(p->cones.v_dim[b]);
-        maxlen = std::max(maxlen, len);
-        for (int i = 0; i < len; ++i) {
-            int j = p->cones.start_idx[b] + i;
-            in_cone[j] = 1;
-            cone_box_ |= std::isfinite(l_[j]) || std::isfinite(u_[j]);
-        }
-    }
-    if (!cone_start_.empty()) {
-        for (int i = 0; i < n_; ++i)
-            if (!in_cone[i])
-                free_idx_.push_back(i);
-        S_ = slots_class(maxlen);
-    }
+    n_ = dp_.n;
+    m_ = dp_.m;
+    qtype_ = dp_.qtype;
+    has_g_ = dp_.has_g;
+    box_free_ = dp_.box_free;
+    eq_rows_ = dp_.eq_rows;
+    cone_box_ = dp_.cone_box;
+    cone_start_ = dp_.cone_start;
+    cone_len_ = dp_.cone_len;
+    cone_type_ = dp_.cone_type;
+    cone_vdim_ = dp_.cone_vdim;
+    free_idx_ = dp_.free_idx;
+    S_ = dp_.S;
 }
 
 void Solve::upload_and_preprocess()
 {
     cudaStream_t s = st_;
+    auto mut = [&](double *src, size_t k) -> double * { // arrays the solve rescales in place
+        if (own_)
+            return src;
+        double *d = ar_.alloc<double>(k);
+        if (k)
+            CK(cudaMemcpyAsync(d, src, k * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        return d;
+    };
     A_.rows = m_;
     A_.cols = n_;
-    A_.nnz = (int)A_v_.size();
-    A_.rp = ar_.upload(A_rp_.data(), A_rp_.size(), s);
-    A_.ci = ar_.upload(A_ci_.data(), A_ci_.size(), s);
-    A_.v = ar_.upload(A_v_.data(), A_v_.size(), s);
+    A_.nnz = dp_.nnzA;
+    A_.rp = dp_.A_rp;
+    A_.ci = dp_.A_ci;
+    A_.v = mut(dp_.A_v, dp_.nnzA);
     At_ = transpose(A_, ar_, s);
-    c_d_ = ar_.upload(c_.data(), n_, s);
-    l_d_ = ar_.upload(l_.data(), n_, s);
-    u_d_ = ar_.upload(u_.data(), n_, s);
-    lc_d_ = ar_.upload(lc_.data(), m_, s);
-    uc_d_ = ar_.upload(uc_.data(), m_, s);
-    g_d_ = ar_.upload(g_.data(), m_, s);
+    c_d_ = mut(dp_.c, n_);
+    l_d_ = mut(dp_.l, n_);
+    u_d_ = mut(dp_.u, n_);
+    lc_d_ = mut(dp_.lc, m_);
+    uc_d_ = mut(dp_.uc, m_);
+    g_d_ = mut(dp_.g, m_);
     if (qtype_ != PDHCG_NON_Q) {
-        const CsrComponent *Q = P_->objective_sparse_matrix;
         Q_.rows = n_;
         Q_.cols = n_;
-        Q_.nnz = P_->objective_sparse_matrix_num_nonzeros;
-        Q_.rp = ar_.upload(Q->row_ptr, (size_t)n_ + 1, s);
-        Q_.ci = ar_.upload(Q->col_ind, Q_.nnz, s);
-        Q_.v = ar_.upload(Q->val, Q_.nnz, s);
+        Q_.nnz = dp_.nnzQ;
+        Q_.rp = dp_.Q_rp;
+        Q_.ci = dp_.Q_ci;
+        Q_.v = mut(dp_.Q_v, dp_.nnzQ);
     }
-    int nc = (int)cone_start_.size();
-    if (nc > 0) {
-        cst_d_ = ar_.upload(cone_start_.data(), nc, s);
-        clen_d_ = ar_.upload(cone_len_.data(), nc, s);
-        ctype_d_ = ar_.upload(cone_type_.data(), nc, s);
-        cvdim_d_ = ar_.upload(cone_vdim_.data(), nc, s);
-        if (!free_idx_.empty())
-            free_d_ = ar_.upload(free_idx_.data(), free_idx_.size(), s);
-    }
+    cst_d_ = dp_.cst;
+    clen_d_ = dp_.clen;
+    ctype_d_ = dp_.ctype;
+    cvdim_d_ = dp_.cvdim;
+    free_d_ = dp_.free_d;
     GA_ = pick_group(A_.nnz, m_);
     GAt_ = pick_group(At_.nnz, n_);
 }
@@ -521,13 +604,9 @@ void Solve::init_state()
     dy_ = ar_.alloc<double>(m);
     CK(cudaMemsetAsync(x0_, 0, n * sizeof(double), s));
     CK(cudaMemsetAsync(dslack_, 0, n * sizeof(double), s));
-    if (P_->primal_start) {
-        double *ps = ar_.upload(P_->primal_start, n, s);
-        scale_start_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(n, ps, vr_d_, sb_, x0_);
-    }
-    const double *ds = nullptr;
-    if (P_->dual_start && !(P_->num_constraints == 0 || P_->constraint_matrix == nullptr))
-        ds = ar_.upload(P_->dual_start, m, s);
+    if (dp_.pstart)
+        scale_start_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(n, dp_.pstart, vr_d_, sb_, x0_);
+    const double *ds = dp_.dstart;
     dual_start_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(m, ds, cr_d_, sc_, y0_, y_, yp_);
     if (nc > 0) {
         cone_warm_ = ar_.alloc<double>(3 * (size_t)nc);
@@ -972,8 +1051,8 @@ void Solve::read_residual()
     double lin_abs_p = abs_p_;
     abs_d_ = nrm(r[RS_DUAL_RES]) / sc_;
     double half_xqx = qtype_ == PDHCG_NON_Q ? 0.0 : 0.5 * r[RS_XQX];
-    pobj_ = (r[RS_CX] + half_xqx) / (sb_ * sc_) + P_->objective_constant;
-    dobj_ = (r[RS_SLACKX] + r[RS_PRIMAL_SLACK] - half_xqx) / (sb_ * sc_) + P_->objective_constant;
+    pobj_ = (r[RS_CX] + half_xqx) / (sb_ * sc_) + dp_.obj_const;
+    dobj_ = (r[RS_SLACKX] + r[RS_PRIMAL_SLACK] - half_xqx) / (sb_ * sc_) + dp_.obj_const;
     rel_p_ = lin_abs_p / (1.0 + bnorm_);
     double den;
     if (qtype_ == PDHCG_NON_Q)
@@ -1121,7 +1200,22 @@ pdhcg_result_t *Solve::make_result()
 {
     cudaStream_t s = st_;
     int n = n_, m = m_;
-    double *xo = ar_.alloc<double>(n), *yo = ar_.alloc<double>(m), *rco = ar_.alloc<double>(n);
+    bool on_dev = opt_.solution_on_device != 0;
+    double *xo, *yo, *rco;
+    if (on_dev) { // kept with the device problem for pdhcg_b200_device_solution
+        if (!dp_.x_out) {
+            dp_.x_out = dp_.ar.alloc<double>(n);
+            dp_.y_out = dp_.ar.alloc<double>(m);
+            dp_.rc_out = dp_.ar.alloc<double>(n);
+        }
+        xo = dp_.x_out;
+        yo = dp_.y_out;
+        rco = dp_.rc_out;
+    } else {
+        xo = ar_.alloc<double>(n);
+        yo = ar_.alloc<double>(m);
+        rco = ar_.alloc<double>(n);
+    }
     if (fp32_)
         result_kernel<float><<<grid_for((long long)n + m, TPB), TPB, 0, s>>>(
             n, m, At_.rp, At_.ci, At_.v, c_d_, q_d_, nullptr, qtype_ == PDHCG_DIAG_Q ? 1 : 0, l_d_, u_d_, vr_d_,
@@ -1131,16 +1225,18 @@ pdhcg_result_t *Solve::make_result()
             n, m, At_.rp, At_.ci, At_.v, c_d_, q_d_, nullptr, qtype_ == PDHCG_DIAG_Q ? 1 : 0, l_d_, u_d_, vr_d_,
             cr_d_, sb_, sc_, xp_, yp_, xo, yo, rco);
     pdhcg_result_t *r = (pdhcg_result_t *)std::calloc(1, sizeof(pdhcg_result_t));
-    r->primal_solution = (double *)std::malloc(std::max(n, 1) * sizeof(double));
-    r->dual_solution = (double *)std::malloc(std::max(m, 1) * sizeof(double));
-    r->reduced_cost = (double *)std::malloc(std::max(n, 1) * sizeof(double));
-    CK(cudaMemcpyAsync(r->primal_solution, xo, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(r->dual_solution, yo, m * sizeof(double), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(r->reduced_cost, rco, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (!on_dev) {
+        r->primal_solution = (double *)std::malloc(std::max(n, 1) * sizeof(double));
+        r->dual_solution = (double *)std::malloc(std::max(m, 1) * sizeof(double));
+        r->reduced_cost = (double *)std::malloc(std::max(n, 1) * sizeof(double));
+        CK(cudaMemcpyAsync(r->primal_solution, xo, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(r->dual_solution, yo, m * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(r->reduced_cost, rco, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
     CK(cudaStreamSynchronize(s));
-    r->num_variables = P_->num_variables;
-    r->num_constraints = P_->num_constraints;
-    r->num_nonzeros = P_->constraint_matrix_num_nonzeros;
+    r->num_variables = dp_.orig_vars;
+    r->num_constraints = dp_.orig_cons;
+    r->num_nonzeros = dp_.orig_nnz;
     r->total_count = k_;
     r->total_inner_count = (int)inner_total_;
     r->cumulative_time_sec = cum_time_;
@@ -1163,17 +1259,8 @@ pdhcg_result_t *Solve::run()
     build_host();
     auto t_host = std::chrono::steady_clock::now();
     stats_.host_copy_ms = std::chrono::duration<double, std::milli>(t_host - t_setup).count();
-    if (qtype_ != PDHCG_NON_Q && qtype_ != PDHCG_DIAG_Q)
-        throw CudaError("non-diagonal Q (inner BB solve) is not available yet");
-    if (S_ < 0)
-        throw CudaError("cone blocks longer than 256 slots are not supported yet");
-    for (int t : cone_type_)
-        if (t != CONE_STANDARD_SOC && t != CONE_ROTATED_SOC)
-            throw CudaError("only SOC and rotated SOC cones are available on the device path yet");
-    if (P_->cones.is_fixed)
-        throw CudaError("fixed cone slots are not available on the device path yet");
-    if (P_->affine_cones.num_cones > 0)
-        throw CudaError("affine cones are not available on the device path yet");
+    if (!dp_.unsupported.empty())
+        throw CudaError(dp_.unsupported);
     upload_and_preprocess();
     CK(cudaStreamSynchronize(st_));
     stats_.upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host).count();
@@ -1217,7 +1304,7 @@ pdhcg_result_t *Solve::run()
             cnorm_ = std::sqrt(h[NS_C2]);
             bnorm_ = std::sqrt(h[NS_B2]);
         }
-        if (P_->num_constraints == 0 || P_->constraint_matrix == nullptr)
+        if (dp_.dummy)
             bnorm_ = 0.0; // the dummy row has infinite bounds and no offset
     }
     rescale();
@@ -1349,7 +1436,18 @@ pdhcg_result_t *pdhcg_b200_solve(const qp_problem_t *prob, const pdhg_parameters
         auto t0 = std::chrono::steady_clock::now();
         pdhcg_result_t *r = nullptr;
         {
-            Solve s(prob, prm, opt);
+            cudaStream_t us = nullptr;
+            CK(cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking));
+            std::unique_ptr<DeviceProblem> dp;
+            try {
+                dp = make_device_problem(prob, us);
+            } catch (...) {
+                cudaStreamDestroy(us);
+                throw;
+            }
+            cudaStreamDestroy(us);
+            opt.solution_on_device = 0; // the temporary device problem dies with this call
+            Solve s(*dp, true, prm, opt);
             r = s.run();
         }
         g_last_stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -1369,6 +1467,82 @@ pdhcg_result_t *pdhcg_b200_solve(const qp_problem_t *prob, const pdhg_parameters
         std::fprintf(stderr, "[pdhcg_b200] solve failed: %s\n", e.what());
         return nullptr;
     }
+}
+
+struct pdhcg_b200_device_problem_s {
+    std::unique_ptr<DeviceProblem> dp;
+};
+
+pdhcg_b200_device_problem_t *pdhcg_b200_upload(const qp_problem_t *prob)
+{
+    if (!prob) {
+        std::fprintf(stderr, "[pdhcg_b200_upload] prob is NULL\n");
+        return nullptr;
+    }
+    cudaStream_t us = nullptr;
+    try {
+        CK(cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking));
+        auto h = new pdhcg_b200_device_problem_s;
+        h->dp = make_device_problem(prob, us);
+        cudaStreamDestroy(us);
+        return h;
+    } catch (const std::exception &e) {
+        if (us)
+            cudaStreamDestroy(us);
+        std::fprintf(stderr, "[pdhcg_b200_upload] failed: %s\n", e.what());
+        return nullptr;
+    }
+}
+
+pdhcg_result_t *pdhcg_b200_solve_device(pdhcg_b200_device_problem_t *h, const pdhg_parameters_t *params,
+                                        const pdhcg_b200_options_t *opts)
+{
+    if (!h || !h->dp) {
+        std::fprintf(stderr, "[pdhcg_b200_solve_device] invalid handle\n");
+        return nullptr;
+    }
+    pdhg_parameters_t prm;
+    if (params)
+        prm = *params;
+    else
+        set_default_parameters(&prm);
+    pdhcg_b200_options_t opt;
+    if (opts)
+        opt = *opts;
+    else
+        pdhcg_b200_default_options(&opt);
+    try {
+        auto t0 = std::chrono::steady_clock::now();
+        pdhcg_result_t *r = nullptr;
+        {
+            Solve s(*h->dp, false, prm, opt);
+            r = s.run();
+        }
+        g_last_stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return r;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "[pdhcg_b200] solve failed: %s\n", e.what());
+        return nullptr;
+    }
+}
+
+int pdhcg_b200_device_solution(const pdhcg_b200_device_problem_t *h, const double **x, const double **y,
+                               const double **reduced_cost)
+{
+    if (!h || !h->dp || !h->dp->x_out)
+        return -1;
+    if (x)
+        *x = h->dp->x_out;
+    if (y)
+        *y = h->dp->y_out;
+    if (reduced_cost)
+        *reduced_cost = h->dp->rc_out;
+    return 0;
+}
+
+void pdhcg_b200_device_problem_free(pdhcg_b200_device_problem_t *h)
+{
+    delete h;
 }
 
 pdhcg_result_t *solve_qp_problem(const qp_problem_t *prob, const pdhg_parameters_t *params)

@@ -20,7 +20,8 @@ class Options(C.Structure):
     """pdhcg_b200_options_t (include/pdhcg_b200.h)."""
     _fields_ = [("precision", C.c_int), ("polish_threshold", C.c_double),
                 ("has_initial_primal_weight", C.c_int), ("initial_primal_weight", C.c_double),
-                ("use_graphs", C.c_int), ("time_steps", C.c_int), ("reserved", C.c_int * 6)]
+                ("use_graphs", C.c_int), ("time_steps", C.c_int), ("solution_on_device", C.c_int),
+                ("reserved", C.c_int * 5)]
 
 
 class Stats(C.Structure):
@@ -56,7 +57,8 @@ EXPORTS = [
     "solve_qp_problem_distributed", "set_default_parameters", "pdhcg_result_free", "qp_problem_free",
     # additive entry points (include/pdhcg_b200.h)
     "pdhcg_b200_default_options", "pdhcg_b200_solve", "pdhcg_b200_last_stats", "pdhcg_b200_csr_spmv",
-    "pdhcg_b200_project_cones", "pdhcg_b200_pdhg_step",
+    "pdhcg_b200_project_cones", "pdhcg_b200_pdhg_step", "pdhcg_b200_upload", "pdhcg_b200_solve_device",
+    "pdhcg_b200_device_solution", "pdhcg_b200_device_problem_free",
 ]
 
 
@@ -90,6 +92,14 @@ def load(build: bool = True) -> C.CDLL:
                                              C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
     lib.pdhcg_b200_pdhg_step.restype = C.c_int
     lib.pdhcg_b200_pdhg_step.argtypes = [P(StepArgs), C.c_void_p]
+    lib.pdhcg_b200_upload.restype = C.c_void_p
+    lib.pdhcg_b200_upload.argtypes = [P(capi.QpProblem)]
+    lib.pdhcg_b200_solve_device.restype = P(capi.PdhcgResult)
+    lib.pdhcg_b200_solve_device.argtypes = [C.c_void_p, P(capi.PdhgParameters), P(Options)]
+    lib.pdhcg_b200_device_solution.restype = C.c_int
+    lib.pdhcg_b200_device_solution.argtypes = [C.c_void_p, P(C.c_void_p), P(C.c_void_p), P(C.c_void_p)]
+    lib.pdhcg_b200_device_problem_free.restype = None
+    lib.pdhcg_b200_device_problem_free.argtypes = [C.c_void_p]
     _LIB = lib
     return lib
 

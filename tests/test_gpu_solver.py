@@ -116,3 +116,41 @@ def test_mixed_precision_reaches_fp64_answer(lib, name):
     assert mix["rel_kkt"] < 1e-6
     assert abs(mix["primal_objective_value"] - ref["primal_objective_value"]) <= 1e-5 * (
         1 + abs(ref["primal_objective_value"]))
+
+
+def test_device_resident_handle_matches_host_path(lib):
+    """pdhcg_b200_upload + pdhcg_b200_solve_device give the same answer as the
+    host-buffer call, the handle can be solved repeatedly, and the solution
+    can stay on the device."""
+    import torch
+    p = instances.conic_lp(seed=31, with_q=True)
+    prm_over = {"termination_criteria.iteration_limit": 50000}
+    host = _solve_gpu(lib, p, prm_over)
+    prob, keep = capi.build(lib, p)
+    prm = capi.default_params(lib, **prm_over)
+    h = lib.pdhcg_b200_upload(prob)
+    assert h
+    for _ in range(2):
+        r = lib.pdhcg_b200_solve_device(h, C.byref(prm), None)
+        assert r
+        d = capi.result_dict(r, p.n, p.A.m)
+        lib.pdhcg_result_free(r)
+        assert d["status"] == host["status"]
+        assert d["total_count"] == host["total_count"]
+        np.testing.assert_allclose(d["x"], host["x"], rtol=1e-12, atol=1e-12)
+    o = native.default_options(solution_on_device=1)
+    r = lib.pdhcg_b200_solve_device(h, C.byref(prm), C.byref(o))
+    assert r and not r.contents.primal_solution
+    lib.pdhcg_result_free(r)
+    xp, yp, rp = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    assert lib.pdhcg_b200_device_solution(h, C.byref(xp), C.byref(yp), C.byref(rp)) == 0
+    torch.cuda.synchronize()
+
+    class _DeviceArray:  # wraps the library's device pointer for torch
+        def __init__(self, ptr, n):
+            self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, True), "version": 2}
+
+    xt = torch.as_tensor(_DeviceArray(xp.value, p.n), device="cuda")
+    np.testing.assert_allclose(xt.cpu().numpy(), host["x"], rtol=1e-12, atol=1e-12)
+    lib.pdhcg_b200_device_problem_free(h)
+    lib.qp_problem_free(prob)
