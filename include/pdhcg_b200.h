@@ -9,6 +9,8 @@
  */
 #pragma once
 
+#include <signal.h>
+
 #include "pdhcg_types.h"
 
 #ifdef __cplusplus
@@ -81,10 +83,21 @@ typedef struct {
 
 int pdhcg_b200_last_stats(pdhcg_b200_stats_t *out);
 
+/* Cancellation.  g_pdhcg_cancel_request is the reference's flag (reference
+ * src/pdhcg.c:31), exported under the same name so that its Python binding
+ * (which declares it extern and sets it from a SIGINT handler, reference
+ * python_bindings/_core_bindings.cpp:41-47) links unchanged.  A non-zero
+ * value ends the running solve at its next evaluation with
+ * TERMINATION_REASON_USER_INTERRUPT. */
+extern volatile sig_atomic_t g_pdhcg_cancel_request;
+void pdhcg_b200_request_cancel(int on);
+
 /* ---- kernel-level entry points on device pointers ------------------------
  * For parity tests and embedding.  Pointers are device memory of the current
- * device; stream may be NULL (legacy default stream).  They allocate nothing
- * and return after enqueueing (call cudaStreamSynchronize to wait). */
+ * device; stream may be NULL (legacy default stream).  They return after
+ * enqueueing (call cudaStreamSynchronize to wait).  pdhcg_b200_csr_spmv
+ * allocates nothing; pdhcg_b200_project_cones and pdhcg_b200_pdhg_step take
+ * small stream-ordered temporaries (cudaMallocAsync / cudaFreeAsync). */
 
 /* y = M x for a CSR matrix (int32 indices, FP64 values). */
 int pdhcg_b200_csr_spmv(int rows, const int *row_ptr, const int *col_ind, const double *val, const double *x,

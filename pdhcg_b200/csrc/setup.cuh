@@ -163,6 +163,16 @@ __global__ void scale_csr_kernel(const int *rp, const int *ci, double *v, int ro
     }
 }
 
+// v_k /= rs[r] for every entry of row r
+__global__ void scale_rows_kernel(const int *rp, double *v, int rows, const double *rs)
+{
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        double a = rs[r];
+        for (int k = rp[r]; k < rp[r + 1]; ++k)
+            v[k] /= a;
+    }
+}
+
 __global__ void scale_cols_kernel(const int *rp, const int *ci, double *v, int rows, const double *cs)
 {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)

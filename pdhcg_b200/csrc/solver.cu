@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "bb.cuh"
 #include "residual.cuh"
 #include "setup.cuh"
 
@@ -200,6 +201,10 @@ struct DeviceProblem {
     Arena ar;
     int *A_rp = nullptr, *A_ci = nullptr, *Q_rp = nullptr, *Q_ci = nullptr;
     double *A_v = nullptr, *Q_v = nullptr;
+    // low-rank term R (k rows, CSR) and its middle matrix D
+    int rank = 0, nnzR = 0, dkind = 0; // dkind 0 none (identity), 1 diagonal, 2 dense
+    int *R_rp = nullptr, *R_ci = nullptr;
+    double *R_v = nullptr, *Ddiag = nullptr, *Ddense = nullptr;
     double *c = nullptr, *l = nullptr, *u = nullptr, *lc = nullptr, *uc = nullptr, *g = nullptr;
     int *cst = nullptr, *clen = nullptr, *ctype = nullptr, *cvdim = nullptr, *free_d = nullptr;
     double *pstart = nullptr, *dstart = nullptr;
@@ -279,12 +284,51 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
                     break;
                 }
     }
-    if (d.qtype != PDHCG_NON_Q) {
+    if (d.qtype != PDHCG_NON_Q && nnzq > 0) {
         const CsrComponent *Q = p->objective_sparse_matrix;
         d.nnzQ = p->objective_sparse_matrix_num_nonzeros;
         d.Q_rp = ar.upload(Q->row_ptr, (size_t)d.n + 1, s);
         d.Q_ci = ar.upload(Q->col_ind, d.nnzQ, s);
         d.Q_v = ar.upload(Q->val, d.nnzQ, s);
+    }
+    if (nnzr > 0) {
+        const CsrComponent *R = p->objective_lowrank_matrix;
+        d.rank = p->num_rank_lowrank_obj;
+        d.nnzR = nnzr;
+        d.R_rp = ar.upload(R->row_ptr, (size_t)d.rank + 1, s);
+        d.R_ci = ar.upload(R->col_ind, d.nnzR, s);
+        d.R_v = ar.upload(R->val, d.nnzR, s);
+        // middle matrix kind (reference preprocess_qp_problem, src/preconditioner.c:742-791)
+        const CsrComponent *Dm = p->objective_lowrank_middle_matrix;
+        int k = d.rank;
+        if (Dm && Dm->row_ptr && p->objective_lowrank_middle_matrix_num_nonzeros > 0) {
+            bool diag_only = true;
+            for (int r = 0; r < k && diag_only; ++r)
+                for (int j = Dm->row_ptr[r]; j < Dm->row_ptr[r + 1]; ++j)
+                    if (Dm->col_ind[j] != r) {
+                        diag_only = false;
+                        break;
+                    }
+            if (diag_only) {
+                std::vector<double> dd(k, 0.0);
+                for (int r = 0; r < k; ++r)
+                    for (int j = Dm->row_ptr[r]; j < Dm->row_ptr[r + 1]; ++j)
+                        dd[r] = Dm->val[j];
+                d.dkind = 1;
+                d.Ddiag = ar.upload(dd.data(), k, s);
+                CK(cudaStreamSynchronize(s));
+            } else {
+                std::vector<double> dd((size_t)k * k, 0.0);
+                for (int r = 0; r < k; ++r)
+                    for (int j = Dm->row_ptr[r]; j < Dm->row_ptr[r + 1]; ++j)
+                        dd[(size_t)r * k + Dm->col_ind[j]] = Dm->val[j];
+                d.dkind = 2;
+                d.Ddense = ar.upload(dd.data(), (size_t)k * k, s);
+                CK(cudaStreamSynchronize(s));
+            }
+        }
+        if (k > BB_MAX_RANK)
+            d.unsupported = "low-rank terms of rank above 512 are not supported yet";
     }
 
     int maxlen = 0;
@@ -317,8 +361,6 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
         if (!d.free_idx.empty())
             d.free_d = ar.upload(d.free_idx.data(), d.free_idx.size(), s);
     }
-    if (d.qtype != PDHCG_NON_Q && d.qtype != PDHCG_DIAG_Q)
-        d.unsupported = "non-diagonal Q (inner BB solve) is not available yet";
     if (d.S < 0)
         d.unsupported = "cone blocks longer than 256 slots are not supported yet";
     if (p->cones.is_fixed)
@@ -355,6 +397,9 @@ private:
     void step_size();
     void loop();
     void enqueue_step(bool store_primal, bool store_dual, bool want_fpe, double w);
+    void enqueue_step_bb(bool store_dual, bool want_fpe, double w);
+    template <typename T>
+    void launch_dual(const StepData<T> &D, const StepParams &P);
     template <typename T>
     void enqueue_step_t(bool store_primal, bool store_dual, bool want_fpe, double w);
     template <typename T>
@@ -386,7 +431,18 @@ private:
     int S_ = 1;
 
     // device
-    DevCsr A_, At_, Q_;
+    DevCsr A_, At_, Q_, R_, Rt_;
+    // inner BB solve (non-diagonal Q)
+    bool bb_ = false;
+    int bb_grid_ = 0, bb_limit_ = 1, GQ_ = 1;
+    double *bb_aty_ = nullptr, *bb_grad_ = nullptr, *bb_dir_ = nullptr, *bb_qx_ = nullptr, *qx_res_ = nullptr;
+    double *bb_part_ = nullptr, *bb_rxp_ = nullptr, *bb_rx_ = nullptr, *bb_tol_ = nullptr, *bb_tscale_ = nullptr;
+    double *bb_diag_h_ = nullptr, *bb_m_ = nullptr, *bb_minv_ = nullptr;
+    int *bb_inner_ = nullptr;
+    double bb_cached_inv_tau_ = -1.0, bb_min_tol_ = 1e-9;
+    BBData bb_data() const;
+    void setup_bb();
+    void enqueue_q_apply(const double *v, double *qx);
     double *c_d_ = nullptr, *l_d_ = nullptr, *u_d_ = nullptr, *q_d_ = nullptr, *lc_d_ = nullptr, *uc_d_ = nullptr,
            *g_d_ = nullptr, *cr_d_ = nullptr, *vr_d_ = nullptr;
     int *free_d_ = nullptr, *cst_d_ = nullptr, *clen_d_ = nullptr, *ctype_d_ = nullptr, *cvdim_d_ = nullptr;
@@ -519,6 +575,15 @@ void Solve::upload_and_preprocess()
         Q_.ci = dp_.Q_ci;
         Q_.v = mut(dp_.Q_v, dp_.nnzQ);
     }
+    if (dp_.nnzR > 0) {
+        R_.rows = dp_.rank;
+        R_.cols = n_;
+        R_.nnz = dp_.nnzR;
+        R_.rp = dp_.R_rp;
+        R_.ci = dp_.R_ci;
+        R_.v = mut(dp_.R_v, dp_.nnzR);
+        Rt_ = transpose(R_, ar_, s);
+    }
     cst_d_ = dp_.cst;
     clen_d_ = dp_.clen;
     ctype_d_ = dp_.ctype;
@@ -554,6 +619,10 @@ void Solve::rescale()
         scale_csr_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.ci, At_.v, n, fvr, fcr, 1);
         if (Q_.nnz > 0)
             scale_csr_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(Q_.rp, Q_.ci, Q_.v, n, fvr, fvr, 0);
+        if (R_.nnz > 0) { // R /= D_var by columns (reference scale_problem, src/preconditioner.c:295-307)
+            scale_cols_kernel<<<grid_for(R_.rows, TPB), TPB, 0, s>>>(R_.rp, R_.ci, R_.v, R_.rows, fvr);
+            scale_rows_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(Rt_.rp, Rt_.v, n, fvr);
+        }
         scale_vectors_kernel<<<grid_for((long long)n + m, TPB), TPB, 0, s>>>(n, m, c_d_, l_d_, u_d_, fvr, lc_d_,
                                                                              uc_d_, g_d_, fcr, vr_d_, cr_d_);
         CK(cudaGetLastError());
@@ -584,6 +653,11 @@ void Solve::rescale()
                                                                                lc_d_, uc_d_, g_d_);
         if (Q_.nnz > 0)
             mul_scalar_kernel<<<grid_for(Q_.nnz, TPB), TPB, 0, s>>>(Q_.v, Q_.nnz, sc_ / sb_);
+        if (R_.nnz > 0) {
+            double f = std::sqrt(sc_ / sb_);
+            mul_scalar_kernel<<<grid_for(R_.nnz, TPB), TPB, 0, s>>>(R_.v, R_.nnz, f);
+            mul_scalar_kernel<<<grid_for(Rt_.nnz, TPB), TPB, 0, s>>>(Rt_.v, Rt_.nnz, f);
+        }
     }
     CK(cudaGetLastError());
 }
@@ -633,6 +707,156 @@ void Solve::init_state()
         nonconvexity_ = mn; // reference initialize_quadratic_term_information, src/solver_state.cu:400-418
     }
     CK(cudaGetLastError());
+}
+
+// ---- inner BB solve set-up (reference initialize_inner_solver and
+// initialize_quadratic_term_information, src/solver_state.cu:280-420) -------
+BBData Solve::bb_data() const
+{
+    BBData D{};
+    D.n = n_;
+    D.c = c_d_;
+    D.l = l_d_;
+    D.u = u_d_;
+    D.aty = bb_aty_;
+    D.sparse = Q_.nnz > 0;
+    D.Q_rp = Q_.rp;
+    D.Q_ci = Q_.ci;
+    D.Q_v = Q_.v;
+    D.k = R_.nnz > 0 ? R_.rows : 0;
+    D.R_rp = R_.rp;
+    D.R_ci = R_.ci;
+    D.R_v = R_.v;
+    D.Rt_rp = Rt_.rp;
+    D.Rt_ci = Rt_.ci;
+    D.Rt_v = Rt_.v;
+    D.dkind = dp_.dkind;
+    D.Ddiag = dp_.Ddiag;
+    D.Ddense = dp_.Ddense;
+    D.m_diag = bb_m_;
+    D.m_inv = bb_minv_;
+    D.tol_scale = bb_tscale_;
+    D.free_idx = free_d_;
+    D.n_free = (int)free_idx_.size();
+    D.cone_start = cst_d_;
+    D.cone_len = clen_d_;
+    D.cone_type = ctype_d_;
+    D.n_cones = (int)cone_start_.size();
+    D.vr = vr_d_;
+    D.cone_warm = cone_warm_;
+    D.x0 = x0_;
+    D.x = x_;
+    D.xp = xp_;
+    D.xr = xr_;
+    D.dx = dx_;
+    D.grad = bb_grad_;
+    D.dir = bb_dir_;
+    D.qx = bb_qx_;
+    D.part = bb_part_;
+    D.rx_part = bb_rxp_;
+    D.rx = bb_rx_;
+    D.tol = bb_tol_;
+    D.limit = bb_limit_;
+    D.inner_total = bb_inner_;
+    return D;
+}
+
+void Solve::setup_bb()
+{
+    cudaStream_t s = st_;
+    int n = n_;
+    GQ_ = residual_group(pick_group((long long)Q_.nnz + Rt_.nnz, n));
+    // cooperative grid: every block resident at once
+    int dev = 0, nsm = 0, per_sm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    dispatch_rg(GQ_, [&](auto GC) {
+        dispatch_s(S_, [&](auto SC) {
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bb_kernel<GC.value, SC.value>, TPB, 0));
+        });
+    });
+    int q_per_sm = 0;
+    dispatch_rg(GQ_, [&](auto GC) {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&q_per_sm, q_apply_kernel<GC.value>, TPB, 0));
+    });
+    per_sm = std::min(per_sm, q_per_sm);
+    if (per_sm < 1)
+        throw CudaError("inner BB kernel cannot be made resident");
+    bb_grid_ = nsm * std::min(per_sm, 4);
+    int k = R_.nnz > 0 ? R_.rows : 0;
+    bb_aty_ = ar_.alloc<double>(n);
+    bb_grad_ = ar_.alloc<double>(n);
+    bb_dir_ = ar_.alloc<double>(n);
+    bb_qx_ = ar_.alloc<double>(n);
+    qx_res_ = ar_.alloc<double>(n);
+    bb_part_ = ar_.alloc<double>((size_t)4 * bb_grid_);
+    bb_rxp_ = ar_.alloc<double>((size_t)bb_grid_ * std::max(k, 1));
+    bb_rx_ = ar_.alloc<double>(std::max(k, 1));
+    bb_tol_ = ar_.alloc<double>(2);
+    bb_tscale_ = bb_tol_ + 1;
+    bb_inner_ = ar_.alloc<int>(1);
+    CK(cudaMemsetAsync(bb_inner_, 0, sizeof(int), s));
+    int lim = prm_.inner_solver_parameters.iteration_limit;
+    double it0 = prm_.inner_solver_parameters.initial_tolerance;
+    double mt = prm_.inner_solver_parameters.min_tolerance;
+    if (lim < 1)
+        lim = 1;
+    if (it0 <= 0.0)
+        it0 = 1e-3;
+    if (mt <= 0.0)
+        mt = 1e-9;
+    bb_limit_ = lim;
+    bb_min_tol_ = mt;
+    double init[2] = {it0, 1.0};
+    CK(cudaMemcpyAsync(bb_tol_, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    if (prm_.diag_jacobi_precond) {
+        bb_diag_h_ = ar_.alloc<double>(n);
+        bb_m_ = ar_.alloc<double>(n);
+        bb_minv_ = ar_.alloc<double>(n);
+        bb_diag_h_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(n, Q_.nnz > 0, Q_.rp, Q_.ci, Q_.v, k, Rt_.rp, Rt_.ci,
+                                                          Rt_.v, dp_.dkind, dp_.Ddiag, dp_.Ddense, bb_diag_h_);
+    }
+    // eigenvalues of a sparse Q (the reference computes them for SPARSE_Q only)
+    if (qtype_ == PDHCG_SPARSE_Q) {
+        std::vector<double> v0(n);
+        unsigned int seed = 1234;
+        for (int i = 0; i < n; ++i)
+            v0[i] = (double)rand_r(&seed) / RAND_MAX;
+        double *v = ar_.alloc<double>(n), *av = ar_.alloc<double>(n), *out = ar_.alloc<double>(2);
+        double *part = ar_.alloc<double>((size_t)2 * bb_grid_);
+        int eper = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&eper, power_eig_kernel, TPB, 0));
+        int eg = std::max(1, std::min(bb_grid_, nsm * std::max(eper, 1)));
+        double lmax = 0.0;
+        for (int shifted = 0; shifted < 2; ++shifted) {
+            CK(cudaMemcpyAsync(v, v0.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+            int maxit = prm_.sv_max_iter;
+            double tol = prm_.sv_tol;
+            void *args[] = {&n, &Q_.rp, &Q_.ci, &Q_.v, &v, &av, &part, &maxit, &tol, &shifted, &lmax, &out};
+            CK(cudaLaunchCooperativeKernel((void *)power_eig_kernel, eg, TPB, args, 0, s));
+            double h[2];
+            CK(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            if (shifted)
+                nonconvexity_ = h[0];
+            else
+                lmax = h[0];
+        }
+    }
+    if (nonconvexity_ < 0)
+        bb_limit_ = 1; // reference optimize, src/solver.cu:109-112
+    CK(cudaGetLastError());
+}
+
+void Solve::enqueue_q_apply(const double *v, double *qx)
+{
+    BBData D = bb_data();
+    int grid = bb_grid_;
+    dispatch_rg(GQ_, [&](auto GC) {
+        void *args[] = {&D, (void *)&v, &qx};
+        CK(cudaLaunchCooperativeKernel((void *)q_apply_kernel<GC.value>, grid, TPB, args, 0, st_));
+    });
+    stats_.kernel_launches++;
 }
 
 // ---- step size (reference initialize_step_size_and_primal_weight,
@@ -747,8 +971,94 @@ StepData<T> Solve::step_data()
     return D;
 }
 
+template <typename T>
+void Solve::launch_dual(const StepData<T> &D, const StepParams &P)
+{
+    cudaStream_t s = st_;
+    dispatch_g(GA_, [&](auto GC) {
+        constexpr int G = GC.value;
+        int grid = grid_for((long long)m_, TPB / G);
+        if (eq_rows_) {
+            if (has_g_)
+                dual_kernel<G, T, true, true><<<grid, TPB, 0, s>>>(D, P);
+            else
+                dual_kernel<G, T, true, false><<<grid, TPB, 0, s>>>(D, P);
+        } else {
+            if (has_g_)
+                dual_kernel<G, T, false, true><<<grid, TPB, 0, s>>>(D, P);
+            else
+                dual_kernel<G, T, false, false><<<grid, TPB, 0, s>>>(D, P);
+        }
+    });
+    stats_.kernel_launches++;
+}
+
+// BB path: A^T y, preconditioner refresh when tau changed, the cooperative
+// inner solve (which also writes x_refl and the Halpern x), then the dual step.
+void Solve::enqueue_step_bb(bool store_dual, bool want_fpe, double w)
+{
+    cudaStream_t s = st_;
+    if (opt_.time_steps) {
+        if (ev_used_ + 2 > ev_pool_.size()) {
+            for (int i = 0; i < 64; ++i) {
+                cudaEvent_t e;
+                CK(cudaEventCreate(&e));
+                ev_pool_.push_back(e);
+            }
+        }
+        CK(cudaEventRecord(ev_pool_[ev_used_++], s));
+    }
+    double tau = step_ / omega_;
+    if (nonconvexity_ < 0) {
+        tau = std::fmax(tau, -1.01 * std::fmin(0.0, nonconvexity_));
+        tau /= 100;
+    }
+    dispatch_g(GAt_, [&](auto GC) {
+        constexpr int G = GC.value;
+        spmv_kernel<G><<<grid_for(n_, TPB / G), TPB, 0, s>>>(n_, At_.rp, At_.ci, At_.v, y_, bb_aty_);
+    });
+    double inv_tau = 1.0 / tau;
+    if (bb_m_ && inv_tau != bb_cached_inv_tau_) {
+        int nb = grid_for(n_, TPB, 148 * 4);
+        bb_precond_kernel<<<nb, TPB, 0, s>>>(n_, bb_diag_h_, inv_tau, bb_m_, bb_minv_, partials_);
+        fold_partials_kernel<<<1, TPB, 0, s>>>(partials_, nb, 1, fpe_ops_d_, bb_part_);
+        bb_tol_scale_kernel<<<1, 1, 0, s>>>(bb_part_, n_, bb_tscale_);
+        bb_cached_inv_tau_ = inv_tau;
+        stats_.kernel_launches += 3;
+    }
+    BBData D = bb_data();
+    BBParams BP{tau, w, prm_.reflection_coefficient, want_fpe ? 1 : 0};
+    dispatch_rg(GQ_, [&](auto GC) {
+        dispatch_s(S_, [&](auto SC) {
+            void *args[] = {&D, &BP};
+            CK(cudaLaunchCooperativeKernel((void *)bb_kernel<GC.value, SC.value>, bb_grid_, TPB, args, 0, s));
+        });
+    });
+    StepParams P{};
+    P.tau = tau;
+    P.sigma = step_ * omega_;
+    P.w = w;
+    P.rho = prm_.reflection_coefficient;
+    P.store_primal = 1;
+    P.store_dual = store_dual;
+    P.want_fpe = want_fpe;
+    P.lp_slack = 0;
+    P.cone_box = cone_box_;
+    StepData<double> SD = step_data<double>();
+    launch_dual<double>(SD, P);
+    stats_.kernel_launches += 2;
+    stats_.step_kernel_launches++;
+    step_bytes_sum_ += step_bytes(sizeof(double), true, store_dual);
+    if (opt_.time_steps)
+        CK(cudaEventRecord(ev_pool_[ev_used_++], s));
+}
+
 void Solve::enqueue_step(bool store_primal, bool store_dual, bool want_fpe, double w)
 {
+    if (bb_) {
+        enqueue_step_bb(store_dual, want_fpe, w);
+        return;
+    }
     if (fp32_)
         enqueue_step_t<float>(store_primal, store_dual, want_fpe, w);
     else
@@ -818,22 +1128,7 @@ void Solve::enqueue_step_t(bool store_primal, bool store_dual, bool want_fpe, do
         });
         stats_.kernel_launches++;
     }
-    dispatch_g(GA_, [&](auto GC) {
-        constexpr int G = GC.value;
-        int grid = grid_for((long long)m_, TPB / G);
-        if (eq_rows_) {
-            if (has_g_)
-                dual_kernel<G, T, true, true><<<grid, TPB, 0, s>>>(D, P);
-            else
-                dual_kernel<G, T, true, false><<<grid, TPB, 0, s>>>(D, P);
-        } else {
-            if (has_g_)
-                dual_kernel<G, T, false, true><<<grid, TPB, 0, s>>>(D, P);
-            else
-                dual_kernel<G, T, false, false><<<grid, TPB, 0, s>>>(D, P);
-        }
-    });
-    stats_.kernel_launches++;
+    launch_dual<T>(D, P);
     stats_.step_kernel_launches++;
     step_bytes_sum_ += step_bytes(sizeof(T), store_primal || !cone_start_.empty(), store_dual);
     if (fp32_)
@@ -924,6 +1219,12 @@ void Solve::enqueue_residual_t(bool want_dist)
     P.l2 = prm_.optimality_norm == NORM_TYPE_L2;
     P.is_lp = qtype_ == PDHCG_NON_Q;
     P.qmode = qtype_ == PDHCG_DIAG_Q ? 1 : 0;
+    if (bb_) { // Q x_pdhg for the residual (reference update_obj_product in compute_residual)
+        if constexpr (std::is_same<VT, double>::value)
+            enqueue_q_apply(xp_, qx_res_);
+        D.qx = qx_res_;
+        P.qmode = 2;
+    }
     P.has_cones = D.n_cones > 0;
     P.want_dist = want_dist;
     P.tau = step_ / omega_;
@@ -957,6 +1258,11 @@ void Solve::enqueue_fpe(int slot)
     });
     fold_partials_kernel<<<1, TPB, 0, s>>>(part, nb, FP_COUNT, fpe_ops_d_, scal_d_ + RS_COUNT + slot * FP_COUNT);
     stats_.kernel_launches += 2;
+    if (bb_) {
+        bb_tol_update_kernel<<<1, 1, 0, s>>>(scal_d_ + RS_COUNT + slot * FP_COUNT + FP_DX2, step_, omega_, bb_min_tol_,
+                                             bb_tol_);
+        stats_.kernel_launches++;
+    }
 }
 
 // ---- mixed precision (FP32 bulk phase, then FP64 polish) ----------------
@@ -1216,7 +1522,12 @@ pdhcg_result_t *Solve::make_result()
         yo = ar_.alloc<double>(m);
         rco = ar_.alloc<double>(n);
     }
-    if (fp32_)
+    if (bb_) {
+        enqueue_q_apply(xp_, qx_res_);
+        result_kernel<double><<<grid_for((long long)n + m, TPB), TPB, 0, s>>>(
+            n, m, At_.rp, At_.ci, At_.v, c_d_, q_d_, qx_res_, 2, l_d_, u_d_, vr_d_, cr_d_, sb_, sc_, xp_, yp_, xo, yo,
+            rco);
+    } else if (fp32_)
         result_kernel<float><<<grid_for((long long)n + m, TPB), TPB, 0, s>>>(
             n, m, At_.rp, At_.ci, At_.v, c_d_, q_d_, nullptr, qtype_ == PDHCG_DIAG_Q ? 1 : 0, l_d_, u_d_, vr_d_,
             cr_d_, sb_, sc_, f_.xp, f_.yp, xo, yo, rco);
@@ -1311,10 +1622,19 @@ pdhcg_result_t *Solve::run()
     init_state();
     step_size();
     CK(cudaStreamSynchronize(st_));
-    if (opt_.precision == PDHCG_B200_MIXED)
+    bb_ = qtype_ != PDHCG_NON_Q && qtype_ != PDHCG_DIAG_Q;
+    if (bb_)
+        setup_bb();
+    if (opt_.precision == PDHCG_B200_MIXED && !bb_) // the inner BB solve runs in FP64 only
         enter_fp32();
     stats_.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_setup).count();
     loop();
+    if (bb_) {
+        int inner = 0;
+        CK(cudaMemcpyAsync(&inner, bb_inner_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+        CK(cudaStreamSynchronize(st_));
+        inner_total_ += inner;
+    }
     auto t_res = std::chrono::steady_clock::now();
     pdhcg_result_t *r = make_result();
     stats_.result_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_res).count();
@@ -1400,13 +1720,16 @@ int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cuda
 // C entry points
 // ---------------------------------------------------------------------------
 
-static volatile std::sig_atomic_t g_cancel = 0;
-
 extern "C" {
 
-int pdhcg_b200_cancel_requested(void) { return g_cancel != 0; }
+// The reference's cancellation flag (reference src/pdhcg.c:31), written by
+// its Python binding's SIGINT handler (reference
+// python_bindings/_core_bindings.cpp:41-47) and read at every evaluation.
+volatile std::sig_atomic_t g_pdhcg_cancel_request = 0;
 
-void pdhcg_b200_request_cancel(int on) { g_cancel = on ? 1 : 0; }
+int pdhcg_b200_cancel_requested(void) { return g_pdhcg_cancel_request != 0; }
+
+void pdhcg_b200_request_cancel(int on) { g_pdhcg_cancel_request = on ? 1 : 0; }
 
 void pdhcg_b200_default_options(pdhcg_b200_options_t *o)
 {

@@ -150,3 +150,63 @@ def conic_lp(seed: int = 5, nfree: int = 60, nsoc: int = 10, soc_len: int = 12, 
         q = rng.uniform(0.1, 1.0, n)
         p.Q = CsrMatrix(n, n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), q)
     return p
+
+
+def portfolio(seed: int = 3, scale: float = 1.0, rank: int = 100, sectors: int = 500) -> Problem:
+    """Low-rank portfolio QP with a rotated-SOC tracking-error block.
+
+    Variables: weights x (n assets), factor exposures z (rank), s, t.
+    Objective 1/2 x'(R'DR + Q)x - mu'x with R rank x n dense N(0, 1/sqrt(n))
+    (passed as a dense matrix), D = diag U(0.5, 2), Q = diag U(1e-4, 1e-2).
+    Rows: budget sum x = 1; one row per sector with upper bound 0.05; the
+    exposure rows z - diag(sqrt D) R x = 0; s = TE^2 / 2 and t = 1.
+    Cone: [z, s, t] in the rotated SOC, i.e. |sqrt(D) R x|^2 <= TE^2.
+    Box: 0 <= x <= 0.02; z, s, t free (cone slots).
+    """
+    rng = np.random.default_rng(seed)
+    n = max(100, int(200000 * scale))
+    k = rank if scale >= 0.05 else max(4, int(rank * scale * 20))
+    nsec = max(2, min(sectors, n // 20))
+    R = rng.standard_normal((k, n)) / np.sqrt(n)
+    Dd = rng.uniform(0.5, 2.0, k)
+    qd = rng.uniform(1e-4, 1e-2, n)
+    mu = rng.uniform(0.0, 1e-3, n)
+    N = n + k + 2
+    sec = rng.integers(0, nsec, n)
+    x0 = np.full(n, 1.0 / n)
+    z0 = np.sqrt(Dd) * (R @ x0)
+    te2 = 1.5 * float(z0 @ z0) + 1e-8
+    rows, cols, vals = [], [], []
+    # budget
+    rows.append(np.zeros(n, np.int64)); cols.append(np.arange(n)); vals.append(np.ones(n))
+    # sectors
+    rows.append(1 + sec); cols.append(np.arange(n)); vals.append(np.ones(n))
+    # exposures: z_r - sqrt(D_r) R_r x = 0
+    base = 1 + nsec
+    rr = np.repeat(np.arange(k), n)
+    rows.append(base + rr); cols.append(np.tile(np.arange(n), k)); vals.append((-np.sqrt(Dd)[:, None] * R).ravel())
+    rows.append(base + np.arange(k)); cols.append(n + np.arange(k)); vals.append(np.ones(k))
+    # s and t
+    rows.append(np.array([base + k, base + k + 1])); cols.append(np.array([n + k, n + k + 1])); vals.append(np.ones(2))
+    m = base + k + 2
+    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(m, N))
+    A.sort_indices()
+    lo = np.full(m, -np.inf)
+    up = np.full(m, np.inf)
+    lo[0] = up[0] = 1.0
+    up[1:base] = 0.05
+    lo[base:base + k] = up[base:base + k] = 0.0
+    lo[base + k] = up[base + k] = 0.5 * te2
+    lo[base + k + 1] = up[base + k + 1] = 1.0
+    lb = np.concatenate([np.zeros(n), np.full(k + 2, -np.inf)])
+    ub = np.concatenate([np.full(n, 0.02), np.full(k + 2, np.inf)])
+    c = np.concatenate([-mu, np.zeros(k + 2)])
+    Qd = np.concatenate([qd, np.zeros(k + 2)])
+    qidx = np.arange(n)
+    Q = CsrMatrix(N, N, np.concatenate([np.arange(n + 1), np.full(k + 2, n)]).astype(np.int32),
+                  qidx.astype(np.int32), qd)
+    Rfull = np.zeros((k, N))
+    Rfull[:, :n] = R
+    Dm = CsrMatrix(k, k, np.arange(k + 1, dtype=np.int32), np.arange(k, dtype=np.int32), Dd)
+    return Problem(c=c, A=CsrMatrix.from_scipy(A), con_lb=lo, con_ub=up, var_lb=lb, var_ub=ub, Q=Q,
+                   R_dense=Rfull, D=Dm, cones=[Cone(CONE_ROTATED_SOC, n, k)])

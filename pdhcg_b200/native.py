@@ -58,7 +58,7 @@ EXPORTS = [
     # additive entry points (include/pdhcg_b200.h)
     "pdhcg_b200_default_options", "pdhcg_b200_solve", "pdhcg_b200_last_stats", "pdhcg_b200_csr_spmv",
     "pdhcg_b200_project_cones", "pdhcg_b200_pdhg_step", "pdhcg_b200_upload", "pdhcg_b200_solve_device",
-    "pdhcg_b200_device_solution", "pdhcg_b200_device_problem_free",
+    "pdhcg_b200_device_solution", "pdhcg_b200_device_problem_free", "pdhcg_b200_request_cancel",
 ]
 
 
@@ -100,6 +100,8 @@ def load(build: bool = True) -> C.CDLL:
     lib.pdhcg_b200_device_solution.argtypes = [C.c_void_p, P(C.c_void_p), P(C.c_void_p), P(C.c_void_p)]
     lib.pdhcg_b200_device_problem_free.restype = None
     lib.pdhcg_b200_device_problem_free.argtypes = [C.c_void_p]
+    lib.pdhcg_b200_request_cancel.restype = None
+    lib.pdhcg_b200_request_cancel.argtypes = [C.c_int]
     _LIB = lib
     return lib
 

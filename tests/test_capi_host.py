@@ -32,6 +32,19 @@ def test_library_exports_every_declared_symbol(lib):
         assert name in declared, name
 
 
+def test_cancel_flag_is_the_reference_symbol(lib):
+    """The reference's Python binding declares g_pdhcg_cancel_request extern
+    (reference python_bindings/_core_bindings.cpp:41) and writes it; the
+    library must export that data symbol, and pdhcg_b200_request_cancel
+    writes the same word."""
+    flag = C.c_int.in_dll(lib, "g_pdhcg_cancel_request")
+    assert flag.value == 0
+    lib.pdhcg_b200_request_cancel(1)
+    assert flag.value == 1
+    lib.pdhcg_b200_request_cancel(0)
+    assert flag.value == 0
+
+
 def _problem_fields(P):
     p = P.contents
     n, m = p.num_variables, p.num_constraints

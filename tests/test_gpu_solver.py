@@ -42,7 +42,7 @@ def _solve_oracle(oracle, lib, p, params):
     return d
 
 
-@pytest.mark.parametrize("name", sorted(n for n in KNOWN_ANSWERS if n != "sparse_q_soc"))
+@pytest.mark.parametrize("name", sorted(KNOWN_ANSWERS))
 def test_known_answers_on_gpu(lib, name):
     p, prm, expect = KNOWN_ANSWERS[name]()
     res = _solve_gpu(lib, p, prm)
@@ -59,6 +59,10 @@ CASES = {
                       "termination_criteria.eps_feasible_relative": 1e-6}),
     "diag_qp_l2": (lambda: instances.diag_qp(seed=9), {"optimality_norm": capi.NORM_L2}),
     "box_lp_no_bound_obj": (lambda: instances.box_lp(seed=8), {"bound_objective_rescaling": False}),
+    # inner BB solve: sparse Q, and low rank + diagonal Q with a rotated-SOC block
+    "sparse_qp_small": (lambda: instances.sparse_qp(scale=0.05), {}),
+    "sparse_qp_no_precond": (lambda: instances.sparse_qp(seed=7, scale=0.03), {"diag_jacobi_precond": False}),
+    "portfolio_small": (lambda: instances.portfolio(scale=0.01), {}),
 }
 
 
