@@ -92,6 +92,13 @@ int pdhcg_b200_last_stats(pdhcg_b200_stats_t *out);
 extern volatile sig_atomic_t g_pdhcg_cancel_request;
 void pdhcg_b200_request_cancel(int on);
 
+/* Length of cone block `block` (3 for EXP/POW, v_dim + 2 for SOC/RSOC,
+ * v_dim (v_dim + 1) / 2 for PSD), -1 for an invalid block.  Same name and
+ * meaning as the reference's cone_block_length (reference
+ * internal/cone_utils.h:27, src/cone_utils.c:40-45), which its Python binding
+ * calls. */
+int cone_block_length(const cone_blocks_t *blocks, int block);
+
 /* ---- kernel-level entry points on device pointers ------------------------
  * For parity tests and embedding.  Pointers are device memory of the current
  * device; stream may be NULL (legacy default stream).  They return after

@@ -352,7 +352,9 @@ int pdhcg_b200_cone_length(cone_type_t type, int v_dim)
     return -1;
 }
 
-static int block_len(const cone_blocks_t *b, int i)
+// Length of cone block i (reference cone_block_length, src/cone_utils.c:40-45);
+// exported under the reference's name because its Python binding calls it.
+extern "C" int cone_block_length(const cone_blocks_t *b, int i)
 {
     if (!b || i < 0 || i >= b->num_cones || !b->type || !b->v_dim)
         return -1;
@@ -689,7 +691,7 @@ qp_problem_t *create_qp_problem(const double *objective_c, const matrix_desc_t *
     {
         int covered = 0;
         for (int c = 0; c < num_affine_cones; ++c) {
-            covered += block_len(&prob->affine_cones, c);
+            covered += cone_block_length(&prob->affine_cones, c);
             prob->affine_cones.start_idx[c] += m;
         }
         if (covered != p) {
@@ -705,7 +707,7 @@ qp_problem_t *create_qp_problem(const double *objective_c, const matrix_desc_t *
         // cone slots must be free (reference src/pdhcg.c:468-503)
         int n_orig = n;
         for (int c = 0; c < prob->cones.num_cones; ++c) {
-            int st = prob->cones.start_idx[c], len = block_len(&prob->cones, c);
+            int st = prob->cones.start_idx[c], len = cone_block_length(&prob->cones, c);
             for (int v = st; v < st + len; ++v) {
                 double lo = prob->variable_lower_bound[v], hi = prob->variable_upper_bound[v];
                 bool lo_fin = std::isfinite(lo) && lo > -1e30, hi_fin = std::isfinite(hi) && hi < 1e30;
@@ -780,7 +782,7 @@ int set_cone_fixed(qp_problem_t *prob, int cone_idx, int slot, double value)
         std::fprintf(stderr, "[set_cone_fixed] fixed PSD cone sections are not supported.\n");
         return -1;
     }
-    int len = block_len(&prob->cones, cone_idx);
+    int len = cone_block_length(&prob->cones, cone_idx);
     if (slot < 0 || slot >= len) {
         std::fprintf(stderr, "[set_cone_fixed] slot %d out of range [0, %d) for cone %d\n", slot, len, cone_idx);
         return -1;

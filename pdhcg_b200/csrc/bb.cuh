@@ -166,17 +166,19 @@ __device__ void bb_drx_smem(const BBData &D, double *drx)
     __syncthreads();
 }
 
-// qx_j for one variable, G lanes: Q row j . v + R^T row j . drx
+// qx_j for one variable, G lanes: Q row j . v + R^T row j . drx.  Every
+// lane of the warp calls it; ok == false gives 0 without reading a row.
 template <int G>
-__device__ __forceinline__ double bb_q_row(const BBData &D, const double *v, const double *drx, int j, int sub)
+__device__ __forceinline__ double bb_q_row(const BBData &D, const double *v, const double *drx, int j, int sub,
+                                           bool ok)
 {
     double s = 0.0;
-    if (D.sparse) {
+    if (ok && D.sparse) {
         int b = D.Q_rp[j], e = D.Q_rp[j + 1];
         for (int t = b + sub; t < e; t += G)
             s += D.Q_v[t] * v[D.Q_ci[t]];
     }
-    if (D.k > 0) {
+    if (ok && D.k > 0) {
         int b = D.Rt_rp[j], e = D.Rt_rp[j + 1];
         for (int t = b + sub; t < e; t += G)
             s += D.Rt_v[t] * drx[D.Rt_ci[t]];
@@ -337,7 +339,7 @@ __device__ double bb_grad_phase(const BBData &D, const double *drx, double inv_t
     for (int base = gwarp * per; base < D.n; base += nwarps * per) {
         int j = base + lane / G;
         bool ok = j < D.n;
-        double q = bb_q_row<G>(D, D.xp, drx, ok ? j : 0, ok ? sub : G);
+        double q = bb_q_row<G>(D, D.xp, drx, ok ? j : 0, sub, ok);
         if (ok && sub == 0) {
             double gn = q + D.c[j] - D.aty[j] + inv_tau * (D.xp[j] - D.x[j]);
             double pb = gn - D.grad[j];
@@ -499,7 +501,7 @@ __global__ void __launch_bounds__(TPB) q_apply_kernel(BBData D, const double *v,
     for (int base = gwarp * per; base < D.n; base += nwarps * per) {
         int j = base + lane / G;
         bool ok = j < D.n;
-        double q = bb_q_row<G>(D, v, drx, ok ? j : 0, ok ? sub : G);
+        double q = bb_q_row<G>(D, v, drx, ok ? j : 0, sub, ok);
         if (ok && sub == 0)
             qx[j] = q;
     }

@@ -42,12 +42,36 @@ __device__ __forceinline__ double group_sum(double v)
     return v;
 }
 
-// sum_k val[k] * x[col[k]] over row r, G lanes cooperating (lane = lane in group).
+// Row-group loops.  A warp holds 32/G row groups of G lanes, and group_sum
+// shuffles over the full warp, so every lane of a warp must run the same
+// number of passes: the loop runs over the warp's first row `base`
+// (uniform across the warp), each group takes row base + lane / G, and a
+// group past the end computes an empty row (ok == false).
+//   for (int base = warp_row0<G>(); base < rows; base += warp_row_stride<G>()) {
+//       int r = base + (threadIdx.x & 31) / G; bool ok = r < rows;
+//       double a = row_dot<G>(rp, ci, val, x, r, sub, ok); ... }
+template <int G>
+__device__ __forceinline__ int warp_row0(int block = -1)
+{
+    const int b = block < 0 ? (int)blockIdx.x : block;
+    return b * (int)(blockDim.x / G) + (int)(threadIdx.x >> 5) * (32 / G);
+}
+
+template <int G>
+__device__ __forceinline__ int warp_row_stride(int blocks = -1)
+{
+    return (blocks < 0 ? (int)gridDim.x : blocks) * (int)(blockDim.x / G);
+}
+
+// sum_k val[k] * x[col[k]] over row r, G lanes cooperating (lane = lane in
+// group); every lane of the warp must call it, ok == false gives 0 without
+// reading the row.
 template <int G, typename V>
 __device__ __forceinline__ double row_dot(const int *__restrict__ rp, const int *__restrict__ ci,
-                                          const V *__restrict__ val, const double *__restrict__ x, int r, int lane)
+                                          const V *__restrict__ val, const double *__restrict__ x, int r, int lane,
+                                          bool ok = true)
 {
-    int b = __ldg(rp + r), e = __ldg(rp + r + 1);
+    int b = ok ? __ldg(rp + r) : 0, e = ok ? __ldg(rp + r + 1) : 0;
     double s = 0.0;
     for (int k = b + lane; k < e; k += G)
         s += (double)__ldg(val + k) * __ldg(x + __ldg(ci + k));
@@ -57,9 +81,10 @@ __device__ __forceinline__ double row_dot(const int *__restrict__ rp, const int 
 // Same with the vector held in FP32.
 template <int G, typename V>
 __device__ __forceinline__ double row_dot(const int *__restrict__ rp, const int *__restrict__ ci,
-                                          const V *__restrict__ val, const float *__restrict__ x, int r, int lane)
+                                          const V *__restrict__ val, const float *__restrict__ x, int r, int lane,
+                                          bool ok = true)
 {
-    int b = __ldg(rp + r), e = __ldg(rp + r + 1);
+    int b = ok ? __ldg(rp + r) : 0, e = ok ? __ldg(rp + r + 1) : 0;
     double s = 0.0;
     for (int k = b + lane; k < e; k += G)
         s += (double)__ldg(val + k) * (double)__ldg(x + __ldg(ci + k));

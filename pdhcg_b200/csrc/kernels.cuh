@@ -65,13 +65,14 @@ struct StepData {
 template <int G, typename T, bool HAS_Q, bool HAS_BOX>
 __global__ void __launch_bounds__(TPB) primal_free_kernel(StepData<T> D, StepParams P)
 {
-    const int groups_per_block = TPB / G;
     const int lane = threadIdx.x % G;
     const int nrows = D.free_idx ? D.n_free : D.n;
-    for (int r = blockIdx.x * groups_per_block + threadIdx.x / G; r < nrows; r += gridDim.x * groups_per_block) {
-        const int j = D.free_idx ? D.free_idx[r] : r;
-        double aty = row_dot<G>(D.At_rp, D.At_ci, D.At_v, D.y, j, lane);
-        if (lane == 0) {
+    for (int base = warp_row0<G>(); base < nrows; base += warp_row_stride<G>()) {
+        const int r = base + (threadIdx.x & 31) / G;
+        const bool ok = r < nrows;
+        const int j = ok ? (D.free_idx ? D.free_idx[r] : r) : 0;
+        double aty = row_dot<G>(D.At_rp, D.At_ci, D.At_v, D.y, j, lane, ok);
+        if (ok && lane == 0) {
             double xi = D.x[j];
             double t = xi - P.tau * ((double)D.c[j] - aty);
             if (HAS_Q)
@@ -186,11 +187,12 @@ __global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<T> D, StepPar
 template <int G, typename T, bool EQ_ROWS, bool HAS_G>
 __global__ void __launch_bounds__(TPB) dual_kernel(StepData<T> D, StepParams P)
 {
-    const int groups_per_block = TPB / G;
     const int lane = threadIdx.x % G;
-    for (int i = blockIdx.x * groups_per_block + threadIdx.x / G; i < D.m; i += gridDim.x * groups_per_block) {
-        double ax = row_dot<G>(D.A_rp, D.A_ci, D.A_v, D.xr, i, lane);
-        if (lane == 0) {
+    for (int base = warp_row0<G>(); base < D.m; base += warp_row_stride<G>()) {
+        const int i = base + (threadIdx.x & 31) / G;
+        const bool ok = i < D.m;
+        double ax = row_dot<G>(D.A_rp, D.A_ci, D.A_v, D.xr, i, lane, ok);
+        if (ok && lane == 0) {
             double v = HAS_G ? ax + (double)D.g[i] : ax;
             double yi = D.y[i];
             double pr;
@@ -267,10 +269,12 @@ template <int G>
 __global__ void __launch_bounds__(TPB) spmv_kernel(int rows, const int *rp, const int *ci, const double *v,
                                                    const double *x, double *y)
 {
-    const int gpb = TPB / G, lane = threadIdx.x % G;
-    for (int r = blockIdx.x * gpb + threadIdx.x / G; r < rows; r += gridDim.x * gpb) {
-        double a = row_dot<G>(rp, ci, v, x, r, lane);
-        if (lane == 0)
+    const int lane = threadIdx.x % G;
+    for (int base = warp_row0<G>(); base < rows; base += warp_row_stride<G>()) {
+        const int r = base + (threadIdx.x & 31) / G;
+        const bool ok = r < rows;
+        double a = row_dot<G>(rp, ci, v, x, r, lane, ok);
+        if (ok && lane == 0)
             y[r] = a;
     }
 }

@@ -75,10 +75,12 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
 
     int b = blockIdx.x;
     if (b < D.rows_blocks) {
-        const int gpb = TPB / G, lane = threadIdx.x % G;
-        for (int i = b * gpb + threadIdx.x / G; i < D.m; i += D.rows_blocks * gpb) {
-            double ax = row_dot<G>(D.A_rp, D.A_ci, D.A_v, D.xp, i, lane);
-            if (lane == 0) {
+        const int lane = threadIdx.x % G;
+        for (int base = warp_row0<G>(b); base < D.m; base += warp_row_stride<G>(D.rows_blocks)) {
+            const int i = base + (threadIdx.x & 31) / G;
+            const bool ok = i < D.m;
+            double ax = row_dot<G>(D.A_rp, D.A_ci, D.A_v, D.xp, i, lane, ok);
+            if (ok && lane == 0) {
                 double v = ax + D.g[i];
                 double proj = clampd(D.lc[i], v, D.uc[i]);
                 fold(RS_PRIMAL_RES, norm_term((v - proj) * D.cr[i], P.l2));
@@ -93,12 +95,14 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
         }
     } else if (b < D.rows_blocks + D.free_blocks) {
         b -= D.rows_blocks;
-        const int gpb = TPB / G, lane = threadIdx.x % G;
+        const int lane = threadIdx.x % G;
         const int nrows = D.free_idx ? D.n_free : D.n;
-        for (int r = b * gpb + threadIdx.x / G; r < nrows; r += D.free_blocks * gpb) {
-            const int j = D.free_idx ? D.free_idx[r] : r;
-            double aty = row_dot<G>(D.At_rp, D.At_ci, D.At_v, D.yp, j, lane);
-            if (lane == 0) {
+        for (int base = warp_row0<G>(b); base < nrows; base += warp_row_stride<G>(D.free_blocks)) {
+            const int r = base + (threadIdx.x & 31) / G;
+            const bool ok = r < nrows;
+            const int j = ok ? (D.free_idx ? D.free_idx[r] : r) : 0;
+            double aty = row_dot<G>(D.At_rp, D.At_ci, D.At_v, D.yp, j, lane, ok);
+            if (ok && lane == 0) {
                 double x = D.xp[j];
                 double qx = P.qmode == 1 ? D.q[j] * x : (P.qmode == 2 ? D.qx[j] : 0.0);
                 double dr, ds;
@@ -214,10 +218,12 @@ __global__ void __launch_bounds__(TPB) fpe_kernel(int n, int m, const int *At_rp
     double acc[FP_COUNT] = {0.0, 0.0, 0.0};
     int b = blockIdx.x;
     if (b < col_blocks) {
-        const int gpb = TPB / G, lane = threadIdx.x % G;
-        for (int j = b * gpb + threadIdx.x / G; j < n; j += col_blocks * gpb) {
-            double a = row_dot<G>(At_rp, At_ci, At_v, dy, j, lane);
-            if (lane == 0) {
+        const int lane = threadIdx.x % G;
+        for (int base = warp_row0<G>(b); base < n; base += warp_row_stride<G>(col_blocks)) {
+            const int j = base + (threadIdx.x & 31) / G;
+            const bool ok = j < n;
+            double a = row_dot<G>(At_rp, At_ci, At_v, dy, j, lane, ok);
+            if (ok && lane == 0) {
                 double d = dx[j];
                 acc[FP_DX2] += d * d;
                 acc[FP_CROSS] += a * d;

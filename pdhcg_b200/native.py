@@ -59,6 +59,7 @@ EXPORTS = [
     "pdhcg_b200_default_options", "pdhcg_b200_solve", "pdhcg_b200_last_stats", "pdhcg_b200_csr_spmv",
     "pdhcg_b200_project_cones", "pdhcg_b200_pdhg_step", "pdhcg_b200_upload", "pdhcg_b200_solve_device",
     "pdhcg_b200_device_solution", "pdhcg_b200_device_problem_free", "pdhcg_b200_request_cancel",
+    "cone_block_length",
 ]
 
 

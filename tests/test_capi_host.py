@@ -45,6 +45,25 @@ def test_cancel_flag_is_the_reference_symbol(lib):
     assert flag.value == 0
 
 
+def test_cone_block_length_matches_reference_rule(lib):
+    """cone_block_length (reference src/cone_utils.c:26-45): 3 for EXP/POW,
+    v_dim + 2 for (R)SOC, the triangle of v_dim for PSD, -1 when invalid."""
+    types = np.array([capi.CONE_EXPONENTIAL, capi.CONE_POWER, capi.CONE_STANDARD_SOC,
+                      capi.CONE_ROTATED_SOC, capi.CONE_PSD, capi.CONE_PSD, capi.CONE_STANDARD_SOC], dtype=np.int32)
+    vdim = np.array([1, 1, 5, 0, 4, 0, -1], dtype=np.int32)
+    blk = capi.ConeBlocks()
+    blk.num_cones = len(types)
+    blk.type = types.ctypes.data_as(C.POINTER(C.c_int))
+    blk.v_dim = vdim.ctypes.data_as(C.POINTER(C.c_int))
+    fn = lib.cone_block_length
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(capi.ConeBlocks), C.c_int]
+    got = [fn(C.byref(blk), i) for i in range(len(types))]
+    assert got == [3, 3, 7, 2, 10, -1, -1]
+    assert fn(C.byref(blk), -1) == -1 and fn(C.byref(blk), len(types)) == -1
+    assert fn(None, 0) == -1
+
+
 def _problem_fields(P):
     p = P.contents
     n, m = p.num_variables, p.num_constraints
