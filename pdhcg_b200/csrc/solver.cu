@@ -1903,12 +1903,24 @@ int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *co
         return -1;
     cone_len_kernel<<<grid_for(num_cones, TPB), TPB, 0, s>>>(num_cones, cone_vdim, cone_type, len);
     int maxlen = 0;
+    bool types_ok = true;
     {
-        std::vector<int> h(num_cones);
+        std::vector<int> h(num_cones), t(num_cones);
         cudaMemcpyAsync(h.data(), len, num_cones * sizeof(int), cudaMemcpyDeviceToHost, s);
-        cudaStreamSynchronize(s);
-        for (int v : h)
-            maxlen = std::max(maxlen, v);
+        cudaMemcpyAsync(t.data(), cone_type, num_cones * sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) {
+            cudaFreeAsync(len, s);
+            return -1;
+        }
+        for (int i = 0; i < num_cones; ++i) {
+            maxlen = std::max(maxlen, h[i]);
+            types_ok = types_ok && (t[i] == CONE_STANDARD_SOC || t[i] == CONE_ROTATED_SOC);
+        }
+    }
+    if (!types_ok) { // the exponential, power and PSD projections are not built
+        std::fprintf(stderr, "[pdhcg_b200_project_cones] only SOC and rotated-SOC blocks are supported.\n");
+        cudaFreeAsync(len, s);
+        return -3;
     }
     int S = slots_class(maxlen);
     if (S < 0) {

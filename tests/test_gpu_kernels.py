@@ -76,6 +76,21 @@ def test_cone_projection_matches_oracle(lib, oracle, weighted, uniform_d):
     np.testing.assert_allclose(got, expect, rtol=tol, atol=tol * np.abs(expect).max())
 
 
+def test_cone_projection_rejects_unbuilt_cone_types(lib):
+    """An exponential block is refused (-3) and x is left untouched."""
+    import torch
+    x = np.arange(8, dtype=np.float64)
+    xd = _dev(x)
+    starts, vdims = _dev([0, 3], np.int32), _dev([1, 3], np.int32)
+    types = _dev([capi.CONE_STANDARD_SOC, capi.CONE_EXPONENTIAL], np.int32)
+    d = _dev(np.ones(8))
+    rc = lib.pdhcg_b200_project_cones(2, _ptr(starts), _ptr(vdims), _ptr(types), None, _ptr(xd), _ptr(d), None,
+                                      1.0, None)
+    torch.cuda.synchronize()
+    assert rc == -3
+    np.testing.assert_array_equal(xd.cpu().numpy(), x)
+
+
 @pytest.mark.parametrize("with_q,with_cones", [(False, False), (True, False), (False, True), (True, True)])
 def test_fused_step_matches_oracle(lib, oracle, with_q, with_cones):
     import torch

@@ -152,7 +152,7 @@ def test_device_resident_handle_matches_host_path(lib):
 
     class _DeviceArray:  # wraps the library's device pointer for torch
         def __init__(self, ptr, n):
-            self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, True), "version": 2}
+            self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 2}
 
     xt = torch.as_tensor(_DeviceArray(xp.value, p.n), device="cuda")
     np.testing.assert_allclose(xt.cpu().numpy(), host["x"], rtol=1e-12, atol=1e-12)
