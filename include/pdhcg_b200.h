@@ -119,6 +119,28 @@ int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *co
                              const double *cone_alpha, double *x, const double *d, const double *q, double tau,
                              void *stream);
 
+/* pdhcg_b200_project_cones for callers that must not allocate device memory
+ * (no cudaMalloc / cudaMallocAsync / cudaFree, no allocating library): e.g.
+ * code whose memory is budgeted up front, or that runs while another
+ * component owns the allocator.  No counterpart in the reference.
+ * Same arguments, results and error codes as pdhcg_b200_project_cones, plus
+ * -4 when num_cones > PDHCG_B200_NOALLOC_MAX_CONES (nothing is launched).
+ * Its scratch is one file-scope device array per device
+ * ((PDHCG_B200_NOALLOC_MAX_CONES + 2) ints); every call writes it before
+ * reading it, so nothing needs to start at zero.
+ * - The first call on each device looks up that array's address
+ *   (cudaGetSymbolAddress with the device current); make that first call
+ *   before any stream capture.
+ * - Calls on the same device share the scratch: two calls that overlap in
+ *   time (other threads, or other streams before the first has finished)
+ *   race.  Serialise them.
+ * - Like pdhcg_b200_project_cones it waits for the stream (it reads the
+ *   longest block length back to the host). */
+#define PDHCG_B200_NOALLOC_MAX_CONES 65536
+int pdhcg_b200_project_cones_noalloc(int num_cones, const int *cone_start, const int *cone_vdim,
+                                     const int *cone_type, const double *cone_alpha, double *x, const double *d,
+                                     const double *q, double tau, void *stream);
+
 /* One restarted-Halpern PDHG step (primal prox with diagonal Q or none, cone
  * projection, dual prox, reflection, Halpern averaging) on device arrays;
  * the layout mirrors oracle_step_t of the oracle.  Sizes: n variables, m rows. */

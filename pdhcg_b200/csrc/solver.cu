@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -1714,6 +1715,65 @@ int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cuda
     return 0;
 }
 
+// ---- scratch of pdhcg_b200_project_cones_noalloc ---------------------------
+// A file-scope device array replaces the stream-ordered temporary of
+// pdhcg_b200_project_cones: [0, nc) the block lengths, then the longest
+// length and a flag for a cone type without a projection.  Every call
+// writes all of them before reading any, so nothing has to start at zero.
+constexpr int NOALLOC_MAX_CONES = PDHCG_B200_NOALLOC_MAX_CONES;
+static __device__ __align__(256) int g_noalloc_scratch[NOALLOC_MAX_CONES + 2];
+
+__global__ void __launch_bounds__(TPB) noalloc_len_kernel(int nc, const int *vdim, const int *type, int *scratch)
+{
+    __shared__ int sh_max[TPB], sh_bad[TPB];
+    int mx = 0, bad = 0;
+    for (int b = threadIdx.x; b < nc; b += TPB) {
+        const int t = type[b], v = vdim[b];
+        const int len = (t == 2 || t == 3) ? 3 : (t == 4 ? v * (v + 1) / 2 : v + 2);
+        scratch[b] = len;
+        mx = max(mx, len);
+        bad |= (t != CONE_STANDARD_SOC && t != CONE_ROTATED_SOC);
+    }
+    sh_max[threadIdx.x] = mx;
+    sh_bad[threadIdx.x] = bad;
+    __syncthreads();
+    for (int o = TPB / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sh_max[threadIdx.x] = max(sh_max[threadIdx.x], sh_max[threadIdx.x + o]);
+            sh_bad[threadIdx.x] |= sh_bad[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        scratch[NOALLOC_MAX_CONES] = sh_max[0];
+        scratch[NOALLOC_MAX_CONES + 1] = sh_bad[0];
+    }
+}
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device (cudaGetSymbolAddress with that device current) and cached.
+int *noalloc_scratch()
+{
+    constexpr int MAX_DEVICES = 64;
+    static std::mutex mu;
+    static int *addr[MAX_DEVICES] = {};
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES)
+        return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            std::fprintf(stderr, "[pdhcg_b200_project_cones_noalloc] cudaGetSymbolAddress: %s\n",
+                         cudaGetErrorString(e));
+            return nullptr;
+        }
+        addr[dev] = (int *)p;
+    }
+    return addr[dev];
+}
+
 } // namespace
 
 // ---------------------------------------------------------------------------
@@ -1932,6 +1992,43 @@ int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *co
                                                                                  cone_type, x, d, q, tau);
     });
     cudaFreeAsync(len, s);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int pdhcg_b200_project_cones_noalloc(int num_cones, const int *cone_start, const int *cone_vdim,
+                                     const int *cone_type, const double *cone_alpha, double *x, const double *d,
+                                     const double *q, double tau, void *stream)
+{
+    (void)cone_alpha;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (num_cones <= 0)
+        return 0;
+    if (num_cones > NOALLOC_MAX_CONES) {
+        std::fprintf(stderr,
+                     "[pdhcg_b200_project_cones_noalloc] %d cone blocks exceed the limit of %d "
+                     "(use pdhcg_b200_project_cones)\n",
+                     num_cones, NOALLOC_MAX_CONES);
+        return -4;
+    }
+    int *scratch = noalloc_scratch();
+    if (!scratch)
+        return -1;
+    noalloc_len_kernel<<<1, TPB, 0, s>>>(num_cones, cone_vdim, cone_type, scratch);
+    int info[2] = {0, 0}; // longest block, unsupported-type flag
+    if (cudaMemcpyAsync(info, scratch + NOALLOC_MAX_CONES, sizeof(info), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return -1;
+    if (info[1]) {
+        std::fprintf(stderr, "[pdhcg_b200_project_cones_noalloc] only SOC and rotated-SOC blocks are supported.\n");
+        return -3;
+    }
+    int S = slots_class(info[0]);
+    if (S < 0)
+        return -2;
+    dispatch_s(S, [&](auto SC) {
+        project_cones_kernel<SC.value><<<grid_for(num_cones, WARPS), TPB, 0, s>>>(num_cones, cone_start, scratch,
+                                                                                 cone_type, x, d, q, tau);
+    });
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -59,7 +59,7 @@ EXPORTS = [
     "pdhcg_b200_default_options", "pdhcg_b200_solve", "pdhcg_b200_last_stats", "pdhcg_b200_csr_spmv",
     "pdhcg_b200_project_cones", "pdhcg_b200_pdhg_step", "pdhcg_b200_upload", "pdhcg_b200_solve_device",
     "pdhcg_b200_device_solution", "pdhcg_b200_device_problem_free", "pdhcg_b200_request_cancel",
-    "cone_block_length",
+    "cone_block_length", "pdhcg_b200_project_cones_noalloc",
 ]
 
 
@@ -91,6 +91,8 @@ def load(build: bool = True) -> C.CDLL:
     lib.pdhcg_b200_project_cones.restype = C.c_int
     lib.pdhcg_b200_project_cones.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
+    lib.pdhcg_b200_project_cones_noalloc.restype = C.c_int
+    lib.pdhcg_b200_project_cones_noalloc.argtypes = lib.pdhcg_b200_project_cones.argtypes
     lib.pdhcg_b200_pdhg_step.restype = C.c_int
     lib.pdhcg_b200_pdhg_step.argtypes = [P(StepArgs), C.c_void_p]
     lib.pdhcg_b200_upload.restype = C.c_void_p
