@@ -1,6 +1,6 @@
 // device.cuh -- device building blocks of the PDHCG-B200 kernels:
-// warp/block reductions, CSR row dot products with a configurable number
-// of lanes per row, and warp-cooperative weighted cone projections.
+// warp/block reductions, CSR row products (stream mode for the hot kernels,
+// row groups for set-up), and warp-cooperative weighted cone projections.
 #pragma once
 
 #include <cfloat>
@@ -42,27 +42,6 @@ __device__ __forceinline__ double group_sum(double v)
     return v;
 }
 
-// Row-group loops.  A warp holds 32/G row groups of G lanes, and group_sum
-// shuffles over the full warp, so every lane of a warp must run the same
-// number of passes: the loop runs over the warp's first row `base`
-// (uniform across the warp), each group takes row base + lane / G, and a
-// group past the end computes an empty row (ok == false).
-//   for (int base = warp_row0<G>(); base < rows; base += warp_row_stride<G>()) {
-//       int r = base + (threadIdx.x & 31) / G; bool ok = r < rows;
-//       double a = row_dot<G>(rp, ci, val, x, r, sub, ok); ... }
-template <int G>
-__device__ __forceinline__ int warp_row0(int block = -1)
-{
-    const int b = block < 0 ? (int)blockIdx.x : block;
-    return b * (int)(blockDim.x / G) + (int)(threadIdx.x >> 5) * (32 / G);
-}
-
-template <int G>
-__device__ __forceinline__ int warp_row_stride(int blocks = -1)
-{
-    return (blocks < 0 ? (int)gridDim.x : blocks) * (int)(blockDim.x / G);
-}
-
 // sum_k val[k] * x[col[k]] over row r, G lanes cooperating (lane = lane in
 // group); every lane of the warp must call it, ok == false gives 0 without
 // reading the row.
@@ -91,16 +70,121 @@ __device__ __forceinline__ double row_dot(const int *__restrict__ rp, const int 
     return group_sum<G>(s);
 }
 
-// Entries [b, e) of one row, G lanes cooperating; every lane of the warp
-// must call it (the group reduction shuffles over the full warp).
-template <int G, typename V, typename X>
-__device__ __forceinline__ double range_dot(const int *__restrict__ ci, const V *__restrict__ val,
-                                            const X *__restrict__ x, int b, int e, int lane)
+// ---------------------------------------------------------------------------
+// Stream-mode CSR products for the hot step kernels.
+//
+// A warp owns up to 32 * S consecutive rows [r0, r0 + nr); lane l owns rows
+// r0 + l + 32 s.  Their entries are one contiguous range [rp[r0], rp[r0+nr])
+// of the CSR arrays, so the warp streams that range in chunks of
+// STREAM_CHUNK entries: every lane issues STREAM_U independent coalesced
+// loads of (col, val), then STREAM_U gathers of x, and stores the products in
+// a per-warp shared buffer; each lane then adds the products of its own rows
+// in entry order (the same order as a sequential row loop).
+//
+// A row longer than STREAM_ROW_MAX would leave one lane adding alone while
+// the warp waits, so a warp whose rows include such a row reduces its rows
+// one at a time across all 32 lanes instead (warp_sum; a different but
+// fixed summation order).
+// ---------------------------------------------------------------------------
+#ifndef PDHCG_STREAM_U
+#define PDHCG_STREAM_U 8
+#endif
+constexpr int STREAM_U = PDHCG_STREAM_U;
+constexpr int STREAM_CHUNK = 32 * STREAM_U;
+constexpr int STREAM_ROW_MAX = 64;
+
+__device__ __forceinline__ int warp_max_int(int v)
 {
-    double s = 0.0;
-    for (int k = b + lane; k < e; k += G)
-        s += (double)__ldg(val + k) * (double)__ldg(x + __ldg(ci + k));
-    return group_sum<G>(s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v = max(v, __shfl_xor_sync(FULL, v, o));
+    return v;
+}
+
+// out[s] = sum_k val[k] * x[ci[k]] over row r0 + lane + 32 s (0 when that
+// row is past nr).  Every lane of the warp must call it with the same r0,
+// nr (1 <= nr <= 32 S) and stage (STREAM_CHUNK doubles of this warp's
+// shared memory).
+template <int S, typename V, typename X>
+__device__ __forceinline__ void warp_stream_rows(const int *__restrict__ rp, const int *__restrict__ ci,
+                                                 const V *__restrict__ val, const X *__restrict__ x, int r0, int nr,
+                                                 int lane, double *stage, double (&out)[S])
+{
+    int rb[S], re[S];
+    int longest = 0;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int i = lane + 32 * s;
+        rb[s] = re[s] = 0;
+        if (i < nr) {
+            rb[s] = __ldg(rp + r0 + i);
+            re[s] = __ldg(rp + r0 + i + 1);
+        }
+        longest = max(longest, re[s] - rb[s]);
+        out[s] = 0.0;
+    }
+    longest = warp_max_int(longest);
+    const int b = __shfl_sync(FULL, rb[0], 0);
+    int e = 0;
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+        if (s == ((nr - 1) >> 5))
+            e = re[s];
+    e = __shfl_sync(FULL, e, (nr - 1) & 31);
+
+    if (longest <= STREAM_ROW_MAX) {
+        for (int cb = b; cb < e; cb += STREAM_CHUNK) {
+            int col[STREAM_U];
+            double v[STREAM_U];
+#pragma unroll
+            for (int u = 0; u < STREAM_U; ++u) {
+                const int k = cb + 32 * u + lane;
+                col[u] = k < e ? __ldg(ci + k) : -1;
+                v[u] = k < e ? (double)__ldg(val + k) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < STREAM_U; ++u)
+                stage[32 * u + lane] = col[u] >= 0 ? v[u] * (double)__ldg(x + col[u]) : 0.0;
+            __syncwarp();
+            const int ce = min(e, cb + STREAM_CHUNK);
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const int lo = max(rb[s], cb), hi = min(re[s], ce);
+                double a = out[s];
+                for (int k = lo; k < hi; ++k)
+                    a += stage[k - cb];
+                out[s] = a;
+            }
+            __syncwarp();
+        }
+    } else {
+        for (int i = 0; i < nr; ++i) {
+            int bi = 0, ei = 0;
+#pragma unroll
+            for (int s = 0; s < S; ++s)
+                if (s == (i >> 5)) {
+                    bi = rb[s];
+                    ei = re[s];
+                }
+            bi = __shfl_sync(FULL, bi, i & 31);
+            ei = __shfl_sync(FULL, ei, i & 31);
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+            int k = bi + lane;
+            for (; k + 96 < ei; k += 128) {
+                a0 += (double)__ldg(val + k) * (double)__ldg(x + __ldg(ci + k));
+                a1 += (double)__ldg(val + k + 32) * (double)__ldg(x + __ldg(ci + k + 32));
+                a2 += (double)__ldg(val + k + 64) * (double)__ldg(x + __ldg(ci + k + 64));
+                a3 += (double)__ldg(val + k + 96) * (double)__ldg(x + __ldg(ci + k + 96));
+            }
+            for (; k < ei; k += 32)
+                a0 += (double)__ldg(val + k) * (double)__ldg(x + __ldg(ci + k));
+            const double a = warp_sum((a0 + a1) + (a2 + a3));
+#pragma unroll
+            for (int s = 0; s < S; ++s)
+                if (s == (i >> 5) && lane == (i & 31))
+                    out[s] = a;
+        }
+    }
 }
 
 __device__ __forceinline__ double clampd(double lo, double x, double hi) { return fmax(lo, fmin(x, hi)); }

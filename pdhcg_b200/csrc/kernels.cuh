@@ -55,6 +55,10 @@ struct StepData {
     const T *vr; // variable rescaling (cone metric)
     const int *free_idx;
     int n_free; // variables outside cones (NULL: all)
+    // the free variables as tiles of <= 32 consecutive rows {first, count}
+    // (NULL: rows [32 t, 32 t + 32) of all n variables)
+    const int2 *free_tiles;
+    int n_free_tiles;
     const int *cone_start, *cone_len, *cone_type;
     int n_cones;
     double *cone_warm; // per-cone multiplier warm start (may be NULL)
@@ -62,153 +66,204 @@ struct StepData {
     T *y0, *y, *yp, *dy;
 };
 
-template <int G, typename T, bool HAS_Q, bool HAS_BOX>
+// The step kernels are written as warp bodies (one tile or one cone block per
+// call) so that the launch shape is chosen in one place; every body takes
+// its warp's STREAM_CHUNK-double shared staging buffer.  The loads of each
+// lane's own vector entries are issued before the row products, so they are
+// in flight together with the matrix stream.
+
+// Variables outside cones: one tile of <= 32 consecutive rows of A^T:
+// A^T y by stream-mode products, then the prox step, box clamp, reflection
+// and Halpern average of each row's variable in its lane.
+template <typename T, bool HAS_Q, bool HAS_BOX>
+__device__ __forceinline__ void primal_free_tile(const StepData<T> &D, const StepParams &P, int r0, int nr, int lane,
+                                                 double *stage)
+{
+    const bool own = lane < nr;
+    const int j = r0 + (own ? lane : 0);
+    double xi = 0.0, c = 0.0, q = 0.0, lo = 0.0, hi = 0.0, x0 = 0.0;
+    if (own) {
+        xi = D.x[j];
+        c = D.c[j];
+        x0 = D.x0[j];
+        if (HAS_Q)
+            q = D.q[j];
+        if (HAS_BOX) {
+            lo = D.l[j];
+            hi = D.u[j];
+        }
+    }
+    double aty[1];
+    warp_stream_rows<1>(D.At_rp, D.At_ci, D.At_v, D.y, r0, nr, lane, stage, aty);
+    if (own) {
+        double t = xi - P.tau * (c - aty[0]);
+        if (HAS_Q)
+            t /= (1.0 + P.tau * q);
+        double p = HAS_BOX ? clampd(lo, t, hi) : t;
+        double xr = 2.0 * p - xi;
+        D.xr[j] = (T)xr;
+        if (P.store_primal) {
+            D.xp[j] = (T)p;
+            if (P.lp_slack)
+                D.dual_slack[j] = (T)((p - t) / P.tau);
+        }
+        if (P.want_fpe)
+            D.dx[j] = (T)(xr - xi);
+        double refl = P.rho * xr + (1.0 - P.rho) * xi;
+        D.x[j] = (T)(P.w * refl + (1.0 - P.w) * x0);
+    }
+}
+
+template <typename T, bool HAS_Q, bool HAS_BOX>
 __global__ void __launch_bounds__(TPB) primal_free_kernel(StepData<T> D, StepParams P)
 {
-    const int lane = threadIdx.x % G;
-    const int nrows = D.free_idx ? D.n_free : D.n;
-    for (int base = warp_row0<G>(); base < nrows; base += warp_row_stride<G>()) {
-        const int r = base + (threadIdx.x & 31) / G;
-        const bool ok = r < nrows;
-        const int j = ok ? (D.free_idx ? D.free_idx[r] : r) : 0;
-        double aty = row_dot<G>(D.At_rp, D.At_ci, D.At_v, D.y, j, lane, ok);
-        if (ok && lane == 0) {
-            double xi = D.x[j];
-            double t = xi - P.tau * ((double)D.c[j] - aty);
-            if (HAS_Q)
-                t /= (1.0 + P.tau * (double)D.q[j]);
-            double p = HAS_BOX ? clampd(D.l[j], t, D.u[j]) : t;
-            double xr = 2.0 * p - xi;
-            D.xr[j] = (T)xr;
-            if (P.store_primal) {
-                D.xp[j] = (T)p;
-                if (P.lp_slack)
-                    D.dual_slack[j] = (T)((p - t) / P.tau);
-            }
-            if (P.want_fpe)
-                D.dx[j] = (T)(xr - xi);
-            double refl = P.rho * xr + (1.0 - P.rho) * xi;
-            D.x[j] = (T)(P.w * refl + (1.0 - P.w) * (double)D.x0[j]);
+    __shared__ double stage_all[WARPS][STREAM_CHUNK];
+    const int lane = threadIdx.x & 31;
+    double *stage = stage_all[threadIdx.x >> 5];
+    const int ntiles = D.free_tiles ? D.n_free_tiles : (D.n + 31) / 32;
+    for (int t = blockIdx.x * WARPS + (threadIdx.x >> 5); t < ntiles; t += gridDim.x * WARPS) {
+        int r0, nr;
+        if (D.free_tiles) {
+            const int2 ft = D.free_tiles[t];
+            r0 = ft.x;
+            nr = ft.y;
+        } else {
+            r0 = 32 * t;
+            nr = min(32, D.n - r0);
         }
+        primal_free_tile<T, HAS_Q, HAS_BOX>(D, P, r0, nr, lane, stage);
     }
 }
 
-// One warp per cone block.  The prox candidate of every slot is projected
-// onto the cone in the (1 + tau q) d^2 metric (diagonal Q) or d^2 metric (LP).
-// A^T y for the L consecutive rows [st, st+L) of one cone block into a
-// per-warp staging buffer, G lanes per row so each load instruction reads
-// G consecutive entries of 32/G rows.
-template <int G, typename V, typename X>
-__device__ __forceinline__ void warp_rows_dot(const int *__restrict__ rp, const int *__restrict__ ci,
-                                              const V *__restrict__ val, const X *__restrict__ x, int st, int L,
-                                              int lane, double *out_sm)
+// One cone block [st, st + L): A^T y for the block's rows by stream-mode
+// products, the prox candidate of every slot, then the projection onto the
+// cone in the (1 + tau q) d^2 metric (diagonal Q) or d^2 metric (LP).
+template <int S, typename T, bool HAS_Q>
+__device__ __forceinline__ void primal_cone_block(const StepData<T> &D, const StepParams &P, int cb, int lane,
+                                                  double *stage)
 {
-    const int sub = lane % G;
-    for (int base = 0; base < L; base += 32 / G) {
-        int slot = base + lane / G;
-        int b = 0, e = 0;
-        if (slot < L) {
-            b = __ldg(rp + st + slot);
-            e = __ldg(rp + st + slot + 1);
+    const int st = D.cone_start[cb], L = D.cone_len[cb], type = D.cone_type[cb];
+    WarpSlots<S> sl;
+    double xi[S], cc[S], x0[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int i = lane + 32 * s;
+        sl.x[s] = 0.0;
+        sl.d[s] = 1.0;
+        sl.w[s] = 1.0;
+        xi[s] = cc[s] = x0[s] = 0.0;
+        if (i < L) {
+            const int j = st + i;
+            xi[s] = D.x[j];
+            cc[s] = D.c[j];
+            x0[s] = D.x0[j];
+            sl.d[s] = D.vr[j];
+            if (HAS_Q)
+                sl.w[s] = 1.0 + P.tau * (double)D.q[j];
         }
-        double a = range_dot<G>(ci, val, x, b, e, sub);
-        if (sub == 0 && slot < L)
-            out_sm[slot] = a;
     }
-    __syncwarp();
+    double aty[S];
+    warp_stream_rows<S>(D.At_rp, D.At_ci, D.At_v, D.y, st, L, lane, stage, aty);
+    double tt[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int i = lane + 32 * s;
+        tt[s] = 0.0;
+        if (i < L) {
+            const int j = st + i;
+            double t = xi[s] - P.tau * (cc[s] - aty[s]);
+            if (HAS_Q)
+                t /= sl.w[s];
+            tt[s] = t;
+            sl.x[s] = P.cone_box ? clampd(D.l[j], t, D.u[j]) : t;
+        }
+    }
+    // LP dual slack of the box step is recorded before the cone projection
+    // (reference compute_lp_next_pdhg_primal_solution_major_kernel then
+    // project_cone_runtime, src/pdhg_core_op.cu:426-455, 729-735)
+    if (P.lp_slack) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const int i = lane + 32 * s;
+            if (i < L)
+                D.dual_slack[st + i] = (T)((sl.x[s] - tt[s]) / P.tau);
+        }
+    }
+    bool uni = warp_uniform_unit<S>(sl, L, lane);
+    warp_project<S>(type, sl, L, lane, uni, D.cone_warm ? D.cone_warm + cb : nullptr);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int i = lane + 32 * s;
+        if (i < L) {
+            const int j = st + i;
+            double p = sl.x[s];
+            double xr = 2.0 * p - xi[s];
+            D.xr[j] = (T)xr;
+            D.xp[j] = (T)p; // cones force the pdhg store (reference :428, :460)
+            if (P.want_fpe)
+                D.dx[j] = (T)(xr - xi[s]);
+            double refl = P.rho * xr + (1.0 - P.rho) * xi[s];
+            D.x[j] = (T)(P.w * refl + (1.0 - P.w) * x0[s]);
+        }
+    }
 }
 
-template <int S, int G, typename T, bool HAS_Q>
+template <int S, typename T, bool HAS_Q>
 __global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<T> D, StepParams P)
 {
-    __shared__ double aty_all[WARPS][32 * S];
+    __shared__ double stage_all[WARPS][STREAM_CHUNK];
     const int lane = threadIdx.x & 31;
     const int warp = blockIdx.x * WARPS + (threadIdx.x >> 5);
     const int nwarps = gridDim.x * WARPS;
-    double *aty_sm = aty_all[threadIdx.x >> 5];
-    for (int cb = warp; cb < D.n_cones; cb += nwarps) {
-        const int st = D.cone_start[cb], L = D.cone_len[cb], type = D.cone_type[cb];
-        warp_rows_dot<G>(D.At_rp, D.At_ci, D.At_v, D.y, st, L, lane, aty_sm);
-        WarpSlots<S> sl;
-        double xi[S], tt[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            int i = lane + 32 * s;
-            sl.x[s] = 0.0;
-            sl.d[s] = 1.0;
-            sl.w[s] = 1.0;
-            xi[s] = 0.0;
-            tt[s] = 0.0;
-            if (i < L) {
-                int j = st + i;
-                double aty = aty_sm[i];
-                xi[s] = D.x[j];
-                double t = xi[s] - P.tau * ((double)D.c[j] - aty);
-                if (HAS_Q)
-                    t /= (1.0 + P.tau * (double)D.q[j]);
-                tt[s] = t;
-                sl.x[s] = P.cone_box ? clampd(D.l[j], t, D.u[j]) : t;
-                sl.d[s] = D.vr[j];
-                sl.w[s] = HAS_Q ? 1.0 + P.tau * (double)D.q[j] : 1.0;
-            }
-        }
-        __syncwarp(); // the staging buffer is reused by the next block
-        // LP dual slack of the box step is recorded before the cone
-        // projection (reference compute_lp_next_pdhg_primal_solution_major_kernel
-        // then project_cone_runtime, src/pdhg_core_op.cu:426-455, 729-735)
-        if (P.lp_slack) {
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                int i = lane + 32 * s;
-                if (i < L)
-                    D.dual_slack[st + i] = (T)((sl.x[s] - tt[s]) / P.tau);
-            }
-        }
-        bool uni = warp_uniform_unit<S>(sl, L, lane);
-        warp_project<S>(type, sl, L, lane, uni, D.cone_warm ? D.cone_warm + cb : nullptr);
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            int i = lane + 32 * s;
-            if (i < L) {
-                int j = st + i;
-                double p = sl.x[s];
-                double xr = 2.0 * p - xi[s];
-                D.xr[j] = (T)xr;
-                D.xp[j] = (T)p; // cones force the pdhg store (reference :428, :460)
-                if (P.want_fpe)
-                    D.dx[j] = (T)(xr - xi[s]);
-                double refl = P.rho * xr + (1.0 - P.rho) * xi[s];
-                D.x[j] = (T)(P.w * refl + (1.0 - P.w) * (double)D.x0[j]);
-            }
-        }
+    double *stage = stage_all[threadIdx.x >> 5];
+    for (int cb = warp; cb < D.n_cones; cb += nwarps)
+        primal_cone_block<S, T, HAS_Q>(D, P, cb, lane, stage);
+}
+
+// One tile of 32 consecutive rows of A: A x_refl by stream-mode products,
+// then the dual prox, reflection and Halpern average of y.
+template <typename T, bool EQ_ROWS, bool HAS_G>
+__device__ __forceinline__ void dual_tile(const StepData<T> &D, const StepParams &P, int r0, int nr, int lane,
+                                          double *stage)
+{
+    const bool own = lane < nr;
+    const int i = r0 + (own ? lane : 0);
+    double yi = 0.0, y0 = 0.0, lc = 0.0, uc = 0.0, g = 0.0;
+    if (own) {
+        yi = D.y[i];
+        y0 = D.y0[i];
+        lc = D.lc[i];
+        if (!EQ_ROWS)
+            uc = D.uc[i];
+        if (HAS_G)
+            g = D.g[i];
+    }
+    double axr[1];
+    warp_stream_rows<1>(D.A_rp, D.A_ci, D.A_v, D.xr, r0, nr, lane, stage, axr);
+    if (own) {
+        double v = HAS_G ? axr[0] + g : axr[0];
+        double pr = EQ_ROWS ? lc : clampd(lc, v - yi / P.sigma, uc);
+        double yn = yi - P.sigma * v + P.sigma * pr;
+        if (P.store_dual)
+            D.yp[i] = (T)yn;
+        double yr = 2.0 * yn - yi;
+        if (P.want_fpe)
+            D.dy[i] = (T)(yr - yi);
+        double refl = P.rho * yr + (1.0 - P.rho) * yi;
+        D.y[i] = (T)(P.w * refl + (1.0 - P.w) * y0);
     }
 }
 
-template <int G, typename T, bool EQ_ROWS, bool HAS_G>
+template <typename T, bool EQ_ROWS, bool HAS_G>
 __global__ void __launch_bounds__(TPB) dual_kernel(StepData<T> D, StepParams P)
 {
-    const int lane = threadIdx.x % G;
-    for (int base = warp_row0<G>(); base < D.m; base += warp_row_stride<G>()) {
-        const int i = base + (threadIdx.x & 31) / G;
-        const bool ok = i < D.m;
-        double ax = row_dot<G>(D.A_rp, D.A_ci, D.A_v, D.xr, i, lane, ok);
-        if (ok && lane == 0) {
-            double v = HAS_G ? ax + (double)D.g[i] : ax;
-            double yi = D.y[i];
-            double pr;
-            if (EQ_ROWS)
-                pr = D.lc[i];
-            else
-                pr = clampd(D.lc[i], v - yi / P.sigma, D.uc[i]);
-            double yn = yi - P.sigma * v + P.sigma * pr;
-            if (P.store_dual)
-                D.yp[i] = (T)yn;
-            double yr = 2.0 * yn - yi;
-            if (P.want_fpe)
-                D.dy[i] = (T)(yr - yi);
-            double refl = P.rho * yr + (1.0 - P.rho) * yi;
-            D.y[i] = (T)(P.w * refl + (1.0 - P.w) * (double)D.y0[i]);
-        }
+    __shared__ double stage_all[WARPS][STREAM_CHUNK];
+    const int lane = threadIdx.x & 31;
+    double *stage = stage_all[threadIdx.x >> 5];
+    const int ntiles = (D.m + 31) / 32;
+    for (int t = blockIdx.x * WARPS + (threadIdx.x >> 5); t < ntiles; t += gridDim.x * WARPS) {
+        const int r0 = 32 * t;
+        dual_tile<T, EQ_ROWS, HAS_G>(D, P, r0, min(32, D.m - r0), lane, stage);
     }
 }
 
@@ -265,17 +320,19 @@ __global__ void fold_partials_kernel(const double *partials, int nblocks, int ns
     }
 }
 
-template <int G>
+// y = M x, one warp per tile of 32 rows (stream-mode products)
 __global__ void __launch_bounds__(TPB) spmv_kernel(int rows, const int *rp, const int *ci, const double *v,
                                                    const double *x, double *y)
 {
-    const int lane = threadIdx.x % G;
-    for (int base = warp_row0<G>(); base < rows; base += warp_row_stride<G>()) {
-        const int r = base + (threadIdx.x & 31) / G;
-        const bool ok = r < rows;
-        double a = row_dot<G>(rp, ci, v, x, r, lane, ok);
-        if (ok && lane == 0)
-            y[r] = a;
+    __shared__ double stage_all[WARPS][STREAM_CHUNK];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int ntiles = (rows + 31) / 32;
+    for (int tile = blockIdx.x * WARPS + wib; tile < ntiles; tile += gridDim.x * WARPS) {
+        const int r0 = 32 * tile, nr = min(32, rows - r0);
+        double a[1];
+        warp_stream_rows<1>(rp, ci, v, x, r0, nr, lane, stage_all[wib], a);
+        if (lane < nr)
+            y[r0 + lane] = a[0];
     }
 }
 

@@ -53,6 +53,7 @@ struct ResidualData {
     const VT *xp, *yp, *x0, *y0;
     const VT *dual_slack;
     const int *free_idx; int n_free;
+    const int2 *free_tiles; int n_free_tiles; // tiles of consecutive free rows (NULL: all n rows)
     const int *cone_start, *cone_len, *cone_type; int n_cones;
     double *warm_dual, *warm_aug; // per-cone warm starts of the two projections
     double *partials;
@@ -61,10 +62,10 @@ struct ResidualData {
 
 __device__ __forceinline__ double norm_term(double v, int l2) { return l2 ? v * v : abs_or_inf(v); }
 
-template <int G, int S, typename VT>
+template <int S, typename VT>
 __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, ResidualParams P)
 {
-    __shared__ double aty_all[WARPS][32 * S];
+    __shared__ double stage_all[WARPS][STREAM_CHUNK];
     const int NOP = P.l2 ? RSUM : RMAX;
     const int ops[RS_COUNT] = {NOP, RSUM, NOP, RSUM, RSUM, RSUM, NOP, NOP, RSUM, RSUM};
     double acc[RS_COUNT];
@@ -72,16 +73,20 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
     for (int s = 0; s < RS_COUNT; ++s)
         acc[s] = 0.0;
     auto fold = [&](int s, double v) { acc[s] = ops[s] == RMAX ? fmax(acc[s], v) : acc[s] + v; };
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double *stage = stage_all[wib];
 
     int b = blockIdx.x;
     if (b < D.rows_blocks) {
-        const int lane = threadIdx.x % G;
-        for (int base = warp_row0<G>(b); base < D.m; base += warp_row_stride<G>(D.rows_blocks)) {
-            const int i = base + (threadIdx.x & 31) / G;
-            const bool ok = i < D.m;
-            double ax = row_dot<G>(D.A_rp, D.A_ci, D.A_v, D.xp, i, lane, ok);
-            if (ok && lane == 0) {
-                double v = ax + D.g[i];
+        // constraint rows, one warp per tile of 32
+        const int ntiles = (D.m + 31) / 32;
+        for (int tile = b * WARPS + wib; tile < ntiles; tile += D.rows_blocks * WARPS) {
+            const int r0 = 32 * tile, nr = min(32, D.m - r0);
+            double axr[1];
+            warp_stream_rows<1>(D.A_rp, D.A_ci, D.A_v, D.xp, r0, nr, lane, stage, axr);
+            if (lane < nr) {
+                const int i = r0 + lane;
+                double v = axr[0] + D.g[i];
                 double proj = clampd(D.lc[i], v, D.uc[i]);
                 fold(RS_PRIMAL_RES, norm_term((v - proj) * D.cr[i], P.l2));
                 double y = D.yp[i];
@@ -94,15 +99,24 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
             }
         }
     } else if (b < D.rows_blocks + D.free_blocks) {
+        // variables outside cones, one warp per tile of consecutive rows
         b -= D.rows_blocks;
-        const int lane = threadIdx.x % G;
-        const int nrows = D.free_idx ? D.n_free : D.n;
-        for (int base = warp_row0<G>(b); base < nrows; base += warp_row_stride<G>(D.free_blocks)) {
-            const int r = base + (threadIdx.x & 31) / G;
-            const bool ok = r < nrows;
-            const int j = ok ? (D.free_idx ? D.free_idx[r] : r) : 0;
-            double aty = row_dot<G>(D.At_rp, D.At_ci, D.At_v, D.yp, j, lane, ok);
-            if (ok && lane == 0) {
+        const int ntiles = D.free_tiles ? D.n_free_tiles : (D.n + 31) / 32;
+        for (int tile = b * WARPS + wib; tile < ntiles; tile += D.free_blocks * WARPS) {
+            int r0, nr;
+            if (D.free_tiles) {
+                const int2 ft = D.free_tiles[tile];
+                r0 = ft.x;
+                nr = ft.y;
+            } else {
+                r0 = 32 * tile;
+                nr = min(32, D.n - r0);
+            }
+            double atyr[1];
+            warp_stream_rows<1>(D.At_rp, D.At_ci, D.At_v, D.yp, r0, nr, lane, stage, atyr);
+            if (lane < nr) {
+                const int j = r0 + lane;
+                const double aty = atyr[0];
                 double x = D.xp[j];
                 double qx = P.qmode == 1 ? D.q[j] * x : (P.qmode == 2 ? D.qx[j] : 0.0);
                 double dr, ds;
@@ -139,12 +153,11 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
         }
     } else {
         b -= D.rows_blocks + D.free_blocks;
-        const int lane = threadIdx.x & 31;
         const int nwarps = D.cone_blocks * WARPS;
-        double *aty_sm = aty_all[threadIdx.x >> 5];
-        for (int cb = b * WARPS + (threadIdx.x >> 5); cb < D.n_cones; cb += nwarps) {
+        for (int cb = b * WARPS + wib; cb < D.n_cones; cb += nwarps) {
             const int st = D.cone_start[cb], L = D.cone_len[cb], type = D.cone_type[cb];
-            warp_rows_dot<4>(D.At_rp, D.At_ci, D.At_v, D.yp, st, L, lane, aty_sm);
+            double atys[S];
+            warp_stream_rows<S>(D.At_rp, D.At_ci, D.At_v, D.yp, st, L, lane, stage, atys);
             WarpSlots<S> dual, aug;
             double xv[S], rc[S], qxv[S], atyv[S];
 #pragma unroll
@@ -156,7 +169,7 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
                 xv[s] = rc[s] = qxv[s] = atyv[s] = 0.0;
                 if (i < L) {
                     int j = st + i;
-                    double aty = aty_sm[i];
+                    double aty = atys[s];
                     double x = D.xp[j];
                     double qx = P.qmode == 1 ? D.q[j] * x : (P.qmode == 2 ? D.qx[j] : 0.0);
                     double eff = P.qmode ? D.c[j] + qx : D.c[j];
@@ -171,7 +184,6 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
                     aug.d[s] = D.vr[j];
                 }
             }
-            __syncwarp(); // staging buffer reused by the next block
             bool uni = warp_uniform_unit<S>(aug, L, lane); // d uniform <=> 1/d uniform
             warp_project<S>(type, dual, L, lane, uni, D.warm_dual ? D.warm_dual + cb : nullptr);
             warp_project<S>(type, aug, L, lane, uni, D.warm_aug ? D.warm_aug + cb : nullptr);
@@ -209,24 +221,27 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
 // dx = x_refl - x_cur and dy = y_refl - y_cur written by the step kernels.
 enum FpeScalar { FP_DX2 = 0, FP_DY2, FP_CROSS, FP_COUNT };
 
-template <int G, typename VT>
+template <typename VT>
 __global__ void __launch_bounds__(TPB) fpe_kernel(int n, int m, const int *At_rp, const int *At_ci, const double *At_v,
                                                   const VT *dx, const VT *dy, double *partials,
                                                   int col_blocks)
 {
+    __shared__ double stage_all[WARPS][STREAM_CHUNK];
     const int ops[FP_COUNT] = {RSUM, RSUM, RSUM};
     double acc[FP_COUNT] = {0.0, 0.0, 0.0};
     int b = blockIdx.x;
     if (b < col_blocks) {
-        const int lane = threadIdx.x % G;
-        for (int base = warp_row0<G>(b); base < n; base += warp_row_stride<G>(col_blocks)) {
-            const int j = base + (threadIdx.x & 31) / G;
-            const bool ok = j < n;
-            double a = row_dot<G>(At_rp, At_ci, At_v, dy, j, lane, ok);
-            if (ok && lane == 0) {
-                double d = dx[j];
+        // (A^T dy)_j dx_j, one warp per tile of 32 rows of A^T
+        const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+        const int ntiles = (n + 31) / 32;
+        for (int tile = b * WARPS + wib; tile < ntiles; tile += col_blocks * WARPS) {
+            const int r0 = 32 * tile, nr = min(32, n - r0);
+            double a[1];
+            warp_stream_rows<1>(At_rp, At_ci, At_v, dy, r0, nr, lane, stage_all[wib], a);
+            if (lane < nr) {
+                double d = dx[r0 + lane];
                 acc[FP_DX2] += d * d;
-                acc[FP_CROSS] += a * d;
+                acc[FP_CROSS] += a[0] * d;
             }
         }
     } else {
@@ -238,6 +253,132 @@ __global__ void __launch_bounds__(TPB) fpe_kernel(int n, int m, const int *At_rp
         }
     }
     block_reduce_store<FP_COUNT>(acc, ops, partials);
+}
+
+// ---------------------------------------------------------------------------
+// Infeasibility certificates (reference compute_infeasibility_information,
+// src/pdhg_core_op.cu:1296-1429, kernels src/kernels/pdhcg_kernels.cu:
+// 760-859), from the last step's differences dx = x_refl - x_cur and
+// dy = y_refl - y_cur, in three launches plus fixed-order folds:
+//   ray_project_kernel : dx, dy onto the recession cones of the bounds (in
+//                        place), max |dx|, max |dy|
+//   ray_scale_kernel   : dx /= max |dx|
+//   ray_kernel         : A dx and A^T dy by stream-mode products and the
+//                        certificate pieces below
+// ---------------------------------------------------------------------------
+enum RayNorm { RN_DX = 0, RN_DY, RN_COUNT };
+enum RayScalar {
+    RY_PSLACK = 0, // sum over rows of the dual-ray objective terms
+    RY_DSLACK,     // sum over columns of the reduced-cost objective terms
+    RY_CDX,        // c . dx
+    RY_PINF,       // max primal-ray infeasibility (scaled by D_con)
+    RY_DINF,       // max dual-ray infeasibility (scaled by D_var)
+    RY_QDX,        // max |Q dx|
+    RY_COUNT
+};
+
+template <typename VT>
+__global__ void __launch_bounds__(TPB) ray_project_kernel(int n, int m, VT *dx, VT *dy, const double *l,
+                                                          const double *u, const double *lc, const double *uc,
+                                                          double *partials)
+{
+    const int ops[RN_COUNT] = {RMAX, RMAX};
+    double acc[RN_COUNT] = {0.0, 0.0};
+    for (int i = blockIdx.x * TPB + threadIdx.x; i < n + m; i += gridDim.x * TPB) {
+        if (i < n) {
+            double d = dx[i];
+            if (isfinite(l[i]))
+                d = fmax(d, 0.0);
+            if (isfinite(u[i]))
+                d = fmin(d, 0.0);
+            dx[i] = (VT)d;
+            acc[RN_DX] = fmax(acc[RN_DX], abs_or_inf((double)(VT)d));
+        } else {
+            const int r = i - n;
+            double d = dy[r];
+            if (!isfinite(lc[r]))
+                d = fmin(d, 0.0);
+            if (!isfinite(uc[r]))
+                d = fmax(d, 0.0);
+            dy[r] = (VT)d;
+            acc[RN_DY] = fmax(acc[RN_DY], abs_or_inf((double)(VT)d));
+        }
+    }
+    block_reduce_store<RN_COUNT>(acc, ops, partials);
+}
+
+template <typename VT>
+__global__ void ray_scale_kernel(int n, VT *dx, const double *norms)
+{
+    const double nx = norms[RN_DX];
+    if (!(nx > 0.0))
+        return;
+    const double inv = 1.0 / nx;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        dx[i] = (VT)((double)dx[i] * inv);
+}
+
+struct RayData {
+    int n, m;
+    const int *A_rp, *A_ci;
+    const double *A_v;
+    const int *At_rp, *At_ci;
+    const double *At_v;
+    const double *c, *l, *u, *q, *qx; // q: diagonal Q (qmode 1); qx: Q dx precomputed (qmode 2)
+    const double *lc, *uc, *g, *cr, *vr;
+    int qmode;
+    int rows_blocks; // blocks [0, rows_blocks) take rows of A, the rest columns
+    double *partials;
+};
+
+template <typename VT>
+__global__ void __launch_bounds__(TPB) ray_kernel(RayData D, const VT *dx, const VT *dy)
+{
+    __shared__ double stage_all[WARPS][STREAM_CHUNK];
+    const int ops[RY_COUNT] = {RSUM, RSUM, RSUM, RMAX, RMAX, RMAX};
+    double acc[RY_COUNT] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double *stage = stage_all[wib];
+    auto fin = [](double v) { return isfinite(v) ? v : 0.0; };
+    if ((int)blockIdx.x < D.rows_blocks) {
+        const int ntiles = (D.m + 31) / 32;
+        for (int tile = blockIdx.x * WARPS + wib; tile < ntiles; tile += D.rows_blocks * WARPS) {
+            const int r0 = 32 * tile, nr = min(32, D.m - r0);
+            double pp[1];
+            warp_stream_rows<1>(D.A_rp, D.A_ci, D.A_v, dx, r0, nr, lane, stage, pp);
+            if (lane < nr) {
+                const int i = r0 + lane;
+                const double y = dy[i];
+                acc[RY_PSLACK] += fmax(y, 0.0) * fin(D.lc[i]) + fmin(y, 0.0) * fin(D.uc[i]) - D.g[i] * y;
+                const double pinf = (fmax(0.0, -pp[0]) * (double)isfinite(D.lc[i]) +
+                                     fmax(0.0, pp[0]) * (double)isfinite(D.uc[i])) * D.cr[i];
+                acc[RY_PINF] = fmax(acc[RY_PINF], abs_or_inf(pinf));
+            }
+        }
+    } else {
+        const int b = blockIdx.x - D.rows_blocks, nb = gridDim.x - D.rows_blocks;
+        const int ntiles = (D.n + 31) / 32;
+        for (int tile = b * WARPS + wib; tile < ntiles; tile += nb * WARPS) {
+            const int r0 = 32 * tile, nr = min(32, D.n - r0);
+            double dpr[1];
+            warp_stream_rows<1>(D.At_rp, D.At_ci, D.At_v, dy, r0, nr, lane, stage, dpr);
+            if (lane < nr) {
+                const int j = r0 + lane;
+                const double dp = -dpr[0];
+                const double x = dx[j];
+                acc[RY_DSLACK] += fmax(dp, 0.0) * fin(D.l[j]) + fmin(dp, 0.0) * fin(D.u[j]);
+                const double dinf =
+                    (fmax(0.0, dp) * (double)!isfinite(D.l[j]) - fmin(0.0, dp) * (double)!isfinite(D.u[j])) * D.vr[j];
+                acc[RY_DINF] = fmax(acc[RY_DINF], abs_or_inf(dinf));
+                acc[RY_CDX] += D.c[j] * x;
+                if (D.qmode) {
+                    const double qx = D.qmode == 1 ? D.q[j] * x : D.qx[j];
+                    acc[RY_QDX] = fmax(acc[RY_QDX], abs_or_inf(qx));
+                }
+            }
+        }
+    }
+    block_reduce_store<RY_COUNT>(acc, ops, D.partials);
 }
 
 } // namespace pdhcg

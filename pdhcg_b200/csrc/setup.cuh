@@ -438,8 +438,11 @@ __global__ void __launch_bounds__(TPB) power_sigma_kernel(int m, int n, const in
                                                           double *out /* [sigma, iterations] */)
 {
     cg::grid_group grid = cg::this_grid();
+    __shared__ double stage_all[WARPS][STREAM_CHUNK];
     const int nb = gridDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31, gw = blockIdx.x * WARPS + (threadIdx.x >> 5), nw = gridDim.x * WARPS;
+    double *stage = stage_all[threadIdx.x >> 5];
     double *p0 = part, *p1 = part + nb, *p2 = part + 2 * nb, *p3 = part + 3 * nb;
     // normalize the start vector
     double a = 0.0;
@@ -454,14 +457,24 @@ __global__ void __launch_bounds__(TPB) power_sigma_kernel(int m, int n, const in
     double s2 = 1.0;
     int it = 0;
     for (; it < max_iter; ++it) {
-        for (int j = tid; j < n; j += nth)
-            dp[j] = row_dot<1>(At_rp, At_ci, At_v, v, j, 0);
+        // dp = A^T v and nv = A dp, one warp per tile of 32 rows
+        for (int t = gw; t < (n + 31) / 32; t += nw) {
+            const int r0 = 32 * t, nr = min(32, n - r0);
+            double r[1];
+            warp_stream_rows<1>(At_rp, At_ci, At_v, v, r0, nr, lane, stage, r);
+            if (lane < nr)
+                dp[r0 + lane] = r[0];
+        }
         grid.sync();
         a = 0.0;
-        for (int i = tid; i < m; i += nth) {
-            double t = row_dot<1>(A_rp, A_ci, A_v, dp, i, 0);
-            nv[i] = t;
-            a += t * v[i];
+        for (int t = gw; t < (m + 31) / 32; t += nw) {
+            const int r0 = 32 * t, nr = min(32, m - r0);
+            double r[1];
+            warp_stream_rows<1>(A_rp, A_ci, A_v, dp, r0, nr, lane, stage, r);
+            if (lane < nr) {
+                nv[r0 + lane] = r[0];
+                a += r[0] * v[r0 + lane];
+            }
         }
         coop_block_partial(a, p1);
         grid.sync();

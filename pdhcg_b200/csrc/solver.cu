@@ -93,6 +93,21 @@ int print_frequency(int iter)
     return step;
 }
 
+// Runs of consecutive rows in a sorted index list, cut into tiles of at
+// most 32 rows {first row, count} (one warp each in the step kernels).
+std::vector<int2> row_tiles(const std::vector<int> &rows)
+{
+    std::vector<int2> t;
+    for (size_t i = 0; i < rows.size();) {
+        size_t j = i + 1;
+        while (j < rows.size() && j - i < 32 && rows[j] == rows[j - 1] + 1)
+            ++j;
+        t.push_back(make_int2(rows[i], (int)(j - i)));
+        i = j;
+    }
+    return t;
+}
+
 // lanes per row from the mean row length
 int pick_group(long long nnz, int rows)
 {
@@ -123,22 +138,6 @@ int slots_class(int maxlen)
     if (s <= 8)
         return 8;
     return -1;
-}
-
-// lanes per row of the cone kernels' staging SpMV
-int cone_group(int g)
-{
-    return g <= 2 ? 2 : (g <= 4 ? 4 : 8);
-}
-
-template <typename F>
-void dispatch_cg(int G, F &&f)
-{
-    switch (G) {
-    case 2: f(std::integral_constant<int, 2>{}); break;
-    case 4: f(std::integral_constant<int, 4>{}); break;
-    default: f(std::integral_constant<int, 8>{}); break;
-    }
 }
 
 // lanes per row of the residual kernel (one kernel serves A and A^T rows)
@@ -208,6 +207,8 @@ struct DeviceProblem {
     double *R_v = nullptr, *Ddiag = nullptr, *Ddense = nullptr;
     double *c = nullptr, *l = nullptr, *u = nullptr, *lc = nullptr, *uc = nullptr, *g = nullptr;
     int *cst = nullptr, *clen = nullptr, *ctype = nullptr, *cvdim = nullptr, *free_d = nullptr;
+    int2 *free_tiles = nullptr; // free variables as tiles of consecutive rows
+    int n_free_tiles = 0;
     double *pstart = nullptr, *dstart = nullptr;
     // solution kept on the device when a solve is asked to leave it there
     double *x_out = nullptr, *y_out = nullptr, *rc_out = nullptr;
@@ -359,8 +360,13 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
         d.clen = ar.upload(d.cone_len.data(), nc, s);
         d.ctype = ar.upload(d.cone_type.data(), nc, s);
         d.cvdim = ar.upload(d.cone_vdim.data(), nc, s);
-        if (!d.free_idx.empty())
+        if (!d.free_idx.empty()) {
             d.free_d = ar.upload(d.free_idx.data(), d.free_idx.size(), s);
+            std::vector<int2> ft = row_tiles(d.free_idx);
+            d.n_free_tiles = (int)ft.size();
+            d.free_tiles = ar.upload(ft.data(), ft.size(), s);
+            CK(cudaStreamSynchronize(s)); // ft goes out of scope
+        }
     }
     if (d.S < 0)
         d.unsupported = "cone blocks longer than 256 slots are not supported yet";
@@ -414,8 +420,6 @@ private:
     void read_residual();
     void enqueue_fpe(int slot);
     pdhcg_result_t *make_result();
-    template <typename F>
-    void dispatch_g(int G, F &&f);
 
     DeviceProblem &dp_;
     bool own_;
@@ -462,9 +466,13 @@ private:
     int fp32_stall_ = 0;
     double *partials_ = nullptr, *scal_d_ = nullptr, *h_scal_ = nullptr;
     int *res_ops_d_ = nullptr, *fpe_ops_d_ = nullptr, *norm_ops_d_ = nullptr;
+    int *rayn_ops_d_ = nullptr, *ray_ops_d_ = nullptr;
+    double *ray_d_ = nullptr; // [RN_COUNT + RY_COUNT] folded certificate scalars
+    // infeasibility certificates of the last computation (zero until then)
+    double p_ray_obj_ = 0.0, d_ray_obj_ = 0.0, max_p_ray_ = 0.0, max_d_ray_ = 0.0;
+    void compute_infeasibility();
     int res_rows_blocks_ = 0, res_free_blocks_ = 0, res_cone_blocks_ = 0;
     int fpe_col_blocks_ = 0, fpe_row_blocks_ = 0;
-    int GA_ = 1, GAt_ = 1;
 
     // scaling
     double sb_ = 1.0, sc_ = 1.0, cnorm_ = 0.0, bnorm_ = 0.0;
@@ -492,18 +500,6 @@ private:
     void harvest_step_events();
 };
 
-template <typename F>
-void Solve::dispatch_g(int G, F &&f)
-{
-    switch (G) {
-    case 1: f(std::integral_constant<int, 1>{}); break;
-    case 2: f(std::integral_constant<int, 2>{}); break;
-    case 4: f(std::integral_constant<int, 4>{}); break;
-    case 8: f(std::integral_constant<int, 8>{}); break;
-    case 16: f(std::integral_constant<int, 16>{}); break;
-    default: f(std::integral_constant<int, 32>{}); break;
-    }
-}
 
 template <typename F>
 void dispatch_s(int S, F &&f)
@@ -590,8 +586,6 @@ void Solve::upload_and_preprocess()
     ctype_d_ = dp_.ctype;
     cvdim_d_ = dp_.cvdim;
     free_d_ = dp_.free_d;
-    GA_ = pick_group(A_.nnz, m_);
-    GAt_ = pick_group(At_.nnz, n_);
 }
 
 // ---- rescaling (reference rescale_problem, src/preconditioner.c:654-713) --
@@ -922,6 +916,8 @@ StepData<T> Solve::step_data()
     D.At_ci = At_.ci;
     D.free_idx = free_d_;
     D.n_free = (int)free_idx_.size();
+    D.free_tiles = dp_.free_tiles;
+    D.n_free_tiles = dp_.n_free_tiles;
     D.cone_start = cst_d_;
     D.cone_len = clen_d_;
     D.cone_type = ctype_d_;
@@ -976,21 +972,18 @@ template <typename T>
 void Solve::launch_dual(const StepData<T> &D, const StepParams &P)
 {
     cudaStream_t s = st_;
-    dispatch_g(GA_, [&](auto GC) {
-        constexpr int G = GC.value;
-        int grid = grid_for((long long)m_, TPB / G);
-        if (eq_rows_) {
-            if (has_g_)
-                dual_kernel<G, T, true, true><<<grid, TPB, 0, s>>>(D, P);
-            else
-                dual_kernel<G, T, true, false><<<grid, TPB, 0, s>>>(D, P);
-        } else {
-            if (has_g_)
-                dual_kernel<G, T, false, true><<<grid, TPB, 0, s>>>(D, P);
-            else
-                dual_kernel<G, T, false, false><<<grid, TPB, 0, s>>>(D, P);
-        }
-    });
+    int grid = grid_for(((long long)m_ + 31) / 32, WARPS);
+    if (eq_rows_) {
+        if (has_g_)
+            dual_kernel<T, true, true><<<grid, TPB, 0, s>>>(D, P);
+        else
+            dual_kernel<T, true, false><<<grid, TPB, 0, s>>>(D, P);
+    } else {
+        if (has_g_)
+            dual_kernel<T, false, true><<<grid, TPB, 0, s>>>(D, P);
+        else
+            dual_kernel<T, false, false><<<grid, TPB, 0, s>>>(D, P);
+    }
     stats_.kernel_launches++;
 }
 
@@ -1014,10 +1007,7 @@ void Solve::enqueue_step_bb(bool store_dual, bool want_fpe, double w)
         tau = std::fmax(tau, -1.01 * std::fmin(0.0, nonconvexity_));
         tau /= 100;
     }
-    dispatch_g(GAt_, [&](auto GC) {
-        constexpr int G = GC.value;
-        spmv_kernel<G><<<grid_for(n_, TPB / G), TPB, 0, s>>>(n_, At_.rp, At_.ci, At_.v, y_, bb_aty_);
-    });
+    spmv_kernel<<<grid_for(((long long)n_ + 31) / 32, WARPS), TPB, 0, s>>>(n_, At_.rp, At_.ci, At_.v, y_, bb_aty_);
     double inv_tau = 1.0 / tau;
     if (bb_m_ && inv_tau != bb_cached_inv_tau_) {
         int nb = grid_for(n_, TPB, 148 * 4);
@@ -1098,34 +1088,28 @@ void Solve::enqueue_step_t(bool store_primal, bool store_dual, bool want_fpe, do
     bool hasq = qtype_ == PDHCG_DIAG_Q;
     int nfree = D.n_cones > 0 ? D.n_free : n_;
     if (nfree > 0) {
-        dispatch_g(GAt_, [&](auto GC) {
-            constexpr int G = GC.value;
-            int grid = grid_for((long long)nfree, TPB / G);
-            if (hasq) {
-                if (box_free_)
-                    primal_free_kernel<G, T, true, false><<<grid, TPB, 0, s>>>(D, P);
-                else
-                    primal_free_kernel<G, T, true, true><<<grid, TPB, 0, s>>>(D, P);
-            } else {
-                if (box_free_)
-                    primal_free_kernel<G, T, false, false><<<grid, TPB, 0, s>>>(D, P);
-                else
-                    primal_free_kernel<G, T, false, true><<<grid, TPB, 0, s>>>(D, P);
-            }
-        });
+        int ntiles = D.free_tiles ? D.n_free_tiles : (n_ + 31) / 32;
+        int grid = grid_for(ntiles, WARPS);
+        if (hasq) {
+            if (box_free_)
+                primal_free_kernel<T, true, false><<<grid, TPB, 0, s>>>(D, P);
+            else
+                primal_free_kernel<T, true, true><<<grid, TPB, 0, s>>>(D, P);
+        } else {
+            if (box_free_)
+                primal_free_kernel<T, false, false><<<grid, TPB, 0, s>>>(D, P);
+            else
+                primal_free_kernel<T, false, true><<<grid, TPB, 0, s>>>(D, P);
+        }
         stats_.kernel_launches++;
     }
     if (D.n_cones > 0) {
         dispatch_s(S_, [&](auto SC) {
             int grid = grid_for(D.n_cones, WARPS);
             if (hasq)
-                dispatch_cg(cone_group(GAt_), [&](auto GC) {
-                    primal_cone_kernel<SC.value, GC.value, T, true><<<grid, TPB, 0, s>>>(D, P);
-                });
+                primal_cone_kernel<SC.value, T, true><<<grid, TPB, 0, s>>>(D, P);
             else
-                dispatch_cg(cone_group(GAt_), [&](auto GC) {
-                    primal_cone_kernel<SC.value, GC.value, T, false><<<grid, TPB, 0, s>>>(D, P);
-                });
+                primal_cone_kernel<SC.value, T, false><<<grid, TPB, 0, s>>>(D, P);
         });
         stats_.kernel_launches++;
     }
@@ -1208,6 +1192,8 @@ void Solve::enqueue_residual_t(bool want_dist)
     }
     D.free_idx = free_d_;
     D.n_free = (int)free_idx_.size();
+    D.free_tiles = dp_.free_tiles;
+    D.n_free_tiles = dp_.n_free_tiles;
     D.cone_start = cst_d_;
     D.cone_len = clen_d_;
     D.cone_type = ctype_d_;
@@ -1234,11 +1220,7 @@ void Solve::enqueue_residual_t(bool want_dist)
         sa = 1.0;
     P.s_aug = sa;
     int nb = D.rows_blocks + D.free_blocks + D.cone_blocks;
-    // one row-group width serves both the A rows and the A^T rows
-    int G = residual_group(std::min(GA_, GAt_));
-    dispatch_rg(G, [&](auto GC) {
-        dispatch_s(S_, [&](auto SC) { residual_kernel<GC.value, SC.value, VT><<<nb, TPB, 0, s>>>(D, P); });
-    });
+    dispatch_s(S_, [&](auto SC) { residual_kernel<SC.value, VT><<<nb, TPB, 0, s>>>(D, P); });
     fold_partials_kernel<<<1, TPB, 0, s>>>(partials_, nb, RS_COUNT, res_ops_d_, scal_d_);
     stats_.kernel_launches += 2;
     stats_.evaluations++;
@@ -1249,20 +1231,86 @@ void Solve::enqueue_fpe(int slot)
     cudaStream_t s = st_;
     int nb = fpe_col_blocks_ + fpe_row_blocks_;
     double *part = partials_; // stream order serialises every user of the partials buffer
-    dispatch_rg(residual_group(GAt_), [&](auto GC) {
-        if (fp32_)
-            fpe_kernel<GC.value, float><<<nb, TPB, 0, s>>>(n_, m_, At_.rp, At_.ci, At_.v, f_.dx, f_.dy, part,
-                                                             fpe_col_blocks_);
-        else
-            fpe_kernel<GC.value, double><<<nb, TPB, 0, s>>>(n_, m_, At_.rp, At_.ci, At_.v, dx_, dy_, part,
-                                                              fpe_col_blocks_);
-    });
+    if (fp32_)
+        fpe_kernel<float><<<nb, TPB, 0, s>>>(n_, m_, At_.rp, At_.ci, At_.v, f_.dx, f_.dy, part, fpe_col_blocks_);
+    else
+        fpe_kernel<double><<<nb, TPB, 0, s>>>(n_, m_, At_.rp, At_.ci, At_.v, dx_, dy_, part, fpe_col_blocks_);
     fold_partials_kernel<<<1, TPB, 0, s>>>(part, nb, FP_COUNT, fpe_ops_d_, scal_d_ + RS_COUNT + slot * FP_COUNT);
     stats_.kernel_launches += 2;
     if (bb_) {
         bb_tol_update_kernel<<<1, 1, 0, s>>>(scal_d_ + RS_COUNT + slot * FP_COUNT + FP_DX2, step_, omega_, bb_min_tol_,
                                              bb_tol_);
         stats_.kernel_launches++;
+    }
+}
+
+// Infeasibility certificates from the differences of the last major step
+// (reference compute_infeasibility_information, src/pdhg_core_op.cu:1296-1429;
+// called, like there, only without cones, at major iterations before
+// 3 * termination_evaluation_frequency).  dx and dy are modified in place,
+// as the reference modifies delta_primal/dual_solution.
+void Solve::compute_infeasibility()
+{
+    cudaStream_t s = st_;
+    int nb = grid_for((long long)n_ + m_, TPB, 148 * 4);
+    if (fp32_)
+        ray_project_kernel<float><<<nb, TPB, 0, s>>>(n_, m_, f_.dx, f_.dy, l_d_, u_d_, lc_d_, uc_d_, partials_);
+    else
+        ray_project_kernel<double><<<nb, TPB, 0, s>>>(n_, m_, dx_, dy_, l_d_, u_d_, lc_d_, uc_d_, partials_);
+    fold_partials_kernel<<<1, TPB, 0, s>>>(partials_, nb, RN_COUNT, rayn_ops_d_, ray_d_);
+    if (fp32_)
+        ray_scale_kernel<float><<<grid_for(n_, TPB), TPB, 0, s>>>(n_, f_.dx, ray_d_);
+    else
+        ray_scale_kernel<double><<<grid_for(n_, TPB), TPB, 0, s>>>(n_, dx_, ray_d_);
+    RayData D{};
+    D.n = n_;
+    D.m = m_;
+    D.A_rp = A_.rp;
+    D.A_ci = A_.ci;
+    D.A_v = A_.v;
+    D.At_rp = At_.rp;
+    D.At_ci = At_.ci;
+    D.At_v = At_.v;
+    D.c = c_d_;
+    D.l = l_d_;
+    D.u = u_d_;
+    D.q = q_d_;
+    D.lc = lc_d_;
+    D.uc = uc_d_;
+    D.g = g_d_;
+    D.cr = cr_d_;
+    D.vr = vr_d_;
+    D.qmode = (qtype_ == PDHCG_NON_Q) ? 0 : (qtype_ == PDHCG_DIAG_Q ? 1 : 2);
+    if (D.qmode == 2) { // Q dx through the BB apply (FP64 only)
+        enqueue_q_apply(dx_, qx_res_);
+        D.qx = qx_res_;
+    }
+    D.rows_blocks = res_rows_blocks_;
+    D.partials = partials_;
+    int grid = res_rows_blocks_ + fpe_col_blocks_;
+    if (fp32_)
+        ray_kernel<float><<<grid, TPB, 0, s>>>(D, f_.dx, f_.dy);
+    else
+        ray_kernel<double><<<grid, TPB, 0, s>>>(D, dx_, dy_);
+    fold_partials_kernel<<<1, TPB, 0, s>>>(partials_, grid, RY_COUNT, ray_ops_d_, ray_d_ + RN_COUNT);
+    stats_.kernel_launches += 6;
+    double h[RN_COUNT + RY_COUNT];
+    CK(cudaMemcpyAsync(h, ray_d_, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const double *r = h + RN_COUNT;
+    p_ray_obj_ = r[RY_CDX] / (sb_ * sc_);
+    d_ray_obj_ = (r[RY_PSLACK] + r[RY_DSLACK]) / (sb_ * sc_);
+    max_p_ray_ = r[RY_PINF];
+    if (qtype_ != PDHCG_NON_Q)
+        max_p_ray_ = std::fmax(max_p_ray_, r[RY_QDX] / sc_);
+    max_d_ray_ = r[RY_DINF];
+    double f = std::fmax(h[RN_DY], r[RY_DINF]);
+    if (f > 0.0) {
+        max_d_ray_ /= f;
+        d_ray_obj_ /= f;
+    } else {
+        max_d_ray_ = 0.0;
+        d_ray_obj_ = 0.0;
     }
 }
 
@@ -1389,18 +1437,24 @@ void Solve::loop()
             bool restart_check = is_major_ || k_ == 0;
             enqueue_residual(restart_check);
             read_residual();
+            // reference src/solver.cu:127-131
+            if (cone_start_.empty() && is_major_ && k_ < 3 * freq)
+                compute_infeasibility();
             cum_time_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-            // check_termination_criteria (reference src/utils.cu:250-289); the
-            // infeasibility certificates stay zero, which never fires
-            if (rel_d_ < tc.eps_feasible_relative && rel_p_ < tc.eps_feasible_relative &&
-                rel_gap_ < tc.eps_optimal_relative)
+            // check_termination_criteria (reference src/utils.cu:250-289)
+            if (pdhcg_b200_cancel_requested())
+                reason_ = TERMINATION_REASON_USER_INTERRUPT;
+            else if (rel_d_ < tc.eps_feasible_relative && rel_p_ < tc.eps_feasible_relative &&
+                     rel_gap_ < tc.eps_optimal_relative)
                 reason_ = TERMINATION_REASON_OPTIMAL;
+            else if (cone_start_.empty() && d_ray_obj_ > 0.0 && max_d_ray_ / d_ray_obj_ <= tc.eps_infeasible)
+                reason_ = TERMINATION_REASON_PRIMAL_INFEASIBLE;
+            else if (cone_start_.empty() && p_ray_obj_ < 0.0 && max_p_ray_ / (-p_ray_obj_) <= tc.eps_infeasible)
+                reason_ = TERMINATION_REASON_DUAL_INFEASIBLE;
             else if (k_ >= tc.iteration_limit)
                 reason_ = TERMINATION_REASON_ITERATION_LIMIT;
             else if (cum_time_ >= tc.time_sec_limit)
                 reason_ = TERMINATION_REASON_TIME_LIMIT;
-            if (pdhcg_b200_cancel_requested())
-                reason_ = TERMINATION_REASON_USER_INTERRUPT;
             if (reason_ != TERMINATION_REASON_UNSPECIFIED)
                 break;
             if (fp32_) {
@@ -1561,6 +1615,10 @@ pdhcg_result_t *Solve::make_result()
     r->objective_gap = gap_;
     r->relative_objective_gap = rel_gap_;
     r->termination_reason = reason_;
+    r->max_primal_ray_infeasibility = max_p_ray_;
+    r->max_dual_ray_infeasibility = max_d_ray_;
+    r->primal_ray_linear_objective = p_ray_obj_;
+    r->dual_ray_objective = d_ray_obj_;
     return r;
 }
 
@@ -1577,16 +1635,17 @@ pdhcg_result_t *Solve::run()
     CK(cudaStreamSynchronize(st_));
     stats_.upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host).count();
     // reduction scratch sized for the widest user
-    int rg = residual_group(std::min(GA_, GAt_));
-    res_rows_blocks_ = grid_for(m_, TPB / rg, 148 * 8);
-    res_free_blocks_ = grid_for(cone_start_.empty() ? n_ : (long long)free_idx_.size(), TPB / rg, 148 * 8);
+    // residual ranges: one warp per tile of 32 rows / per cone block
+    res_rows_blocks_ = grid_for(((long long)m_ + 31) / 32, WARPS, 148 * 8);
+    res_free_blocks_ = grid_for(cone_start_.empty() ? ((long long)n_ + 31) / 32 : (long long)dp_.n_free_tiles, WARPS,
+                                148 * 8);
     if (!cone_start_.empty() && free_idx_.empty())
         res_free_blocks_ = 0;
     res_cone_blocks_ = cone_start_.empty() ? 0 : grid_for((long long)cone_start_.size(), WARPS, 148 * 8);
-    fpe_col_blocks_ = grid_for(n_, TPB / residual_group(GAt_), 148 * 8);
+    fpe_col_blocks_ = grid_for(((long long)n_ + 31) / 32, WARPS, 148 * 8);
     fpe_row_blocks_ = grid_for(m_, TPB, 148 * 4);
     int maxb = std::max({res_rows_blocks_ + res_free_blocks_ + res_cone_blocks_, fpe_col_blocks_ + fpe_row_blocks_,
-                         148 * 4});
+                         res_rows_blocks_ + fpe_col_blocks_, 148 * 4});
     partials_ = ar_.alloc<double>((size_t)maxb * RS_COUNT);
     scal_d_ = ar_.alloc<double>(RS_COUNT + 2 * FP_COUNT);
     CK(cudaMemsetAsync(scal_d_, 0, (RS_COUNT + 2 * FP_COUNT) * sizeof(double), st_));
@@ -1599,6 +1658,11 @@ pdhcg_result_t *Solve::run()
         res_ops_d_ = ar_.upload(res_ops, RS_COUNT, st_);
         fpe_ops_d_ = ar_.upload(fpe_ops, FP_COUNT, st_);
         norm_ops_d_ = ar_.upload(norm_ops, NS_COUNT, st_);
+        int rayn_ops[RN_COUNT] = {RMAX, RMAX};
+        int ray_ops[RY_COUNT] = {RSUM, RSUM, RSUM, RMAX, RMAX, RMAX};
+        rayn_ops_d_ = ar_.upload(rayn_ops, RN_COUNT, st_);
+        ray_ops_d_ = ar_.upload(ray_ops, RY_COUNT, st_);
+        ray_d_ = ar_.alloc<double>(RN_COUNT + RY_COUNT);
         CK(cudaStreamSynchronize(st_)); // the uploads above read stack arrays
     }
     // unscaled norms for the relative errors (reference src/solver_state.cu:854-934)
@@ -1652,6 +1716,7 @@ int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cuda
 {
     int n = t->n, nc = t->num_cones;
     int *len_d = nullptr, *free_d = nullptr;
+    int2 *tiles_d = nullptr;
     int S = 1;
     if (nc > 0) {
         std::vector<int> st(nc), vd(nc), tp(nc), len(nc);
@@ -1674,14 +1739,20 @@ int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cuda
         S = slots_class(maxlen);
         if (S < 0)
             return -2;
+        std::vector<int2> ft = row_tiles(fr);
         CK(cudaMallocAsync((void **)&len_d, nc * sizeof(int), s));
         CK(cudaMallocAsync((void **)&free_d, std::max<size_t>(fr.size(), 1) * sizeof(int), s));
+        CK(cudaMallocAsync((void **)&tiles_d, std::max<size_t>(ft.size(), 1) * sizeof(int2), s));
         CK(cudaMemcpyAsync(len_d, len.data(), nc * sizeof(int), cudaMemcpyHostToDevice, s));
-        if (!fr.empty())
+        if (!fr.empty()) {
             CK(cudaMemcpyAsync(free_d, fr.data(), fr.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(tiles_d, ft.data(), ft.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+        }
         CK(cudaStreamSynchronize(s)); // host vectors go out of scope
         D.free_idx = free_d;
         D.n_free = (int)fr.size();
+        D.free_tiles = tiles_d;
+        D.n_free_tiles = (int)ft.size();
         D.cone_start = t->cone_start;
         D.cone_len = len_d;
         D.cone_type = t->cone_type;
@@ -1690,28 +1761,32 @@ int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cuda
     bool hasq = t->q_diag != nullptr;
     int nfree = nc > 0 ? D.n_free : n;
     if (nfree > 0) {
-        int grid = grid_for(nfree, TPB);
+        int ntiles = nc > 0 ? D.n_free_tiles : (n + 31) / 32;
+        int grid = grid_for(ntiles, WARPS);
         if (hasq)
-            primal_free_kernel<1, double, true, true><<<grid, TPB, 0, s>>>(D, P);
+            primal_free_kernel<double, true, true><<<grid, TPB, 0, s>>>(D, P);
         else
-            primal_free_kernel<1, double, false, true><<<grid, TPB, 0, s>>>(D, P);
+            primal_free_kernel<double, false, true><<<grid, TPB, 0, s>>>(D, P);
     }
     if (nc > 0)
         dispatch_s(S, [&](auto SC) {
             if (hasq)
-                primal_cone_kernel<SC.value, 4, double, true><<<grid_for(nc, WARPS), TPB, 0, s>>>(D, P);
+                primal_cone_kernel<SC.value, double, true><<<grid_for(nc, WARPS), TPB, 0, s>>>(D, P);
             else
-                primal_cone_kernel<SC.value, 4, double, false><<<grid_for(nc, WARPS), TPB, 0, s>>>(D, P);
+                primal_cone_kernel<SC.value, double, false><<<grid_for(nc, WARPS), TPB, 0, s>>>(D, P);
         });
+    int dgrid = grid_for(((long long)t->m + 31) / 32, WARPS);
     if (t->affine_offset)
-        dual_kernel<1, double, false, true><<<grid_for(t->m, TPB), TPB, 0, s>>>(D, P);
+        dual_kernel<double, false, true><<<dgrid, TPB, 0, s>>>(D, P);
     else
-        dual_kernel<1, double, false, false><<<grid_for(t->m, TPB), TPB, 0, s>>>(D, P);
+        dual_kernel<double, false, false><<<dgrid, TPB, 0, s>>>(D, P);
     CK(cudaGetLastError());
     if (len_d)
         CK(cudaFreeAsync(len_d, s));
     if (free_d)
         CK(cudaFreeAsync(free_d, s));
+    if (tiles_d)
+        CK(cudaFreeAsync(tiles_d, s));
     return 0;
 }
 
@@ -1945,7 +2020,7 @@ int pdhcg_b200_csr_spmv(int rows, const int *row_ptr, const int *col_ind, const 
                         double *y, void *stream)
 {
     cudaStream_t s = (cudaStream_t)stream;
-    spmv_kernel<1><<<grid_for(rows, TPB), TPB, 0, s>>>(rows, row_ptr, col_ind, val, x, y);
+    spmv_kernel<<<grid_for(((long long)rows + 31) / 32, WARPS), TPB, 0, s>>>(rows, row_ptr, col_ind, val, x, y);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -96,3 +96,49 @@ def check_known_answer(res: dict, expect: dict):
         assert abs(w - 4.0) <= tol * 5
         assert abs(v * v + w * w - z * z) <= tol
         assert abs((3.0 / v - 1.0) / 2.0 - (1.0 - 4.0 / z) / 2.0) <= 1e-4
+
+
+# ---- infeasible instances (no reference test pins these; the GPU solver is
+# checked against the oracle's restatement of the certificate logic,
+# reference src/pdhg_core_op.cu:1296-1429 and src/utils.cu:230-280) ----------
+
+def primal_infeasible_lp(seed=41, n=60, m=30):
+    """A feasible box LP plus the row sum(x) >= 2 n + 5, which the box
+    [-2, 2]^n cannot meet."""
+    import scipy.sparse as sp
+    from pdhcg_b200 import instances
+    p = instances.box_lp(seed=seed, n=n, m=m)
+    A = sp.vstack([p.A.to_scipy(), sp.csr_matrix(np.ones((1, n)))]).tocsr()
+    return Problem(c=p.c, A=CsrMatrix.from_scipy(A), con_lb=np.concatenate([p.con_lb, [2.0 * n + 5]]),
+                   con_ub=np.concatenate([p.con_ub, [np.inf]]), var_lb=p.var_lb, var_ub=p.var_ub)
+
+
+def dual_infeasible(seed=42, n=60, m=30, diag_q=False):
+    """A feasible box LP (or diagonal QP) whose first variable is free, in no
+    row, has cost -1 and (QP) zero curvature: the objective is unbounded."""
+    from pdhcg_b200 import instances
+    p = instances.box_lp(seed=seed, n=n, m=m)
+    A = p.A.to_scipy().tolil()
+    A[:, 0] = 0.0
+    A = A.tocsr()
+    A.eliminate_zeros()
+    lb, ub, c = p.var_lb.copy(), p.var_ub.copy(), p.c.copy()
+    lb[0], ub[0], c[0] = -np.inf, np.inf, -1.0
+    q = None
+    if diag_q:
+        qd = np.random.default_rng(seed).uniform(0.1, 1.0, n)
+        qd[0] = 0.0
+        q = CsrMatrix(n, n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), qd)
+    return Problem(c=c, A=CsrMatrix.from_scipy(A), con_lb=p.con_lb, con_ub=p.con_ub, var_lb=lb, var_ub=ub, Q=q)
+
+
+# expected status with an iteration limit of 2000.  The QP is unbounded too,
+# but its certificate carries max |Q dx|, which the not yet converged
+# curvature directions keep above eps_infeasible * |c . dx| while certificates
+# are computed (k < 3 * termination_evaluation_frequency), so the reference's
+# logic runs it to the limit.
+INFEASIBLE = {
+    "primal_infeasible_lp": (primal_infeasible_lp, "PRIMAL_INFEASIBLE"),
+    "dual_infeasible_lp": (dual_infeasible, "DUAL_INFEASIBLE"),
+    "dual_infeasible_qp": (lambda: dual_infeasible(diag_q=True), "ITERATION_LIMIT"),
+}

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from pdhcg_b200 import capi, instances, native
-from problems import KNOWN_ANSWERS, check_known_answer
+from problems import INFEASIBLE, KNOWN_ANSWERS, check_known_answer
 
 pytestmark = pytest.mark.gpu
 
@@ -158,3 +158,20 @@ def test_device_resident_handle_matches_host_path(lib):
     np.testing.assert_allclose(xt.cpu().numpy(), host["x"], rtol=1e-12, atol=1e-12)
     lib.pdhcg_b200_device_problem_free(h)
     lib.qp_problem_free(prob)
+
+
+@pytest.mark.parametrize("name", sorted(INFEASIBLE))
+def test_infeasibility_certificates_match_oracle(lib, oracle, name):
+    """Infeasibility detection (reference compute_infeasibility_information,
+    src/pdhg_core_op.cu:1296-1429): same status and iteration count as the
+    oracle, certificate scalars to 1e-6 relative."""
+    make, status = INFEASIBLE[name]
+    p = make()
+    prm = {"termination_criteria.iteration_limit": 2000}
+    g = _solve_gpu(lib, p, prm)
+    o = _solve_oracle(oracle, lib, p, prm)
+    assert g["status"] == o["status"] == status
+    assert g["total_count"] == o["total_count"]
+    for f in ("max_primal_ray_infeasibility", "max_dual_ray_infeasibility", "primal_ray_linear_objective",
+              "dual_ray_objective"):
+        assert abs(g[f] - o[f]) <= 1e-6 * (1.0 + abs(o[f])), (f, g[f], o[f])

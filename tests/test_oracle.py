@@ -15,7 +15,7 @@ import pytest
 
 from pdhcg_b200 import capi
 from golden_problems import SCALING_CASES, scaling_problem
-from problems import KNOWN_ANSWERS, check_known_answer
+from problems import INFEASIBLE, KNOWN_ANSWERS, check_known_answer
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "scaling.npz")
 _dp = C.POINTER(C.c_double)
@@ -112,3 +112,18 @@ def test_oracle_weighted_projection_is_optimal(oracle, typ):
             cand_u = u + t * rng.standard_normal(k + 2) * 0.01
             if in_cone(cand_u, 0.0):
                 assert np.sum(w * (cand_u * d - r) ** 2) >= f0 - 1e-9
+
+
+@pytest.mark.parametrize("name", sorted(INFEASIBLE))
+def test_oracle_detects_infeasibility(lib, oracle, name):
+    """The oracle's certificate logic (reference compute_infeasibility_information)
+    reports the expected status on the constructed infeasible instances."""
+    make, status = INFEASIBLE[name]
+    p = make()
+    prob, keep = capi.build(lib, p)
+    prm = capi.default_params(lib, **{"termination_criteria.iteration_limit": 2000})
+    r = oracle.oracle_solve(prob, C.byref(prm))
+    d = capi.result_dict(r, p.n, p.A.m)
+    oracle.oracle_result_free(r)
+    lib.qp_problem_free(prob)
+    assert d["status"] == status
