@@ -268,18 +268,23 @@ __device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform
         return;
     }
 
-    // u-space data: a = x / d, omega = w d^2; b = omega * a
-    double b[S], om[S];
+    // u-space data: a = x / d, omega = w d^2; b = omega * a = w d x.  The
+    // projection is u_i = b_i / (omega_i + lam), i.e. x_i = x_i omega_i / (omega_i + lam),
+    // so the only per-slot reciprocals are 1/d (for the cone tests) and
+    // 1/(omega_i + lam) (reused for the output).
+    double b[S], om[S], inv[S];
     double n2 = 0.0, p2 = 0.0;
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         int i = lane + 32 * s;
         b[s] = 0.0;
         om[s] = 1.0;
+        inv[s] = 1.0;
         if (i < apex) {
-            double a = sl.x[s] / sl.d[s];
+            double rd = __drcp_rn(sl.d[s]);
+            double a = sl.x[s] * rd;
             om[s] = fmax(sl.w[s] * sl.d[s] * sl.d[s], DBL_MIN);
-            b[s] = om[s] * a;
+            b[s] = sl.w[s] * sl.d[s] * sl.x[s];
             n2 += a * a;
             p2 += b[s] * b[s];
         }
@@ -304,7 +309,8 @@ __device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform
 #pragma unroll
         for (int s = 0; s < S; ++s)
             if (lane + 32 * s < apex) {
-                double t = b[s] / (om[s] + lam);
+                inv[s] = __drcp_rn(om[s] + lam);
+                double t = b[s] * inv[s];
                 t2 += t * t;
             }
         uz = sqrt(warp_sum(t2));
@@ -317,19 +323,21 @@ __device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform
         double hi = lower ? omz * (1.0 - 1e-14) : INFINITY;
         double w0 = warm ? *warm : -1.0;
         lam = (w0 > lo && w0 < hi && isfinite(w0)) ? w0 : (lower ? 0.5 * (lo + hi) : 2.0 * omz);
+        double izl = 0.0;
+        bool done = false;
         for (int it = 0; it < ROOT_ITERS; ++it) {
             double t2 = 0.0, dt2 = 0.0;
 #pragma unroll
             for (int s = 0; s < S; ++s)
                 if (lane + 32 * s < apex) {
-                    double inv = 1.0 / (om[s] + lam);
-                    double t = b[s] * inv;
+                    inv[s] = __drcp_rn(om[s] + lam);
+                    double t = b[s] * inv[s];
                     t2 += t * t;
-                    dt2 += t * t * inv;
+                    dt2 += t * t * inv[s];
                 }
             t2 = warp_sum(t2);
             dt2 = warp_sum(dt2);
-            double izl = 1.0 / (omz - lam);
+            izl = __drcp_rn(omz - lam);
             double z = bz * izl;
             double f = t2 - z * z;
             double df = -2.0 * dt2 - 2.0 * z * z * izl;
@@ -337,14 +345,23 @@ __device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform
                 lo = lam;
             else
                 hi = lam;
-            if (fabs(f) <= 1e-13 * (1.0 + t2 + z * z) || (isfinite(hi) && hi - lo <= 1e-13 * (1.0 + hi + lo)))
+            if (fabs(f) <= 1e-13 * (1.0 + t2 + z * z) || (isfinite(hi) && hi - lo <= 1e-13 * (1.0 + hi + lo))) {
+                done = true;
                 break;
+            }
             double nx = lam - f / df;
             if (!isfinite(nx) || !(nx > lo && nx < hi))
                 nx = isfinite(hi) ? 0.5 * (lo + hi) : 2.0 * lam;
             lam = nx;
         }
-        uz = bz / (omz - lam);
+        if (!done) { // iteration cap: inv and izl of the final lam
+#pragma unroll
+            for (int s = 0; s < S; ++s)
+                if (lane + 32 * s < apex)
+                    inv[s] = __drcp_rn(om[s] + lam);
+            izl = __drcp_rn(omz - lam);
+        }
+        uz = bz * izl;
         if (warm && lane == 0)
             *warm = lam;
     }
@@ -352,7 +369,7 @@ __device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform
     for (int s = 0; s < S; ++s) {
         int i = lane + 32 * s;
         if (i < apex)
-            sl.x[s] = (b[s] / (om[s] + lam)) * sl.d[s];
+            sl.x[s] = sl.x[s] * om[s] * inv[s];
         else if (i == apex)
             sl.x[s] = uz * dz;
     }
