@@ -511,4 +511,69 @@ __global__ void __launch_bounds__(TPB) power_sigma_kernel(int m, int n, const in
     }
 }
 
+// ---- Curtis-Reid scaling (reference curtis_reid_rescaling,
+// src/preconditioner.c:334-495): log-space alternating row / column averages
+// of log|a_ij|, cone blocks averaged together when scaling is
+// cone-preserving.  One thread per row with sequential sums in entry order,
+// the order of the reference's host loops.
+constexpr double CR_LOG_MIN_ABS = 1e-300;
+constexpr double CR_LOG_LIMIT = 69.07755278982137; // log(1e30)
+
+// sum of log max(|a|, 1e-300) over each row of M
+__global__ void cr_logsum_kernel(const int *rp, const double *v, int rows, double *sum)
+{
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int k = rp[r]; k < rp[r + 1]; ++k)
+            s += log(fmax(fabs(v[k]), CR_LOG_MIN_ABS));
+        sum[r] = s;
+    }
+}
+
+// raw[r] = base[r] - sum_{k in row r} other[col k]; out[r] = raw[r] / len(r),
+// 0 for empty rows (raw may be NULL)
+__global__ void cr_average_kernel(const int *rp, const int *ci, int rows, const double *base, const double *other,
+                                  double *out, double *raw)
+{
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        int b = rp[r], e = rp[r + 1];
+        double s = base[r];
+        for (int k = b; k < e; ++k)
+            s -= other[ci[k]];
+        if (raw)
+            raw[r] = s;
+        out[r] = e > b ? s / (double)(e - b) : 0.0;
+    }
+}
+
+// cone-preserving column step: one value per cone block,
+// (sum over the block of cs) / (sum over the block of the column counts)
+__global__ void cr_cone_average_kernel(int nc, const int *start, const int *len, const int *At_rp, const double *cs,
+                                       double *cls)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nc; b += gridDim.x * blockDim.x) {
+        const int st = start[b], L = len[b];
+        double bsum = 0.0;
+        int bcount = 0;
+        for (int c = st; c < st + L; ++c) {
+            bsum += cs[c];
+            bcount += At_rp[c + 1] - At_rp[c];
+        }
+        const double bl = bcount > 0 ? bsum / (double)bcount : 0.0;
+        for (int c = st; c < st + L; ++c)
+            cls[c] = bl;
+    }
+}
+
+__global__ void cr_exp_kernel(double *v, int k)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+        double x = v[i];
+        if (isnan(x))
+            v[i] = 1.0;
+        else
+            v[i] = exp(fmin(fmax(x, -CR_LOG_LIMIT), CR_LOG_LIMIT));
+    }
+}
+
 } // namespace pdhcg

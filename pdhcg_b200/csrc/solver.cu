@@ -600,16 +600,8 @@ void Solve::rescale()
     CK(cudaMemcpyAsync(cr_d_, ones_m.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(vr_d_, ones_n.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
     bool pres = prm_.use_cone_preserving_scaling;
-    auto apply = [&](int ruiz_phase) {
-        CK(cudaGetLastError());
-        sqrt_or_one_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(fvr, n);
-        sqrt_or_one_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(fcr, m);
-        if (nc > 0) {
-            if (pres)
-                cone_scaling_adjust_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(fvr, nc, cst_d_, clen_d_, ruiz_phase);
-            else
-                psd_scaling_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(fvr, nc, cst_d_, cvdim_d_, ctype_d_);
-        }
+    // scale the problem by (fcr, fvr) (reference scale_problem, src/preconditioner.c:231-332)
+    auto apply_scaling = [&]() {
         scale_csr_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.ci, A_.v, m, fcr, fvr, 0);
         scale_csr_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.ci, At_.v, n, fvr, fcr, 1);
         if (Q_.nnz > 0)
@@ -622,8 +614,35 @@ void Solve::rescale()
                                                                              uc_d_, g_d_, fcr, vr_d_, cr_d_);
         CK(cudaGetLastError());
     };
-    if (prm_.curtis_reid_iterations > 0)
-        throw CudaError("Curtis-Reid scaling is not available on the device path yet");
+    // Ruiz / Pock-Chambolle factors: square roots, then the cone adjustment
+    auto apply = [&](int ruiz_phase) {
+        CK(cudaGetLastError());
+        sqrt_or_one_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(fvr, n);
+        sqrt_or_one_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(fcr, m);
+        if (nc > 0) {
+            if (pres)
+                cone_scaling_adjust_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(fvr, nc, cst_d_, clen_d_, ruiz_phase);
+            else
+                psd_scaling_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(fvr, nc, cst_d_, cvdim_d_, ctype_d_);
+        }
+        apply_scaling();
+    };
+    if (prm_.curtis_reid_iterations > 0 && m > 0 && n > 0 && A_.nnz > 0) {
+        // reference curtis_reid_rescaling, src/preconditioner.c:334-495
+        double *rsum = ar_.alloc<double>(m), *csum = ar_.alloc<double>(n), *cs = ar_.alloc<double>(n);
+        CK(cudaMemsetAsync(fvr, 0, n * sizeof(double), s)); // column log-scales start at 0
+        cr_logsum_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.v, m, rsum);
+        cr_logsum_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.v, n, csum);
+        for (int it = 0; it < prm_.curtis_reid_iterations; ++it) {
+            cr_average_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.ci, m, rsum, fvr, fcr, nullptr);
+            cr_average_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.ci, n, csum, fcr, fvr, cs);
+            if (nc > 0 && pres)
+                cr_cone_average_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(nc, cst_d_, clen_d_, At_.rp, cs, fvr);
+        }
+        cr_exp_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(fcr, m);
+        cr_exp_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(fvr, n);
+        apply_scaling();
+    }
     for (int it = 0; it < prm_.l_inf_ruiz_iterations; ++it) {
         row_absmax_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.v, m, fcr);
         row_absmax_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.v, n, fvr);

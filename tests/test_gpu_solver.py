@@ -63,6 +63,11 @@ CASES = {
     "sparse_qp_small": (lambda: instances.sparse_qp(scale=0.05), {}),
     "sparse_qp_no_precond": (lambda: instances.sparse_qp(seed=7, scale=0.03), {"diag_jacobi_precond": False}),
     "portfolio_small": (lambda: instances.portfolio(scale=0.01), {}),
+    # Curtis-Reid scaling before Ruiz (cone-preserving and not)
+    "box_lp_curtis_reid": (lambda: instances.box_lp(seed=10), {"curtis_reid_iterations": 8}),
+    "conic_qp_curtis_reid": (lambda: instances.conic_lp(seed=11, with_q=True), {"curtis_reid_iterations": 5}),
+    "conic_lp_curtis_reid_np": (lambda: instances.conic_lp(seed=12), {"curtis_reid_iterations": 5,
+                                                                       "use_cone_preserving_scaling": False}),
 }
 
 
