@@ -99,6 +99,34 @@ void pdhcg_b200_request_cancel(int on);
  * calls. */
 int cone_block_length(const cone_blocks_t *blocks, int block);
 
+/* ---- batched solve ----------------------------------------------------------
+ * Many small LP / diagonal-QP instances (no cones, at most 65535 rows and
+ * columns, each fitting in one SM's shared memory) in persistent launches:
+ * each instance runs the same restarted Halpern PDHG as solve_qp_problem
+ * inside one thread group with its scaled data held in shared memory, in
+ * FP32 with FP64 accumulation, reductions, residuals and step sizes.
+ * Instances that do not qualify are solved one by one by solve_qp_problem.
+ * No counterpart in the reference (its baseline is one solve_qp_problem call
+ * per instance).  results[i] receives a heap result of problem i (free each
+ * with pdhcg_result_free); returns 0, or -1 on error. */
+typedef struct {
+    int shape;       /* launch shape (index into the shapes below), -1: by size */
+    int reserved[7];
+} pdhcg_b200_batch_options_t;
+
+/* Launch shapes {threads per CTA, threads per instance}:
+ * 0 {128, 32}, 1 {256, 64}, 2 {256, 128}, 3 {256, 256}, 4 {512, 512}. */
+#define PDHCG_B200_BATCH_SHAPES 5
+
+void pdhcg_b200_default_batch_options(pdhcg_b200_batch_options_t *opts);
+int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *probs, const pdhg_parameters_t *params,
+                           const pdhcg_b200_batch_options_t *opts, pdhcg_result_t **results);
+/* Times every launch shape on the given instances (solving them each time)
+ * and stores the fastest in opts->shape; shape_ms (may be NULL) receives
+ * PDHCG_B200_BATCH_SHAPES wall times in milliseconds. */
+int pdhcg_b200_batch_autotune(int count, const qp_problem_t *const *probs, const pdhg_parameters_t *params,
+                              pdhcg_b200_batch_options_t *opts, double *shape_ms);
+
 /* ---- kernel-level entry points on device pointers ------------------------
  * For parity tests and embedding.  Pointers are device memory of the current
  * device; stream may be NULL (legacy default stream).  They return after

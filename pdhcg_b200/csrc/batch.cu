@@ -1,0 +1,1051 @@
+// batch.cu -- many small LP / diagonal-QP instances in one persistent launch.
+//
+// Each instance runs the restarted Halpern PDHG of the single-instance
+// solver (reference optimize, src/solver.cu:121-170, with the step of
+// pdhg_update, the residuals of compute_residual, the restart test and the
+// PID primal weight of perform_restart), but entirely inside one thread
+// group of a CTA: its scaled matrix (A and A^T, FP32 values, 16-bit column
+// indices) and all its vectors live in shared memory for the whole solve,
+// so an iteration is two passes over shared memory separated by group
+// barriers and never touches HBM.  Groups pull instances from a global
+// counter (largest first), so a launch of #SM x k CTAs keeps every SM busy
+// until the batch is done.
+//
+// Precision: FP32 matrix values and iterates, products and every reduction
+// accumulated in FP64; the scaling factors, step sizes, primal weight,
+// residuals and objectives are FP64.
+//
+// Launch shapes (threads per group GROUP, groups per CTA) are template
+// parameters; pdhcg_b200_batch_autotune times the candidates on a sample of
+// the batch and keeps the fastest per size class.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "pdhcg.h"
+#include "pdhcg_b200.h"
+
+namespace {
+
+constexpr double SCALE_EPS = 1e-12;
+// shared memory one instance may use (the opt-in maximum per CTA, less room
+// for the static arrays)
+constexpr int SMEM_CAP = 227 * 1024 - 1024;
+
+struct BInst {            // one instance, offsets into the packed arrays
+    int n, m;
+    long long rp_off;     // A row pointers  (m + 1, local entry offsets)
+    long long trp_off;    // A^T row pointers (n + 1)
+    long long k_off;      // entries of A (and of A^T, same count)
+    long long x_off;      // x-side vectors (n)
+    long long y_off;      // y-side vectors (m)
+    int smem;             // bytes of shared memory the instance needs
+    int qmode;            // 0 LP, 1 diagonal Q
+    double obj_const;
+};
+
+struct BParams {
+    double eps_opt, eps_feas;
+    double time_limit_ns;          // per instance, checked at every evaluation
+    int iter_limit, freq;
+    int l2;
+    int ruiz_iters;
+    int has_pc;
+    double pc_alpha;
+    int bound_obj;
+    int sv_max_iter;
+    double sv_tol;
+    double rho;                    // reflection coefficient
+    double suff, nec, artificial;  // restart thresholds
+    double i_smooth, k_p, k_i, k_d;
+};
+
+struct BData {               // packed inputs and outputs of the whole batch
+    const int *A_rp, *A_ci, *At_rp, *At_ci;
+    const double *A_v, *At_v;
+    const double *c, *l, *u, *q;     // x side (q: diagonal, 0 for LP)
+    const double *lc, *uc;           // y side
+    const double *v0;                // power-method start vector (rand_r(1234) in [-1, 1])
+    const BInst *inst;
+    const int *order;                // instance indices, largest first
+    int count;
+    int *next;                       // work counter (starts at 0)
+    double *x_out, *y_out;           // unscaled solutions
+    double *stats;                   // per instance: BS_COUNT doubles
+};
+
+enum BStat { BS_STATUS = 0, BS_ITERS, BS_POBJ, BS_DOBJ, BS_ABS_P, BS_ABS_D, BS_REL_P, BS_REL_D, BS_GAP, BS_REL_GAP, BS_COUNT };
+
+__host__ __device__ inline int print_freq(int it)
+{
+    int step = 10;
+    long long th = 1000;
+    while (it >= th) {
+        step *= 10;
+        th *= 10;
+    }
+    return step;
+}
+
+// Shared-memory layout of one instance (byte offsets; every array 16-byte aligned).
+struct Layout {
+    int arp, atrp, aci, atci, av, atv;                 // matrices
+    int c, l, u, q, x0, x, xp, xr, dx, ds;             // x side, float
+    int lc, uc, y0, y, yp, dy;                         // y side, float
+    int vr, cr;                                        // scaling, double
+    int red;                                           // reduction scratch, double[32]
+    int total;
+    __host__ __device__ static int al(int b) { return (b + 15) & ~15; }
+    __host__ __device__ Layout(int n, int m, int nnz)
+    {
+        int o = 0;
+        arp = o; o += al(4 * (m + 1));
+        atrp = o; o += al(4 * (n + 1));
+        aci = o; o += al(2 * nnz);
+        atci = o; o += al(2 * nnz);
+        av = o; o += al(4 * nnz);
+        atv = o; o += al(4 * nnz);
+        c = o; o += al(4 * n);
+        l = o; o += al(4 * n);
+        u = o; o += al(4 * n);
+        q = o; o += al(4 * n);
+        x0 = o; o += al(4 * n);
+        x = o; o += al(4 * n);
+        xp = o; o += al(4 * n);
+        xr = o; o += al(4 * n);
+        dx = o; o += al(4 * n);
+        ds = o; o += al(4 * n);
+        lc = o; o += al(4 * m);
+        uc = o; o += al(4 * m);
+        y0 = o; o += al(4 * m);
+        y = o; o += al(4 * m);
+        yp = o; o += al(4 * m);
+        dy = o; o += al(4 * m);
+        vr = o; o += al(8 * n);
+        cr = o; o += al(8 * m);
+        red = o; o += al(8 * 64);
+        total = o;
+    }
+};
+
+// ---- thread group: GROUP threads of a CTA that own one instance ----------
+template <int BT, int GROUP>
+struct Grp {
+    int id, t;
+    __device__ Grp() : id(threadIdx.x / GROUP), t(threadIdx.x % GROUP) {}
+    __device__ void sync() const
+    {
+        if (GROUP == BT)
+            __syncthreads();
+        else if (GROUP == 32)
+            __syncwarp();
+        else
+            asm volatile("bar.sync %0, %1;" ::"r"(1 + id), "r"(GROUP) : "memory");
+    }
+    // sum (or max) over the group in a fixed order; every thread gets the result
+    __device__ double reduce(double v, bool is_max, double *red) const
+    {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double w = __shfl_xor_sync(0xffffffffu, v, o);
+            v = is_max ? fmax(v, w) : v + w;
+        }
+        if (GROUP == 32)
+            return v;
+        constexpr int NW = GROUP / 32;
+        if ((t & 31) == 0)
+            red[t >> 5] = v;
+        sync();
+        double r = red[0];
+        for (int i = 1; i < NW; ++i)
+            r = is_max ? fmax(r, red[i]) : r + red[i];
+        sync();
+        return r;
+    }
+};
+
+__device__ __forceinline__ double clampd(double lo, double x, double hi) { return fmax(lo, fmin(x, hi)); }
+__device__ __forceinline__ double gtimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return (double)t;
+}
+__device__ __forceinline__ double nterm(double v, int l2) { return l2 ? v * v : (isfinite(v) ? fabs(v) : INFINITY); }
+
+template <int BT, int GROUP>
+__device__ void solve_instance(const BData &D, const BParams &P, int idx, char *sm, const Grp<BT, GROUP> &g)
+{
+    const BInst I = D.inst[idx];
+    const int n = I.n, m = I.m;
+    const int *Arp = D.A_rp + I.rp_off, *Atrp = D.At_rp + I.trp_off;
+    const int nnz = Arp[m];
+    const int *Aci = D.A_ci + I.k_off, *Atci = D.At_ci + I.k_off;
+    const double *Av = D.A_v + I.k_off, *Atv = D.At_v + I.k_off;
+    const double *gc = D.c + I.x_off, *gl = D.l + I.x_off, *gu = D.u + I.x_off, *gq = D.q + I.x_off;
+    const double *glc = D.lc + I.y_off, *guc = D.uc + I.y_off;
+    Layout Lo(n, m, nnz);
+    int *arp = (int *)(sm + Lo.arp), *atrp = (int *)(sm + Lo.atrp);
+    unsigned short *aci = (unsigned short *)(sm + Lo.aci), *atci = (unsigned short *)(sm + Lo.atci);
+    float *av = (float *)(sm + Lo.av), *atv = (float *)(sm + Lo.atv);
+    float *c = (float *)(sm + Lo.c), *l = (float *)(sm + Lo.l), *u = (float *)(sm + Lo.u), *q = (float *)(sm + Lo.q);
+    float *x0 = (float *)(sm + Lo.x0), *x = (float *)(sm + Lo.x), *xp = (float *)(sm + Lo.xp);
+    float *xr = (float *)(sm + Lo.xr), *dx = (float *)(sm + Lo.dx), *ds = (float *)(sm + Lo.ds);
+    float *lc = (float *)(sm + Lo.lc), *uc = (float *)(sm + Lo.uc), *y0 = (float *)(sm + Lo.y0);
+    float *y = (float *)(sm + Lo.y), *yp = (float *)(sm + Lo.yp), *dy = (float *)(sm + Lo.dy);
+    double *vr = (double *)(sm + Lo.vr), *cr = (double *)(sm + Lo.cr), *red = (double *)(sm + Lo.red);
+    const int t = g.t;
+    const bool hasq = I.qmode == 1;
+    const double t_start = g.reduce(t == 0 ? gtimer_ns() : 0.0, true, red); // one clock for the group
+
+    // ---- unscaled norms for the relative errors (reference
+    // src/solver_state.cu:854-934) ----------------------------------------
+    double c2 = 0.0, cmax = 0.0, b2 = 0.0, bmax = 0.0;
+    for (int j = t; j < n; j += GROUP) {
+        double v = gc[j];
+        c2 += v * v;
+        cmax = fmax(cmax, fabs(v));
+    }
+    for (int i = t; i < m; i += GROUP) {
+        double lo = glc[i], up = guc[i], bb = 0.0, bm = 0.0;
+        if (isfinite(lo) && lo != up) {
+            bb += lo * lo;
+            bm = fmax(bm, fabs(lo));
+        }
+        if (isfinite(up)) {
+            bb += up * up;
+            bm = fmax(bm, fabs(up));
+        }
+        b2 += bb;
+        bmax = fmax(bmax, bm);
+    }
+    c2 = g.reduce(c2, false, red);
+    cmax = g.reduce(cmax, true, red);
+    b2 = g.reduce(b2, false, red);
+    bmax = g.reduce(bmax, true, red);
+    const double cnorm = P.l2 ? sqrt(c2) : cmax, bnorm = P.l2 ? sqrt(b2) : bmax;
+
+    // ---- rescaling (reference rescale_problem, src/preconditioner.c:654-713):
+    // cumulative factors in FP64, computed from the original FP64 entries ------
+    for (int j = t; j < n; j += GROUP)
+        vr[j] = 1.0;
+    for (int i = t; i < m; i += GROUP)
+        cr[i] = 1.0;
+    g.sync();
+    // Ruiz (max) passes, then one Pock-Chambolle (power-sum) pass; each pass
+    // takes both factors from the same scaled matrix, then applies them.  The
+    // new factors are parked in the still unused float vector areas.
+    double *fr = (double *)(sm + Lo.lc), *fcol = (double *)(sm + Lo.c);
+    for (int it = 0; it < P.ruiz_iters + (P.has_pc ? 1 : 0); ++it) {
+        const bool ruiz = it < P.ruiz_iters;
+        const double a_row = ruiz ? 0.0 : P.pc_alpha, a_col = ruiz ? 0.0 : 2.0 - P.pc_alpha;
+        for (int i = t; i < m; i += GROUP) {
+            double s = 0.0;
+            for (int k = Arp[i]; k < Arp[i + 1]; ++k) {
+                double a = fabs(Av[k]) / (cr[i] * vr[Aci[k]]);
+                s = ruiz ? fmax(s, a) : s + (a_row == 1.0 ? a : pow(a, a_row));
+            }
+            fr[i] = s < SCALE_EPS ? 1.0 : sqrt(s);
+        }
+        for (int j = t; j < n; j += GROUP) {
+            double s = 0.0;
+            for (int k = Atrp[j]; k < Atrp[j + 1]; ++k) {
+                double a = fabs(Atv[k]) / (cr[Atci[k]] * vr[j]);
+                s = ruiz ? fmax(s, a) : s + (a_col == 1.0 ? a : pow(a, a_col));
+            }
+            fcol[j] = s < SCALE_EPS ? 1.0 : sqrt(s);
+        }
+        g.sync();
+        for (int i = t; i < m; i += GROUP)
+            cr[i] *= fr[i];
+        for (int j = t; j < n; j += GROUP)
+            vr[j] *= fcol[j];
+        g.sync();
+    }
+    // bound / objective rescaling (reference bound_obj_rescaling, :602-652)
+    double sb = 1.0, sc = 1.0;
+    if (P.bound_obj) {
+        double bb2 = 0.0, cc2 = 0.0;
+        for (int i = t; i < m; i += GROUP) {
+            double lo = glc[i] / cr[i], up = guc[i] / cr[i];
+            if (isfinite(lo) && lo != up)
+                bb2 += lo * lo;
+            if (isfinite(up))
+                bb2 += up * up;
+        }
+        for (int j = t; j < n; j += GROUP) {
+            double v = gc[j] / vr[j];
+            cc2 += v * v;
+        }
+        bb2 = g.reduce(bb2, false, red);
+        cc2 = g.reduce(cc2, false, red);
+        sb = 1.0 / (sqrt(bb2) + 1.0);
+        sc = 1.0 / (sqrt(cc2) + 1.0);
+    }
+    // ---- scaled data in shared memory --------------------------------------
+    for (int i = t; i <= m; i += GROUP)
+        arp[i] = Arp[i];
+    for (int j = t; j <= n; j += GROUP)
+        atrp[j] = Atrp[j];
+    for (int k = t; k < nnz; k += GROUP) {
+        aci[k] = (unsigned short)Aci[k];
+        atci[k] = (unsigned short)Atci[k];
+    }
+    g.sync();
+    for (int i = t; i < m; i += GROUP)
+        for (int k = arp[i]; k < arp[i + 1]; ++k)
+            av[k] = (float)(Av[k] / (cr[i] * vr[aci[k]]));
+    for (int j = t; j < n; j += GROUP)
+        for (int k = atrp[j]; k < atrp[j + 1]; ++k)
+            atv[k] = (float)(Atv[k] / (vr[j] * cr[atci[k]]));
+    for (int j = t; j < n; j += GROUP) {
+        const double vj = vr[j];
+        c[j] = (float)(gc[j] / vj * sc);
+        l[j] = (float)(gl[j] * vj * sb);
+        u[j] = (float)(gu[j] * vj * sb);
+        q[j] = hasq ? (float)(gq[j] / (vj * vj) * (sc / sb) + 1e-12) : 0.0f;
+        const float x00 = (float)clampd((double)l[j], 0.0, (double)u[j]);
+        x0[j] = x[j] = xp[j] = xr[j] = x00;
+        dx[j] = ds[j] = 0.0f;
+    }
+    for (int i = t; i < m; i += GROUP) {
+        lc[i] = (float)(glc[i] / cr[i] * sb);
+        uc[i] = (float)(guc[i] / cr[i] * sb);
+        y0[i] = y[i] = yp[i] = dy[i] = 0.0f;
+    }
+    g.sync();
+
+    // ---- step size: power method on A A^T (reference
+    // estimate_maximum_singular_value, src/pdhg_core_op.cu:1673-1788) ----------
+    double step = 1.0;
+    if (nnz > 0) {
+        float *v = yp, *nv = dy, *dp = xr; // scratch, reset below
+        double a = 0.0;
+        for (int i = t; i < m; i += GROUP) {
+            v[i] = (float)D.v0[i];
+            a += D.v0[i] * D.v0[i];
+        }
+        a = g.reduce(a, false, red);
+        double inv = 1.0 / sqrt(a);
+        for (int i = t; i < m; i += GROUP)
+            v[i] = (float)((double)v[i] * inv);
+        g.sync();
+        double s2 = 1.0;
+        for (int it = 0; it < P.sv_max_iter; ++it) {
+            for (int j = t; j < n; j += GROUP) {
+                double s = 0.0;
+                for (int k = atrp[j]; k < atrp[j + 1]; ++k)
+                    s += (double)atv[k] * (double)v[atci[k]];
+                dp[j] = (float)s;
+            }
+            g.sync();
+            a = 0.0;
+            for (int i = t; i < m; i += GROUP) {
+                double s = 0.0;
+                for (int k = arp[i]; k < arp[i + 1]; ++k)
+                    s += (double)av[k] * (double)dp[aci[k]];
+                nv[i] = (float)s;
+                a += s * (double)v[i];
+            }
+            s2 = g.reduce(a, false, red);
+            a = 0.0;
+            for (int i = t; i < m; i += GROUP) {
+                double r = (double)nv[i] - s2 * (double)v[i];
+                a += r * r;
+            }
+            a = g.reduce(a, false, red);
+            if (sqrt(a) < P.sv_tol)
+                break;
+            a = 0.0;
+            for (int i = t; i < m; i += GROUP)
+                a += (double)nv[i] * (double)nv[i];
+            a = g.reduce(a, false, red);
+            inv = 1.0 / sqrt(a);
+            for (int i = t; i < m; i += GROUP)
+                v[i] = (float)((double)nv[i] * inv);
+            g.sync();
+        }
+        double sv = sqrt(s2);
+        step = sv < 1e-12 ? 1.0 : 0.998 / sv;
+        for (int i = t; i < m; i += GROUP)
+            yp[i] = dy[i] = 0.0f;
+        for (int j = t; j < n; j += GROUP)
+            xr[j] = x0[j];
+        g.sync();
+    }
+    double omega = P.bound_obj ? 1.0 : (cnorm + 1.0) / (bnorm + 1.0);
+    double best_omega = omega, best_gap = INFINITY, pw_sum = 0.0, pw_last = 0.0;
+    double fpe = 0.0, fpe0 = 0.0, fpe_last = INFINITY;
+    double rel_p = INFINITY, rel_d = INFINITY, rel_gap = INFINITY, abs_p = 0, abs_d = 0, pobj = 0, dobj = 0, gap = 0;
+    double dist_x = 0.0, dist_y = 0.0;
+    int k = 0, inner = 0, status = TERMINATION_REASON_UNSPECIFIED;
+    bool is_major = false, do_restart = false;
+
+    // residual evaluation (compute_residual for LP / diagonal Q without cones)
+    auto evaluate = [&](bool want_dist) {
+        const double tau = step / omega;
+        double pr = 0.0, pslack = 0.0, dy2 = 0.0;
+        for (int i = t; i < m; i += GROUP) {
+            double s = 0.0;
+            for (int kk = arp[i]; kk < arp[i + 1]; ++kk)
+                s += (double)av[kk] * (double)xp[aci[kk]];
+            double proj = clampd((double)lc[i], s, (double)uc[i]);
+            pr = P.l2 ? pr + nterm((s - proj) * cr[i], 1) : fmax(pr, nterm((s - proj) * cr[i], 0));
+            double yv = yp[i];
+            double lo = lc[i], up = uc[i];
+            pslack += fmax(yv, 0.0) * (isfinite(lo) ? lo : 0.0) + fmin(yv, 0.0) * (isfinite(up) ? up : 0.0);
+            if (want_dist) {
+                double d = yv - (double)y0[i];
+                dy2 += d * d;
+            }
+        }
+        double dr = 0.0, cx = 0.0, xqx = 0.0, sx = 0.0, qn = 0.0, an = 0.0, dx2 = 0.0;
+        for (int j = t; j < n; j += GROUP) {
+            double s = 0.0;
+            for (int kk = atrp[j]; kk < atrp[j + 1]; ++kk)
+                s += (double)atv[kk] * (double)yp[atci[kk]];
+            double xv = xp[j], qx = hasq ? (double)q[j] * xv : 0.0;
+            double dsl, drr;
+            if (!hasq) {
+                dsl = ds[j];
+                drr = ((double)c[j] - s - dsl) * vr[j];
+            } else {
+                double gr = qx + (double)c[j] - s;
+                double tt = xv - tau * gr;
+                double p = fmax((double)l[j], fmin((double)u[j], tt));
+                dsl = (p - tt) / tau;
+                drr = (gr - dsl) * vr[j];
+            }
+            dr = P.l2 ? dr + nterm(drr, 1) : fmax(dr, nterm(drr, 0));
+            cx += (double)c[j] * xv;
+            xqx += xv * qx;
+            sx += dsl * xv;
+            qn = P.l2 ? qn + nterm(qx * vr[j], 1) : fmax(qn, nterm(qx * vr[j], 0));
+            an = P.l2 ? an + nterm(s * vr[j], 1) : fmax(an, nterm(s * vr[j], 0));
+            if (want_dist) {
+                double d = xv - (double)x0[j];
+                dx2 += d * d;
+            }
+        }
+        const bool L2 = P.l2 != 0;
+        pr = g.reduce(pr, !L2, red);
+        dr = g.reduce(dr, !L2, red);
+        qn = g.reduce(qn, !L2, red);
+        an = g.reduce(an, !L2, red);
+        pslack = g.reduce(pslack, false, red);
+        cx = g.reduce(cx, false, red);
+        xqx = g.reduce(xqx, false, red);
+        sx = g.reduce(sx, false, red);
+        dx2 = g.reduce(dx2, false, red);
+        dy2 = g.reduce(dy2, false, red);
+        auto nrm = [&](double v) { return L2 ? sqrt(v) : v; };
+        abs_p = nrm(pr) / sb;
+        abs_d = nrm(dr) / sc;
+        double hq = hasq ? 0.5 * xqx : 0.0;
+        pobj = (cx + hq) / (sb * sc) + I.obj_const;
+        dobj = (sx + pslack - hq) / (sb * sc) + I.obj_const;
+        rel_p = abs_p / (1.0 + bnorm);
+        double den = hasq ? 1.0 + fmax(cnorm, fmax(nrm(qn) / sc, nrm(an) / sc)) : 1.0 + cnorm;
+        rel_d = abs_d / den;
+        gap = fabs(pobj - dobj);
+        rel_gap = gap / (1.0 + fabs(pobj) + fabs(dobj));
+        dist_x = sqrt(dx2);
+        dist_y = sqrt(dy2);
+    };
+
+    // fixed-point error of the last step (compute_fixed_point_error)
+    auto fixed_point_error = [&]() {
+        double p2 = 0.0, d2 = 0.0, cross = 0.0;
+        for (int j = t; j < n; j += GROUP) {
+            double s = 0.0;
+            for (int kk = atrp[j]; kk < atrp[j + 1]; ++kk)
+                s += (double)atv[kk] * (double)dy[atci[kk]];
+            double d = dx[j];
+            p2 += d * d;
+            cross += s * d;
+        }
+        for (int i = t; i < m; i += GROUP) {
+            double d = dy[i];
+            d2 += d * d;
+        }
+        p2 = g.reduce(p2, false, red);
+        d2 = g.reduce(d2, false, red);
+        cross = g.reduce(cross, false, red);
+        double mv = p2 * omega + d2 / omega;
+        return sqrt(mv + 2.0 * step * cross);
+    };
+
+    while (k < P.iter_limit) {
+        if (is_major || k == 0 || (k % print_freq(k)) == 0) {
+            evaluate(is_major || k == 0);
+            // elapsed time from thread 0's clock, made uniform by the reduction
+            const double el = g.reduce(t == 0 ? gtimer_ns() - t_start : 0.0, true, red);
+            if (rel_d < P.eps_feas && rel_p < P.eps_feas && rel_gap < P.eps_opt) {
+                status = TERMINATION_REASON_OPTIMAL;
+                break;
+            }
+            if (el >= P.time_limit_ns) {
+                status = TERMINATION_REASON_TIME_LIMIT;
+                break;
+            }
+        }
+        if (is_major || k == 0) {
+            do_restart = false;
+            if (k == P.freq)
+                do_restart = true;
+            else if (k > P.freq) {
+                if (fpe <= P.suff * fpe0)
+                    do_restart = true;
+                if (fpe <= P.nec * fpe0 && fpe > fpe_last)
+                    do_restart = true;
+                if (inner >= P.artificial * k)
+                    do_restart = true;
+            }
+            fpe_last = fpe;
+            if (do_restart) {
+                double pd = dist_x, dd = dist_y, ratio = rel_d / rel_p;
+                if (pd > 1e-16 && dd > 1e-16 && pd < 1e12 && dd < 1e12 && ratio > 1e-8 && ratio < 1e8) {
+                    double err = log(dd) - log(pd) - log(omega);
+                    pw_sum = pw_sum * P.i_smooth + err;
+                    double derr = err - pw_last;
+                    omega *= exp(P.k_p * err + P.k_i * pw_sum + P.k_d * derr);
+                    pw_last = err;
+                } else {
+                    omega = best_omega;
+                    pw_sum = 0.0;
+                    pw_last = 0.0;
+                }
+                double gg = fabs(log10(rel_d / rel_p));
+                if (gg < best_gap) {
+                    best_gap = gg;
+                    best_omega = omega;
+                }
+                for (int j = t; j < n; j += GROUP)
+                    x0[j] = x[j] = xp[j];
+                for (int i = t; i < m; i += GROUP)
+                    y0[i] = y[i] = yp[i];
+                g.sync();
+                inner = 0;
+                fpe_last = INFINITY;
+            }
+        }
+        is_major = ((k + 1) % P.freq) == 0;
+        const bool want_fpe = is_major || do_restart;
+        const double w = (double)(inner + 1) / (double)(inner + 2);
+        const double tau = step / omega, sigma = step * omega;
+        // primal step (reference pdhg_update + halpern_update)
+        for (int j = t; j < n; j += GROUP) {
+            double s = 0.0;
+            for (int kk = atrp[j]; kk < atrp[j + 1]; ++kk)
+                s += (double)atv[kk] * (double)y[atci[kk]];
+            double xi = x[j];
+            double tt = xi - tau * ((double)c[j] - s);
+            if (hasq)
+                tt /= (1.0 + tau * (double)q[j]);
+            double p = clampd((double)l[j], tt, (double)u[j]);
+            double xrr = 2.0 * p - xi;
+            xp[j] = (float)p;
+            xr[j] = (float)xrr;
+            if (!hasq)
+                ds[j] = (float)((p - tt) / tau);
+            dx[j] = (float)(xrr - xi);
+            double refl = P.rho * xrr + (1.0 - P.rho) * xi;
+            x[j] = (float)(w * refl + (1.0 - w) * (double)x0[j]);
+        }
+        g.sync();
+        for (int i = t; i < m; i += GROUP) {
+            double s = 0.0;
+            for (int kk = arp[i]; kk < arp[i + 1]; ++kk)
+                s += (double)av[kk] * (double)xr[aci[kk]];
+            double yi = y[i];
+            double pr = clampd((double)lc[i], s - yi / sigma, (double)uc[i]);
+            double yn = yi - sigma * s + sigma * pr;
+            double yrr = 2.0 * yn - yi;
+            yp[i] = (float)yn;
+            dy[i] = (float)(yrr - yi);
+            double refl = P.rho * yrr + (1.0 - P.rho) * yi;
+            y[i] = (float)(w * refl + (1.0 - w) * (double)y0[i]);
+        }
+        g.sync();
+        if (want_fpe) {
+            fpe = fixed_point_error();
+            if (do_restart) {
+                fpe0 = fpe;
+                do_restart = false;
+            }
+        }
+        ++inner;
+        ++k;
+    }
+    if (status == TERMINATION_REASON_UNSPECIFIED) {
+        status = TERMINATION_REASON_ITERATION_LIMIT;
+        evaluate(false);
+    }
+    // unscaled solution (reference rescale_solution)
+    for (int j = t; j < n; j += GROUP)
+        D.x_out[I.x_off + j] = (double)xp[j] / vr[j] / sb;
+    for (int i = t; i < m; i += GROUP)
+        D.y_out[I.y_off + i] = (double)yp[i] / cr[i] / sc;
+    if (t == 0) {
+        double *st = D.stats + (size_t)idx * BS_COUNT;
+        st[BS_STATUS] = status;
+        st[BS_ITERS] = k;
+        st[BS_POBJ] = pobj;
+        st[BS_DOBJ] = dobj;
+        st[BS_ABS_P] = abs_p;
+        st[BS_ABS_D] = abs_d;
+        st[BS_REL_P] = rel_p;
+        st[BS_REL_D] = rel_d;
+        st[BS_GAP] = gap;
+        st[BS_REL_GAP] = rel_gap;
+    }
+    g.sync();
+}
+
+template <int BT, int GROUP>
+__global__ void __launch_bounds__(BT) batch_kernel(BData D, BParams P, int smem_per_group)
+{
+    extern __shared__ __align__(16) char smem[];
+    __shared__ int s_idx[BT / GROUP];
+    Grp<BT, GROUP> g;
+    char *sm = smem + (size_t)g.id * smem_per_group;
+    for (;;) {
+        if (g.t == 0)
+            s_idx[g.id] = atomicAdd(D.next, 1);
+        g.sync();
+        const int w = s_idx[g.id];
+        g.sync();
+        if (w >= D.count)
+            break;
+        solve_instance<BT, GROUP>(D, P, D.order[w], sm, g);
+    }
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+namespace {
+
+#define BCK(call)                                                                                                      \
+    do {                                                                                                               \
+        cudaError_t e_ = (call);                                                                                       \
+        if (e_ != cudaSuccess) {                                                                                       \
+            std::fprintf(stderr, "[pdhcg_b200_solve_batch] %s: %s\n", #call, cudaGetErrorString(e_));                 \
+            return -1;                                                                                                 \
+        }                                                                                                              \
+    } while (0)
+
+struct DevBuf { // device allocations of one batch solve
+    std::vector<void *> p;
+    template <typename T>
+    T *up(const std::vector<T> &h)
+    {
+        void *d = nullptr;
+        if (cudaMalloc(&d, std::max<size_t>(h.size(), 1) * sizeof(T)) != cudaSuccess)
+            return nullptr;
+        p.push_back(d);
+        if (!h.empty() && cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+            return nullptr;
+        return (T *)d;
+    }
+    template <typename T>
+    T *zeros(size_t k)
+    {
+        void *d = nullptr;
+        if (cudaMalloc(&d, std::max<size_t>(k, 1) * sizeof(T)) != cudaSuccess)
+            return nullptr;
+        p.push_back(d);
+        if (cudaMemset(d, 0, std::max<size_t>(k, 1) * sizeof(T)) != cudaSuccess)
+            return nullptr;
+        return (T *)d;
+    }
+    ~DevBuf()
+    {
+        for (void *q : p)
+            cudaFree(q);
+    }
+};
+
+// A launch shape: threads per CTA, threads per instance group.
+struct Shape {
+    int bt, group;
+};
+const Shape SHAPES[] = {{128, 32}, {256, 64}, {256, 128}, {256, 256}, {512, 512}};
+constexpr int NSHAPES = sizeof(SHAPES) / sizeof(SHAPES[0]);
+
+template <int BT, int GROUP>
+cudaError_t launch_shape(const BData &D, const BParams &P, int smem_group, int sms, cudaStream_t s)
+{
+    constexpr int G = BT / GROUP;
+    size_t smem = (size_t)smem_group * G;
+    auto kern = batch_kernel<BT, GROUP>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT, smem);
+    if (e != cudaSuccess)
+        return e;
+    if (per_sm < 1)
+        return cudaErrorInvalidConfiguration;
+    int groups = (D.count + G - 1) / G;
+    int grid = std::max(1, std::min(groups, sms * per_sm));
+    kern<<<grid, BT, smem, s>>>(D, P, smem_group);
+    return cudaGetLastError();
+}
+
+cudaError_t launch(int shape, const BData &D, const BParams &P, int smem_group, int sms, cudaStream_t s)
+{
+    switch (shape) {
+    case 0: return launch_shape<128, 32>(D, P, smem_group, sms, s);
+    case 1: return launch_shape<256, 64>(D, P, smem_group, sms, s);
+    case 2: return launch_shape<256, 128>(D, P, smem_group, sms, s);
+    case 3: return launch_shape<256, 256>(D, P, smem_group, sms, s);
+    default: return launch_shape<512, 512>(D, P, smem_group, sms, s);
+    }
+}
+
+// Q diagonal-only?  (the batch supports LP and diagonal Q; reference
+// detect_q_type, src/utils.cu:834-885)
+bool diag_q(const qp_problem_t *p, std::vector<double> &q)
+{
+    q.assign(p->num_variables, 0.0);
+    if (p->num_rank_lowrank_obj > 0 && p->objective_lowrank_matrix_num_nonzeros > 0)
+        return false;
+    if (!p->objective_sparse_matrix || p->objective_sparse_matrix_num_nonzeros == 0)
+        return true;
+    const CsrComponent *Q = p->objective_sparse_matrix;
+    for (int r = 0; r < p->num_variables; ++r)
+        for (int k = Q->row_ptr[r]; k < Q->row_ptr[r + 1]; ++k) {
+            if (Q->col_ind[k] != r && Q->val[k] != 0.0)
+                return false;
+            if (Q->col_ind[k] == r)
+                q[r] += Q->val[k];
+        }
+    return true;
+}
+
+// smallest-group shape that holds the class's largest instance
+int default_shape(int max_smem, int max_dim)
+{
+    const int cap = SMEM_CAP;
+    int want = max_dim <= 256 ? 32 : (max_dim <= 1024 ? 128 : 256);
+    for (int sh = 0; sh < NSHAPES; ++sh) {
+        if (SHAPES[sh].group < want)
+            continue;
+        if ((long long)max_smem * (SHAPES[sh].bt / SHAPES[sh].group) <= cap)
+            return sh;
+    }
+    return (long long)max_smem <= cap ? NSHAPES - 1 : -1;
+}
+
+} // namespace
+
+extern "C" void pdhcg_b200_default_batch_options(pdhcg_b200_batch_options_t *o)
+{
+    std::memset(o, 0, sizeof(*o));
+    o->shape = -1;
+}
+
+extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *probs, const pdhg_parameters_t *params,
+                                      const pdhcg_b200_batch_options_t *opts, pdhcg_result_t **results)
+{
+    if (count < 0 || (count > 0 && (!probs || !results))) {
+        std::fprintf(stderr, "[pdhcg_b200_solve_batch] invalid arguments.\n");
+        return -1;
+    }
+    pdhcg_b200_batch_options_t o;
+    if (opts)
+        o = *opts;
+    else
+        pdhcg_b200_default_batch_options(&o);
+    pdhg_parameters_t prm;
+    if (params)
+        prm = *params;
+    else
+        set_default_parameters(&prm);
+    for (int i = 0; i < count; ++i)
+        results[i] = nullptr;
+    if (count == 0)
+        return 0;
+    auto t0 = std::chrono::steady_clock::now();
+    // ---- pack -------------------------------------------------------------
+    std::vector<int> A_rp, A_ci, At_rp, At_ci, batched;
+    std::vector<double> A_v, At_v, c, l, u, q, lc, uc;
+    std::vector<BInst> inst;
+    std::vector<int> fallback;
+    int max_m = 1;
+    std::vector<double> qd;
+    for (int i = 0; i < count; ++i) {
+        const qp_problem_t *p = probs[i];
+        if (!p) {
+            std::fprintf(stderr, "[pdhcg_b200_solve_batch] problem %d is NULL.\n", i);
+            return -1;
+        }
+        const int n = p->num_variables, m = p->num_constraints;
+        bool ok = n > 0 && m > 0 && n < 65536 && m < 65536 && p->cones.num_cones == 0 &&
+                  p->affine_cones.num_cones == 0 && p->constraint_matrix && diag_q(p, qd);
+        BInst b{};
+        if (ok) {
+            const CsrComponent *A = p->constraint_matrix;
+            const int nnz = A->row_ptr[m];
+            Layout Lo(n, m, nnz);
+            ok = Lo.total <= SMEM_CAP;
+            b.smem = Lo.total;
+        }
+        if (!ok) { // solved on its own by the single-instance path
+            fallback.push_back(i);
+            continue;
+        }
+        const CsrComponent *A = p->constraint_matrix;
+        const int nnz = A->row_ptr[m];
+        b.n = n;
+        b.m = m;
+        b.rp_off = (long long)A_rp.size();
+        b.trp_off = (long long)At_rp.size();
+        b.k_off = (long long)A_ci.size();
+        b.x_off = (long long)c.size();
+        b.y_off = (long long)lc.size();
+        b.qmode = (p->objective_sparse_matrix && p->objective_sparse_matrix_num_nonzeros > 0) ? 1 : 0;
+        b.obj_const = p->objective_constant;
+        for (int r = 0; r <= m; ++r)
+            A_rp.push_back(A->row_ptr[r]);
+        for (int k = 0; k < nnz; ++k) {
+            A_ci.push_back(A->col_ind[k]);
+            A_v.push_back(A->val[k]);
+        }
+        // A^T by counting sort (entries of each column in increasing row order)
+        std::vector<int> trp(n + 1, 0), tci(nnz);
+        std::vector<double> tv(nnz);
+        for (int k = 0; k < nnz; ++k)
+            trp[A->col_ind[k] + 1]++;
+        for (int j = 0; j < n; ++j)
+            trp[j + 1] += trp[j];
+        std::vector<int> pos(trp.begin(), trp.end() - 1);
+        for (int r = 0; r < m; ++r)
+            for (int k = A->row_ptr[r]; k < A->row_ptr[r + 1]; ++k) {
+                int d = pos[A->col_ind[k]]++;
+                tci[d] = r;
+                tv[d] = A->val[k];
+            }
+        At_rp.insert(At_rp.end(), trp.begin(), trp.end());
+        At_ci.insert(At_ci.end(), tci.begin(), tci.end());
+        At_v.insert(At_v.end(), tv.begin(), tv.end());
+        for (int j = 0; j < n; ++j) {
+            c.push_back(p->objective_vector ? p->objective_vector[j] : 0.0);
+            l.push_back(p->variable_lower_bound[j]);
+            u.push_back(p->variable_upper_bound[j]);
+            q.push_back(qd[j]);
+        }
+        for (int r = 0; r < m; ++r) {
+            lc.push_back(p->constraint_lower_bound[r]);
+            uc.push_back(p->constraint_upper_bound[r]);
+        }
+        max_m = std::max(max_m, m);
+        inst.push_back(b);
+        batched.push_back(i);
+    }
+    const int nb = (int)inst.size();
+    // power-method start vector (reference: rand_r with seed 1234 in [-1, 1])
+    std::vector<double> v0(max_m);
+    unsigned int seed = 1234;
+    for (int i = 0; i < max_m; ++i)
+        v0[i] = ((double)rand_r(&seed) / (double)RAND_MAX) * 2.0 - 1.0;
+    BParams P{};
+    P.eps_opt = prm.termination_criteria.eps_optimal_relative;
+    P.eps_feas = prm.termination_criteria.eps_feasible_relative;
+    P.time_limit_ns = prm.termination_criteria.time_sec_limit * 1e9;
+    P.iter_limit = prm.termination_criteria.iteration_limit;
+    P.freq = prm.termination_evaluation_frequency > 0 ? prm.termination_evaluation_frequency : 200;
+    P.l2 = prm.optimality_norm == NORM_TYPE_L2;
+    P.ruiz_iters = prm.l_inf_ruiz_iterations;
+    P.has_pc = prm.has_pock_chambolle_alpha;
+    P.pc_alpha = prm.pock_chambolle_alpha;
+    P.bound_obj = prm.bound_objective_rescaling;
+    P.sv_max_iter = prm.sv_max_iter;
+    P.sv_tol = prm.sv_tol;
+    P.rho = prm.reflection_coefficient;
+    P.suff = prm.restart_params.sufficient_reduction_for_restart;
+    P.nec = prm.restart_params.necessary_reduction_for_restart;
+    P.artificial = prm.restart_params.artificial_restart_threshold;
+    P.i_smooth = prm.restart_params.i_smooth;
+    P.k_p = prm.restart_params.k_p;
+    P.k_i = prm.restart_params.k_i;
+    P.k_d = prm.restart_params.k_d;
+
+    std::vector<double> xo(c.size()), yo(lc.size()), st((size_t)std::max(nb, 1) * BS_COUNT);
+    double kernel_ms = 0.0;
+    if (nb > 0) {
+        // classes by size: instances sorted by shared-memory need, largest first;
+        // one launch per class of similar size
+        std::vector<int> order(nb);
+        for (int i = 0; i < nb; ++i)
+            order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return inst[a].smem > inst[b].smem; });
+        DevBuf B;
+        BData D{};
+        D.A_rp = B.up(A_rp);
+        D.A_ci = B.up(A_ci);
+        D.A_v = B.up(A_v);
+        D.At_rp = B.up(At_rp);
+        D.At_ci = B.up(At_ci);
+        D.At_v = B.up(At_v);
+        D.c = B.up(c);
+        D.l = B.up(l);
+        D.u = B.up(u);
+        D.q = B.up(q);
+        D.lc = B.up(lc);
+        D.uc = B.up(uc);
+        D.v0 = B.up(v0);
+        D.inst = B.up(inst);
+        D.x_out = B.zeros<double>(xo.size());
+        D.y_out = B.zeros<double>(yo.size());
+        D.stats = B.zeros<double>(st.size());
+        if (!D.A_rp || !D.A_ci || !D.A_v || !D.At_rp || !D.At_ci || !D.At_v || !D.c || !D.l || !D.u || !D.q ||
+            !D.lc || !D.uc || !D.v0 || !D.inst || !D.x_out || !D.y_out || !D.stats) {
+            std::fprintf(stderr, "[pdhcg_b200_solve_batch] device allocation or upload failed.\n");
+            return -1;
+        }
+        int dev = 0, sms = 0;
+        BCK(cudaGetDevice(&dev));
+        BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        // size classes: a new class starts when the need drops below half
+        std::vector<std::pair<int, int>> classes; // [begin, end) in order
+        for (int b = 0; b < nb;) {
+            int e = b + 1;
+            while (e < nb && inst[order[e]].smem * 2 > inst[order[b]].smem)
+                ++e;
+            classes.push_back({b, e});
+            b = e;
+        }
+        int *d_order = B.up(order);
+        int *d_next = B.zeros<int>(classes.size());
+        if (!d_order || !d_next)
+            return -1;
+        cudaEvent_t e0, e1;
+        BCK(cudaEventCreate(&e0));
+        BCK(cudaEventCreate(&e1));
+        BCK(cudaEventRecord(e0, 0));
+        for (size_t ci = 0; ci < classes.size(); ++ci) {
+            const int b = classes[ci].first, e = classes[ci].second;
+            int max_smem = 0, max_dim = 0;
+            for (int i = b; i < e; ++i) {
+                max_smem = std::max(max_smem, inst[order[i]].smem);
+                max_dim = std::max(max_dim, std::max(inst[order[i]].n, inst[order[i]].m));
+            }
+            int sh = o.shape >= 0 && o.shape < NSHAPES ? o.shape : default_shape(max_smem, max_dim);
+            if (sh < 0 || (long long)max_smem * (SHAPES[sh].bt / SHAPES[sh].group) > SMEM_CAP)
+                sh = default_shape(max_smem, max_dim);
+            BData Dc = D;
+            Dc.order = d_order + b;
+            Dc.count = e - b;
+            Dc.next = d_next + ci;
+            cudaError_t err = launch(sh, Dc, P, max_smem, sms, 0);
+            if (err != cudaSuccess) {
+                std::fprintf(stderr, "[pdhcg_b200_solve_batch] launch: %s\n", cudaGetErrorString(err));
+                return -1;
+            }
+        }
+        BCK(cudaEventRecord(e1, 0));
+        BCK(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        BCK(cudaEventElapsedTime(&ms, e0, e1));
+        kernel_ms = ms;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        BCK(cudaMemcpy(xo.data(), D.x_out, xo.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        BCK(cudaMemcpy(yo.data(), D.y_out, yo.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        BCK(cudaMemcpy(st.data(), D.stats, st.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    // ---- results ----------------------------------------------------------
+    for (int bi = 0; bi < nb; ++bi) {
+        const int i = batched[bi];
+        const qp_problem_t *p = probs[i];
+        const BInst &b = inst[bi];
+        const double *s = st.data() + (size_t)bi * BS_COUNT;
+        pdhcg_result_t *r = (pdhcg_result_t *)std::calloc(1, sizeof(pdhcg_result_t));
+        if (!r)
+            return -1;
+        r->num_variables = b.n;
+        r->num_constraints = b.m;
+        r->primal_solution = (double *)std::malloc(b.n * sizeof(double));
+        r->dual_solution = (double *)std::malloc(b.m * sizeof(double));
+        r->reduced_cost = (double *)std::malloc(b.n * sizeof(double));
+        std::memcpy(r->primal_solution, xo.data() + b.x_off, b.n * sizeof(double));
+        std::memcpy(r->dual_solution, yo.data() + b.y_off, b.m * sizeof(double));
+        // reduced cost c + Qx - A^T y, clamped on infinite bounds (reference
+        // compute_and_rescale_reduced_cost_qp_kernel)
+        for (int j = 0; j < b.n; ++j)
+            r->reduced_cost[j] = (p->objective_vector ? p->objective_vector[j] : 0.0) + q[b.x_off + j] * r->primal_solution[j];
+        const int *arp = A_rp.data() + b.rp_off;
+        for (int row = 0; row < b.m; ++row)
+            for (int k = arp[row]; k < arp[row + 1]; ++k)
+                r->reduced_cost[A_ci[b.k_off + k]] -= A_v[b.k_off + k] * r->dual_solution[row];
+        for (int j = 0; j < b.n; ++j) {
+            if (!std::isfinite(p->variable_lower_bound[j]))
+                r->reduced_cost[j] = std::fmin(r->reduced_cost[j], 0.0);
+            if (!std::isfinite(p->variable_upper_bound[j]))
+                r->reduced_cost[j] = std::fmax(r->reduced_cost[j], 0.0);
+        }
+        r->termination_reason = (termination_reason_t)(int)s[BS_STATUS];
+        r->total_count = (int)s[BS_ITERS];
+        r->primal_objective_value = s[BS_POBJ];
+        r->dual_objective_value = s[BS_DOBJ];
+        r->absolute_primal_residual = s[BS_ABS_P];
+        r->absolute_dual_residual = s[BS_ABS_D];
+        r->relative_primal_residual = s[BS_REL_P];
+        r->relative_dual_residual = s[BS_REL_D];
+        r->objective_gap = s[BS_GAP];
+        r->relative_objective_gap = s[BS_REL_GAP];
+        r->cumulative_time_sec = kernel_ms * 1e-3;
+        results[i] = r;
+    }
+    for (int i : fallback) {
+        results[i] = solve_qp_problem(probs[i], &prm);
+        if (!results[i])
+            return -1;
+    }
+    (void)t0;
+    return 0;
+}
+
+extern "C" int pdhcg_b200_batch_autotune(int count, const qp_problem_t *const *probs, const pdhg_parameters_t *params,
+                                         pdhcg_b200_batch_options_t *opts, double *shape_ms)
+{
+    if (count <= 0 || !probs || !opts) {
+        std::fprintf(stderr, "[pdhcg_b200_batch_autotune] invalid arguments.\n");
+        return -1;
+    }
+    std::vector<pdhcg_result_t *> res(count);
+    double best = INFINITY;
+    int best_shape = -1;
+    for (int sh = 0; sh < NSHAPES; ++sh) {
+        pdhcg_b200_batch_options_t o = *opts;
+        o.shape = sh;
+        cudaDeviceSynchronize();
+        auto t0 = std::chrono::steady_clock::now();
+        int rc = pdhcg_b200_solve_batch(count, probs, params, &o, res.data());
+        double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        for (auto *r : res)
+            if (r)
+                pdhcg_result_free(r);
+        if (rc != 0)
+            return rc;
+        if (shape_ms)
+            shape_ms[sh] = ms;
+        if (ms < best) {
+            best = ms;
+            best_shape = sh;
+        }
+    }
+    opts->shape = best_shape;
+    return 0;
+}

@@ -210,3 +210,52 @@ def portfolio(seed: int = 3, scale: float = 1.0, rank: int = 100, sectors: int =
     Dm = CsrMatrix(k, k, np.arange(k + 1, dtype=np.int32), np.arange(k, dtype=np.int32), Dd)
     return Problem(c=c, A=CsrMatrix.from_scipy(A), con_lb=lo, con_ub=up, var_lb=lb, var_ub=ub, Q=Q,
                    R_dense=Rfull, D=Dm, cones=[Cone(CONE_ROTATED_SOC, n, k)])
+
+
+def mpc_qp(seed: int, horizon: int, nx: int = 8, nu: int = 4) -> Problem:
+    """One MPC-style QP: states x_1..x_T (nx each) and inputs u_0..u_{T-1}
+    (nu each), n = (nx + nu) T, dynamics rows x_{t+1} - A_t x_t - B_t u_t = 0
+    (the first block row carries A_0 x_0 as its right-hand side), so each
+    row has 1 + nx + nu nonzeros.  A_t = I + E_t with E_t entries
+    N(0, (0.3 / sqrt(nx))^2), rescaled to spectral radius <= 1 so a horizon
+    of 100 stays bounded; B_t entries N(0, 0.3^2); x_0 ~ N(0, I);
+    Q = diag U(0.1, 1); inputs in [-1, 1]; states free; c = 0."""
+    rng = np.random.default_rng(seed)
+    T = horizon
+    nxT, nuT = nx * T, nu * T
+    n = nxT + nuT
+    m = nxT
+    rows, cols, vals = [], [], []
+    b = np.zeros(m)
+    x0 = rng.standard_normal(nx)
+    for t in range(T):
+        At = np.eye(nx) + rng.standard_normal((nx, nx)) * (0.3 / np.sqrt(nx))
+        rad = np.max(np.abs(np.linalg.eigvals(At)))
+        if rad > 1.0:
+            At /= rad
+        Bt = rng.standard_normal((nx, nu)) * 0.3
+        r0 = t * nx
+        # + x_{t+1}
+        rows.append(r0 + np.arange(nx)); cols.append(t * nx + np.arange(nx)); vals.append(np.ones(nx))
+        if t == 0:
+            b[:nx] = At @ x0
+        else:
+            rr, cc = np.meshgrid(np.arange(nx), np.arange(nx), indexing="ij")
+            rows.append((r0 + rr).ravel()); cols.append(((t - 1) * nx + cc).ravel()); vals.append(-At.ravel())
+        rr, cc = np.meshgrid(np.arange(nx), np.arange(nu), indexing="ij")
+        rows.append((r0 + rr).ravel()); cols.append((nxT + t * nu + cc).ravel()); vals.append(-Bt.ravel())
+    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(m, n))
+    A.sort_indices()
+    q = rng.uniform(0.1, 1.0, n)
+    lb = np.concatenate([np.full(nxT, -np.inf), np.full(nuT, -1.0)])
+    ub = np.concatenate([np.full(nxT, np.inf), np.full(nuT, 1.0)])
+    Q = CsrMatrix(n, n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), q)
+    return Problem(c=np.zeros(n), A=CsrMatrix.from_scipy(A), con_lb=b, con_ub=b.copy(), var_lb=lb, var_ub=ub, Q=Q)
+
+
+def mpc_batch(seed: int = 4, count: int = 4096, tmin: int = 10, tmax: int = 100) -> list:
+    """`count` MPC QPs of uneven horizons T ~ U{tmin..tmax}, instance i seeded
+    by (seed, i)."""
+    rng = np.random.default_rng(seed)
+    horizons = rng.integers(tmin, tmax + 1, size=count)
+    return [mpc_qp(seed * 1000003 + i, int(horizons[i])) for i in range(count)]

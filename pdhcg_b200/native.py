@@ -34,6 +34,14 @@ class Stats(C.Structure):
                 ("total_ms", C.c_double), ("reserved", C.c_double * 2)]
 
 
+class BatchOptions(C.Structure):
+    """pdhcg_b200_batch_options_t (include/pdhcg_b200.h)."""
+    _fields_ = [("shape", C.c_int), ("reserved", C.c_int * 7)]
+
+
+BATCH_SHAPES = 5
+
+
 class StepArgs(C.Structure):
     """pdhcg_b200_step_t (include/pdhcg_b200.h); every pointer is a device address."""
     _fields_ = [("n", C.c_int), ("m", C.c_int),
@@ -59,7 +67,8 @@ EXPORTS = [
     "pdhcg_b200_default_options", "pdhcg_b200_solve", "pdhcg_b200_last_stats", "pdhcg_b200_csr_spmv",
     "pdhcg_b200_project_cones", "pdhcg_b200_pdhg_step", "pdhcg_b200_upload", "pdhcg_b200_solve_device",
     "pdhcg_b200_device_solution", "pdhcg_b200_device_problem_free", "pdhcg_b200_request_cancel",
-    "cone_block_length", "pdhcg_b200_project_cones_noalloc",
+    "cone_block_length", "pdhcg_b200_project_cones_noalloc", "pdhcg_b200_default_batch_options",
+    "pdhcg_b200_solve_batch", "pdhcg_b200_batch_autotune",
 ]
 
 
@@ -103,6 +112,14 @@ def load(build: bool = True) -> C.CDLL:
     lib.pdhcg_b200_device_solution.argtypes = [C.c_void_p, P(C.c_void_p), P(C.c_void_p), P(C.c_void_p)]
     lib.pdhcg_b200_device_problem_free.restype = None
     lib.pdhcg_b200_device_problem_free.argtypes = [C.c_void_p]
+    lib.pdhcg_b200_default_batch_options.restype = None
+    lib.pdhcg_b200_default_batch_options.argtypes = [P(BatchOptions)]
+    lib.pdhcg_b200_solve_batch.restype = C.c_int
+    lib.pdhcg_b200_solve_batch.argtypes = [C.c_int, P(P(capi.QpProblem)), P(capi.PdhgParameters), P(BatchOptions),
+                                           P(P(capi.PdhcgResult))]
+    lib.pdhcg_b200_batch_autotune.restype = C.c_int
+    lib.pdhcg_b200_batch_autotune.argtypes = [C.c_int, P(P(capi.QpProblem)), P(capi.PdhgParameters),
+                                              P(BatchOptions), P(C.c_double)]
     lib.pdhcg_b200_request_cancel.restype = None
     lib.pdhcg_b200_request_cancel.argtypes = [C.c_int]
     _LIB = lib
@@ -141,4 +158,31 @@ def solve(p: capi.Problem, params: dict | None = None, options: Options | None =
         lib.pdhcg_result_free(r)
     finally:
         lib.qp_problem_free(prob)
+    return out
+
+
+def solve_batch(problems, params: dict | None = None, shape: int = -1) -> list:
+    """Build every problem with create_qp_problem and solve them together with
+    pdhcg_b200_solve_batch; returns one result dict per problem."""
+    lib = load()
+    built = [capi.build(lib, p) for p in problems]
+    if any(not b[0] for b in built):
+        raise ValueError("create_qp_problem rejected a problem")
+    arr = (C.POINTER(capi.QpProblem) * len(built))(*[b[0] for b in built])
+    prm = capi.default_params(lib, **(params or {}))
+    opts = BatchOptions()
+    lib.pdhcg_b200_default_batch_options(C.byref(opts))
+    opts.shape = shape
+    res = (C.POINTER(capi.PdhcgResult) * len(built))()
+    try:
+        rc = lib.pdhcg_b200_solve_batch(len(built), arr, C.byref(prm), C.byref(opts), res)
+        if rc != 0:
+            raise RuntimeError("pdhcg_b200_solve_batch failed (see stderr)")
+        out = []
+        for p, r in zip(problems, res):
+            out.append(capi.result_dict(r, p.n, p.A.m))
+            lib.pdhcg_result_free(r)
+    finally:
+        for b in built:
+            lib.qp_problem_free(b[0])
     return out

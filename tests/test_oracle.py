@@ -127,3 +127,14 @@ def test_oracle_detects_infeasibility(lib, oracle, name):
     oracle.oracle_result_free(r)
     lib.qp_problem_free(prob)
     assert d["status"] == status
+
+
+def test_mpc_instances_have_the_batched_shape():
+    """MPC generator: n = 12 T, m = 8 T, 13 nonzeros per dynamics row
+    (5 in the first block row), inputs boxed, states free."""
+    from pdhcg_b200 import instances
+    for T in (10, 37, 100):
+        p = instances.mpc_qp(3, T)
+        assert p.n == 12 * T and p.A.m == 8 * T
+        assert p.A.nnz == 8 * (1 + 4) + 8 * (T - 1) * 13
+        assert np.all(p.var_lb[8 * T:] == -1.0) and np.all(np.isinf(p.var_lb[:8 * T]))
