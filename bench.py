@@ -249,6 +249,134 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+BATCH_METRIC = "batched instance throughput (instances/s) at 1e-5 KKT, vs sequential plain solves, 1 B200"
+BATCH_WORKLOAD = ("mpc_batch: 4096 MPC QPs, horizon T ~ U{10..100}, n = 12 T, m = 8 T, 13 nnz/row, "
+                  "diag Q ~ U(0.1, 1), inputs in [-1, 1], eps 1e-5")
+BATCH_EPS = 1e-5
+
+
+def _batch_params(lib):
+    return capi.default_params(lib, **{"termination_criteria.eps_optimal_relative": BATCH_EPS,
+                                       "termination_criteria.eps_feasible_relative": BATCH_EPS,
+                                       "termination_criteria.time_sec_limit": 600.0})
+
+
+def run_batch(args):
+    """The batched workload: all instances in pdhcg_b200_solve_batch (value:
+    kernel time, problem arrays already uploaded; e2e: the whole call from
+    host problems), against one solve_qp_problem per instance on a sample."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", init_method="env://")
+    lib = native.load()
+    count = max(1, int(4096 * args.scale))
+    # instances partition across ranks: rank r solves its own seeded share
+    probs = instances.mpc_batch(seed=4 + rank, count=count)
+    built = [capi.build(lib, p) for p in probs]
+    arr = (C.POINTER(capi.QpProblem) * count)(*[b[0] for b in built])
+    prm = _batch_params(lib)
+    opts = native.BatchOptions()
+    lib.pdhcg_b200_default_batch_options(C.byref(opts))
+    shape_ms = (C.c_double * native.BATCH_SHAPES)()
+    tune = min(count, 512)
+    if lib.pdhcg_b200_batch_autotune(tune, arr, C.byref(prm), C.byref(opts), shape_ms) != 0:
+        raise RuntimeError("batch autotune failed")
+    res = (C.POINTER(capi.PdhcgResult) * count)()
+    launches = [0]
+
+    def solve():
+        t0 = time.perf_counter()
+        if lib.pdhcg_b200_solve_batch(count, arr, C.byref(prm), C.byref(opts), res) != 0:
+            raise RuntimeError("batch solve failed")
+        wall = time.perf_counter() - t0
+        bst = native.BatchStats()
+        lib.pdhcg_b200_last_batch_stats(C.byref(bst))
+        kern = bst.kernel_ms * 1e-3
+        launches[0] += bst.launches
+        stat = {}
+        iters = 0
+        for r in res:
+            st = capi.TERMINATION_REASONS[r.contents.termination_reason]
+            stat[st] = stat.get(st, 0) + 1
+            iters += r.contents.total_count
+            lib.pdhcg_result_free(r)
+        return wall, kern, stat, iters / count
+
+    for _ in range(args.warmup):
+        solve()
+    launches[0] = 0
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    walls, kerns = [], []
+    for _ in range(args.steps):
+        if world > 1:
+            torch.distributed.barrier()
+        w, k, stat, mean_it = solve()
+        walls.append(w)
+        kerns.append(k)
+    clocks = sampler.stop()
+    wall, kern = max(walls), max(kerns)
+    if world > 1:
+        t = torch.tensor([wall, kern], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        wall, kern = t[0].item(), t[1].item()
+    # sequential plain solves (the reference's way: one solve_qp_problem per instance)
+    k_seq = min(16, count)
+    t0 = time.perf_counter()
+    for i in range(k_seq):
+        r = lib.solve_qp_problem(arr[i], C.byref(prm))
+        lib.pdhcg_result_free(r)
+    seq = k_seq / (time.perf_counter() - t0)
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    total = count * world
+    nnz = sum(p.A.nnz for p in probs)
+    line = {
+        "metric": BATCH_METRIC, "value": total / kern, "unit": "instances/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": kern * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": BATCH_WORKLOAD, "instances_per_gpu": count, "parallelism":
+                   "instances partitioned across ranks" if world > 1 else "single",
+                   "shape": int(opts.shape), "autotune_ms": list(shape_ms),
+                   "l2_flush": "not needed: each instance lives in shared memory for its whole solve",
+                   "inputs": "value: kernel time, problem arrays already on the device; e2e: the whole "
+                             "pdhcg_b200_solve_batch call from host problems"},
+        "statuses": stat, "mean_iterations": mean_it, "nnz_per_gpu": int(nnz),
+        "e2e": {"value": total / wall, "unit": "instances/s",
+                "h2d_bytes_per_step": int(sum(p.A.nnz * 24 + (p.A.m + 1) * 4 + (p.n + 1) * 4 + p.n * 32 +
+                                              p.A.m * 16 for p in probs)),
+                "d2h_bytes_per_step": int(sum(8 * (p.n + p.A.m) for p in probs))},
+        "sequential_plain_solves": {"value": seq, "unit": "instances/s", "sample": k_seq,
+                                    "call": "solve_qp_problem per instance"},
+        "speedup_vs_sequential": (total / wall) / (seq * world),
+        "gpu_launches": launches[0],
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        oracle = C.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
+        oracle.oracle_solve.restype = C.POINTER(capi.PdhcgResult)
+        oracle.oracle_solve.argtypes = [C.POINTER(capi.QpProblem), C.POINTER(capi.PdhgParameters)]
+        t0, done = time.perf_counter(), 0
+        while done < count and time.perf_counter() - t0 < 10.0:
+            r = oracle.oracle_solve(arr[done], C.byref(prm))
+            oracle.oracle_result_free(r)
+            done += 1
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": done / dt, "unit": "instances/s", "cores": 1, "kind": "port",
+                                "sample": f"oracle FP64 on the first {done} instances ({dt:.1f}s)"}
+    print(json.dumps(line))
+    for b in built:
+        lib.qp_problem_free(b[0])
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def run_reference(args):
     """The reference's own solver (built from its sources into oracle/_ref)
     on the same instance through its C API; falls back to the oracle port
@@ -304,9 +432,13 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = the benchmark size)")
     ap.add_argument("--iters", type=int, default=None, help="iteration cap (profiling only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="soc_qp", choices=["soc_qp", "mpc_batch"],
+                    help="soc_qp: the headline single-instance workload; mpc_batch: the batched workload")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "mpc_batch":
+        run_batch(args)
     else:
         run_ours(args)
 

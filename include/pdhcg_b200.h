@@ -121,6 +121,17 @@ typedef struct {
 void pdhcg_b200_default_batch_options(pdhcg_b200_batch_options_t *opts);
 int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *probs, const pdhg_parameters_t *params,
                            const pdhcg_b200_batch_options_t *opts, pdhcg_result_t **results);
+/* Figures of the last pdhcg_b200_solve_batch on the calling thread. */
+typedef struct {
+    double kernel_ms;   /* the batch kernels, first launch to last (CUDA events) */
+    double total_ms;    /* the whole call, wall clock */
+    int launches;       /* kernel launches (one per size class) */
+    int batched;        /* instances solved by the batch kernels */
+    int fallback;       /* instances handed to solve_qp_problem */
+    int reserved[5];
+} pdhcg_b200_batch_stats_t;
+int pdhcg_b200_last_batch_stats(pdhcg_b200_batch_stats_t *out);
+
 /* Times every launch shape on the given instances (solving them each time)
  * and stores the fastest in opts->shape; shape_ms (may be NULL) receives
  * PDHCG_B200_BATCH_SHAPES wall times in milliseconds. */

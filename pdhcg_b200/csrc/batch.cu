@@ -21,11 +21,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "pdhcg.h"
@@ -634,6 +636,30 @@ __global__ void __launch_bounds__(BT) batch_kernel(BData D, BParams P, int smem_
 // ---------------------------------------------------------------------------
 namespace {
 
+thread_local pdhcg_b200_batch_stats_t g_batch_stats;
+
+// f(0) .. f(count - 1) on up to hardware_concurrency host threads
+template <typename F>
+void parallel_for(int count, F &&f)
+{
+    int nt = (int)std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), 32u);
+    nt = std::min(nt, std::max(1, count / 16));
+    if (nt <= 1) {
+        for (int i = 0; i < count; ++i)
+            f(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([&]() {
+            for (int i; (i = next.fetch_add(1)) < count;)
+                f(i);
+        });
+    for (auto &th : pool)
+        th.join();
+}
+
 #define BCK(call)                                                                                                      \
     do {                                                                                                               \
         cudaError_t e_ = (call);                                                                                       \
@@ -777,82 +803,91 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
     if (count == 0)
         return 0;
     auto t0 = std::chrono::steady_clock::now();
-    // ---- pack -------------------------------------------------------------
-    std::vector<int> A_rp, A_ci, At_rp, At_ci, batched;
-    std::vector<double> A_v, At_v, c, l, u, q, lc, uc;
+    // ---- pack: a sizing pass, then every instance copied (and A transposed)
+    // by a pool of host threads into its slot of the packed arrays ----------
+    std::vector<int> batched, fallback;
     std::vector<BInst> inst;
-    std::vector<int> fallback;
+    long long tot_rp = 0, tot_trp = 0, tot_k = 0, tot_x = 0, tot_y = 0;
     int max_m = 1;
-    std::vector<double> qd;
-    for (int i = 0; i < count; ++i) {
-        const qp_problem_t *p = probs[i];
-        if (!p) {
-            std::fprintf(stderr, "[pdhcg_b200_solve_batch] problem %d is NULL.\n", i);
-            return -1;
+    {
+        std::vector<double> qd;
+        for (int i = 0; i < count; ++i) {
+            const qp_problem_t *p = probs[i];
+            if (!p) {
+                std::fprintf(stderr, "[pdhcg_b200_solve_batch] problem %d is NULL.\n", i);
+                return -1;
+            }
+            const int n = p->num_variables, m = p->num_constraints;
+            bool ok = n > 0 && m > 0 && n < 65536 && m < 65536 && p->cones.num_cones == 0 &&
+                      p->affine_cones.num_cones == 0 && p->constraint_matrix && diag_q(p, qd);
+            BInst b{};
+            int nnz = 0;
+            if (ok) {
+                nnz = p->constraint_matrix->row_ptr[m];
+                Layout Lo(n, m, nnz);
+                ok = Lo.total <= SMEM_CAP;
+                b.smem = Lo.total;
+            }
+            if (!ok) { // solved on its own by the single-instance path
+                fallback.push_back(i);
+                continue;
+            }
+            b.n = n;
+            b.m = m;
+            b.rp_off = tot_rp;
+            b.trp_off = tot_trp;
+            b.k_off = tot_k;
+            b.x_off = tot_x;
+            b.y_off = tot_y;
+            b.qmode = (p->objective_sparse_matrix && p->objective_sparse_matrix_num_nonzeros > 0) ? 1 : 0;
+            b.obj_const = p->objective_constant;
+            tot_rp += m + 1;
+            tot_trp += n + 1;
+            tot_k += nnz;
+            tot_x += n;
+            tot_y += m;
+            max_m = std::max(max_m, m);
+            inst.push_back(b);
+            batched.push_back(i);
         }
-        const int n = p->num_variables, m = p->num_constraints;
-        bool ok = n > 0 && m > 0 && n < 65536 && m < 65536 && p->cones.num_cones == 0 &&
-                  p->affine_cones.num_cones == 0 && p->constraint_matrix && diag_q(p, qd);
-        BInst b{};
-        if (ok) {
-            const CsrComponent *A = p->constraint_matrix;
-            const int nnz = A->row_ptr[m];
-            Layout Lo(n, m, nnz);
-            ok = Lo.total <= SMEM_CAP;
-            b.smem = Lo.total;
-        }
-        if (!ok) { // solved on its own by the single-instance path
-            fallback.push_back(i);
-            continue;
-        }
+    }
+    std::vector<int> A_rp(tot_rp), A_ci(tot_k), At_rp(tot_trp), At_ci(tot_k);
+    std::vector<double> A_v(tot_k), At_v(tot_k), c(tot_x), l(tot_x), u(tot_x), q(tot_x), lc(tot_y), uc(tot_y);
+    auto fill = [&](int bi) {
+        const qp_problem_t *p = probs[batched[bi]];
+        const BInst &b = inst[bi];
+        const int n = b.n, m = b.m;
         const CsrComponent *A = p->constraint_matrix;
         const int nnz = A->row_ptr[m];
-        b.n = n;
-        b.m = m;
-        b.rp_off = (long long)A_rp.size();
-        b.trp_off = (long long)At_rp.size();
-        b.k_off = (long long)A_ci.size();
-        b.x_off = (long long)c.size();
-        b.y_off = (long long)lc.size();
-        b.qmode = (p->objective_sparse_matrix && p->objective_sparse_matrix_num_nonzeros > 0) ? 1 : 0;
-        b.obj_const = p->objective_constant;
-        for (int r = 0; r <= m; ++r)
-            A_rp.push_back(A->row_ptr[r]);
-        for (int k = 0; k < nnz; ++k) {
-            A_ci.push_back(A->col_ind[k]);
-            A_v.push_back(A->val[k]);
-        }
+        std::memcpy(&A_rp[b.rp_off], A->row_ptr, (m + 1) * sizeof(int));
+        std::memcpy(&A_ci[b.k_off], A->col_ind, nnz * sizeof(int));
+        std::memcpy(&A_v[b.k_off], A->val, nnz * sizeof(double));
         // A^T by counting sort (entries of each column in increasing row order)
-        std::vector<int> trp(n + 1, 0), tci(nnz);
-        std::vector<double> tv(nnz);
+        int *trp = &At_rp[b.trp_off];
+        std::fill(trp, trp + n + 1, 0);
         for (int k = 0; k < nnz; ++k)
             trp[A->col_ind[k] + 1]++;
         for (int j = 0; j < n; ++j)
             trp[j + 1] += trp[j];
-        std::vector<int> pos(trp.begin(), trp.end() - 1);
+        std::vector<int> pos(trp, trp + n);
         for (int r = 0; r < m; ++r)
             for (int k = A->row_ptr[r]; k < A->row_ptr[r + 1]; ++k) {
                 int d = pos[A->col_ind[k]]++;
-                tci[d] = r;
-                tv[d] = A->val[k];
+                At_ci[b.k_off + d] = r;
+                At_v[b.k_off + d] = A->val[k];
             }
-        At_rp.insert(At_rp.end(), trp.begin(), trp.end());
-        At_ci.insert(At_ci.end(), tci.begin(), tci.end());
-        At_v.insert(At_v.end(), tv.begin(), tv.end());
+        std::vector<double> qd;
+        diag_q(p, qd);
         for (int j = 0; j < n; ++j) {
-            c.push_back(p->objective_vector ? p->objective_vector[j] : 0.0);
-            l.push_back(p->variable_lower_bound[j]);
-            u.push_back(p->variable_upper_bound[j]);
-            q.push_back(qd[j]);
+            c[b.x_off + j] = p->objective_vector ? p->objective_vector[j] : 0.0;
+            l[b.x_off + j] = p->variable_lower_bound[j];
+            u[b.x_off + j] = p->variable_upper_bound[j];
+            q[b.x_off + j] = qd[j];
         }
-        for (int r = 0; r < m; ++r) {
-            lc.push_back(p->constraint_lower_bound[r]);
-            uc.push_back(p->constraint_upper_bound[r]);
-        }
-        max_m = std::max(max_m, m);
-        inst.push_back(b);
-        batched.push_back(i);
-    }
+        std::memcpy(&lc[b.y_off], p->constraint_lower_bound, m * sizeof(double));
+        std::memcpy(&uc[b.y_off], p->constraint_upper_bound, m * sizeof(double));
+    };
+    parallel_for((int)inst.size(), fill);
     const int nb = (int)inst.size();
     // power-method start vector (reference: rand_r with seed 1234 in [-1, 1])
     std::vector<double> v0(max_m);
@@ -883,6 +918,7 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
 
     std::vector<double> xo(c.size()), yo(lc.size()), st((size_t)std::max(nb, 1) * BS_COUNT);
     double kernel_ms = 0.0;
+    int launches = 0;
     if (nb > 0) {
         // classes by size: instances sorted by shared-memory need, largest first;
         // one launch per class of similar size
@@ -949,6 +985,7 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
             Dc.count = e - b;
             Dc.next = d_next + ci;
             cudaError_t err = launch(sh, Dc, P, max_smem, sms, 0);
+            ++launches;
             if (err != cudaSuccess) {
                 std::fprintf(stderr, "[pdhcg_b200_solve_batch] launch: %s\n", cudaGetErrorString(err));
                 return -1;
@@ -966,14 +1003,17 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
         BCK(cudaMemcpy(st.data(), D.stats, st.size() * sizeof(double), cudaMemcpyDeviceToHost));
     }
     // ---- results ----------------------------------------------------------
-    for (int bi = 0; bi < nb; ++bi) {
+    std::atomic<int> alloc_failed{0};
+    parallel_for(nb, [&](int bi) {
         const int i = batched[bi];
         const qp_problem_t *p = probs[i];
         const BInst &b = inst[bi];
         const double *s = st.data() + (size_t)bi * BS_COUNT;
         pdhcg_result_t *r = (pdhcg_result_t *)std::calloc(1, sizeof(pdhcg_result_t));
-        if (!r)
-            return -1;
+        if (!r) {
+            alloc_failed = 1;
+            return;
+        }
         r->num_variables = b.n;
         r->num_constraints = b.m;
         r->primal_solution = (double *)std::malloc(b.n * sizeof(double));
@@ -1007,13 +1047,34 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
         r->relative_objective_gap = s[BS_REL_GAP];
         r->cumulative_time_sec = kernel_ms * 1e-3;
         results[i] = r;
+    });
+    if (alloc_failed) {
+        for (int i = 0; i < count; ++i)
+            if (results[i]) {
+                pdhcg_result_free(results[i]);
+                results[i] = nullptr;
+            }
+        return -1;
     }
     for (int i : fallback) {
         results[i] = solve_qp_problem(probs[i], &prm);
         if (!results[i])
             return -1;
     }
-    (void)t0;
+    std::memset(&g_batch_stats, 0, sizeof(g_batch_stats));
+    g_batch_stats.kernel_ms = kernel_ms;
+    g_batch_stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    g_batch_stats.launches = launches;
+    g_batch_stats.batched = nb;
+    g_batch_stats.fallback = (int)fallback.size();
+    return 0;
+}
+
+extern "C" int pdhcg_b200_last_batch_stats(pdhcg_b200_batch_stats_t *out)
+{
+    if (!out)
+        return -1;
+    *out = g_batch_stats;
     return 0;
 }
 

@@ -42,6 +42,12 @@ class BatchOptions(C.Structure):
 BATCH_SHAPES = 5
 
 
+class BatchStats(C.Structure):
+    """pdhcg_b200_batch_stats_t (include/pdhcg_b200.h)."""
+    _fields_ = [("kernel_ms", C.c_double), ("total_ms", C.c_double), ("launches", C.c_int), ("batched", C.c_int),
+                ("fallback", C.c_int), ("reserved", C.c_int * 5)]
+
+
 class StepArgs(C.Structure):
     """pdhcg_b200_step_t (include/pdhcg_b200.h); every pointer is a device address."""
     _fields_ = [("n", C.c_int), ("m", C.c_int),
@@ -68,7 +74,7 @@ EXPORTS = [
     "pdhcg_b200_project_cones", "pdhcg_b200_pdhg_step", "pdhcg_b200_upload", "pdhcg_b200_solve_device",
     "pdhcg_b200_device_solution", "pdhcg_b200_device_problem_free", "pdhcg_b200_request_cancel",
     "cone_block_length", "pdhcg_b200_project_cones_noalloc", "pdhcg_b200_default_batch_options",
-    "pdhcg_b200_solve_batch", "pdhcg_b200_batch_autotune",
+    "pdhcg_b200_solve_batch", "pdhcg_b200_batch_autotune", "pdhcg_b200_last_batch_stats",
 ]
 
 
@@ -120,6 +126,8 @@ def load(build: bool = True) -> C.CDLL:
     lib.pdhcg_b200_batch_autotune.restype = C.c_int
     lib.pdhcg_b200_batch_autotune.argtypes = [C.c_int, P(P(capi.QpProblem)), P(capi.PdhgParameters),
                                               P(BatchOptions), P(C.c_double)]
+    lib.pdhcg_b200_last_batch_stats.restype = C.c_int
+    lib.pdhcg_b200_last_batch_stats.argtypes = [P(BatchStats)]
     lib.pdhcg_b200_request_cancel.restype = None
     lib.pdhcg_b200_request_cancel.argtypes = [C.c_int]
     _LIB = lib
