@@ -78,7 +78,8 @@ typedef struct {
     double upload_ms;            /* allocation and host->device copies */
     double result_ms;            /* result kernel and device->host copies */
     double total_ms;             /* the whole call, wall clock */
-    double reserved[2];
+    double primal_weight;        /* primal weight at termination (a warm start for a similar solve) */
+    double reserved[1];
 } pdhcg_b200_stats_t;
 
 int pdhcg_b200_last_stats(pdhcg_b200_stats_t *out);
@@ -137,6 +138,36 @@ int pdhcg_b200_last_batch_stats(pdhcg_b200_batch_stats_t *out);
  * PDHCG_B200_BATCH_SHAPES wall times in milliseconds. */
 int pdhcg_b200_batch_autotune(int count, const qp_problem_t *const *probs, const pdhg_parameters_t *params,
                               pdhcg_b200_batch_options_t *opts, double *shape_ms);
+
+/* ---- learned warm start --------------------------------------------------------
+ * A small MLP from a parametric instance's parameters theta to a starting
+ * point and a primal weight (no counterpart in the reference):
+ *   h1 = relu(W1 theta + b1), h2 = relu(W2 h1 + b2)      (hidden)
+ *   z  = W3 h2 + b3                                       (rank: low-rank head)
+ *   o  = U z + bu                                         (out_dim, e.g. n + m)
+ *   lw = wp . h2 + bp                                     (log primal weight)
+ * BF16 weights in the products with FP32 accumulation, FP32 master weights
+ * updated by Adam.  Loss: mean over the batch and the outputs of (o - t)^2,
+ * plus the batch mean of (lw - t_lw)^2.  Host arrays are row-major FP32.
+ * Parameters are packed in the order W1, b1, W2, b2, W3, b3, U, bu, wp, bp,
+ * each weight [out_features x in_features] row-major. */
+typedef struct pdhcg_b200_mlp_s pdhcg_b200_mlp_t;
+
+pdhcg_b200_mlp_t *pdhcg_b200_mlp_create(int in_dim, int hidden, int rank, int out_dim, unsigned long long seed);
+void pdhcg_b200_mlp_free(pdhcg_b200_mlp_t *net);
+long long pdhcg_b200_mlp_num_params(const pdhcg_b200_mlp_t *net);
+int pdhcg_b200_mlp_get_params(const pdhcg_b200_mlp_t *net, float *params);
+int pdhcg_b200_mlp_set_params(pdhcg_b200_mlp_t *net, const float *params); /* also resets Adam */
+/* out: batch x out_dim; logw (may be NULL): batch */
+int pdhcg_b200_mlp_predict(pdhcg_b200_mlp_t *net, int batch, const float *theta, float *out, float *logw);
+/* loss of one batch and its gradient (packed order; grad may be NULL) */
+int pdhcg_b200_mlp_loss_grad(pdhcg_b200_mlp_t *net, int batch, const float *theta, const float *target,
+                             const float *target_logw, double *loss, float *grad);
+/* `epochs` passes of Adam over `count` samples in minibatches of `batch`
+ * (in order, the last partial batch dropped); loss receives the last
+ * epoch's mean minibatch loss. */
+int pdhcg_b200_mlp_train(pdhcg_b200_mlp_t *net, int count, const float *theta, const float *target,
+                         const float *target_logw, int epochs, int batch, float lr, double *loss);
 
 /* ---- kernel-level entry points on device pointers ------------------------
  * For parity tests and embedding.  Pointers are device memory of the current

@@ -1726,6 +1726,7 @@ pdhcg_result_t *Solve::run()
     double nnz = (double)A_.nnz;
     stats_.spmv_bytes = 2.0 * nnz * (8 + 4) + 4.0 * ((double)n_ + m_ + 2) + 8.0 * ((double)n_ + m_);
     stats_.step_bytes = stats_.step_kernel_launches > 0 ? step_bytes_sum_ / stats_.step_kernel_launches : 0.0;
+    stats_.primal_weight = omega_;
     g_last_stats = stats_;
     return r;
 }

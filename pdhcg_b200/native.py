@@ -31,7 +31,7 @@ class Stats(C.Structure):
                 ("iterations", C.c_int), ("fp32_iterations", C.c_int), ("restarts", C.c_int),
                 ("evaluations", C.c_int), ("step_bytes", C.c_double), ("spmv_bytes", C.c_double),
                 ("host_copy_ms", C.c_double), ("upload_ms", C.c_double), ("result_ms", C.c_double),
-                ("total_ms", C.c_double), ("reserved", C.c_double * 2)]
+                ("total_ms", C.c_double), ("primal_weight", C.c_double), ("reserved", C.c_double * 1)]
 
 
 class BatchOptions(C.Structure):
@@ -75,6 +75,8 @@ EXPORTS = [
     "pdhcg_b200_device_solution", "pdhcg_b200_device_problem_free", "pdhcg_b200_request_cancel",
     "cone_block_length", "pdhcg_b200_project_cones_noalloc", "pdhcg_b200_default_batch_options",
     "pdhcg_b200_solve_batch", "pdhcg_b200_batch_autotune", "pdhcg_b200_last_batch_stats",
+    "pdhcg_b200_mlp_create", "pdhcg_b200_mlp_free", "pdhcg_b200_mlp_num_params", "pdhcg_b200_mlp_get_params",
+    "pdhcg_b200_mlp_set_params", "pdhcg_b200_mlp_predict", "pdhcg_b200_mlp_loss_grad", "pdhcg_b200_mlp_train",
 ]
 
 
@@ -128,6 +130,24 @@ def load(build: bool = True) -> C.CDLL:
                                               P(BatchOptions), P(C.c_double)]
     lib.pdhcg_b200_last_batch_stats.restype = C.c_int
     lib.pdhcg_b200_last_batch_stats.argtypes = [P(BatchStats)]
+    fp = P(C.c_float)
+    lib.pdhcg_b200_mlp_create.restype = C.c_void_p
+    lib.pdhcg_b200_mlp_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong]
+    lib.pdhcg_b200_mlp_free.restype = None
+    lib.pdhcg_b200_mlp_free.argtypes = [C.c_void_p]
+    lib.pdhcg_b200_mlp_num_params.restype = C.c_longlong
+    lib.pdhcg_b200_mlp_num_params.argtypes = [C.c_void_p]
+    lib.pdhcg_b200_mlp_get_params.restype = C.c_int
+    lib.pdhcg_b200_mlp_get_params.argtypes = [C.c_void_p, fp]
+    lib.pdhcg_b200_mlp_set_params.restype = C.c_int
+    lib.pdhcg_b200_mlp_set_params.argtypes = [C.c_void_p, fp]
+    lib.pdhcg_b200_mlp_predict.restype = C.c_int
+    lib.pdhcg_b200_mlp_predict.argtypes = [C.c_void_p, C.c_int, fp, fp, fp]
+    lib.pdhcg_b200_mlp_loss_grad.restype = C.c_int
+    lib.pdhcg_b200_mlp_loss_grad.argtypes = [C.c_void_p, C.c_int, fp, fp, fp, P(C.c_double), fp]
+    lib.pdhcg_b200_mlp_train.restype = C.c_int
+    lib.pdhcg_b200_mlp_train.argtypes = [C.c_void_p, C.c_int, fp, fp, fp, C.c_int, C.c_int, C.c_float,
+                                         P(C.c_double)]
     lib.pdhcg_b200_request_cancel.restype = None
     lib.pdhcg_b200_request_cancel.argtypes = [C.c_int]
     _LIB = lib

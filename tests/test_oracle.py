@@ -138,3 +138,26 @@ def test_mpc_instances_have_the_batched_shape():
         assert p.n == 12 * T and p.A.m == 8 * T
         assert p.A.nnz == 8 * (1 + 4) + 8 * (T - 1) * 13
         assert np.all(p.var_lb[8 * T:] == -1.0) and np.all(np.isinf(p.var_lb[:8 * T]))
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """The oracle's backward formulas (without BF16 rounding) against central
+    differences of its own loss."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mlp_oracle", os.path.join(os.path.dirname(
+        os.path.dirname(os.path.abspath(__file__))), "oracle", "mlp_oracle.py"))
+    mo = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mo)
+    rng = np.random.default_rng(0)
+    dims = (3, 6, 2, 5)
+    npar = sum(int(np.prod(s)) for s in mo.shapes(*dims))
+    w = rng.standard_normal(npar) * 0.5
+    x, t, tl = rng.standard_normal((4, 3)), rng.standard_normal((4, 5)), rng.standard_normal(4)
+    _, g, _, _ = mo.loss_grad(w, x, t, tl, *dims, quantize=False)
+    h = 1e-6
+    for k in rng.choice(npar, 25, replace=False):
+        e = np.zeros(npar)
+        e[k] = h
+        lp = mo.loss_grad(w + e, x, t, tl, *dims, quantize=False)[0]
+        lm = mo.loss_grad(w - e, x, t, tl, *dims, quantize=False)[0]
+        assert abs((lp - lm) / (2 * h) - g[k]) <= 1e-6 * (1 + abs(g[k]))
