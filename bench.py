@@ -377,6 +377,82 @@ def run_batch(args):
         torch.distributed.destroy_process_group()
 
 
+WS_METRIC = "learned warm start: time-to-1e-6 KKT (s) per held-out instance, warm vs cold start, 1 B200"
+WS_EPS = 1e-6
+
+
+def run_warm_start(args):
+    """The parametric family: cold solves of the training parameters, the MLP
+    trained on the GPU, then held-out instances solved cold and warm (each
+    warm answer must meet the same tolerance).  value = mean warm time per
+    held-out solve; the cold mean is the comparison."""
+    import torch
+    from pdhcg_b200 import warmstart
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if rank != 0:  # one family, one GPU: the other ranks idle
+        return
+    n = max(1000, int(50000 * args.scale))
+    fam = warmstart.ParametricQP(seed=5, n=n)
+    params = {"termination_criteria.eps_optimal_relative": WS_EPS,
+              "termination_criteria.eps_feasible_relative": WS_EPS, "termination_criteria.time_sec_limit": 600.0}
+    ws = warmstart.WarmStart(fam, hidden=512, rank=64, seed=1)
+    t0 = time.perf_counter()
+    train = fam.thetas(args.train, seed=1)
+    X, lw, train_its = ws.collect(train, params)
+    t_collect = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    loss = ws.fit(train, X, lw, epochs=args.epochs, batch=64, lr=1e-3)
+    t_fit = time.perf_counter() - t0
+    held = fam.thetas(args.heldout + args.warmup, seed=2)
+    for th in held[:args.warmup]:
+        ws.solve(th, params)
+        ws.solve(th, params, warm=True)
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    cold_t, warm_t, cold_it, warm_it, ok = [], [], [], [], 0
+    cold_st, warm_st = [], []
+    keys = ("setup_ms", "loop_ms", "result_ms", "upload_ms", "evaluations", "restarts")
+    for th in held[args.warmup:]:
+        c = ws.solve(th, params)
+        st = native.last_stats()
+        cold_t.append(st["total_ms"] * 1e-3)
+        cold_st.append([st[k] for k in keys])
+        w = ws.solve(th, params, warm=True)
+        st = native.last_stats()
+        warm_t.append(st["total_ms"] * 1e-3)
+        warm_st.append([st[k] for k in keys])
+        cold_it.append(c["total_count"])
+        warm_it.append(w["total_count"])
+        ok += int(c["status"] == w["status"] == "OPTIMAL" and abs(c["primal_objective_value"] - w[
+            "primal_objective_value"]) <= 10 * WS_EPS * (1 + abs(c["primal_objective_value"])))
+    clocks = sampler.stop()
+    ws.close()
+    line = {
+        "metric": WS_METRIC, "value": float(np.mean(warm_t)), "unit": "s", "n_gpus": 1, "steps": args.heldout,
+        "warmup": args.warmup, "ms_per_step": float(np.mean(warm_t)) * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 solve, bf16/f32 network", "data": "synthetic",
+        "config": {"workload": f"parametric QP family: n={n}, m={n // 2}, A 6 nnz/row, diag Q, theta in R^32, "
+                               f"c = c0 + C theta, row bounds + L theta, eps 1e-6",
+                   "network": "32-512-512 MLP, rank-64 output head to n + m, log primal-weight head",
+                   "training_solves": args.train, "heldout_solves": args.heldout, "epochs": args.epochs},
+        "cold": {"value": float(np.mean(cold_t)), "unit": "s", "mean_iterations": float(np.mean(cold_it)),
+                 "mean_breakdown": dict(zip(keys, np.mean(cold_st, 0).tolist()))},
+        "warm": {"value": float(np.mean(warm_t)), "unit": "s", "mean_iterations": float(np.mean(warm_it)),
+                 "mean_breakdown": dict(zip(keys, np.mean(warm_st, 0).tolist()))},
+        "speedup_warm_vs_cold": float(np.mean(cold_t) / np.mean(warm_t)),
+        "iteration_ratio_cold_over_warm": float(np.mean(cold_it) / np.mean(warm_it)),
+        "heldout_passing_same_tolerance": f"{ok}/{args.heldout}",
+        "training": {"collect_s": t_collect, "fit_s": t_fit, "final_loss": loss,
+                     "mean_training_iterations": float(np.mean(train_its))},
+        "e2e": {"value": float(np.mean(warm_t)), "unit": "s",
+                "h2d_bytes_per_step": int(fam.A.nnz * 12 + n * 8 * 6 + (n // 2) * 8 * 3),
+                "d2h_bytes_per_step": int(8 * (2 * n + n // 2))},
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+
+
 def run_reference(args):
     """The reference's own solver (built from its sources into oracle/_ref)
     on the same instance through its C API; falls back to the oracle port
@@ -432,13 +508,19 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = the benchmark size)")
     ap.add_argument("--iters", type=int, default=None, help="iteration cap (profiling only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="soc_qp", choices=["soc_qp", "mpc_batch"],
-                    help="soc_qp: the headline single-instance workload; mpc_batch: the batched workload")
+    ap.add_argument("--workload", default="soc_qp", choices=["soc_qp", "mpc_batch", "warm_start"],
+                    help="soc_qp: the headline single-instance workload; mpc_batch: the batched workload; "
+                         "warm_start: the learned warm start on the parametric family")
+    ap.add_argument("--train", type=int, default=2000, help="warm_start: training solves")
+    ap.add_argument("--heldout", type=int, default=200, help="warm_start: held-out solves")
+    ap.add_argument("--epochs", type=int, default=100, help="warm_start: training epochs")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "mpc_batch":
         run_batch(args)
+    elif args.workload == "warm_start":
+        run_warm_start(args)
     else:
         run_ours(args)
 

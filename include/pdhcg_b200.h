@@ -34,7 +34,11 @@ typedef struct {
     int time_steps;                /* bracket every fused step with CUDA events (fills step_kernel_ms) */
     int solution_on_device;        /* pdhcg_b200_solve_device only: leave x, y, reduced cost in device
                                       memory (result arrays are NULL); see pdhcg_b200_device_solution */
-    int reserved[5];
+    int has_initial_step_size;     /* skip the power method and use initial_step_size (0.998 / sigma_max
+                                      of the scaled A): valid for another problem with the same A and
+                                      scaling parameters, e.g. from pdhcg_b200_stats_t.step_size */
+    double initial_step_size;
+    int reserved[4];
 } pdhcg_b200_options_t;
 
 void pdhcg_b200_default_options(pdhcg_b200_options_t *opts);
@@ -79,7 +83,7 @@ typedef struct {
     double result_ms;            /* result kernel and device->host copies */
     double total_ms;             /* the whole call, wall clock */
     double primal_weight;        /* primal weight at termination (a warm start for a similar solve) */
-    double reserved[1];
+    double step_size;            /* 0.998 / sigma_max(scaled A), reusable for the same A */
 } pdhcg_b200_stats_t;
 
 int pdhcg_b200_last_stats(pdhcg_b200_stats_t *out);

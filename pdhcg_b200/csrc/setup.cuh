@@ -437,73 +437,58 @@ __global__ void __launch_bounds__(TPB) power_sigma_kernel(int m, int n, const in
                                                           double *part /* 4 * gridDim */, int max_iter, double tol,
                                                           double *out /* [sigma, iterations] */)
 {
+    // The iterate is u with |u| = 1 / inv (v = inv * u is the unit vector):
+    //   dp = inv * A^T u;  w = A dp = A A^T v
+    //   s2 = v . w = inv * (u . w);  |w - s2 v|^2 = |w|^2 - s2^2  (|v| = 1)
+    // then u <- w, inv <- 1 / |w|: two grid barriers per iteration, the
+    // buffers of u and w alternate.
     cg::grid_group grid = cg::this_grid();
     __shared__ double stage_all[WARPS][STREAM_CHUNK];
     const int nb = gridDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
     const int lane = threadIdx.x & 31, gw = blockIdx.x * WARPS + (threadIdx.x >> 5), nw = gridDim.x * WARPS;
     double *stage = stage_all[threadIdx.x >> 5];
-    double *p0 = part, *p1 = part + nb, *p2 = part + 2 * nb, *p3 = part + 3 * nb;
-    // normalize the start vector
+    double *p0 = part, *p1 = part + nb, *p2 = part + 2 * nb;
     double a = 0.0;
     for (int i = tid; i < m; i += nth)
         a += v[i] * v[i];
     coop_block_partial(a, p0);
     grid.sync();
     double inv = 1.0 / sqrt(coop_fold(p0, nb));
-    for (int i = tid; i < m; i += nth)
-        v[i] *= inv;
-    grid.sync();
+    double *u = v, *w = nv;
     double s2 = 1.0;
     int it = 0;
     for (; it < max_iter; ++it) {
-        // dp = A^T v and nv = A dp, one warp per tile of 32 rows
         for (int t = gw; t < (n + 31) / 32; t += nw) {
             const int r0 = 32 * t, nr = min(32, n - r0);
             double r[1];
-            warp_stream_rows<1>(At_rp, At_ci, At_v, v, r0, nr, lane, stage, r);
+            warp_stream_rows<1>(At_rp, At_ci, At_v, u, r0, nr, lane, stage, r);
             if (lane < nr)
-                dp[r0 + lane] = r[0];
+                dp[r0 + lane] = r[0] * inv;
         }
         grid.sync();
-        a = 0.0;
+        double uw = 0.0, ww = 0.0;
         for (int t = gw; t < (m + 31) / 32; t += nw) {
             const int r0 = 32 * t, nr = min(32, m - r0);
             double r[1];
             warp_stream_rows<1>(A_rp, A_ci, A_v, dp, r0, nr, lane, stage, r);
             if (lane < nr) {
-                nv[r0 + lane] = r[0];
-                a += r[0] * v[r0 + lane];
+                w[r0 + lane] = r[0];
+                uw += r[0] * u[r0 + lane];
+                ww += r[0] * r[0];
             }
         }
-        coop_block_partial(a, p1);
+        coop_block_partial(uw, p1);
+        coop_block_partial(ww, p2);
         grid.sync();
-        s2 = coop_fold(p1, nb);
-        a = 0.0;
-        for (int i = tid; i < m; i += nth) {
-            double t = nv[i] + (-s2) * v[i];
-            nv[i] = t;
-            a += t * t;
-        }
-        coop_block_partial(a, p2);
-        grid.sync();
-        if (sqrt(coop_fold(p2, nb)) < tol)
+        s2 = inv * coop_fold(p1, nb);
+        const double w2 = coop_fold(p2, nb);
+        if (sqrt(fmax(w2 - s2 * s2, 0.0)) < tol)
             break;
-        a = 0.0;
-        for (int i = tid; i < m; i += nth) {
-            double t = nv[i] + s2 * v[i];
-            nv[i] = t;
-            a += t * t;
-        }
-        coop_block_partial(a, p3);
-        grid.sync();
-        inv = 1.0 / sqrt(coop_fold(p3, nb));
-        for (int i = tid; i < m; i += nth)
-            nv[i] *= inv;
-        double *t = v;
-        v = nv;
-        nv = t;
-        grid.sync();
+        inv = 1.0 / sqrt(w2);
+        double *t = u;
+        u = w;
+        w = t;
     }
     if (tid == 0) {
         out[0] = sqrt(s2);

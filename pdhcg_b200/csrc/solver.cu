@@ -46,14 +46,58 @@ struct CudaError : std::runtime_error {
 
 thread_local pdhcg_b200_stats_t g_last_stats;
 
-// device allocations owned by one solve
+// pinned host mirror of a solve's scalar block, one per host thread, kept
+// for the thread's lifetime (a solve runs on one thread)
+double *pinned_scalars()
+{
+    struct Buf {
+        double *p = nullptr;
+        ~Buf()
+        {
+            if (p)
+                cudaFreeHost(p);
+        }
+    };
+    thread_local Buf b;
+    if (!b.p)
+        CK(cudaMallocHost(&b.p, 64 * sizeof(double)));
+    return b.p;
+}
+
+// The device's default memory pool keeps what solves free (no release
+// threshold), so the allocations of the next solve are served from the pool
+// instead of cudaMalloc; set once per device.
+void keep_pool_memory()
+{
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev])
+        return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        unsigned long long keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done[dev] = true;
+}
+
+// Device allocations owned by one solve or one device problem: stream-ordered
+// from the default pool on the owner's stream s, returned to the pool on the
+// legacy stream when the owner (which has synchronised its streams by then)
+// goes away.
 struct Arena {
     std::vector<void *> ptrs;
+    cudaStream_t s = nullptr;
     template <typename T>
     T *alloc(size_t count)
     {
         void *p = nullptr;
-        CK(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+        keep_pool_memory();
+        CK(cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), s));
         ptrs.push_back(p);
         return (T *)p;
     }
@@ -68,7 +112,7 @@ struct Arena {
     ~Arena()
     {
         for (void *p : ptrs)
-            cudaFree(p);
+            cudaFreeAsync(p, 0);
     }
 };
 
@@ -220,6 +264,7 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
 {
     auto dp = std::make_unique<DeviceProblem>();
     DeviceProblem &d = *dp;
+    d.ar.s = s;
     d.n = p->num_variables;
     d.orig_vars = p->num_variables;
     d.orig_cons = p->num_constraints;
@@ -389,10 +434,11 @@ public:
     {
         for (cudaEvent_t e : ev_pool_)
             cudaEventDestroy(e);
-        if (h_scal_)
-            cudaFreeHost(h_scal_);
-        if (st_)
+        if (st_) {
+            cudaStreamSynchronize(st_); // the arena returns its memory on the legacy stream
             cudaStreamDestroy(st_);
+            dp_.ar.s = nullptr;
+        }
     }
     pdhcg_result_t *run();
 
@@ -880,6 +926,8 @@ void Solve::step_size()
     cudaStream_t s = st_;
     if (A_.nnz == 0) {
         step_ = 1.0;
+    } else if (opt_.has_initial_step_size && opt_.initial_step_size > 0.0) {
+        step_ = opt_.initial_step_size; // from a previous solve with the same scaled A
     } else {
         int m = m_, n = n_;
         std::vector<double> v0(m);
@@ -1645,6 +1693,8 @@ pdhcg_result_t *Solve::run()
 {
     auto t_setup = std::chrono::steady_clock::now();
     CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    ar_.s = st_;
+    dp_.ar.s = st_; // outputs kept with the device problem are allocated in this solve's order
     build_host();
     auto t_host = std::chrono::steady_clock::now();
     stats_.host_copy_ms = std::chrono::duration<double, std::milli>(t_host - t_setup).count();
@@ -1668,7 +1718,7 @@ pdhcg_result_t *Solve::run()
     partials_ = ar_.alloc<double>((size_t)maxb * RS_COUNT);
     scal_d_ = ar_.alloc<double>(RS_COUNT + 2 * FP_COUNT);
     CK(cudaMemsetAsync(scal_d_, 0, (RS_COUNT + 2 * FP_COUNT) * sizeof(double), st_));
-    CK(cudaMallocHost(&h_scal_, (RS_COUNT + 2 * FP_COUNT) * sizeof(double)));
+    h_scal_ = pinned_scalars();
     {
         int nop = prm_.optimality_norm == NORM_TYPE_L2 ? RSUM : RMAX;
         int res_ops[RS_COUNT] = {nop, RSUM, nop, RSUM, RSUM, RSUM, nop, nop, RSUM, RSUM};
@@ -1727,6 +1777,7 @@ pdhcg_result_t *Solve::run()
     stats_.spmv_bytes = 2.0 * nnz * (8 + 4) + 4.0 * ((double)n_ + m_ + 2) + 8.0 * ((double)n_ + m_);
     stats_.step_bytes = stats_.step_kernel_launches > 0 ? step_bytes_sum_ / stats_.step_kernel_launches : 0.0;
     stats_.primal_weight = omega_;
+    stats_.step_size = step_;
     g_last_stats = stats_;
     return r;
 }

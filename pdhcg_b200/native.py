@@ -21,7 +21,7 @@ class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("polish_threshold", C.c_double),
                 ("has_initial_primal_weight", C.c_int), ("initial_primal_weight", C.c_double),
                 ("use_graphs", C.c_int), ("time_steps", C.c_int), ("solution_on_device", C.c_int),
-                ("reserved", C.c_int * 5)]
+                ("has_initial_step_size", C.c_int), ("initial_step_size", C.c_double), ("reserved", C.c_int * 4)]
 
 
 class Stats(C.Structure):
@@ -31,7 +31,7 @@ class Stats(C.Structure):
                 ("iterations", C.c_int), ("fp32_iterations", C.c_int), ("restarts", C.c_int),
                 ("evaluations", C.c_int), ("step_bytes", C.c_double), ("spmv_bytes", C.c_double),
                 ("host_copy_ms", C.c_double), ("upload_ms", C.c_double), ("result_ms", C.c_double),
-                ("total_ms", C.c_double), ("primal_weight", C.c_double), ("reserved", C.c_double * 1)]
+                ("total_ms", C.c_double), ("primal_weight", C.c_double), ("step_size", C.c_double)]
 
 
 class BatchOptions(C.Structure):

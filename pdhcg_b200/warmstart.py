@@ -7,7 +7,8 @@ collects cold solves of training parameters with the library's own solver,
 fits the MLP of ``pdhcg_b200_mlp_*`` (trained on the GPU by the library's
 kernels) from theta to the solution (x, y) and the final primal weight, and
 solves a new instance from the predicted point
-(``set_start_values`` + ``initial_primal_weight``).  The cold solve stays the
+(``set_start_values`` + ``initial_primal_weight``), reusing the step size of
+the family's fixed constraint matrix (``initial_step_size``).  The cold solve stays the
 reference: a warm solve must meet the same termination tolerance.
 """
 from __future__ import annotations
@@ -15,7 +16,6 @@ from __future__ import annotations
 import ctypes as C
 
 import numpy as np
-import scipy.sparse as sp
 
 from . import capi, native
 from .capi import CsrMatrix, Problem
@@ -68,6 +68,9 @@ class WarmStart:
             raise RuntimeError("pdhcg_b200_mlp_create failed")
         self.mean = np.zeros(self.out_dim)
         self.scale = np.ones(self.out_dim)
+        # 0.998 / sigma_max of the scaled A, shared by the whole family (A and
+        # the scaling parameters are fixed), recorded by the first cold solve
+        self.step_size = None
 
     def close(self):
         if self.net:
@@ -94,13 +97,19 @@ class WarmStart:
             lib.set_start_values(prob, xs.ctypes.data_as(dp), ys.ctypes.data_as(dp))
             opts.has_initial_primal_weight = 1
             opts.initial_primal_weight = float(w[0])
+            if self.step_size:
+                opts.has_initial_step_size = 1
+                opts.initial_step_size = self.step_size
         prm = capi.default_params(lib, **params)
         r = lib.pdhcg_b200_solve(prob, C.byref(prm), C.byref(opts))
         if not r:
             lib.qp_problem_free(prob)
             raise RuntimeError("solve failed")
         d = capi.result_dict(r, p.n, p.A.m)
-        d["final_primal_weight"] = native.last_stats()["primal_weight"]
+        st = native.last_stats()
+        d["final_primal_weight"] = st["primal_weight"]
+        if not warm and self.step_size is None:
+            self.step_size = st["step_size"]
         lib.pdhcg_result_free(r)
         lib.qp_problem_free(prob)
         return d
