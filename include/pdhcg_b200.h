@@ -186,9 +186,11 @@ int pdhcg_b200_csr_spmv(int rows, const int *row_ptr, const int *col_ind, const 
 
 /* Project each cone block of x (scaled space) onto {x : x_i / d_i in K} in the
  * metric sum_i (1 + tau q_i)(x_i - r_i)^2; q may be NULL.  cone_type holds
- * cone_type_t values; only CONE_STANDARD_SOC and CONE_ROTATED_SOC blocks of
- * at most 256 slots are supported (-3: another cone type, -2: a longer
- * block).  Waits for the stream (it reads the block lengths on the host). */
+ * cone_type_t values: SOC and rotated-SOC blocks of at most 256 slots,
+ * exponential blocks, and power blocks (exponents in cone_alpha, which may
+ * be NULL without power blocks); -3 for a PSD block or a power block
+ * without cone_alpha, -2 for a longer block.  Waits for the stream (it reads
+ * the block lengths on the host). */
 int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *cone_vdim, const int *cone_type,
                              const double *cone_alpha, double *x, const double *d, const double *q, double tau,
                              void *stream);

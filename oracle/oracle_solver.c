@@ -939,6 +939,47 @@ static void compute_residual(ostate *S, norm_type_t nt)
     }
     S->abs_p = vnorm(S->primal_residual, m, nt) / S->sb;
     double lin_abs_p = S->abs_p;
+    /* power-cone primal violation (reference compute_power_cone_primal_violation,
+     * src/pdhg_core_op.cu:214-250, kernel src/kernels/pdhcg_power_cone_kernels.cu:623-669) */
+    double pv_abs = 0.0, pv_rel = 0.0;
+    for (int b = 0; cones && b < S->P.ncones; ++b) {
+        if (S->P.ctype[b] != CONE_POWER) continue;
+        int st = S->P.cstart[b];
+        double x = S->xp[st] / S->vr[st], y = S->xp[st + 1] / S->vr[st + 1], z = S->xp[st + 2] / S->vr[st + 2];
+        double va, vrel;
+        if (!isfinite(x) || !isfinite(y) || !isfinite(z)) {
+            va = vrel = INFINITY;
+        } else {
+            double v = fmax(-x, -y), az = fabs(z);
+            int inside = 0;
+            if (az > 0.0) {
+                double bound = 0.0;
+                if (x > 0.0 && y > 0.0) {
+                    double a = S->P.calpha[b];
+                    double lb = a * log(x) + (1.0 - a) * log(y), lz = log(az);
+                    double tol = 64.0 * DBL_EPSILON * (1.0 + fabs(lb) + fabs(lz));
+                    if (lb + tol >= lz) inside = 1;
+                    else bound = exp(lb);
+                }
+                if (!inside) v = fmax(v, az - bound);
+            }
+            va = fmax(v, 0.0);
+            vrel = va / (S->sb + fmax(fabs(x), fmax(fabs(y), az)));
+        }
+        if (nt == NORM_TYPE_L_INF) {
+            pv_abs = fmax(pv_abs, va);
+            pv_rel = fmax(pv_rel, vrel);
+        } else {
+            pv_abs += va * va;
+            pv_rel += vrel * vrel;
+        }
+    }
+    if (nt != NORM_TYPE_L_INF) {
+        pv_abs = sqrt(pv_abs);
+        pv_rel = sqrt(pv_rel);
+    }
+    if (cones)
+        S->abs_p = nt == NORM_TYPE_L_INF ? fmax(S->abs_p, pv_abs) : hypot(S->abs_p, pv_abs);
     S->abs_d = vnorm(S->dual_residual, n, nt); /* complementarity residual is 0 without fixed sections */
     S->abs_d /= S->sc;
     double half_xqx = S->qtype == PDHCG_NON_Q ? 0.0 : 0.5 * dot(S->xp, S->qx, n);
@@ -953,6 +994,8 @@ static void compute_residual(ostate *S, norm_type_t nt)
     for (int i = 0; i < m; ++i) ssum += S->primal_slack[i];
     S->dobj = (base + ssum - half_xqx) / (S->sb * S->sc) + S->P.c0;
     S->rel_p = lin_abs_p / (1.0 + S->bnorm);
+    if (cones)
+        S->rel_p = nt == NORM_TYPE_L_INF ? fmax(S->rel_p, pv_rel) : hypot(S->rel_p, pv_rel);
     double den;
     if (S->is_lp) {
         den = 1.0 + S->cnorm;

@@ -46,6 +46,7 @@ struct BBData {
     const int *free_idx;
     int n_free;
     const int *cone_start, *cone_len, *cone_type;
+    const double *cone_alpha; // power-cone exponents (NULL: none)
     int n_cones;
     const double *vr;
     double *cone_warm;
@@ -199,6 +200,83 @@ struct BBWork {
     }
 };
 
+// One cone block of bb_var_phase: the warp computes the candidates,
+// projects, and takes the step from the values before the update.
+template <int G, int S>
+__device__ __forceinline__ double bb_cone_block(const BBData &D, const double *drx, bool init, double alpha, int lane,
+                                                double *stage, int cb)
+{
+    const int sub = lane % G;
+    double part = 0.0;
+    int st = D.cone_start[cb], L = D.cone_len[cb], type = D.cone_type[cb];
+    if (init) {
+        // Q x for the block's rows, staged through shared memory
+        for (int base = 0; base < L; base += 32 / G) {
+            int slot = base + lane / G;
+            bool ok = slot < L;
+            int j = st + (ok ? slot : 0);
+            double s = 0.0;
+            if (ok && D.sparse) {
+                int b = D.Q_rp[j], e = D.Q_rp[j + 1];
+                for (int t = b + sub; t < e; t += G)
+                    s += D.Q_v[t] * D.x[D.Q_ci[t]];
+            }
+            if (ok && D.k > 0) {
+                int b = D.Rt_rp[j], e = D.Rt_rp[j + 1];
+                for (int t = b + sub; t < e; t += G)
+                    s += D.Rt_v[t] * drx[D.Rt_ci[t]];
+            }
+            s = group_sum<G>(s);
+            if (ok && sub == 0)
+                stage[slot] = s;
+        }
+        __syncwarp();
+    }
+    WarpSlots<S> sl;
+    double xo[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        int i = lane + 32 * s;
+        sl.x[s] = 0.0;
+        sl.d[s] = 1.0;
+        sl.w[s] = 1.0;
+        xo[s] = 0.0;
+        if (i < L) {
+            int j = st + i;
+            double mi = D.m_inv ? D.m_inv[j] : 1.0;
+            double g;
+            if (init) {
+                double q = stage[i];
+                g = q + D.c[j] - D.aty[j];
+                xo[s] = D.x[j];
+                D.grad[j] = g;
+                D.qx[j] = q;
+            } else {
+                g = D.grad[j];
+                xo[s] = D.xp[j];
+            }
+            sl.x[s] = clampd(D.l[j], xo[s] - alpha * mi * g, D.u[j]);
+            sl.d[s] = D.vr[j];
+        }
+    }
+    __syncwarp();
+    bool uni = warp_uniform_unit<S>(sl, L, lane);
+    warp_project<S>(type, sl, L, lane, uni, D.cone_warm ? D.cone_warm + cb : nullptr,
+                    D.cone_alpha ? D.cone_alpha[cb] : 0.0);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        int i = lane + 32 * s;
+        if (i < L) {
+            int j = st + i;
+            D.xp[j] = sl.x[s];
+            double dd = sl.x[s] - xo[s];
+            D.dir[j] = dd;
+            part += D.m_diag ? dd * D.m_diag[j] * dd : dd * dd;
+        }
+    }
+    return part;
+}
+
 // init: grad = Qx + c - A^T y; x_p = P(x - alpha0 M^-1 grad); dir = x_p - x
 // (reference primal_gradient_descent_kernel_bb_init[_precond] and the cone
 // projection that follows, src/pdhg_core_op.cu:531-566)
@@ -255,74 +333,13 @@ __device__ double bb_var_phase(const BBData &D, const double *drx, bool init, do
                 part += D.m_diag ? dd * D.m_diag[j] * dd : dd * dd;
             }
         } else {
-            // cone block: the warp computes the candidates, projects, and
-            // takes the step from the values before the update
-            int cb = task - W.free_tasks;
-            int st = D.cone_start[cb], L = D.cone_len[cb], type = D.cone_type[cb];
-            if (init) {
-                // Q x for the block's rows, staged through shared memory
-                for (int base = 0; base < L; base += 32 / G) {
-                    int slot = base + lane / G;
-                    bool ok = slot < L;
-                    int j = st + (ok ? slot : 0);
-                    double s = 0.0;
-                    if (ok && D.sparse) {
-                        int b = D.Q_rp[j], e = D.Q_rp[j + 1];
-                        for (int t = b + sub; t < e; t += G)
-                            s += D.Q_v[t] * D.x[D.Q_ci[t]];
-                    }
-                    if (ok && D.k > 0) {
-                        int b = D.Rt_rp[j], e = D.Rt_rp[j + 1];
-                        for (int t = b + sub; t < e; t += G)
-                            s += D.Rt_v[t] * drx[D.Rt_ci[t]];
-                    }
-                    s = group_sum<G>(s);
-                    if (ok && sub == 0)
-                        stage[slot] = s;
-                }
-                __syncwarp();
-            }
-            WarpSlots<S> sl;
-            double xo[S];
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                int i = lane + 32 * s;
-                sl.x[s] = 0.0;
-                sl.d[s] = 1.0;
-                sl.w[s] = 1.0;
-                xo[s] = 0.0;
-                if (i < L) {
-                    int j = st + i;
-                    double mi = D.m_inv ? D.m_inv[j] : 1.0;
-                    double g;
-                    if (init) {
-                        double q = stage[i];
-                        g = q + D.c[j] - D.aty[j];
-                        xo[s] = D.x[j];
-                        D.grad[j] = g;
-                        D.qx[j] = q;
-                    } else {
-                        g = D.grad[j];
-                        xo[s] = D.xp[j];
-                    }
-                    sl.x[s] = clampd(D.l[j], xo[s] - alpha * mi * g, D.u[j]);
-                    sl.d[s] = D.vr[j];
-                }
-            }
-            __syncwarp();
-            bool uni = warp_uniform_unit<S>(sl, L, lane);
-            warp_project<S>(type, sl, L, lane, uni, D.cone_warm ? D.cone_warm + cb : nullptr);
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                int i = lane + 32 * s;
-                if (i < L) {
-                    int j = st + i;
-                    D.xp[j] = sl.x[s];
-                    double dd = sl.x[s] - xo[s];
-                    D.dir[j] = dd;
-                    part += D.m_diag ? dd * D.m_diag[j] * dd : dd * dd;
-                }
-            }
+            // cone block; 3-slot blocks (exponential, power) take the one-slot
+            // instantiation, which alone carries their projection
+            const int cb = task - W.free_tasks;
+            if (S > 1 && D.cone_type[cb] >= 2)
+                part += bb_cone_block<G, 1>(D, drx, init, alpha, lane, stage, cb);
+            else
+                part += bb_cone_block<G, S>(D, drx, init, alpha, lane, stage, cb);
         }
     }
     return part;

@@ -562,14 +562,202 @@ __device__ void warp_project_rsoc(WarpSlots<S> &sl, int L, int lane, bool unifor
     }
 }
 
-template <int S>
-__device__ __forceinline__ void warp_project(int type, WarpSlots<S> &sl, int L, int lane, bool uniform_unit,
-                                             double *warm)
+// ---------------------------------------------------------------------------
+// Three-dimensional cones, projected by one thread.
+//
+// Exponential cone K = cl{(x, y, z) : y > 0, y exp(x / y) <= z}: the
+// projection of r onto {v : v / d in K} in the unit metric of r's space,
+// with the reference's sequence of tests and its Newton iteration on
+// rho = x / y (src/kernels/pdhcg_exp_cone_kernels.cu:26-131): in-cone test,
+// polar-cone test, the x <= 0, y <= 0 case, then at most 100 capped Newton
+// steps with the same fallbacks.
+// ---------------------------------------------------------------------------
+__device__ inline void exp_cone_point(double r1, double r2, double r3, double d1, double d2, double d3, double &o1,
+                                      double &o2, double &o3)
 {
-    if (type == 1) // CONE_STANDARD_SOC
+    const double a1 = r1 / d1, a2 = r2 / d2, a3 = r3 / d3;
+    const bool inside = a2 > 0.0 ? (a1 / a2 < 700.0 && a2 * exp(a1 / a2) <= a3)
+                                 : (a2 == 0.0 && a1 <= 0.0 && a3 >= 0.0);
+    if (inside) {
+        o1 = r1;
+        o2 = r2;
+        o3 = r3;
+        return;
+    }
+    const bool polar = r1 > 0.0 ? ((d2 * r2) / (d1 * r1) < 700.0 &&
+                                   d1 * r1 * exp((d2 * r2) / (d1 * r1)) + 2.718281828459045 * d3 * r3 <= 0.0)
+                                : (r1 == 0.0 && r2 <= 0.0 && r3 <= 0.0);
+    if (polar) {
+        o1 = o2 = o3 = 0.0;
+        return;
+    }
+    if (a1 <= 0.0 && a2 <= 0.0) {
+        o1 = r1;
+        o2 = 0.0;
+        o3 = a3 < 0.0 ? 0.0 : r3;
+        return;
+    }
+    const double al = (d3 / d1) * (d3 / d1), be = (d3 / d2) * (d3 / d2);
+    double rho = 0.0;
+    bool diverged = false;
+    for (int it = 0; it < 100; ++it) {
+        if (fabs(rho) >= 299.0) {
+            diverged = true;
+            break;
+        }
+        const double er = exp(rho), e2 = er * er, omr = 1.0 - rho;
+        const double A = al - be * rho * omr, B = be * a1 * omr - al * a2;
+        const double f = a1 - a2 * rho + a3 * er * A + e2 * B;
+        const double df = -a2 + a3 * er * (A - be * (1.0 - 2.0 * rho)) + e2 * (2.0 * B - be * a1);
+        if (fabs(df) < 1e-300)
+            break;
+        const double step = fmin(fmax(f / df, -10.0), 10.0);
+        rho -= step;
+        if (fabs(step) < 1e-13 * (1.0 + fabs(rho)))
+            break;
+    }
+    const double er = exp(rho);
+    const double u2 = (a1 + al * a3 * er) / (rho + al * er * er);
+    if (diverged || !isfinite(u2) || u2 <= 0.0) {
+        o1 = r1 < 0.0 ? r1 : 0.0;
+        o2 = 0.0;
+        o3 = r3 > 0.0 ? r3 : 0.0;
+        return;
+    }
+    o1 = d1 * rho * u2;
+    o2 = d2 * u2;
+    o3 = d3 * u2 * er;
+}
+
+// Power cone K_a = {(x, y, z) : x, y >= 0, x^a y^(1-a) >= |z|}: weighted
+// projection min sum w_i (v_i - r_i)^2 over K_a, by the reference's steps
+// (src/kernels/pdhcg_power_cone_kernels.cu:25-133): in-cone and
+// opposite-cone tests, then 80 bisection steps on log |v_z| with x, y the
+// positive roots of the KKT quadratics, on the point scaled by its largest
+// magnitude.
+__device__ inline double pow_pos_root(double r, double q)
+{
+    if (!(q > 0.0))
+        return fmax(r, 0.0);
+    const double disc = hypot(r, 2.0 * sqrt(q));
+    return r >= 0.0 ? 0.5 * (r + disc) : (2.0 * q) / (disc - r);
+}
+
+__device__ inline void pow_cone_point(double rx, double ry, double rz, double wx, double wy, double wz, double a,
+                                      double &ox, double &oy, double &oz)
+{
+    double s = fmax(fabs(rx), fmax(fabs(ry), fabs(rz)));
+    if (!(s > 0.0) || !isfinite(s))
+        s = 1.0;
+    rx /= s;
+    ry /= s;
+    rz /= s;
+    const double az = fabs(rz), om = 1.0 - a;
+    if (az == 0.0) {
+        ox = fmax(rx, 0.0) * s;
+        oy = fmax(ry, 0.0) * s;
+        oz = 0.0;
+        return;
+    }
+    if (rx > 0.0 && ry > 0.0 && a * log(rx) + om * log(ry) >= log(az)) {
+        ox = rx * s;
+        oy = ry * s;
+        oz = rz * s;
+        return;
+    }
+    if (rx <= 0.0 && ry <= 0.0) {
+        const double u = rx < 0.0 ? (-wx * rx) / a : 0.0, v = ry < 0.0 ? (-wy * ry) / om : 0.0;
+        if (u > 0.0 && v > 0.0 && a * log(u) + om * log(v) >= log(wz) + log(az)) {
+            ox = oy = oz = 0.0;
+            return;
+        }
+    }
+    const double cx = 4.0 * a * (wz / wx), cy = 4.0 * om * (wz / wy);
+    double lo = log(DBL_MIN), hi = log(az);
+    if (!(hi > lo)) {
+        ox = fmax(rx, 0.0) * s;
+        oy = fmax(ry, 0.0) * s;
+        oz = 0.0;
+        return;
+    }
+    for (int it = 0; it < 80; ++it) {
+        const double lr = lo + 0.5 * (hi - lo), rho = exp(lr);
+        const double x = pow_pos_root(rx, 0.25 * cx * rho * (az - rho));
+        const double y = pow_pos_root(ry, 0.25 * cy * rho * (az - rho));
+        if (x > 0.0 && y > 0.0 && a * log(x) + om * log(y) > lr)
+            lo = lr;
+        else
+            hi = lr;
+    }
+    const double rho = exp(lo + 0.5 * (hi - lo));
+    const double x = pow_pos_root(rx, 0.25 * cx * rho * (az - rho));
+    const double y = pow_pos_root(ry, 0.25 * cy * rho * (az - rho));
+    ox = x * s;
+    oy = y * s;
+    oz = (rz >= 0.0 ? 1.0 : -1.0) * fmin(rho, exp(a * log(x) + om * log(y))) * s;
+}
+
+// Projection of one 3-slot EXP (type 2) or POW (type 3) block: metric w,
+// scaling d.  Only the one-slot (S = 1) instantiations of the cone-block
+// bodies reach it, so its Newton / bisection loops stay out of the wide SOC
+// bodies' register allocation.
+__device__ __forceinline__ double3 cone3_point(int type, double3 x, double3 d, double3 w, double alpha)
+{
+    double3 o;
+    if (type == 2) { // exponential: the sqrt(w) change of variables
+        const double s0 = sqrt(w.x > 0.0 ? w.x : 1.0), s1 = sqrt(w.y > 0.0 ? w.y : 1.0),
+                     s2 = sqrt(w.z > 0.0 ? w.z : 1.0);
+        exp_cone_point(s0 * x.x, s1 * x.y, s2 * x.z, s0 * d.x, s1 * d.y, s2 * d.z, o.x, o.y, o.z);
+        o.x /= s0;
+        o.y /= s1;
+        o.z /= s2;
+    } else { // power: scaled space, weights w d^2
+        pow_cone_point(x.x / d.x, x.y / d.y, x.z / d.z, w.x * d.x * d.x, w.y * d.y * d.y, w.z * d.z * d.z, alpha,
+                       o.x, o.y, o.z);
+        o.x *= d.x;
+        o.y *= d.y;
+        o.z *= d.z;
+    }
+    return o;
+}
+
+// A 3-slot block held in lanes 0..2 (S = 1 slot each): lane 0 gathers it,
+// projects it and hands the result back.
+template <int S>
+__device__ __forceinline__ void warp_project3(int type, WarpSlots<S> &sl, int lane, double alpha)
+{
+    double3 x, d, w;
+    x.x = __shfl_sync(FULL, sl.x[0], 0);
+    x.y = __shfl_sync(FULL, sl.x[0], 1);
+    x.z = __shfl_sync(FULL, sl.x[0], 2);
+    d.x = __shfl_sync(FULL, sl.d[0], 0);
+    d.y = __shfl_sync(FULL, sl.d[0], 1);
+    d.z = __shfl_sync(FULL, sl.d[0], 2);
+    w.x = __shfl_sync(FULL, sl.w[0], 0);
+    w.y = __shfl_sync(FULL, sl.w[0], 1);
+    w.z = __shfl_sync(FULL, sl.w[0], 2);
+    double3 o = make_double3(0.0, 0.0, 0.0);
+    if (lane == 0)
+        o = cone3_point(type, x, d, w, alpha);
+    const double r0 = __shfl_sync(FULL, o.x, 0), r1 = __shfl_sync(FULL, o.y, 0), r2 = __shfl_sync(FULL, o.z, 0);
+    if (lane < 3)
+        sl.x[0] = lane == 0 ? r0 : (lane == 1 ? r1 : r2);
+}
+
+// Cone kinds an instantiation carries: SOC / RSOC (any S), and the 3-slot
+// exponential / power cones (S = 1 only; callers route those blocks there).
+enum ConeKinds { CONES_WIDE = 1, CONES_THREE = 2, CONES_ALL = 3 };
+
+template <int S, int KINDS = CONES_ALL>
+__device__ __forceinline__ void warp_project(int type, WarpSlots<S> &sl, int L, int lane, bool uniform_unit,
+                                             double *warm, double alpha = 0.0)
+{
+    if ((KINDS & CONES_WIDE) && type == 1) // CONE_STANDARD_SOC
         warp_project_soc<S>(sl, L, lane, uniform_unit, warm);
-    else if (type == 0) // CONE_ROTATED_SOC
+    else if ((KINDS & CONES_WIDE) && type == 0) // CONE_ROTATED_SOC
         warp_project_rsoc<S>(sl, L, lane, uniform_unit, warm);
+    else if ((KINDS & CONES_THREE) && S == 1 && (type == 2 || type == 3)) // CONE_EXPONENTIAL, CONE_POWER
+        warp_project3<S>(type, sl, lane, alpha);
 }
 
 // Is d uniform over the block and w == 1 everywhere?  (warp vote)

@@ -60,6 +60,7 @@ struct StepData {
     const int2 *free_tiles;
     int n_free_tiles;
     const int *cone_start, *cone_len, *cone_type;
+    const double *cone_alpha; // power-cone exponents (NULL: none)
     int n_cones;
     double *cone_warm; // per-cone multiplier warm start (may be NULL)
     T *x0, *x, *xp, *xr, *dx, *dual_slack;
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(TPB) primal_free_kernel(StepData<T> D, StepPar
 // One cone block [st, st + L): A^T y for the block's rows by stream-mode
 // products, the prox candidate of every slot, then the projection onto the
 // cone in the (1 + tau q) d^2 metric (diagonal Q) or d^2 metric (LP).
-template <int S, typename T, bool HAS_Q>
+template <int S, typename T, bool HAS_Q, int KINDS>
 __device__ __forceinline__ void primal_cone_block(const StepData<T> &D, const StepParams &P, int cb, int lane,
                                                   double *stage)
 {
@@ -190,7 +191,8 @@ __device__ __forceinline__ void primal_cone_block(const StepData<T> &D, const St
         }
     }
     bool uni = warp_uniform_unit<S>(sl, L, lane);
-    warp_project<S>(type, sl, L, lane, uni, D.cone_warm ? D.cone_warm + cb : nullptr);
+    warp_project<S, KINDS>(type, sl, L, lane, uni, D.cone_warm ? D.cone_warm + cb : nullptr,
+                           D.cone_alpha ? D.cone_alpha[cb] : 0.0);
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         const int i = lane + 32 * s;
@@ -208,16 +210,19 @@ __device__ __forceinline__ void primal_cone_block(const StepData<T> &D, const St
     }
 }
 
-template <int S, typename T, bool HAS_Q>
-__global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<T> D, StepParams P)
+// One warp per cone block of the list ids (NULL: blocks 0 .. nids - 1);
+// KINDS = CONES_WIDE for SOC / RSOC blocks, CONES_THREE (S = 1) for the
+// 3-slot exponential and power blocks.
+template <int S, typename T, bool HAS_Q, int KINDS>
+__global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<T> D, StepParams P, const int *ids, int nids)
 {
     __shared__ double stage_all[WARPS][STREAM_CHUNK];
     const int lane = threadIdx.x & 31;
     const int warp = blockIdx.x * WARPS + (threadIdx.x >> 5);
     const int nwarps = gridDim.x * WARPS;
     double *stage = stage_all[threadIdx.x >> 5];
-    for (int cb = warp; cb < D.n_cones; cb += nwarps)
-        primal_cone_block<S, T, HAS_Q>(D, P, cb, lane, stage);
+    for (int i = warp; i < nids; i += nwarps)
+        primal_cone_block<S, T, HAS_Q, KINDS>(D, P, ids ? ids[i] : i, lane, stage);
 }
 
 // One tile of 32 consecutive rows of A: A x_refl by stream-mode products,

@@ -25,6 +25,8 @@ enum ResidualScalar {
     RS_ATY_NORM,       // |A^T y * D_var|
     RS_DIST_X,         // |x_pdhg - x_init|^2
     RS_DIST_Y,         // |y_pdhg - y_init|^2
+    RS_POW_ABS,        // power-cone primal violation (max, or sum of squares)
+    RS_POW_REL,        // the same relative to the point's size
     RS_COUNT
 };
 
@@ -36,6 +38,7 @@ struct ResidualParams {
     int want_dist;    // restart distances
     double tau;       // step / primal weight (QP dual slack)
     double s_aug;     // step of the projected-gradient augmentation
+    double sb;        // constraint-bound rescaling (power-cone relative violation)
 };
 
 // VT: storage type of the iterates (FP32 during the mixed bulk phase); the
@@ -55,6 +58,7 @@ struct ResidualData {
     const int *free_idx; int n_free;
     const int2 *free_tiles; int n_free_tiles; // tiles of consecutive free rows (NULL: all n rows)
     const int *cone_start, *cone_len, *cone_type; int n_cones;
+    const double *cone_alpha;     // power-cone exponents (NULL: none)
     double *warm_dual, *warm_aug; // per-cone warm starts of the two projections
     double *partials;
     int rows_blocks, free_blocks, cone_blocks;
@@ -62,12 +66,130 @@ struct ResidualData {
 
 __device__ __forceinline__ double norm_term(double v, int l2) { return l2 ? v * v : abs_or_inf(v); }
 
+// One cone block of the residual: A^T y over the block, the dual-cone
+// residual and the augmented projected gradient, folded into acc.
+template <int S, typename VT>
+__device__ __forceinline__ void residual_cone_block(const ResidualData<VT> &D, const ResidualParams &P, int cb,
+                                                    int lane, double *stage, double (&acc)[RS_COUNT],
+                                                    const int (&ops)[RS_COUNT])
+{
+    auto fold = [&](int s, double v) { acc[s] = ops[s] == RMAX ? fmax(acc[s], v) : acc[s] + v; };
+    const int st = D.cone_start[cb], L = D.cone_len[cb], type = D.cone_type[cb];
+    double atys[S];
+    warp_stream_rows<S>(D.At_rp, D.At_ci, D.At_v, D.yp, st, L, lane, stage, atys);
+    WarpSlots<S> dual, aug;
+    double xv[S], rc[S], qxv[S], atyv[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        int i = lane + 32 * s;
+        dual.x[s] = aug.x[s] = 0.0;
+        dual.d[s] = aug.d[s] = 1.0;
+        dual.w[s] = aug.w[s] = 1.0;
+        xv[s] = rc[s] = qxv[s] = atyv[s] = 0.0;
+        if (i < L) {
+            int j = st + i;
+            double aty = atys[s];
+            double x = D.xp[j];
+            double qx = P.qmode == 1 ? D.q[j] * x : (P.qmode == 2 ? D.qx[j] : 0.0);
+            double eff = P.qmode ? D.c[j] + qx : D.c[j];
+            xv[s] = x;
+            atyv[s] = aty;
+            qxv[s] = qx;
+            rc[s] = eff - aty;
+            // dual cone of {x : x/d in K} is {s : s*d in K}: metric 1/d
+            dual.x[s] = rc[s];
+            dual.d[s] = 1.0 / D.vr[j];
+            aug.x[s] = clampd(D.l[j], x - P.s_aug * rc[s], D.u[j]);
+            aug.d[s] = D.vr[j];
+        }
+    }
+    const double alpha = D.cone_alpha ? D.cone_alpha[cb] : 0.0;
+    bool uni = warp_uniform_unit<S>(aug, L, lane); // d uniform <=> 1/d uniform
+    if (type == 0 || type == 1) {
+        // self-dual: projection onto the dual cone in the 1/d metric
+        warp_project<S>(type, dual, L, lane, uni, D.warm_dual ? D.warm_dual + cb : nullptr);
+    } else {
+        // Moreau: rc - proj_{K*}(rc) = -proj_K(-rc), in the inverse scaling
+        // (exponential) or on rc d in the unit metric (power) (reference
+        // compute_cone_dual_residual_exp_kernel / _power_kernel)
+        WarpSlots<S> neg;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const double vr = dual.d[s] > 0.0 ? 1.0 / dual.d[s] : 1.0;
+            neg.x[s] = type == 2 ? -dual.x[s] : -dual.x[s] * vr;
+            neg.d[s] = type == 2 ? dual.d[s] : 1.0;
+            neg.w[s] = 1.0;
+        }
+        warp_project<S>(type, neg, L, lane, false, nullptr, alpha);
+        // keep dual.x = proj_{K*} so that (rc - dual.x) vr is the residual below
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const double vr = dual.d[s] > 0.0 ? 1.0 / dual.d[s] : 1.0;
+            dual.x[s] = type == 2 ? rc[s] + neg.x[s] : rc[s] + neg.x[s] / vr;
+        }
+    }
+    warp_project<S>(type, aug, L, lane, uni, D.warm_aug ? D.warm_aug + cb : nullptr, alpha);
+    if (type == 3 && lane == 0) {
+        // power-cone primal violation (reference compute_power_cone_primal_violation_kernel,
+        // src/kernels/pdhcg_power_cone_kernels.cu:623-669): lane 0 holds slot 0 and
+        // reads slots 1, 2 from the block's storage
+        const double x = xv[0] / D.vr[st], y = (double)D.xp[st + 1] / D.vr[st + 1],
+                     z = (double)D.xp[st + 2] / D.vr[st + 2];
+        double va, vrel;
+        if (!isfinite(x) || !isfinite(y) || !isfinite(z)) {
+            va = vrel = INFINITY;
+        } else {
+            double v = fmax(-x, -y);
+            const double az = fabs(z);
+            if (az > 0.0) {
+                double bound = 0.0;
+                bool in = false;
+                if (x > 0.0 && y > 0.0) {
+                    const double lb = alpha * log(x) + (1.0 - alpha) * log(y), lz = log(az);
+                    in = lb + 64.0 * DBL_EPSILON * (1.0 + fabs(lb) + fabs(lz)) >= lz;
+                    bound = in ? 0.0 : exp(lb);
+                }
+                if (!in)
+                    v = fmax(v, az - bound);
+            }
+            va = fmax(v, 0.0);
+            vrel = va / (P.sb + fmax(fabs(x), fmax(fabs(y), az)));
+        }
+        fold(RS_POW_ABS, norm_term(va, P.l2));
+        fold(RS_POW_REL, norm_term(vrel, P.l2));
+    }
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        int i = lane + 32 * s;
+        if (i < L) {
+            int j = st + i;
+            double vr = D.vr[j];
+            double dr = (rc[s] - dual.x[s]) * vr;
+            double rr = (xv[s] - aug.x[s]) / P.s_aug * vr;
+            if (!isfinite(rr))
+                rr = copysign(INFINITY, rr);
+            if (fabs(rr) > fabs(dr))
+                dr = rr;
+            fold(RS_DUAL_RES, norm_term(dr, P.l2));
+            fold(RS_CX, D.c[j] * xv[s]);
+            fold(RS_XQX, xv[s] * qxv[s]);
+            fold(RS_SLACKX, rc[s] * xv[s]);
+            fold(RS_QX_NORM, norm_term(qxv[s] * vr, P.l2));
+            fold(RS_ATY_NORM, norm_term(atyv[s] * vr, P.l2));
+            if (P.want_dist) {
+                double d = xv[s] - D.x0[j];
+                fold(RS_DIST_X, d * d);
+            }
+        }
+    }
+}
+
 template <int S, typename VT>
 __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, ResidualParams P)
 {
     __shared__ double stage_all[WARPS][STREAM_CHUNK];
     const int NOP = P.l2 ? RSUM : RMAX;
-    const int ops[RS_COUNT] = {NOP, RSUM, NOP, RSUM, RSUM, RSUM, NOP, NOP, RSUM, RSUM};
+    const int ops[RS_COUNT] = {NOP, RSUM, NOP, RSUM, RSUM, RSUM, NOP, NOP, RSUM, RSUM, NOP, NOP};
     double acc[RS_COUNT];
 #pragma unroll
     for (int s = 0; s < RS_COUNT; ++s)
@@ -155,62 +277,12 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
         b -= D.rows_blocks + D.free_blocks;
         const int nwarps = D.cone_blocks * WARPS;
         for (int cb = b * WARPS + wib; cb < D.n_cones; cb += nwarps) {
-            const int st = D.cone_start[cb], L = D.cone_len[cb], type = D.cone_type[cb];
-            double atys[S];
-            warp_stream_rows<S>(D.At_rp, D.At_ci, D.At_v, D.yp, st, L, lane, stage, atys);
-            WarpSlots<S> dual, aug;
-            double xv[S], rc[S], qxv[S], atyv[S];
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                int i = lane + 32 * s;
-                dual.x[s] = aug.x[s] = 0.0;
-                dual.d[s] = aug.d[s] = 1.0;
-                dual.w[s] = aug.w[s] = 1.0;
-                xv[s] = rc[s] = qxv[s] = atyv[s] = 0.0;
-                if (i < L) {
-                    int j = st + i;
-                    double aty = atys[s];
-                    double x = D.xp[j];
-                    double qx = P.qmode == 1 ? D.q[j] * x : (P.qmode == 2 ? D.qx[j] : 0.0);
-                    double eff = P.qmode ? D.c[j] + qx : D.c[j];
-                    xv[s] = x;
-                    atyv[s] = aty;
-                    qxv[s] = qx;
-                    rc[s] = eff - aty;
-                    // dual cone of {x : x/d in K} is {s : s*d in K}: metric 1/d
-                    dual.x[s] = rc[s];
-                    dual.d[s] = 1.0 / D.vr[j];
-                    aug.x[s] = clampd(D.l[j], x - P.s_aug * rc[s], D.u[j]);
-                    aug.d[s] = D.vr[j];
-                }
-            }
-            bool uni = warp_uniform_unit<S>(aug, L, lane); // d uniform <=> 1/d uniform
-            warp_project<S>(type, dual, L, lane, uni, D.warm_dual ? D.warm_dual + cb : nullptr);
-            warp_project<S>(type, aug, L, lane, uni, D.warm_aug ? D.warm_aug + cb : nullptr);
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                int i = lane + 32 * s;
-                if (i < L) {
-                    int j = st + i;
-                    double vr = D.vr[j];
-                    double dr = (rc[s] - dual.x[s]) * vr;
-                    double rr = (xv[s] - aug.x[s]) / P.s_aug * vr;
-                    if (!isfinite(rr))
-                        rr = copysign(INFINITY, rr);
-                    if (fabs(rr) > fabs(dr))
-                        dr = rr;
-                    fold(RS_DUAL_RES, norm_term(dr, P.l2));
-                    fold(RS_CX, D.c[j] * xv[s]);
-                    fold(RS_XQX, xv[s] * qxv[s]);
-                    fold(RS_SLACKX, rc[s] * xv[s]);
-                    fold(RS_QX_NORM, norm_term(qxv[s] * vr, P.l2));
-                    fold(RS_ATY_NORM, norm_term(atyv[s] * vr, P.l2));
-                    if (P.want_dist) {
-                        double d = xv[s] - D.x0[j];
-                        fold(RS_DIST_X, d * d);
-                    }
-                }
-            }
+            // 3-slot blocks (exponential, power) take the one-slot
+            // instantiation, which alone carries their projection
+            if (S > 1 && D.cone_type[cb] >= 2)
+                residual_cone_block<1, VT>(D, P, cb, lane, stage, acc, ops);
+            else
+                residual_cone_block<S, VT>(D, P, cb, lane, stage, acc, ops);
         }
     }
     block_reduce_store<RS_COUNT>(acc, ops, D.partials);

@@ -315,29 +315,40 @@ __global__ void dual_start_kernel(int m, const double *start, const double *cr, 
 
 // warp-per-cone projection of a vector (unit metric, d = rescaling)
 template <int S>
+__device__ __forceinline__ void project_cone_block(int st, int L, int tp, double alpha, double *x, const double *d,
+                                                   const double *q, double tau, int lane)
+{
+    WarpSlots<S> sl;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        int i = lane + 32 * s;
+        sl.x[s] = i < L ? x[st + i] : 0.0;
+        sl.d[s] = i < L ? d[st + i] : 1.0;
+        sl.w[s] = (i < L && q) ? 1.0 + tau * q[st + i] : 1.0;
+    }
+    bool uni = warp_uniform_unit<S>(sl, L, lane);
+    warp_project<S>(tp, sl, L, lane, uni, nullptr, alpha);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        int i = lane + 32 * s;
+        if (i < L)
+            x[st + i] = sl.x[s];
+    }
+}
+
+template <int S>
 __global__ void __launch_bounds__(TPB) project_cones_kernel(int ncones, const int *start, const int *len,
-                                                            const int *type, double *x, const double *d,
-                                                            const double *q, double tau)
+                                                            const int *type, const double *alpha, double *x,
+                                                            const double *d, const double *q, double tau)
 {
     const int lane = threadIdx.x & 31;
     for (int cb = blockIdx.x * WARPS + (threadIdx.x >> 5); cb < ncones; cb += gridDim.x * WARPS) {
         const int st = start[cb], L = len[cb], tp = type[cb];
-        WarpSlots<S> sl;
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            int i = lane + 32 * s;
-            sl.x[s] = i < L ? x[st + i] : 0.0;
-            sl.d[s] = i < L ? d[st + i] : 1.0;
-            sl.w[s] = (i < L && q) ? 1.0 + tau * q[st + i] : 1.0;
-        }
-        bool uni = warp_uniform_unit<S>(sl, L, lane);
-        warp_project<S>(tp, sl, L, lane, uni, nullptr);
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            int i = lane + 32 * s;
-            if (i < L)
-                x[st + i] = sl.x[s];
-        }
+        const double a = alpha ? alpha[cb] : 0.0;
+        if (S > 1 && tp >= 2) // 3-slot blocks: the one-slot instantiation
+            project_cone_block<1>(st, L, tp, a, x, d, q, tau, lane);
+        else
+            project_cone_block<S>(st, L, tp, a, x, d, q, tau, lane);
     }
 }
 

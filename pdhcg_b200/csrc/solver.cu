@@ -152,6 +152,27 @@ std::vector<int2> row_tiles(const std::vector<int> &rows)
     return t;
 }
 
+// The primal step launches the SOC / RSOC blocks and the 3-slot blocks
+// (exponential, power) separately: the 3-slot projections would otherwise
+// sit in the wide kernels' register allocation.  A list pointer stays null
+// when its launch covers every block (all of one kind).
+struct ConeSplit {
+    std::vector<int> wide, three;
+    int *wide_d = nullptr, *three_d = nullptr;
+    int n_wide = 0, n_three = 0;
+
+    void build(const std::vector<int> &types)
+    {
+        wide.clear();
+        three.clear();
+        for (int b = 0; b < (int)types.size(); ++b)
+            (types[b] == CONE_EXPONENTIAL || types[b] == CONE_POWER ? three : wide).push_back(b);
+        n_wide = (int)wide.size();
+        n_three = (int)three.size();
+    }
+    bool mixed() const { return n_wide > 0 && n_three > 0; }
+};
+
 // lanes per row from the mean row length
 int pick_group(long long nnz, int rows)
 {
@@ -239,6 +260,7 @@ struct DeviceProblem {
     int n = 0, m = 0, nnzA = 0, nnzQ = 0, qtype = PDHCG_NON_Q, S = 1;
     bool dummy = false, has_g = false, box_free = true, eq_rows = true, cone_box = false;
     std::vector<int> cone_start, cone_len, cone_type, cone_vdim, free_idx;
+    std::vector<double> cone_alpha;
     double obj_const = 0.0;
     int orig_vars = 0, orig_cons = 0, orig_nnz = 0;
     std::string unsupported; // non-empty: reason the device path cannot solve it
@@ -251,6 +273,8 @@ struct DeviceProblem {
     double *R_v = nullptr, *Ddiag = nullptr, *Ddense = nullptr;
     double *c = nullptr, *l = nullptr, *u = nullptr, *lc = nullptr, *uc = nullptr, *g = nullptr;
     int *cst = nullptr, *clen = nullptr, *ctype = nullptr, *cvdim = nullptr, *free_d = nullptr;
+    double *calpha = nullptr; // power-cone exponents per cone block
+    ConeSplit split;            // cone blocks by launch (wide / 3-slot)
     int2 *free_tiles = nullptr; // free variables as tiles of consecutive rows
     int n_free_tiles = 0;
     double *pstart = nullptr, *dstart = nullptr;
@@ -392,8 +416,9 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
             in_cone[j] = 1;
             d.cone_box |= std::isfinite(p->variable_lower_bound[j]) || std::isfinite(p->variable_upper_bound[j]);
         }
-        if (p->cones.type[b] != CONE_STANDARD_SOC && p->cones.type[b] != CONE_ROTATED_SOC)
-            d.unsupported = "only SOC and rotated SOC cones are available on the device path yet";
+        if (p->cones.type[b] == CONE_PSD)
+            d.unsupported = "PSD cones are not available on the device path yet";
+        d.cone_alpha.push_back(p->cones.power_alpha ? p->cones.power_alpha[b] : 0.0);
     }
     int nc = (int)d.cone_start.size();
     if (nc > 0) {
@@ -405,6 +430,13 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
         d.clen = ar.upload(d.cone_len.data(), nc, s);
         d.ctype = ar.upload(d.cone_type.data(), nc, s);
         d.cvdim = ar.upload(d.cone_vdim.data(), nc, s);
+        d.calpha = ar.upload(d.cone_alpha.data(), nc, s);
+        d.split.build(d.cone_type);
+        if (d.split.mixed()) {
+            d.split.wide_d = ar.upload(d.split.wide.data(), d.split.n_wide, s);
+            d.split.three_d = ar.upload(d.split.three.data(), d.split.n_three, s);
+            CK(cudaStreamSynchronize(s));
+        }
         if (!d.free_idx.empty()) {
             d.free_d = ar.upload(d.free_idx.data(), d.free_idx.size(), s);
             std::vector<int2> ft = row_tiles(d.free_idx);
@@ -556,6 +588,36 @@ void dispatch_s(int S, F &&f)
     case 4: f(std::integral_constant<int, 4>{}); break;
     default: f(std::integral_constant<int, 8>{}); break;
     }
+}
+
+// Primal step over the cone blocks: the SOC / RSOC blocks with S slots per
+// lane, the 3-slot blocks with one; returns the number of launches.
+template <typename T>
+int launch_primal_cones(const StepData<T> &D, const StepParams &P, const ConeSplit &sp, int S, bool hasq,
+                        cudaStream_t s)
+{
+    int launches = 0;
+    if (sp.n_wide > 0) {
+        dispatch_s(S, [&](auto SC) {
+            int grid = grid_for(sp.n_wide, WARPS);
+            if (hasq)
+                primal_cone_kernel<SC.value, T, true, CONES_WIDE>
+                    <<<grid, TPB, 0, s>>>(D, P, sp.wide_d, sp.n_wide);
+            else
+                primal_cone_kernel<SC.value, T, false, CONES_WIDE>
+                    <<<grid, TPB, 0, s>>>(D, P, sp.wide_d, sp.n_wide);
+        });
+        ++launches;
+    }
+    if (sp.n_three > 0) {
+        int grid = grid_for(sp.n_three, WARPS);
+        if (hasq)
+            primal_cone_kernel<1, T, true, CONES_THREE><<<grid, TPB, 0, s>>>(D, P, sp.three_d, sp.n_three);
+        else
+            primal_cone_kernel<1, T, false, CONES_THREE><<<grid, TPB, 0, s>>>(D, P, sp.three_d, sp.n_three);
+        ++launches;
+    }
+    return launches;
 }
 
 template <typename F>
@@ -749,8 +811,8 @@ void Solve::init_state()
         CK(cudaMemsetAsync(cone_warm_, 0, 3 * (size_t)nc * sizeof(double), s)); // 0 = no warm start
         cone_aux_init_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(nc, cst_d_, cvdim_d_, ctype_d_, vr_d_, sb_, x0_);
         dispatch_s(S_, [&](auto SC) {
-            project_cones_kernel<SC.value><<<grid_for(nc, WARPS), TPB, 0, s>>>(nc, cst_d_, clen_d_, ctype_d_, x0_,
-                                                                             vr_d_, nullptr, 0.0);
+            project_cones_kernel<SC.value><<<grid_for(nc, WARPS), TPB, 0, s>>>(nc, cst_d_, clen_d_, ctype_d_,
+                                                                             dp_.calpha, x0_, vr_d_, nullptr, 0.0);
         });
     }
     box_clamp_copy_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(n, l_d_, u_d_, x0_, x_, xp_, xr_);
@@ -801,6 +863,7 @@ BBData Solve::bb_data() const
     D.cone_start = cst_d_;
     D.cone_len = clen_d_;
     D.cone_type = ctype_d_;
+    D.cone_alpha = dp_.calpha;
     D.n_cones = (int)cone_start_.size();
     D.vr = vr_d_;
     D.cone_warm = cone_warm_;
@@ -988,6 +1051,7 @@ StepData<T> Solve::step_data()
     D.cone_start = cst_d_;
     D.cone_len = clen_d_;
     D.cone_type = ctype_d_;
+    D.cone_alpha = dp_.calpha;
     D.n_cones = (int)cone_start_.size();
     if constexpr (std::is_same<T, double>::value) {
         D.A_v = A_.v;
@@ -1170,16 +1234,8 @@ void Solve::enqueue_step_t(bool store_primal, bool store_dual, bool want_fpe, do
         }
         stats_.kernel_launches++;
     }
-    if (D.n_cones > 0) {
-        dispatch_s(S_, [&](auto SC) {
-            int grid = grid_for(D.n_cones, WARPS);
-            if (hasq)
-                primal_cone_kernel<SC.value, T, true><<<grid, TPB, 0, s>>>(D, P);
-            else
-                primal_cone_kernel<SC.value, T, false><<<grid, TPB, 0, s>>>(D, P);
-        });
-        stats_.kernel_launches++;
-    }
+    if (D.n_cones > 0)
+        stats_.kernel_launches += launch_primal_cones(D, P, dp_.split, S_, hasq, s);
     launch_dual<T>(D, P);
     stats_.step_kernel_launches++;
     step_bytes_sum_ += step_bytes(sizeof(T), store_primal || !cone_start_.empty(), store_dual);
@@ -1264,6 +1320,7 @@ void Solve::enqueue_residual_t(bool want_dist)
     D.cone_start = cst_d_;
     D.cone_len = clen_d_;
     D.cone_type = ctype_d_;
+    D.cone_alpha = dp_.calpha;
     D.n_cones = (int)cone_start_.size();
     D.partials = partials_;
     D.rows_blocks = res_rows_blocks_;
@@ -1286,6 +1343,7 @@ void Solve::enqueue_residual_t(bool want_dist)
     if (!(sa > 0.0) || !std::isfinite(sa))
         sa = 1.0;
     P.s_aug = sa;
+    P.sb = sb_;
     int nb = D.rows_blocks + D.free_blocks + D.cone_blocks;
     dispatch_s(S_, [&](auto SC) { residual_kernel<SC.value, VT><<<nb, TPB, 0, s>>>(D, P); });
     fold_partials_kernel<<<1, TPB, 0, s>>>(partials_, nb, RS_COUNT, res_ops_d_, scal_d_);
@@ -1471,11 +1529,20 @@ void Solve::read_residual()
     // compute_residual scalars (reference src/pdhg_core_op.cu:1169-1293)
     abs_p_ = nrm(r[RS_PRIMAL_RES]) / sb_;
     double lin_abs_p = abs_p_;
+    // power-cone primal violation joins the primal residual
+    // (reference src/pdhg_core_op.cu:1156-1163 and 1235-1239)
+    const bool cones = !cone_type_.empty();
+    const double pv_abs = nrm(r[RS_POW_ABS]), pv_rel = nrm(r[RS_POW_REL]);
+    auto join = [&](double a, double b) { return l2 ? std::hypot(a, b) : std::fmax(a, b); };
+    if (cones)
+        abs_p_ = join(abs_p_, pv_abs);
     abs_d_ = nrm(r[RS_DUAL_RES]) / sc_;
     double half_xqx = qtype_ == PDHCG_NON_Q ? 0.0 : 0.5 * r[RS_XQX];
     pobj_ = (r[RS_CX] + half_xqx) / (sb_ * sc_) + dp_.obj_const;
     dobj_ = (r[RS_SLACKX] + r[RS_PRIMAL_SLACK] - half_xqx) / (sb_ * sc_) + dp_.obj_const;
     rel_p_ = lin_abs_p / (1.0 + bnorm_);
+    if (cones)
+        rel_p_ = join(rel_p_, pv_rel);
     double den;
     if (qtype_ == PDHCG_NON_Q)
         den = 1.0 + cnorm_;
@@ -1721,7 +1788,7 @@ pdhcg_result_t *Solve::run()
     h_scal_ = pinned_scalars();
     {
         int nop = prm_.optimality_norm == NORM_TYPE_L2 ? RSUM : RMAX;
-        int res_ops[RS_COUNT] = {nop, RSUM, nop, RSUM, RSUM, RSUM, nop, nop, RSUM, RSUM};
+        int res_ops[RS_COUNT] = {nop, RSUM, nop, RSUM, RSUM, RSUM, nop, nop, RSUM, RSUM, nop, nop};
         int fpe_ops[FP_COUNT] = {RSUM, RSUM, RSUM};
         int norm_ops[NS_COUNT] = {RSUM, RSUM, RMAX, RMAX};
         res_ops_d_ = ar_.upload(res_ops, RS_COUNT, st_);
@@ -1786,9 +1853,10 @@ pdhcg_result_t *Solve::run()
 int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cudaStream_t s)
 {
     int n = t->n, nc = t->num_cones;
-    int *len_d = nullptr, *free_d = nullptr;
+    int *len_d = nullptr, *free_d = nullptr, *ids_d = nullptr;
     int2 *tiles_d = nullptr;
     int S = 1;
+    ConeSplit split;
     if (nc > 0) {
         std::vector<int> st(nc), vd(nc), tp(nc), len(nc);
         CK(cudaMemcpyAsync(st.data(), t->cone_start, nc * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1811,6 +1879,15 @@ int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cuda
         if (S < 0)
             return -2;
         std::vector<int2> ft = row_tiles(fr);
+        split.build(tp);
+        if (split.mixed()) {
+            CK(cudaMallocAsync((void **)&ids_d, nc * sizeof(int), s));
+            CK(cudaMemcpyAsync(ids_d, split.wide.data(), split.n_wide * sizeof(int), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(ids_d + split.n_wide, split.three.data(), split.n_three * sizeof(int),
+                               cudaMemcpyHostToDevice, s));
+            split.wide_d = ids_d;
+            split.three_d = ids_d + split.n_wide;
+        }
         CK(cudaMallocAsync((void **)&len_d, nc * sizeof(int), s));
         CK(cudaMallocAsync((void **)&free_d, std::max<size_t>(fr.size(), 1) * sizeof(int), s));
         CK(cudaMallocAsync((void **)&tiles_d, std::max<size_t>(ft.size(), 1) * sizeof(int2), s));
@@ -1827,6 +1904,7 @@ int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cuda
         D.cone_start = t->cone_start;
         D.cone_len = len_d;
         D.cone_type = t->cone_type;
+        D.cone_alpha = t->cone_alpha;
         D.n_cones = nc;
     }
     bool hasq = t->q_diag != nullptr;
@@ -1840,12 +1918,7 @@ int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cuda
             primal_free_kernel<double, false, true><<<grid, TPB, 0, s>>>(D, P);
     }
     if (nc > 0)
-        dispatch_s(S, [&](auto SC) {
-            if (hasq)
-                primal_cone_kernel<SC.value, double, true><<<grid_for(nc, WARPS), TPB, 0, s>>>(D, P);
-            else
-                primal_cone_kernel<SC.value, double, false><<<grid_for(nc, WARPS), TPB, 0, s>>>(D, P);
-        });
+        launch_primal_cones(D, P, split, S, hasq, s);
     int dgrid = grid_for(((long long)t->m + 31) / 32, WARPS);
     if (t->affine_offset)
         dual_kernel<double, false, true><<<dgrid, TPB, 0, s>>>(D, P);
@@ -1858,6 +1931,8 @@ int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cuda
         CK(cudaFreeAsync(free_d, s));
     if (tiles_d)
         CK(cudaFreeAsync(tiles_d, s));
+    if (ids_d)
+        CK(cudaFreeAsync(ids_d, s));
     return 0;
 }
 
@@ -1869,7 +1944,8 @@ int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cuda
 constexpr int NOALLOC_MAX_CONES = PDHCG_B200_NOALLOC_MAX_CONES;
 static __device__ __align__(256) int g_noalloc_scratch[NOALLOC_MAX_CONES + 2];
 
-__global__ void __launch_bounds__(TPB) noalloc_len_kernel(int nc, const int *vdim, const int *type, int *scratch)
+__global__ void __launch_bounds__(TPB) noalloc_len_kernel(int nc, const int *vdim, const int *type, int has_alpha,
+                                                          int *scratch)
 {
     __shared__ int sh_max[TPB], sh_bad[TPB];
     int mx = 0, bad = 0;
@@ -1878,7 +1954,8 @@ __global__ void __launch_bounds__(TPB) noalloc_len_kernel(int nc, const int *vdi
         const int len = (t == 2 || t == 3) ? 3 : (t == 4 ? v * (v + 1) / 2 : v + 2);
         scratch[b] = len;
         mx = max(mx, len);
-        bad |= (t != CONE_STANDARD_SOC && t != CONE_ROTATED_SOC);
+        bad |= !(t == CONE_STANDARD_SOC || t == CONE_ROTATED_SOC || t == CONE_EXPONENTIAL ||
+                 (t == CONE_POWER && has_alpha));
     }
     sh_max[threadIdx.x] = mx;
     sh_bad[threadIdx.x] = bad;
@@ -2099,7 +2176,6 @@ int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *co
                              const double *cone_alpha, double *x, const double *d, const double *q, double tau,
                              void *stream)
 {
-    (void)cone_alpha;
     cudaStream_t s = (cudaStream_t)stream;
     if (num_cones <= 0)
         return 0;
@@ -2120,11 +2196,13 @@ int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *co
         }
         for (int i = 0; i < num_cones; ++i) {
             maxlen = std::max(maxlen, h[i]);
-            types_ok = types_ok && (t[i] == CONE_STANDARD_SOC || t[i] == CONE_ROTATED_SOC);
+            types_ok = types_ok && (t[i] == CONE_STANDARD_SOC || t[i] == CONE_ROTATED_SOC ||
+                                    t[i] == CONE_EXPONENTIAL || (t[i] == CONE_POWER && cone_alpha));
         }
     }
-    if (!types_ok) { // the exponential, power and PSD projections are not built
-        std::fprintf(stderr, "[pdhcg_b200_project_cones] only SOC and rotated-SOC blocks are supported.\n");
+    if (!types_ok) { // the PSD projection is not built; a power block needs its exponent
+        std::fprintf(stderr, "[pdhcg_b200_project_cones] only SOC, rotated-SOC, exponential and power blocks "
+                             "(with cone_alpha) are supported.\n");
         cudaFreeAsync(len, s);
         return -3;
     }
@@ -2135,7 +2213,8 @@ int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *co
     }
     dispatch_s(S, [&](auto SC) {
         project_cones_kernel<SC.value><<<grid_for(num_cones, WARPS), TPB, 0, s>>>(num_cones, cone_start, len,
-                                                                                 cone_type, x, d, q, tau);
+                                                                                 cone_type, cone_alpha, x, d, q,
+                                                                                 tau);
     });
     cudaFreeAsync(len, s);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
@@ -2145,7 +2224,6 @@ int pdhcg_b200_project_cones_noalloc(int num_cones, const int *cone_start, const
                                      const int *cone_type, const double *cone_alpha, double *x, const double *d,
                                      const double *q, double tau, void *stream)
 {
-    (void)cone_alpha;
     cudaStream_t s = (cudaStream_t)stream;
     if (num_cones <= 0)
         return 0;
@@ -2159,13 +2237,14 @@ int pdhcg_b200_project_cones_noalloc(int num_cones, const int *cone_start, const
     int *scratch = noalloc_scratch();
     if (!scratch)
         return -1;
-    noalloc_len_kernel<<<1, TPB, 0, s>>>(num_cones, cone_vdim, cone_type, scratch);
+    noalloc_len_kernel<<<1, TPB, 0, s>>>(num_cones, cone_vdim, cone_type, cone_alpha != nullptr, scratch);
     int info[2] = {0, 0}; // longest block, unsupported-type flag
     if (cudaMemcpyAsync(info, scratch + NOALLOC_MAX_CONES, sizeof(info), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
         return -1;
     if (info[1]) {
-        std::fprintf(stderr, "[pdhcg_b200_project_cones_noalloc] only SOC and rotated-SOC blocks are supported.\n");
+        std::fprintf(stderr, "[pdhcg_b200_project_cones_noalloc] only SOC, rotated-SOC, exponential and power "
+                             "blocks (with cone_alpha) are supported.\n");
         return -3;
     }
     int S = slots_class(info[0]);
@@ -2173,7 +2252,8 @@ int pdhcg_b200_project_cones_noalloc(int num_cones, const int *cone_start, const
         return -2;
     dispatch_s(S, [&](auto SC) {
         project_cones_kernel<SC.value><<<grid_for(num_cones, WARPS), TPB, 0, s>>>(num_cones, cone_start, scratch,
-                                                                                 cone_type, x, d, q, tau);
+                                                                                 cone_type, cone_alpha, x, d, q,
+                                                                                 tau);
     });
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

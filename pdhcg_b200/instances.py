@@ -20,7 +20,7 @@ from __future__ import annotations
 import numpy as np
 import scipy.sparse as sp
 
-from .capi import CONE_ROTATED_SOC, CONE_STANDARD_SOC, Cone, CsrMatrix, Problem
+from .capi import CONE_EXPONENTIAL, CONE_POWER, CONE_ROTATED_SOC, CONE_STANDARD_SOC, Cone, CsrMatrix, Problem
 
 
 def random_csr(rng: np.random.Generator, m: int, n: int, per_row: int, values: str = "normal") -> CsrMatrix:
@@ -104,11 +104,13 @@ def diag_qp(seed: int = 4, n: int = 300, m: int = 150) -> Problem:
 
 
 def conic_lp(seed: int = 5, nfree: int = 60, nsoc: int = 10, soc_len: int = 12, nrsoc: int = 4,
-             rsoc_len: int = 8, with_q: bool = False) -> Problem:
-    """Free box variables plus SOC and rotated-SOC blocks, equality rows
-    through a strictly feasible point (so the problem is feasible)."""
+             rsoc_len: int = 8, with_q: bool = False, nexp: int = 0, npow: int = 0) -> Problem:
+    """Free box variables plus SOC, rotated-SOC, exponential and power
+    blocks (exponents U(0.2, 0.8)), equality rows through a strictly
+    feasible point (so the problem is feasible) and an objective inside the
+    dual cone on the cone slots (so it is bounded)."""
     rng = np.random.default_rng(seed)
-    n = nfree + nsoc * soc_len + nrsoc * rsoc_len
+    n = nfree + nsoc * soc_len + nrsoc * rsoc_len + 3 * (nexp + npow)
     m = n // 3
     A = random_csr(rng, m, n, 5)
     x0 = np.zeros(n)
@@ -129,6 +131,17 @@ def conic_lp(seed: int = 5, nfree: int = 60, nsoc: int = 10, soc_len: int = 12, 
         x0[st + rsoc_len - 1] = (v @ v) / (2 * s_) + 1.0
         cones.append(Cone(CONE_ROTATED_SOC, st, rsoc_len - 2))
         st += rsoc_len
+    for _ in range(nexp):  # y exp(x / y) < z
+        xe, ye = rng.standard_normal(), 1.0 + rng.random()
+        x0[st:st + 3] = xe, ye, ye * np.exp(xe / ye) + 1.0
+        cones.append(Cone(CONE_EXPONENTIAL, st, 1))
+        st += 3
+    for _ in range(npow):  # x^a y^(1-a) > |z|
+        a = rng.uniform(0.2, 0.8)
+        xp_, yp_ = 1.0 + rng.random(), 1.0 + rng.random()
+        x0[st:st + 3] = xp_, yp_, 0.5 * xp_ ** a * yp_ ** (1 - a) * rng.choice([-1.0, 1.0])
+        cones.append(Cone(CONE_POWER, st, 1, a))
+        st += 3
     b = A.to_scipy() @ x0
     lb = np.full(n, -np.inf)
     ub = np.full(n, np.inf)
@@ -141,6 +154,14 @@ def conic_lp(seed: int = 5, nfree: int = 60, nsoc: int = 10, soc_len: int = 12, 
         L = k.v_dim + 2
         if k.type == CONE_STANDARD_SOC:
             c[st + L - 1] = np.linalg.norm(c[st:st + L - 1]) + 1.0
+        elif k.type == CONE_EXPONENTIAL:  # K* = {(u, v, w): u < 0, -u exp(v / u) <= e w}
+            u = -(0.5 + rng.random())
+            c[st] = u
+            c[st + 2] = -u * np.exp(c[st + 1] / u) / np.e + 1.0
+        elif k.type == CONE_POWER:  # K* = {(u, v, w): (u / a)^a (v / (1 - a))^(1 - a) >= |w|}
+            a = k.alpha
+            c[st], c[st + 1] = 0.5 + rng.random(), 0.5 + rng.random()
+            c[st + 2] = 0.5 * (c[st] / a) ** a * (c[st + 1] / (1 - a)) ** (1 - a) * np.sign(c[st + 2])
         else:
             c[st + L - 2] = abs(c[st + L - 2]) + 1.0
             c[st + L - 1] = (c[st:st + L - 2] @ c[st:st + L - 2]) / (2 * c[st + L - 2]) + 1.0

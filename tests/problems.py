@@ -6,7 +6,8 @@ CUDA solver are both checked against the answers the reference asserts.
 """
 import numpy as np
 
-from pdhcg_b200.capi import (CONE_ROTATED_SOC, CONE_STANDARD_SOC, Cone, CsrMatrix, Problem)
+from pdhcg_b200.capi import (CONE_EXPONENTIAL, CONE_POWER, CONE_ROTATED_SOC, CONE_STANDARD_SOC, NORM_L2, Cone, CsrMatrix,
+                             Problem)
 
 BIG = 1e30
 
@@ -71,7 +72,56 @@ def rsoc_diag_q_asym():
                     "tol": 1e-3}
 
 
+def exp_cone_linear():
+    """test/test_conic_e2e.c:148-215: min -x s.t. y = 1, z = 2, (x, y, z) in
+    K_exp.  Expected x = log 2, y = 1, z = 2 (tol 5e-3)."""
+    A = CsrMatrix(2, 3, np.array([0, 1, 2]), np.array([1, 2]), np.array([1.0, 1.0]))
+    p = Problem(c=np.array([-1.0, 0.0, 0.0]), A=A, con_lb=np.array([1.0, 2.0]), con_ub=np.array([1.0, 2.0]),
+                var_lb=np.full(3, -BIG), var_ub=np.full(3, BIG), cones=[Cone(CONE_EXPONENTIAL, 0, 1)])
+    prm = {"termination_criteria.eps_optimal_relative": 1e-6, "termination_criteria.eps_feasible_relative": 1e-6,
+           "termination_criteria.iteration_limit": 1000000}
+    return p, prm, {"x": [np.log(2.0), 1.0, 2.0], "tol": 5e-3}
+
+
+_POW_PRM = {"termination_evaluation_frequency": 10, "termination_criteria.eps_optimal_relative": 1e-8,
+            "termination_criteria.eps_feasible_relative": 1e-8, "termination_criteria.iteration_limit": 1000000}
+
+
+def pow_full_cone(alpha, l2=False):
+    """test/test_power_cone.c:109-152: max z s.t. x + y = 2, (x, y, z) in
+    K_alpha, started from (1, 1, 0).  Expected (2a, 2(1-a), (2a)^a (2(1-a))^(1-a))
+    (tol 2e-5)."""
+    A = CsrMatrix(1, 3, np.array([0, 2]), np.array([0, 1]), np.array([1.0, 1.0]))
+    p = Problem(c=np.array([0.0, 0.0, -1.0]), A=A, con_lb=np.array([2.0]), con_ub=np.array([2.0]),
+                var_lb=np.full(3, -np.inf), var_ub=np.full(3, np.inf), cones=[Cone(CONE_POWER, 0, 1, alpha=alpha)],
+                primal_start=np.array([1.0, 1.0, 0.0]), dual_start=np.array([0.0]))
+    om = 1.0 - alpha
+    prm = dict(_POW_PRM)
+    if l2:
+        prm["optimality_norm"] = NORM_L2
+    return p, prm, {"x": [2 * alpha, 2 * om, (2 * alpha) ** alpha * (2 * om) ** om], "tol": 2e-5, "nonzero_iters": True}
+
+
+def pow_diag_q():
+    """test/test_power_cone.c:196-209: min sum w_i (x_i - c_i)^2 / 2 over the
+    power cone (a = 0.7, no rows), center (1.5, -0.4, -2.2), weights
+    (0.3, 2, 5).  Expected (3.427365210244501, 0.4816579589566281,
+    -1.902365192823554) (tol 2e-4)."""
+    center, w = np.array([1.5, -0.4, -2.2]), np.array([0.3, 2.0, 5.0])
+    A = CsrMatrix(0, 3, np.array([0]), np.zeros(0, np.int32), np.zeros(0))
+    Q = CsrMatrix(3, 3, np.array([0, 1, 2, 3]), np.array([0, 1, 2]), w)
+    p = Problem(c=-w * center, A=A, Q=Q, var_lb=np.full(3, -np.inf), var_ub=np.full(3, np.inf),
+                cones=[Cone(CONE_POWER, 0, 1, alpha=0.7)])
+    return p, dict(_POW_PRM), {"x": [3.427365210244501, 0.4816579589566281, -1.902365192823554], "tol": 2e-4}
+
+
 KNOWN_ANSWERS = {
+    "exp_cone_linear": exp_cone_linear,
+    "pow_full_cone_0.2": lambda: pow_full_cone(0.2),
+    "pow_full_cone_0.5": lambda: pow_full_cone(0.5),
+    "pow_full_cone_0.8": lambda: pow_full_cone(0.8),
+    "pow_full_cone_0.5_l2": lambda: pow_full_cone(0.5, l2=True),
+    "pow_diag_q": pow_diag_q,
     "lp_small": lp_small,
     "sparse_q_soc": sparse_q_soc,
     "soc_diag_q": soc_diag_q,
@@ -86,11 +136,14 @@ def check_known_answer(res: dict, expect: dict):
     tol = expect["tol"]
     x = res["x"]
     if "x" in expect:
-        np.testing.assert_allclose(x, expect["x"], atol=tol * (1 + np.abs(expect["x"])).max())
+        e = np.asarray(expect["x"], dtype=float)
+        assert np.all(np.abs(np.asarray(x) - e) <= tol * (1 + np.abs(e))), (x, e)
     if "y" in expect:
         np.testing.assert_allclose(res["y"], expect["y"], atol=tol * 10)
     if "obj" in expect:
         assert abs(res["primal_objective_value"] - expect["obj"]) <= 10 * tol * (1 + abs(expect["obj"]))
+    if expect.get("nonzero_iters"):
+        assert res["total_count"] > 0  # a feasible non-optimal start must not pass at iteration 0
     if expect.get("soc_kkt"):
         v, w, z = x
         assert abs(w - 4.0) <= tol * 5

@@ -76,13 +76,52 @@ def test_cone_projection_matches_oracle(lib, oracle, weighted, uniform_d):
     np.testing.assert_allclose(got, expect, rtol=tol, atol=tol * np.abs(expect).max())
 
 
+@pytest.mark.parametrize("weighted", [False, True])
+def test_exp_pow_projection_matches_oracle(lib, oracle, weighted):
+    """Exponential and power blocks (one thread per block on the device)
+    against the oracle's restatement of the reference's point projections:
+    points inside, in the polar / opposite cone and in general position,
+    power exponents across (0, 1).  Tolerance 1e-9 (math-library round-off
+    through the Newton / bisection steps)."""
+    import torch
+    rng = np.random.default_rng(11 + weighted)
+    nb = 600
+    types = rng.choice([capi.CONE_EXPONENTIAL, capi.CONE_POWER], nb)
+    alpha = rng.uniform(0.1, 0.9, nb)
+    x = rng.standard_normal(3 * nb) * rng.choice([0.1, 1.0, 10.0], 3 * nb)
+    x[0:30:3] = -np.abs(x[0:30:3])  # some x <= 0, y <= 0 points
+    x[1:30:3] = -np.abs(x[1:30:3])
+    d = np.repeat(rng.uniform(0.5, 2.0, nb), 3) * rng.uniform(0.8, 1.25, 3 * nb)
+    q = rng.uniform(0.0, 2.0, 3 * nb) if weighted else None
+    tau = 0.37
+    expect = x.copy()
+    for b in range(nb):
+        blk = expect[3 * b:3 * b + 3].copy()
+        dd = d[3 * b:3 * b + 3].copy()
+        qq = q[3 * b:3 * b + 3].copy() if weighted else None
+        oracle.oracle_project_cone_block(int(types[b]), 1, float(alpha[b]), blk.ctypes.data_as(_dp),
+                                         dd.ctypes.data_as(_dp), qq.ctypes.data_as(_dp) if weighted else None, tau)
+        expect[3 * b:3 * b + 3] = blk
+    starts = _dev(np.arange(nb) * 3, np.int32)
+    vdims = _dev(np.ones(nb), np.int32)
+    tp = _dev(types, np.int32)
+    al = _dev(alpha)
+    xd, dd_, qd = _dev(x), _dev(d), (_dev(q) if weighted else None)
+    rc = lib.pdhcg_b200_project_cones(nb, _ptr(starts), _ptr(vdims), _ptr(tp), _ptr(al), _ptr(xd), _ptr(dd_),
+                                      _ptr(qd), tau, None)
+    torch.cuda.synchronize()
+    assert rc == 0
+    got = xd.cpu().numpy()
+    np.testing.assert_allclose(got, expect, rtol=1e-9, atol=1e-9 * np.abs(expect).max())
+
+
 def test_cone_projection_rejects_unbuilt_cone_types(lib):
-    """An exponential block is refused (-3) and x is left untouched."""
+    """A PSD block is refused (-3) and x is left untouched."""
     import torch
     x = np.arange(8, dtype=np.float64)
     xd = _dev(x)
-    starts, vdims = _dev([0, 3], np.int32), _dev([1, 3], np.int32)
-    types = _dev([capi.CONE_STANDARD_SOC, capi.CONE_EXPONENTIAL], np.int32)
+    starts, vdims = _dev([0, 3], np.int32), _dev([1, 2], np.int32)
+    types = _dev([capi.CONE_STANDARD_SOC, capi.CONE_PSD], np.int32)
     d = _dev(np.ones(8))
     rc = lib.pdhcg_b200_project_cones(2, _ptr(starts), _ptr(vdims), _ptr(types), None, _ptr(xd), _ptr(d), None,
                                       1.0, None)

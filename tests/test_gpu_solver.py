@@ -68,6 +68,10 @@ CASES = {
     "conic_qp_curtis_reid": (lambda: instances.conic_lp(seed=11, with_q=True), {"curtis_reid_iterations": 5}),
     "conic_lp_curtis_reid_np": (lambda: instances.conic_lp(seed=12), {"curtis_reid_iterations": 5,
                                                                        "use_cone_preserving_scaling": False}),
+    # every cone kind in one problem: the SOC / RSOC launch and the 3-slot launch of the step
+    "mixed_cones_lp": (lambda: instances.conic_lp(seed=13, nexp=12, npow=12), {}),
+    "mixed_cones_qp": (lambda: instances.conic_lp(seed=14, with_q=True, nexp=10, npow=10), {}),
+    "exp_pow_only_qp": (lambda: instances.conic_lp(seed=15, nsoc=0, nrsoc=0, with_q=True, nexp=15, npow=15), {}),
 }
 
 

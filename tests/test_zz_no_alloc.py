@@ -67,7 +67,7 @@ def test_noalloc_projection_limits_and_errors(lib):
     assert lib.pdhcg_b200_project_cones_noalloc(NOALLOC_MAX_CONES + 1, None, None, None, None, None, None, None,
                                                 1.0, None) == -4
     # a cone type without a projection: -3, x untouched
-    blocks, x, d, _ = _case(13, [(3, 1), (3, capi.CONE_EXPONENTIAL)], False)
+    blocks, x, d, _ = _case(13, [(3, 1), (3, capi.CONE_PSD)], False)
     rc, got = _run(lib.pdhcg_b200_project_cones_noalloc, blocks, x, d, None, 1.0)
     assert rc == -3
     np.testing.assert_array_equal(got, x)
