@@ -36,6 +36,38 @@ EPS = 1e-6
 METRIC = "time-to-1e-6 KKT (s) & SpMV GB/s: mixed/warm-start vs plain FP64, 1 B200"
 WORKLOAD = "soc_qp: n=1e6 (20000 SOC blocks x 50), m=5e5 eq rows, 10 nnz/row, diag Q, eps 1e-6"
 
+# Single-instance workloads: the generator, the forms the solver has for the
+# problem class (the inner BB solve of sparse / low-rank Q runs in FP64
+# only) and what keeps the timed solves out of L2.
+WORKLOADS = {
+    "soc_qp": {"make": lambda scale, r: instances.soc_qp(seed=2 + r, scale=scale), "desc": WORKLOAD,
+               "mixed": True, "l2": "working set (>=134 MB) larger than L2"},
+    "sparse_qp": {"make": lambda scale, r: instances.sparse_qp(seed=1 + r, scale=scale),
+                  "desc": "sparse_qp: n=1e4, m=5e3, 8 nnz/row, Q = B'B + 0.1 I (B 2000 x 1e4, 4 nnz/row; "
+                          "sparse Q, inner BB solve), box [-10, 10], eps 1e-6",
+                  "mixed": False, "l2": "L2-resident working set (< 3 MB): latency-bound, time to tolerance"},
+    "portfolio": {"make": lambda scale, r: instances.portfolio(seed=3 + r, scale=scale),
+                  "desc": "portfolio: n=2e5 assets, R 100 x 2e5 dense N(0, 1/sqrt n), D diag U(0.5, 2), "
+                          "Q diag U(1e-4, 1e-2), budget + 500 sector + 100 exposure rows, RSOC tracking-error "
+                          "block, x in [0, 0.02], eps 1e-6",
+                  "mixed": False, "l2": "working set (A, R and R^T, >700 MB) larger than L2"},
+}
+
+
+def _h2d_bytes(p) -> int:
+    """Bytes of the problem arrays a host-buffer solve copies to the device."""
+    n, m = p.n, (p.A.m if p.A is not None else 0)
+    b = 3 * n * 8 + 2 * m * 8
+    for M in (p.A, p.Q):
+        if M is not None:
+            b += M.nnz * 12 + (M.m + 1) * 4
+    if getattr(p, "R_dense", None) is not None:
+        b += p.R_dense.size * 8
+    if getattr(p, "D", None) is not None:
+        b += p.D.nnz * 12 + (p.D.m + 1) * 4
+    b += 12 * len(p.cones or [])
+    return int(b)
+
 
 def _params(lib, iters=None):
     over = {"termination_criteria.eps_optimal_relative": EPS, "termination_criteria.eps_feasible_relative": EPS,
@@ -135,10 +167,11 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", init_method="env://")
     lib = native.load()
-    problem = instances.soc_qp(seed=2 + rank, scale=args.scale)
+    W = WORKLOADS[args.workload]
+    problem = W["make"](args.scale, rank)
     prob, keep = capi.build(lib, problem)
     prm = _params(lib, args.iters)
-    forms = {"fp64": 0, "mixed": 1}
+    forms = {"fp64": 0, "mixed": 1} if W["mixed"] else {"fp64": 0}
     handle = lib.pdhcg_b200_upload(prob)
     if not handle:
         raise RuntimeError("pdhcg_b200_upload failed")
@@ -160,7 +193,7 @@ def run_ours(args):
             rr = r.contents
             d = {"status": capi.TERMINATION_REASONS[rr.termination_reason], "total_count": rr.total_count,
                  "rel_kkt": max(rr.relative_primal_residual, rr.relative_dual_residual, rr.relative_objective_gap),
-                 "primal_objective_value": rr.primal_objective_value}
+                 "primal_objective_value": rr.primal_objective_value, "total_inner_count": rr.total_inner_count}
         else:
             d = capi.result_dict(r, problem.n, problem.A.m)
         lib.pdhcg_result_free(r)
@@ -209,30 +242,27 @@ def run_ours(args):
                 "frac": (ach / peak) if ach else None, "traffic": None, "peak_kind": peak_kind,
                 "bytes_per_step": tstats["step_bytes"], "step_kernel_ms": step_ms}
 
-    mixed, fp64 = out["mixed"], out["fp64"]
-    per_solve, _, res, stats, clocks = mixed["device"]
-    e2e_solve, _, e2e_res, e2e_stats, _ = mixed["host"]
-    rl = roof(mixed["tstats"])
+    head = out["mixed"] if W["mixed"] else out["fp64"]
+    fp64 = out["fp64"]
+    per_solve, _, res, stats, clocks = head["device"]
+    e2e_solve, _, e2e_res, e2e_stats, _ = head["host"]
+    rl = roof(head["tstats"])
     line = {
         "metric": METRIC, "value": per_solve, "unit": "s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_solve * 1e3,
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "parallelism": "replicas" if world > 1 else "single",
-                   "eps": EPS, "form": "mixed: FP32 bulk, FP64 polish below 1e-5",
-                   "l2_flush": "working set (>=134 MB) larger than L2",
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if W["mixed"] else "f64", "data": "synthetic",
+        "config": {"workload": W["desc"], "parallelism": "replicas" if world > 1 else "single",
+                   "eps": EPS, "form": "mixed: FP32 bulk, FP64 polish below 1e-5" if W["mixed"] else "FP64",
+                   "l2_flush": W["l2"],
                    "inputs": "value: problem resident in HBM (pdhcg_b200_upload once), solution left on device; "
                              "e2e: host buffers through pdhcg_b200_solve"},
         "status": res["status"], "iterations": res["total_count"], "rel_kkt": res["rel_kkt"],
         "objective": res["primal_objective_value"], "fp32_iterations": stats["fp32_iterations"],
-        "fp64_form": {"value": fp64["device"][0], "e2e": fp64["host"][0], "status": fp64["device"][2]["status"],
-                      "iterations": fp64["device"][2]["total_count"], "rel_kkt": fp64["device"][2]["rel_kkt"],
-                      "objective": fp64["device"][2]["primal_objective_value"], "roofline": roof(fp64["tstats"])},
-        "speedup_mixed_vs_fp64": fp64["device"][0] / per_solve,
         "spmv_gbs": rl["achieved"],
         "roofline": rl,
         "e2e": {"value": e2e_solve, "unit": "s",
-                "h2d_bytes_per_step": int(problem.A.nnz * 12 + (problem.A.m + 1) * 4 + problem.n * 8 * 4 +
-                                          problem.A.m * 8 * 3 + problem.n * 12),
+                "h2d_bytes_per_step": _h2d_bytes(problem),
                 "d2h_bytes_per_step": int(8 * (2 * problem.n + problem.A.m)),
                 "status": e2e_res["status"], "iterations": e2e_res["total_count"]},
         "gpu_launches": int(stats["kernel_launches"]) * args.steps,
@@ -242,6 +272,15 @@ def run_ours(args):
         "e2e_breakdown_ms": {k: e2e_stats[k] for k in ("host_copy_ms", "upload_ms", "setup_ms", "loop_ms",
                                                        "result_ms", "total_ms")},
     }
+    if W["mixed"]:
+        line["fp64_form"] = {"value": fp64["device"][0], "e2e": fp64["host"][0],
+                             "status": fp64["device"][2]["status"], "iterations": fp64["device"][2]["total_count"],
+                             "rel_kkt": fp64["device"][2]["rel_kkt"],
+                             "objective": fp64["device"][2]["primal_objective_value"],
+                             "roofline": roof(fp64["tstats"])}
+        line["speedup_mixed_vs_fp64"] = fp64["device"][0] / per_solve
+    else:
+        line["inner_iterations"] = res.get("total_inner_count")
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(problem, res["total_count"])
     print(json.dumps(line))
@@ -461,13 +500,14 @@ def run_reference(args):
     if rank != 0:
         return
     path = os.path.join(ROOT, "oracle", "_ref", "libpdhcg_ref.so")
-    problem = instances.soc_qp(seed=2, scale=args.scale)
+    W = WORKLOADS.get(args.workload, WORKLOADS["soc_qp"])
+    problem = W["make"](args.scale, 0)
     if not os.path.exists(path):
         lib = native.load(build=False)
         cb = cpu_baseline(problem, 3000)
         print(json.dumps({"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "s",
                           "higher_is_better": False, "n_gpus": 1, "steps": 1, "warmup": 0,
-                          "config": {"workload": WORKLOAD}, "cpu_baseline": cb,
+                          "config": {"workload": W["desc"]}, "cpu_baseline": cb,
                           "e2e": {"value": cb["value"], "unit": "s", "h2d_bytes_per_step": 0,
                                   "d2h_bytes_per_step": 0}}))
         return
@@ -491,7 +531,7 @@ def run_reference(args):
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": per, "unit": "s", "higher_is_better": False,
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": WORKLOAD, "eps": EPS},
+        "data": "synthetic", "config": {"workload": W["desc"], "eps": EPS},
         "status": res["status"], "iterations": res["total_count"], "rel_kkt": res["rel_kkt"],
         "objective": res["primal_objective_value"], "reference_loop_s": res["cumulative_time_sec"],
         "cpu_baseline": {"value": per, "unit": "s", "cores": 1, "kind": "reference",
@@ -508,8 +548,10 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = the benchmark size)")
     ap.add_argument("--iters", type=int, default=None, help="iteration cap (profiling only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="soc_qp", choices=["soc_qp", "mpc_batch", "warm_start"],
-                    help="soc_qp: the headline single-instance workload; mpc_batch: the batched workload; "
+    ap.add_argument("--workload", default="soc_qp",
+                    choices=["soc_qp", "sparse_qp", "portfolio", "mpc_batch", "warm_start"],
+                    help="soc_qp: the headline single-instance workload; sparse_qp: sparse-Q QP (inner BB "
+                         "solve); portfolio: low-rank portfolio QP; mpc_batch: the batched workload; "
                          "warm_start: the learned warm start on the parametric family")
     ap.add_argument("--train", type=int, default=2000, help="warm_start: training solves")
     ap.add_argument("--heldout", type=int, default=200, help="warm_start: held-out solves")

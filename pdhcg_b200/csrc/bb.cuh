@@ -35,8 +35,10 @@ struct BBData {
     int k;                   // low-rank rank (0: none)
     const int *R_rp, *R_ci;  // R, k rows
     const double *R_v;
-    const int *Rt_rp, *Rt_ci; // R^T, n rows
+    const int *Rt_rp, *Rt_ci; // R^T, n rows (not built when r_width > 0)
     const double *Rt_v;
+    int r_width;              // > 0: every row of R holds columns 0..r_width-1 in order, so R_v is
+                              // row-major k x r_width (R^T not built); 0: R and R^T as CSR
     int dkind;               // 0 none (D = I), 1 diagonal, 2 dense (row-major, upper triangle used)
     const double *Ddiag, *Ddense;
     // Jacobi preconditioner M = diag(Q) + 1/tau (NULL: none)
@@ -115,8 +117,12 @@ __device__ void bb_rx_partials(const BBData &D, const double *v)
         long long len = e0 - b0;
         int cb = b0 + (int)(len * blockIdx.x / nb), ce = b0 + (int)(len * (blockIdx.x + 1) / nb);
         double s = 0.0;
-        for (int e = cb + lane; e < ce; e += 32)
-            s += D.R_v[e] * v[D.R_ci[e]];
+        if (D.r_width) // column of entry e is e - b0
+            for (int e = cb + lane; e < ce; e += 32)
+                s += D.R_v[e] * v[e - b0];
+        else
+            for (int e = cb + lane; e < ce; e += 32)
+                s += D.R_v[e] * v[D.R_ci[e]];
         s = warp_sum(s);
         if (lane == 0)
             D.rx_part[(size_t)blockIdx.x * D.k + r] = s;
@@ -167,6 +173,25 @@ __device__ void bb_drx_smem(const BBData &D, double *drx)
     __syncthreads();
 }
 
+// This lane's share (lanes sub, sub + G, ...) of R^T row j . drx
+template <int G>
+__device__ __forceinline__ double bb_rt_part(const BBData &D, const double *drx, int j, int sub)
+{
+    double s = 0.0;
+    if (D.r_width) { // column j of the row-major R, rows in increasing order (the order of R^T row j)
+        if (j < D.r_width) {
+            const double *col = D.R_v + j;
+            for (int r = sub; r < D.k; r += G)
+                s += col[(size_t)r * D.r_width] * drx[r];
+        }
+    } else {
+        int b = D.Rt_rp[j], e = D.Rt_rp[j + 1];
+        for (int t = b + sub; t < e; t += G)
+            s += D.Rt_v[t] * drx[D.Rt_ci[t]];
+    }
+    return s;
+}
+
 // qx_j for one variable, G lanes: Q row j . v + R^T row j . drx.  Every
 // lane of the warp calls it; ok == false gives 0 without reading a row.
 template <int G>
@@ -180,9 +205,7 @@ __device__ __forceinline__ double bb_q_row(const BBData &D, const double *v, con
             s += D.Q_v[t] * v[D.Q_ci[t]];
     }
     if (ok && D.k > 0) {
-        int b = D.Rt_rp[j], e = D.Rt_rp[j + 1];
-        for (int t = b + sub; t < e; t += G)
-            s += D.Rt_v[t] * drx[D.Rt_ci[t]];
+        s += bb_rt_part<G>(D, drx, j, sub);
     }
     return group_sum<G>(s);
 }
@@ -221,11 +244,8 @@ __device__ __forceinline__ double bb_cone_block(const BBData &D, const double *d
                 for (int t = b + sub; t < e; t += G)
                     s += D.Q_v[t] * D.x[D.Q_ci[t]];
             }
-            if (ok && D.k > 0) {
-                int b = D.Rt_rp[j], e = D.Rt_rp[j + 1];
-                for (int t = b + sub; t < e; t += G)
-                    s += D.Rt_v[t] * drx[D.Rt_ci[t]];
-            }
+            if (ok && D.k > 0)
+                s += bb_rt_part<G>(D, drx, j, sub);
             s = group_sum<G>(s);
             if (ok && sub == 0)
                 stage[slot] = s;
@@ -306,11 +326,8 @@ __device__ double bb_var_phase(const BBData &D, const double *drx, bool init, do
                         for (int t = b + sub; t < e; t += G)
                             s += D.Q_v[t] * D.x[D.Q_ci[t]];
                     }
-                    if (ok && D.k > 0) {
-                        int b = D.Rt_rp[j], e = D.Rt_rp[j + 1];
-                        for (int t = b + sub; t < e; t += G)
-                            s += D.Rt_v[t] * drx[D.Rt_ci[t]];
-                    }
+                    if (ok && D.k > 0)
+                        s += bb_rt_part<G>(D, drx, j, sub);
                     q = group_sum<G>(s);
                 }
             }
@@ -470,9 +487,10 @@ __global__ void bb_tol_update_kernel(const double *fpe_sums, double step, double
 
 // diag(Q) + diag(R^T D R) for the preconditioner (reference
 // initialize_inner_solver, src/solver_state.cu:321-367)
+// R_dense: R row-major k x width over columns 0..width-1 (then R^T is not used)
 __global__ void bb_diag_h_kernel(int n, int sparse, const int *Q_rp, const int *Q_ci, const double *Q_v, int k,
-                                 const int *Rt_rp, const int *Rt_ci, const double *Rt_v, int dkind,
-                                 const double *Ddiag, const double *Ddense, double *diag_h)
+                                 const int *Rt_rp, const int *Rt_ci, const double *Rt_v, const double *R_dense,
+                                 int width, int dkind, const double *Ddiag, const double *Ddense, double *diag_h)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double s = 0.0;
@@ -481,7 +499,22 @@ __global__ void bb_diag_h_kernel(int n, int sparse, const int *Q_rp, const int *
                 if (Q_ci[t] == i)
                     s += Q_v[t];
         double r = 0.0;
-        if (k > 0) {
+        if (k > 0 && R_dense) { // column i (empty past the width), rows in increasing order
+            const double *col = R_dense + i;
+            const size_t w = width;
+            if (i >= width)
+                r = 0.0;
+            else if (dkind == 1)
+                for (int a = 0; a < k; ++a)
+                    r += Ddiag[a] * col[a * w] * col[a * w];
+            else if (dkind == 2)
+                for (int a = 0; a < k; ++a)
+                    for (int b = 0; b < k; ++b)
+                        r += col[a * w] * col[b * w] * Ddense[(size_t)a * k + b];
+            else
+                for (int a = 0; a < k; ++a)
+                    r += col[a * w] * col[a * w];
+        } else if (k > 0) {
             int b = Rt_rp[i], e = Rt_rp[i + 1];
             if (dkind == 1)
                 for (int t = b; t < e; ++t)

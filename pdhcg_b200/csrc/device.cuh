@@ -101,14 +101,123 @@ __device__ __forceinline__ int warp_max_int(int v)
     return v;
 }
 
+// ---------------------------------------------------------------------------
+// Long rows.  A row of more than LONG_ROW entries (a dense constraint row, a
+// variable in many rows) is too long for the stream mode below, and one warp
+// per row would leave the product to the few warps whose tiles hold such
+// rows.  So these rows are cut into segments of at most LONG_SEG entries:
+// long_partials_kernel writes one partial product per segment (one warp
+// each, fixed order), and the product that reads the row adds its
+// segments' partials in segment order, each lane for its own row.  The
+// partials belong to the last vector passed to that kernel: every product
+// of a matrix with long rows is preceded by its pass.
+// ---------------------------------------------------------------------------
+constexpr int LONG_ROW = STREAM_ROW_MAX; // every row beyond stream mode
+constexpr int LONG_SEG = 4096;
+
+struct LongRows {
+    const int *rows;      // [n] long row ids, ascending
+    const int *seg_first; // [n + 1] first segment of each long row
+    const int2 *seg;      // [nseg] entry range {begin, end} of each segment
+    double *part;         // [nseg] partial products of the last pass
+    int n, nseg;
+};
+
+// index of the first long row >= row (L.n when none)
+__device__ __forceinline__ int long_lower_bound(const LongRows &L, int row)
+{
+    int lo = 0, hi = L.n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(L.rows + mid) < row)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// the same sum computed by the whole warp for one row (every lane calls it)
+__device__ __forceinline__ double long_row_sum_warp(const LongRows &L, int row, int lane)
+{
+    const int i = long_lower_bound(L, row);
+    const int f = __ldg(L.seg_first + i), e = __ldg(L.seg_first + i + 1);
+    double a = 0.0;
+    for (int k = f + lane; k < e; k += 32)
+        a += L.part[k];
+    return warp_sum(a);
+}
+
+// sum of long row i's segment partials, in segment order (one lane)
+__device__ __forceinline__ double long_row_fold(const LongRows &L, int i)
+{
+    const int f = __ldg(L.seg_first + i), e = __ldg(L.seg_first + i + 1);
+    double a = 0.0;
+    for (int k = f; k < e; ++k)
+        a += L.part[k];
+    return a;
+}
+
+// one warp's dot product over entries [b, e), lane-strided, 4 partial sums
+template <typename V, typename X>
+__device__ __forceinline__ double warp_range_dot(const int *__restrict__ ci, const V *__restrict__ val,
+                                                 const X *__restrict__ x, int b, int e, int lane)
+{
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int k = b + lane;
+    for (; k + 96 < e; k += 128) {
+        a0 += (double)__ldg(val + k) * (double)__ldg(x + __ldg(ci + k));
+        a1 += (double)__ldg(val + k + 32) * (double)__ldg(x + __ldg(ci + k + 32));
+        a2 += (double)__ldg(val + k + 64) * (double)__ldg(x + __ldg(ci + k + 64));
+        a3 += (double)__ldg(val + k + 96) * (double)__ldg(x + __ldg(ci + k + 96));
+    }
+    for (; k < e; k += 32)
+        a0 += (double)__ldg(val + k) * (double)__ldg(x + __ldg(ci + k));
+    return warp_sum((a0 + a1) + (a2 + a3));
+}
+
+// the segment pass over warps gw, gw + nw, ... (a kernel body, or a phase
+// of a cooperative kernel followed by a grid barrier)
+template <typename V, typename X>
+__device__ __forceinline__ void long_partials(const LongRows &L, const int *__restrict__ ci,
+                                              const V *__restrict__ val, const X *__restrict__ x, int gw, int nw,
+                                              int lane)
+{
+    for (int sg = gw; sg < L.nseg; sg += nw) {
+        const int2 r = L.seg[sg];
+        const double a = warp_range_dot(ci, val, x, r.x, r.y, lane);
+        if (lane == 0)
+            L.part[sg] = a;
+    }
+}
+
+template <typename V, typename X>
+__global__ void __launch_bounds__(256) long_partials_kernel(LongRows L, const int *ci, const V *val, const X *x)
+{
+    long_partials(L, ci, val, x, (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5),
+                  (int)((gridDim.x * blockDim.x) >> 5), (int)(threadIdx.x & 31));
+}
+
+// number of rows longer than LONG_ROW entries
+__global__ void long_count_kernel(int rows, const int *rp, int *count)
+{
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+        if (rp[r + 1] - rp[r] > LONG_ROW)
+            atomicAdd(count, 1);
+}
+
 // out[s] = sum_k val[k] * x[ci[k]] over row r0 + lane + 32 s (0 when that
 // row is past nr).  Every lane of the warp must call it with the same r0,
 // nr (1 <= nr <= 32 S) and stage (STREAM_CHUNK doubles of this warp's
-// shared memory).
+// shared memory).  Rows longer than LONG_ROW entries take their value from
+// the segment partials of lr, which must hold this product's pass.  A tile
+// holding such a row is otherwise reduced one row at a time by the whole
+// warp (no table, lr.n = 0; or S > 2, where the lane-wise form would cost
+// the wide cone kernels their registers).
 template <int S, typename V, typename X>
 __device__ __forceinline__ void warp_stream_rows(const int *__restrict__ rp, const int *__restrict__ ci,
                                                  const V *__restrict__ val, const X *__restrict__ x, int r0, int nr,
-                                                 int lane, double *stage, double (&out)[S])
+                                                 int lane, double *stage, double (&out)[S], const LongRows &lr)
 {
     int rb[S], re[S];
     int longest = 0;
@@ -157,6 +266,27 @@ __device__ __forceinline__ void warp_stream_rows(const int *__restrict__ rp, con
             }
             __syncwarp();
         }
+    } else if (S <= 2 && lr.n > 0) {
+        // every row longer than LONG_ROW is in lr: each lane folds its own
+        // long row's partials (its table index from one search per tile and
+        // a ballot) or adds its own short row in entry order
+        const int base = long_lower_bound(lr, r0);
+        int before = 0;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const bool valid = lane + 32 * s < nr;
+            const bool lg = valid && re[s] - rb[s] > LONG_ROW;
+            const unsigned mask = __ballot_sync(FULL, lg);
+            if (lg) {
+                out[s] = long_row_fold(lr, base + before + __popc(mask & ((1u << lane) - 1u)));
+            } else if (valid) {
+                double a = 0.0;
+                for (int k = rb[s]; k < re[s]; ++k)
+                    a += (double)__ldg(val + k) * (double)__ldg(x + __ldg(ci + k));
+                out[s] = a;
+            }
+            before += __popc(mask);
+        }
     } else {
         for (int i = 0; i < nr; ++i) {
             int bi = 0, ei = 0;
@@ -168,17 +298,9 @@ __device__ __forceinline__ void warp_stream_rows(const int *__restrict__ rp, con
                 }
             bi = __shfl_sync(FULL, bi, i & 31);
             ei = __shfl_sync(FULL, ei, i & 31);
-            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-            int k = bi + lane;
-            for (; k + 96 < ei; k += 128) {
-                a0 += (double)__ldg(val + k) * (double)__ldg(x + __ldg(ci + k));
-                a1 += (double)__ldg(val + k + 32) * (double)__ldg(x + __ldg(ci + k + 32));
-                a2 += (double)__ldg(val + k + 64) * (double)__ldg(x + __ldg(ci + k + 64));
-                a3 += (double)__ldg(val + k + 96) * (double)__ldg(x + __ldg(ci + k + 96));
-            }
-            for (; k < ei; k += 32)
-                a0 += (double)__ldg(val + k) * (double)__ldg(x + __ldg(ci + k));
-            const double a = warp_sum((a0 + a1) + (a2 + a3));
+            // (wide tiles with a long-row table: the warp folds each long row)
+            const double a = (lr.n > 0 && ei - bi > LONG_ROW) ? long_row_sum_warp(lr, r0 + i, lane)
+                                                                : warp_range_dot(ci, val, x, bi, ei, lane);
 #pragma unroll
             for (int s = 0; s < S; ++s)
                 if (s == (i >> 5) && lane == (i & 31))

@@ -65,6 +65,7 @@ struct StepData {
     double *cone_warm; // per-cone multiplier warm start (may be NULL)
     T *x0, *x, *xp, *xr, *dx, *dual_slack;
     T *y0, *y, *yp, *dy;
+    LongRows A_long, At_long; // long rows of A (pass over x_refl) and of A^T (pass over y)
 };
 
 // The step kernels are written as warp bodies (one tile or one cone block per
@@ -95,7 +96,7 @@ __device__ __forceinline__ void primal_free_tile(const StepData<T> &D, const Ste
         }
     }
     double aty[1];
-    warp_stream_rows<1>(D.At_rp, D.At_ci, D.At_v, D.y, r0, nr, lane, stage, aty);
+    warp_stream_rows<1>(D.At_rp, D.At_ci, D.At_v, D.y, r0, nr, lane, stage, aty, D.At_long);
     if (own) {
         double t = xi - P.tau * (c - aty[0]);
         if (HAS_Q)
@@ -164,7 +165,7 @@ __device__ __forceinline__ void primal_cone_block(const StepData<T> &D, const St
         }
     }
     double aty[S];
-    warp_stream_rows<S>(D.At_rp, D.At_ci, D.At_v, D.y, st, L, lane, stage, aty);
+    warp_stream_rows<S>(D.At_rp, D.At_ci, D.At_v, D.y, st, L, lane, stage, aty, D.At_long);
     double tt[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
@@ -244,7 +245,7 @@ __device__ __forceinline__ void dual_tile(const StepData<T> &D, const StepParams
             g = D.g[i];
     }
     double axr[1];
-    warp_stream_rows<1>(D.A_rp, D.A_ci, D.A_v, D.xr, r0, nr, lane, stage, axr);
+    warp_stream_rows<1>(D.A_rp, D.A_ci, D.A_v, D.xr, r0, nr, lane, stage, axr, D.A_long);
     if (own) {
         double v = HAS_G ? axr[0] + g : axr[0];
         double pr = EQ_ROWS ? lc : clampd(lc, v - yi / P.sigma, uc);
@@ -325,9 +326,10 @@ __global__ void fold_partials_kernel(const double *partials, int nblocks, int ns
     }
 }
 
-// y = M x, one warp per tile of 32 rows (stream-mode products)
+// y = M x, one warp per tile of 32 rows (stream-mode products); lr: M's
+// long rows with the segment pass over this x done (or none)
 __global__ void __launch_bounds__(TPB) spmv_kernel(int rows, const int *rp, const int *ci, const double *v,
-                                                   const double *x, double *y)
+                                                   const double *x, double *y, LongRows lr)
 {
     __shared__ double stage_all[WARPS][STREAM_CHUNK];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -335,7 +337,7 @@ __global__ void __launch_bounds__(TPB) spmv_kernel(int rows, const int *rp, cons
     for (int tile = blockIdx.x * WARPS + wib; tile < ntiles; tile += gridDim.x * WARPS) {
         const int r0 = 32 * tile, nr = min(32, rows - r0);
         double a[1];
-        warp_stream_rows<1>(rp, ci, v, x, r0, nr, lane, stage_all[wib], a);
+        warp_stream_rows<1>(rp, ci, v, x, r0, nr, lane, stage_all[wib], a, lr);
         if (lane < nr)
             y[r0 + lane] = a[0];
     }

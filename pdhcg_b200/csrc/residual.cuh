@@ -62,6 +62,7 @@ struct ResidualData {
     double *warm_dual, *warm_aug; // per-cone warm starts of the two projections
     double *partials;
     int rows_blocks, free_blocks, cone_blocks;
+    LongRows A_long, At_long; // passes over x_pdhg and y_pdhg
 };
 
 __device__ __forceinline__ double norm_term(double v, int l2) { return l2 ? v * v : abs_or_inf(v); }
@@ -76,7 +77,7 @@ __device__ __forceinline__ void residual_cone_block(const ResidualData<VT> &D, c
     auto fold = [&](int s, double v) { acc[s] = ops[s] == RMAX ? fmax(acc[s], v) : acc[s] + v; };
     const int st = D.cone_start[cb], L = D.cone_len[cb], type = D.cone_type[cb];
     double atys[S];
-    warp_stream_rows<S>(D.At_rp, D.At_ci, D.At_v, D.yp, st, L, lane, stage, atys);
+    warp_stream_rows<S>(D.At_rp, D.At_ci, D.At_v, D.yp, st, L, lane, stage, atys, D.At_long);
     WarpSlots<S> dual, aug;
     double xv[S], rc[S], qxv[S], atyv[S];
 #pragma unroll
@@ -205,7 +206,7 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
         for (int tile = b * WARPS + wib; tile < ntiles; tile += D.rows_blocks * WARPS) {
             const int r0 = 32 * tile, nr = min(32, D.m - r0);
             double axr[1];
-            warp_stream_rows<1>(D.A_rp, D.A_ci, D.A_v, D.xp, r0, nr, lane, stage, axr);
+            warp_stream_rows<1>(D.A_rp, D.A_ci, D.A_v, D.xp, r0, nr, lane, stage, axr, D.A_long);
             if (lane < nr) {
                 const int i = r0 + lane;
                 double v = axr[0] + D.g[i];
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
                 nr = min(32, D.n - r0);
             }
             double atyr[1];
-            warp_stream_rows<1>(D.At_rp, D.At_ci, D.At_v, D.yp, r0, nr, lane, stage, atyr);
+            warp_stream_rows<1>(D.At_rp, D.At_ci, D.At_v, D.yp, r0, nr, lane, stage, atyr, D.At_long);
             if (lane < nr) {
                 const int j = r0 + lane;
                 const double aty = atyr[0];
@@ -296,7 +297,7 @@ enum FpeScalar { FP_DX2 = 0, FP_DY2, FP_CROSS, FP_COUNT };
 template <typename VT>
 __global__ void __launch_bounds__(TPB) fpe_kernel(int n, int m, const int *At_rp, const int *At_ci, const double *At_v,
                                                   const VT *dx, const VT *dy, double *partials,
-                                                  int col_blocks)
+                                                  int col_blocks, LongRows At_long)
 {
     __shared__ double stage_all[WARPS][STREAM_CHUNK];
     const int ops[FP_COUNT] = {RSUM, RSUM, RSUM};
@@ -309,7 +310,7 @@ __global__ void __launch_bounds__(TPB) fpe_kernel(int n, int m, const int *At_rp
         for (int tile = b * WARPS + wib; tile < ntiles; tile += col_blocks * WARPS) {
             const int r0 = 32 * tile, nr = min(32, n - r0);
             double a[1];
-            warp_stream_rows<1>(At_rp, At_ci, At_v, dy, r0, nr, lane, stage_all[wib], a);
+            warp_stream_rows<1>(At_rp, At_ci, At_v, dy, r0, nr, lane, stage_all[wib], a, At_long);
             if (lane < nr) {
                 double d = dx[r0 + lane];
                 acc[FP_DX2] += d * d;
@@ -401,6 +402,7 @@ struct RayData {
     int qmode;
     int rows_blocks; // blocks [0, rows_blocks) take rows of A, the rest columns
     double *partials;
+    LongRows A_long, At_long; // passes over the primal and dual rays
 };
 
 template <typename VT>
@@ -417,7 +419,7 @@ __global__ void __launch_bounds__(TPB) ray_kernel(RayData D, const VT *dx, const
         for (int tile = blockIdx.x * WARPS + wib; tile < ntiles; tile += D.rows_blocks * WARPS) {
             const int r0 = 32 * tile, nr = min(32, D.m - r0);
             double pp[1];
-            warp_stream_rows<1>(D.A_rp, D.A_ci, D.A_v, dx, r0, nr, lane, stage, pp);
+            warp_stream_rows<1>(D.A_rp, D.A_ci, D.A_v, dx, r0, nr, lane, stage, pp, D.A_long);
             if (lane < nr) {
                 const int i = r0 + lane;
                 const double y = dy[i];
@@ -433,7 +435,7 @@ __global__ void __launch_bounds__(TPB) ray_kernel(RayData D, const VT *dx, const
         for (int tile = b * WARPS + wib; tile < ntiles; tile += nb * WARPS) {
             const int r0 = 32 * tile, nr = min(32, D.n - r0);
             double dpr[1];
-            warp_stream_rows<1>(D.At_rp, D.At_ci, D.At_v, dy, r0, nr, lane, stage, dpr);
+            warp_stream_rows<1>(D.At_rp, D.At_ci, D.At_v, dy, r0, nr, lane, stage, dpr, D.At_long);
             if (lane < nr) {
                 const int j = r0 + lane;
                 const double dp = -dpr[0];

@@ -14,11 +14,74 @@ namespace pdhcg {
 
 namespace cg = cooperative_groups;
 
-__global__ void expand_rows_kernel(const int *rp, int rows, int *row_of)
+// Row-wise set-up kernels run one thread per row.  With skip_long set, rows
+// of more than LONG_ROW entries are skipped and left to the companion
+// kernel over the long-row table, one block per long row, so that a dense
+// row does not hold one thread for its whole length.
+
+__global__ void expand_rows_kernel(const int *rp, int rows, int *row_of, int skip_long)
 {
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        if (skip_long && rp[r + 1] - rp[r] > LONG_ROW)
+            continue;
         for (int k = rp[r]; k < rp[r + 1]; ++k)
             row_of[k] = r;
+    }
+}
+
+__global__ void expand_long_rows_kernel(LongRows L, const int *rp, int *row_of)
+{
+    for (int i = blockIdx.x; i < L.n; i += gridDim.x) {
+        const int r = L.rows[i];
+        for (int k = rp[r] + threadIdx.x; k < rp[r + 1]; k += blockDim.x)
+            row_of[k] = r;
+    }
+}
+
+// fixed-order block reductions of one value per thread (blockDim.x == TPB)
+__device__ __forceinline__ double block_sum_fixed(double v)
+{
+    __shared__ double sh[TPB];
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = TPB / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ double block_max(double v)
+{
+    __shared__ double sh[TPB];
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = TPB / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// bad != 0 unless the CSR holds exactly the columns 0..cols-1 in order in every row
+__global__ void dense_rows_check_kernel(int rows, int cols, const int *rp, const int *ci, int *bad)
+{
+    const long long nnz = (long long)rows * cols;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nnz;
+         k += (long long)gridDim.x * blockDim.x) {
+        if (ci[k] != (int)(k % cols))
+            atomicOr(bad, 1);
+        if (k <= rows && rp[k] != (int)(k * cols)) // row pointers (rows + 1 <= nnz + 1 entries)
+            atomicOr(bad, 1);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && rp[rows] != (int)nnz)
+        atomicOr(bad, 1);
 }
 
 __global__ void iota_kernel(int *v, int n)
@@ -53,9 +116,11 @@ __global__ void gather_transpose_kernel(const int *perm, const int *row_of, cons
     }
 }
 
-__global__ void row_absmax_kernel(const int *rp, const double *v, int rows, double *out)
+__global__ void row_absmax_kernel(const int *rp, const double *v, int rows, double *out, int skip_long)
 {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        if (skip_long && rp[r + 1] - rp[r] > LONG_ROW)
+            continue;
         double mx = 0.0;
         for (int k = rp[r]; k < rp[r + 1]; ++k) {
             double a = fabs(v[k]);
@@ -66,16 +131,49 @@ __global__ void row_absmax_kernel(const int *rp, const double *v, int rows, doub
     }
 }
 
+// the maximum is exact in any order, so a long row's value is the same
+__global__ void long_row_absmax_kernel(LongRows L, const int *rp, const double *v, double *out)
+{
+    for (int i = blockIdx.x; i < L.n; i += gridDim.x) {
+        const int r = L.rows[i];
+        double mx = 0.0;
+        for (int k = rp[r] + threadIdx.x; k < rp[r + 1]; k += blockDim.x)
+            mx = fmax(mx, fabs(v[k]));
+        mx = block_max(mx);
+        if (threadIdx.x == 0)
+            out[r] = mx;
+    }
+}
+
 // sum_k |a_k|^p per row; p == 1 uses |a| itself (pow(x, 1) == x exactly)
-__global__ void row_powsum_kernel(const int *rp, const double *v, int rows, double p, double *out)
+__global__ void row_powsum_kernel(const int *rp, const double *v, int rows, double p, double *out, int skip_long)
 {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        if (skip_long && rp[r + 1] - rp[r] > LONG_ROW)
+            continue;
         double s = 0.0;
         for (int k = rp[r]; k < rp[r + 1]; ++k) {
             double a = fabs(v[k]);
             s += (p == 1.0) ? a : pow(a, p);
         }
         out[r] = s;
+    }
+}
+
+// a long row's sum in a fixed order (thread-strided, then a tree): the same
+// on every run, but associated differently from a sequential sum
+__global__ void long_row_powsum_kernel(LongRows L, const int *rp, const double *v, double p, double *out)
+{
+    for (int i = blockIdx.x; i < L.n; i += gridDim.x) {
+        const int r = L.rows[i];
+        double s = 0.0;
+        for (int k = rp[r] + threadIdx.x; k < rp[r + 1]; k += blockDim.x) {
+            const double a = fabs(v[k]);
+            s += (p == 1.0) ? a : pow(a, p);
+        }
+        s = block_sum_fixed(s);
+        if (threadIdx.x == 0)
+            out[r] = s;
     }
 }
 
@@ -152,9 +250,11 @@ __global__ void psd_scaling_kernel(double *s, int ncones, const int *start, cons
 
 // v_k /= (rs[r] * cs[col]) : A with (cr, vr), A^T with (vr, cr), Q with (vr, vr)
 __global__ void scale_csr_kernel(const int *rp, const int *ci, double *v, int rows, const double *rs,
-                                 const double *cs, int cr_first)
+                                 const double *cs, int cr_first, int skip_long)
 {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        if (skip_long && rp[r + 1] - rp[r] > LONG_ROW)
+            continue;
         double a = rs[r];
         for (int k = rp[r]; k < rp[r + 1]; ++k) {
             double b = cs[ci[k]];
@@ -163,7 +263,21 @@ __global__ void scale_csr_kernel(const int *rp, const int *ci, double *v, int ro
     }
 }
 
-// v_k /= rs[r] for every entry of row r
+__global__ void long_scale_csr_kernel(LongRows L, const int *rp, const int *ci, double *v, const double *rs,
+                                      const double *cs, int cr_first)
+{
+    for (int i = blockIdx.x; i < L.n; i += gridDim.x) {
+        const int r = L.rows[i];
+        const double a = rs[r];
+        for (int k = rp[r] + threadIdx.x; k < rp[r + 1]; k += blockDim.x) {
+            const double b = cs[ci[k]];
+            v[k] /= cr_first ? (b * a) : (a * b);
+        }
+    }
+}
+
+// v_k /= rs[r] for every entry of row r (rows of at most LONG_ROW entries:
+// every caller's matrix has none longer)
 __global__ void scale_rows_kernel(const int *rp, double *v, int rows, const double *rs)
 {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
@@ -173,11 +287,12 @@ __global__ void scale_rows_kernel(const int *rp, double *v, int rows, const doub
     }
 }
 
-__global__ void scale_cols_kernel(const int *rp, const int *ci, double *v, int rows, const double *cs)
+// v_k /= cs[ci[k]], one thread per entry (no row needed)
+__global__ void scale_cols_kernel(const int *ci, double *v, long long nnz, const double *cs)
 {
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x)
-        for (int k = rp[r]; k < rp[r + 1]; ++k)
-            v[k] /= cs[ci[k]];
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nnz;
+         k += (long long)gridDim.x * blockDim.x)
+        v[k] /= cs[ci[k]];
 }
 
 __global__ void scale_vectors_kernel(int n, int m, double *c, double *l, double *u, const double *vr, double *lc,
@@ -446,7 +561,8 @@ __global__ void __launch_bounds__(TPB) power_sigma_kernel(int m, int n, const in
                                                           const MT *A_v, const int *At_rp, const int *At_ci,
                                                           const MT *At_v, double *v, double *nv, double *dp,
                                                           double *part /* 4 * gridDim */, int max_iter, double tol,
-                                                          double *out /* [sigma, iterations] */)
+                                                          double *out /* [sigma, iterations] */, LongRows A_long,
+                                                          LongRows At_long)
 {
     // The iterate is u with |u| = 1 / inv (v = inv * u is the unit vector):
     //   dp = inv * A^T u;  w = A dp = A A^T v
@@ -470,19 +586,27 @@ __global__ void __launch_bounds__(TPB) power_sigma_kernel(int m, int n, const in
     double s2 = 1.0;
     int it = 0;
     for (; it < max_iter; ++it) {
+        if (At_long.n > 0) { // segment pass of the long rows, then the rows
+            long_partials(At_long, At_ci, At_v, u, gw, nw, lane);
+            grid.sync();
+        }
         for (int t = gw; t < (n + 31) / 32; t += nw) {
             const int r0 = 32 * t, nr = min(32, n - r0);
             double r[1];
-            warp_stream_rows<1>(At_rp, At_ci, At_v, u, r0, nr, lane, stage, r);
+            warp_stream_rows<1>(At_rp, At_ci, At_v, u, r0, nr, lane, stage, r, At_long);
             if (lane < nr)
                 dp[r0 + lane] = r[0] * inv;
         }
         grid.sync();
+        if (A_long.n > 0) {
+            long_partials(A_long, A_ci, A_v, dp, gw, nw, lane);
+            grid.sync();
+        }
         double uw = 0.0, ww = 0.0;
         for (int t = gw; t < (m + 31) / 32; t += nw) {
             const int r0 = 32 * t, nr = min(32, m - r0);
             double r[1];
-            warp_stream_rows<1>(A_rp, A_ci, A_v, dp, r0, nr, lane, stage, r);
+            warp_stream_rows<1>(A_rp, A_ci, A_v, dp, r0, nr, lane, stage, r, A_long);
             if (lane < nr) {
                 w[r0 + lane] = r[0];
                 uw += r[0] * u[r0 + lane];

@@ -215,10 +215,48 @@ struct DevCsr {
     int rows = 0, cols = 0, nnz = 0;
     int *rp = nullptr, *ci = nullptr;
     double *v = nullptr;
+    LongRows lr{}; // rows of more than LONG_ROW entries, cut into segments (n = 0: none)
 };
 
+// The long rows of M and their segments.  A count on the device decides
+// whether the row pointer is read back at all (most problems have none).
+void build_long_rows(DevCsr &M, Arena &ar, cudaStream_t s)
+{
+    M.lr = LongRows{};
+    if (M.rows == 0 || M.nnz <= LONG_ROW)
+        return;
+    int *cnt = ar.alloc<int>(1);
+    CK(cudaMemsetAsync(cnt, 0, sizeof(int), s));
+    long_count_kernel<<<grid_for(M.rows, 256), 256, 0, s>>>(M.rows, M.rp, cnt);
+    int count = 0;
+    CK(cudaMemcpyAsync(&count, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (count == 0)
+        return;
+    std::vector<int> rp(M.rows + 1);
+    CK(cudaMemcpyAsync(rp.data(), M.rp, rp.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    std::vector<int> rows, first{0};
+    std::vector<int2> seg;
+    for (int r = 0; r < M.rows; ++r) {
+        if (rp[r + 1] - rp[r] <= LONG_ROW)
+            continue;
+        rows.push_back(r);
+        for (int b = rp[r]; b < rp[r + 1]; b += LONG_SEG)
+            seg.push_back(make_int2(b, std::min(rp[r + 1], b + LONG_SEG)));
+        first.push_back((int)seg.size());
+    }
+    M.lr.rows = ar.upload(rows.data(), rows.size(), s);
+    M.lr.seg_first = ar.upload(first.data(), first.size(), s);
+    M.lr.seg = ar.upload(seg.data(), seg.size(), s);
+    M.lr.part = ar.alloc<double>(seg.size());
+    M.lr.n = (int)rows.size();
+    M.lr.nseg = (int)seg.size();
+    CK(cudaStreamSynchronize(s)); // the host tables go out of scope
+}
+
 // stable transpose on the device (entries of each output row in increasing
-// input-row order)
+// input-row order); M's long-row table, when it has one, is built first
 DevCsr transpose(const DevCsr &M, Arena &ar, cudaStream_t s)
 {
     DevCsr T;
@@ -234,7 +272,9 @@ DevCsr transpose(const DevCsr &M, Arena &ar, cudaStream_t s)
     }
     int *row_of = ar.alloc<int>(M.nnz), *idx = ar.alloc<int>(M.nnz), *keys_out = ar.alloc<int>(M.nnz),
         *perm = ar.alloc<int>(M.nnz);
-    expand_rows_kernel<<<grid_for(M.rows, TPB), TPB, 0, s>>>(M.rp, M.rows, row_of);
+    expand_rows_kernel<<<grid_for(M.rows, TPB), TPB, 0, s>>>(M.rp, M.rows, row_of, M.lr.n > 0);
+    if (M.lr.n > 0)
+        expand_long_rows_kernel<<<std::min(M.lr.n, 148 * 16), TPB, 0, s>>>(M.lr, M.rp, row_of);
     iota_kernel<<<grid_for(M.nnz, TPB), TPB, 0, s>>>(idx, M.nnz);
     size_t tmp_bytes = 0;
     int bits = 1;
@@ -490,6 +530,9 @@ private:
     template <typename T>
     StepData<T> step_data();
     double step_bytes(size_t s, bool store_primal, bool store_dual) const;
+    double bb_inner_bytes() const;
+    template <typename V, typename X>
+    void long_pass(const DevCsr &M, const V *val, const X *x);
     void enqueue_residual(bool want_dist);
     template <typename VT>
     void enqueue_residual_t(bool want_dist);
@@ -515,6 +558,7 @@ private:
 
     // device
     DevCsr A_, At_, Q_, R_, Rt_;
+    int r_width_ = 0; // > 0: R dense over columns 0..r_width_-1 (row-major), Rt_ not built
     // inner BB solve (non-diagonal Q)
     bool bb_ = false;
     int bb_grid_ = 0, bb_limit_ = 1, GQ_ = 1;
@@ -665,7 +709,9 @@ void Solve::upload_and_preprocess()
     A_.rp = dp_.A_rp;
     A_.ci = dp_.A_ci;
     A_.v = mut(dp_.A_v, dp_.nnzA);
+    build_long_rows(A_, ar_, s);
     At_ = transpose(A_, ar_, s);
+    build_long_rows(At_, ar_, s);
     c_d_ = mut(dp_.c, n_);
     l_d_ = mut(dp_.l, n_);
     u_d_ = mut(dp_.u, n_);
@@ -687,7 +733,24 @@ void Solve::upload_and_preprocess()
         R_.rp = dp_.R_rp;
         R_.ci = dp_.R_ci;
         R_.v = mut(dp_.R_v, dp_.nnzR);
-        Rt_ = transpose(R_, ar_, s);
+        // an R whose rows all hold the same leading columns 0..w-1 in order
+        // (a dense R, possibly zero on trailing auxiliary columns) is read
+        // row-major by both products and needs no transpose
+        r_width_ = 0;
+        const int w = R_.rows > 0 ? R_.nnz / R_.rows : 0;
+        if (w > 0 && w <= R_.cols && (long long)w * R_.rows == (long long)R_.nnz) {
+            int *bad = ar_.alloc<int>(1);
+            CK(cudaMemsetAsync(bad, 0, sizeof(int), s));
+            dense_rows_check_kernel<<<grid_for(R_.nnz, TPB), TPB, 0, s>>>(R_.rows, w, R_.rp, R_.ci, bad);
+            int h = 1;
+            CK(cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            r_width_ = h == 0 ? w : 0;
+        }
+        if (!r_width_) {
+            build_long_rows(R_, ar_, s);
+            Rt_ = transpose(R_, ar_, s);
+        }
     }
     cst_d_ = dp_.cst;
     clen_d_ = dp_.clen;
@@ -710,13 +773,19 @@ void Solve::rescale()
     bool pres = prm_.use_cone_preserving_scaling;
     // scale the problem by (fcr, fvr) (reference scale_problem, src/preconditioner.c:231-332)
     auto apply_scaling = [&]() {
-        scale_csr_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.ci, A_.v, m, fcr, fvr, 0);
-        scale_csr_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.ci, At_.v, n, fvr, fcr, 1);
+        scale_csr_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.ci, A_.v, m, fcr, fvr, 0, A_.lr.n > 0);
+        scale_csr_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.ci, At_.v, n, fvr, fcr, 1, At_.lr.n > 0);
+        if (A_.lr.n > 0)
+            long_scale_csr_kernel<<<std::min(A_.lr.n, 148 * 16), TPB, 0, s>>>(A_.lr, A_.rp, A_.ci, A_.v, fcr, fvr, 0);
+        if (At_.lr.n > 0)
+            long_scale_csr_kernel<<<std::min(At_.lr.n, 148 * 16), TPB, 0, s>>>(At_.lr, At_.rp, At_.ci, At_.v, fvr,
+                                                                             fcr, 1);
         if (Q_.nnz > 0)
-            scale_csr_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(Q_.rp, Q_.ci, Q_.v, n, fvr, fvr, 0);
+            scale_csr_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(Q_.rp, Q_.ci, Q_.v, n, fvr, fvr, 0, 0);
         if (R_.nnz > 0) { // R /= D_var by columns (reference scale_problem, src/preconditioner.c:295-307)
-            scale_cols_kernel<<<grid_for(R_.rows, TPB), TPB, 0, s>>>(R_.rp, R_.ci, R_.v, R_.rows, fvr);
-            scale_rows_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(Rt_.rp, Rt_.v, n, fvr);
+            scale_cols_kernel<<<grid_for(R_.nnz, TPB), TPB, 0, s>>>(R_.ci, R_.v, R_.nnz, fvr);
+            if (Rt_.nnz > 0)
+                scale_rows_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(Rt_.rp, Rt_.v, n, fvr);
         }
         scale_vectors_kernel<<<grid_for((long long)n + m, TPB), TPB, 0, s>>>(n, m, c_d_, l_d_, u_d_, fvr, lc_d_,
                                                                              uc_d_, g_d_, fcr, vr_d_, cr_d_);
@@ -752,14 +821,22 @@ void Solve::rescale()
         apply_scaling();
     }
     for (int it = 0; it < prm_.l_inf_ruiz_iterations; ++it) {
-        row_absmax_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.v, m, fcr);
-        row_absmax_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.v, n, fvr);
+        row_absmax_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.v, m, fcr, A_.lr.n > 0);
+        row_absmax_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.v, n, fvr, At_.lr.n > 0);
+        if (A_.lr.n > 0)
+            long_row_absmax_kernel<<<std::min(A_.lr.n, 148 * 16), TPB, 0, s>>>(A_.lr, A_.rp, A_.v, fcr);
+        if (At_.lr.n > 0)
+            long_row_absmax_kernel<<<std::min(At_.lr.n, 148 * 16), TPB, 0, s>>>(At_.lr, At_.rp, At_.v, fvr);
         apply(1);
     }
     if (prm_.has_pock_chambolle_alpha) {
         double a = prm_.pock_chambolle_alpha;
-        row_powsum_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.v, m, a, fcr);
-        row_powsum_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.v, n, 2.0 - a, fvr);
+        row_powsum_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.v, m, a, fcr, A_.lr.n > 0);
+        row_powsum_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.v, n, 2.0 - a, fvr, At_.lr.n > 0);
+        if (A_.lr.n > 0)
+            long_row_powsum_kernel<<<std::min(A_.lr.n, 148 * 16), TPB, 0, s>>>(A_.lr, A_.rp, A_.v, a, fcr);
+        if (At_.lr.n > 0)
+            long_row_powsum_kernel<<<std::min(At_.lr.n, 148 * 16), TPB, 0, s>>>(At_.lr, At_.rp, At_.v, 2.0 - a, fvr);
         apply(0);
     }
     if (prm_.bound_objective_rescaling) {
@@ -778,7 +855,8 @@ void Solve::rescale()
         if (R_.nnz > 0) {
             double f = std::sqrt(sc_ / sb_);
             mul_scalar_kernel<<<grid_for(R_.nnz, TPB), TPB, 0, s>>>(R_.v, R_.nnz, f);
-            mul_scalar_kernel<<<grid_for(Rt_.nnz, TPB), TPB, 0, s>>>(Rt_.v, Rt_.nnz, f);
+            if (Rt_.nnz > 0)
+                mul_scalar_kernel<<<grid_for(Rt_.nnz, TPB), TPB, 0, s>>>(Rt_.v, Rt_.nnz, f);
         }
     }
     CK(cudaGetLastError());
@@ -852,6 +930,7 @@ BBData Solve::bb_data() const
     D.Rt_rp = Rt_.rp;
     D.Rt_ci = Rt_.ci;
     D.Rt_v = Rt_.v;
+    D.r_width = r_width_;
     D.dkind = dp_.dkind;
     D.Ddiag = dp_.Ddiag;
     D.Ddense = dp_.Ddense;
@@ -888,7 +967,9 @@ void Solve::setup_bb()
 {
     cudaStream_t s = st_;
     int n = n_;
-    GQ_ = residual_group(pick_group((long long)Q_.nnz + Rt_.nnz, n));
+    // a dense R is read by columns, one thread per variable (coalesced over
+    // the threads of a warp); otherwise lanes per row from the mean row length
+    GQ_ = r_width_ ? 1 : residual_group(pick_group((long long)Q_.nnz + Rt_.nnz, n));
     // cooperative grid: every block resident at once
     int dev = 0, nsm = 0, per_sm = 0;
     CK(cudaGetDevice(&dev));
@@ -937,7 +1018,8 @@ void Solve::setup_bb()
         bb_m_ = ar_.alloc<double>(n);
         bb_minv_ = ar_.alloc<double>(n);
         bb_diag_h_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(n, Q_.nnz > 0, Q_.rp, Q_.ci, Q_.v, k, Rt_.rp, Rt_.ci,
-                                                          Rt_.v, dp_.dkind, dp_.Ddiag, dp_.Ddense, bb_diag_h_);
+                                                          Rt_.v, r_width_ ? R_.v : nullptr, r_width_, dp_.dkind,
+                                                          dp_.Ddiag, dp_.Ddense, bb_diag_h_);
     }
     // eigenvalues of a sparse Q (the reference computes them for SPARSE_Q only)
     if (qtype_ == PDHCG_SPARSE_Q) {
@@ -1007,8 +1089,9 @@ void Solve::step_size()
         double *part = ar_.alloc<double>((size_t)4 * grid);
         int max_iter = prm_.sv_max_iter;
         double tol = prm_.sv_tol;
+        LongRows al = A_.lr, atl = At_.lr;
         void *args[] = {&m, &n, &A_.rp, &A_.ci, &A_.v, &At_.rp, &At_.ci, &At_.v, &v, &nv, &dp, &part, &max_iter,
-                        &tol, &out};
+                        &tol, &out, &al, &atl};
         CK(cudaLaunchCooperativeKernel((void *)power_sigma_kernel<double>, grid, TPB, args, 0, s));
         double h[2];
         CK(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -1037,6 +1120,8 @@ template <typename T>
 StepData<T> Solve::step_data()
 {
     StepData<T> D{};
+    D.A_long = A_.lr;
+    D.At_long = At_.lr;
     D.cone_warm = cone_warm_;
     D.n = n_;
     D.m = m_;
@@ -1103,6 +1188,7 @@ template <typename T>
 void Solve::launch_dual(const StepData<T> &D, const StepParams &P)
 {
     cudaStream_t s = st_;
+    long_pass(A_, D.A_v, D.xr);
     int grid = grid_for(((long long)m_ + 31) / 32, WARPS);
     if (eq_rows_) {
         if (has_g_)
@@ -1138,7 +1224,9 @@ void Solve::enqueue_step_bb(bool store_dual, bool want_fpe, double w)
         tau = std::fmax(tau, -1.01 * std::fmin(0.0, nonconvexity_));
         tau /= 100;
     }
-    spmv_kernel<<<grid_for(((long long)n_ + 31) / 32, WARPS), TPB, 0, s>>>(n_, At_.rp, At_.ci, At_.v, y_, bb_aty_);
+    long_pass(At_, At_.v, y_);
+    spmv_kernel<<<grid_for(((long long)n_ + 31) / 32, WARPS), TPB, 0, s>>>(n_, At_.rp, At_.ci, At_.v, y_, bb_aty_,
+                                                                          At_.lr);
     double inv_tau = 1.0 / tau;
     if (bb_m_ && inv_tau != bb_cached_inv_tau_) {
         int nb = grid_for(n_, TPB, 148 * 4);
@@ -1216,6 +1304,7 @@ void Solve::enqueue_step_t(bool store_primal, bool store_dual, bool want_fpe, do
     P.lp_slack = qtype_ == PDHCG_NON_Q;
     P.cone_box = cone_box_;
     StepData<T> D = step_data<T>();
+    long_pass(At_, D.At_v, D.y); // A^T y of both primal kernels
     bool hasq = qtype_ == PDHCG_DIAG_Q;
     int nfree = D.n_cones > 0 ? D.n_free : n_;
     if (nfree > 0) {
@@ -1265,6 +1354,31 @@ double Solve::step_bytes(size_t s, bool store_primal, bool store_dual) const
     double dual = nnz * (s + 4) + (m + 1) * 4 + n * s + m * s * (2 + (eq_rows_ ? 1 : 2) + (has_g_ ? 1 : 0)) +
                   m * s * (1 + (store_dual ? 1 : 0));
     return primal + dual;
+}
+
+// Algorithmic bytes of one inner BB iteration (bb_kernel): the rows of Q
+// with x_p gathered once, two passes over R (R x_p, then R^T (D R x_p))
+// with x_p gathered once, and fifteen n-vectors of the gradient and
+// projection phases (grad phase: c, A^T y, x_p, x, grad, dir read, grad,
+// Q x written; var phase: grad, x_p, l, u, M^-1 read, x_p, dir written).
+double Solve::bb_inner_bytes() const
+{
+    double n = n_;
+    double q = Q_.nnz > 0 ? Q_.nnz * 12.0 + (n + 1) * 4 + n * 8 : 0.0;
+    double r = R_.nnz == 0 ? 0.0
+               : r_width_ ? 2.0 * R_.nnz * 8.0 + r_width_ * 8.0 // values only, x_p read contiguously
+                          : 2.0 * R_.nnz * 12.0 + (R_.rows + 1) * 4.0 + (n + 1) * 4 + n * 8;
+    return q + r + 15.0 * n * 8;
+}
+
+// Segment pass of M's long rows over x, ahead of a product that reads them.
+template <typename V, typename X>
+void Solve::long_pass(const DevCsr &M, const V *val, const X *x)
+{
+    if (M.lr.n == 0)
+        return;
+    long_partials_kernel<V, X><<<grid_for(M.lr.nseg, WARPS), TPB, 0, st_>>>(M.lr, M.ci, val, x);
+    stats_.kernel_launches++;
 }
 
 void Solve::enqueue_residual(bool want_dist)
@@ -1326,6 +1440,10 @@ void Solve::enqueue_residual_t(bool want_dist)
     D.rows_blocks = res_rows_blocks_;
     D.free_blocks = res_free_blocks_;
     D.cone_blocks = res_cone_blocks_;
+    D.A_long = A_.lr;
+    D.At_long = At_.lr;
+    long_pass(A_, A_.v, D.xp);
+    long_pass(At_, At_.v, D.yp);
     ResidualParams P;
     P.l2 = prm_.optimality_norm == NORM_TYPE_L2;
     P.is_lp = qtype_ == PDHCG_NON_Q;
@@ -1356,10 +1474,15 @@ void Solve::enqueue_fpe(int slot)
     cudaStream_t s = st_;
     int nb = fpe_col_blocks_ + fpe_row_blocks_;
     double *part = partials_; // stream order serialises every user of the partials buffer
-    if (fp32_)
-        fpe_kernel<float><<<nb, TPB, 0, s>>>(n_, m_, At_.rp, At_.ci, At_.v, f_.dx, f_.dy, part, fpe_col_blocks_);
-    else
-        fpe_kernel<double><<<nb, TPB, 0, s>>>(n_, m_, At_.rp, At_.ci, At_.v, dx_, dy_, part, fpe_col_blocks_);
+    if (fp32_) {
+        long_pass(At_, At_.v, f_.dy);
+        fpe_kernel<float><<<nb, TPB, 0, s>>>(n_, m_, At_.rp, At_.ci, At_.v, f_.dx, f_.dy, part, fpe_col_blocks_,
+                                             At_.lr);
+    } else {
+        long_pass(At_, At_.v, dy_);
+        fpe_kernel<double><<<nb, TPB, 0, s>>>(n_, m_, At_.rp, At_.ci, At_.v, dx_, dy_, part, fpe_col_blocks_,
+                                              At_.lr);
+    }
     fold_partials_kernel<<<1, TPB, 0, s>>>(part, nb, FP_COUNT, fpe_ops_d_, scal_d_ + RS_COUNT + slot * FP_COUNT);
     stats_.kernel_launches += 2;
     if (bb_) {
@@ -1412,11 +1535,18 @@ void Solve::compute_infeasibility()
     }
     D.rows_blocks = res_rows_blocks_;
     D.partials = partials_;
+    D.A_long = A_.lr;
+    D.At_long = At_.lr;
     int grid = res_rows_blocks_ + fpe_col_blocks_;
-    if (fp32_)
+    if (fp32_) {
+        long_pass(A_, A_.v, f_.dx);
+        long_pass(At_, At_.v, f_.dy);
         ray_kernel<float><<<grid, TPB, 0, s>>>(D, f_.dx, f_.dy);
-    else
+    } else {
+        long_pass(A_, A_.v, dx_);
+        long_pass(At_, At_.v, dy_);
         ray_kernel<double><<<grid, TPB, 0, s>>>(D, dx_, dy_);
+    }
     fold_partials_kernel<<<1, TPB, 0, s>>>(partials_, grid, RY_COUNT, ray_ops_d_, ray_d_ + RN_COUNT);
     stats_.kernel_launches += 6;
     double h[RN_COUNT + RY_COUNT];
@@ -1842,7 +1972,10 @@ pdhcg_result_t *Solve::run()
     r->rescaling_time_sec = stats_.setup_ms * 1e-3;
     double nnz = (double)A_.nnz;
     stats_.spmv_bytes = 2.0 * nnz * (8 + 4) + 4.0 * ((double)n_ + m_ + 2) + 8.0 * ((double)n_ + m_);
-    stats_.step_bytes = stats_.step_kernel_launches > 0 ? step_bytes_sum_ / stats_.step_kernel_launches : 0.0;
+    double bytes = step_bytes_sum_;
+    if (bb_) // the inner solve: one first pass per step plus every further inner iteration
+        bytes += (double)inner_total_ * bb_inner_bytes();
+    stats_.step_bytes = stats_.step_kernel_launches > 0 ? bytes / stats_.step_kernel_launches : 0.0;
     stats_.primal_weight = omega_;
     stats_.step_size = step_;
     g_last_stats = stats_;
@@ -2168,7 +2301,8 @@ int pdhcg_b200_csr_spmv(int rows, const int *row_ptr, const int *col_ind, const 
                         double *y, void *stream)
 {
     cudaStream_t s = (cudaStream_t)stream;
-    spmv_kernel<<<grid_for(((long long)rows + 31) / 32, WARPS), TPB, 0, s>>>(rows, row_ptr, col_ind, val, x, y);
+    spmv_kernel<<<grid_for(((long long)rows + 31) / 32, WARPS), TPB, 0, s>>>(rows, row_ptr, col_ind, val, x, y,
+                                                                            LongRows{});
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

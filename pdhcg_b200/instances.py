@@ -95,6 +95,31 @@ def box_lp(seed: int = 3, n: int = 300, m: int = 150) -> Problem:
                    var_ub=np.full(n, 2.0))
 
 
+def dense_rows_qp(seed: int = 21, n: int = 6000, m: int = 3000, ndense: int = 3, with_q: bool = False) -> Problem:
+    """Box LP (or diagonal QP) whose A has ``ndense`` dense rows (n entries)
+    among rows of 6 random entries, and one dense column (variable 0 in
+    every row): rows and columns longer than the products' long-row
+    threshold.  Row ranges through a random point, so it is feasible."""
+    rng = np.random.default_rng(seed)
+    B = random_csr(rng, m, n, 6).to_scipy().tolil()
+    dense = rng.choice(m, ndense, replace=False)
+    for r in dense:
+        B[int(r), :] = rng.standard_normal(n) / np.sqrt(n)
+    B[:, 0] = rng.standard_normal((m, 1))
+    A = B.tocsr()
+    A.sort_indices()
+    x0 = rng.uniform(-1, 1, n)
+    ax = A @ x0
+    lo = ax - rng.uniform(0, 1, m)
+    up = ax + rng.uniform(0, 1, m)
+    p = Problem(c=rng.standard_normal(n), A=CsrMatrix.from_scipy(A), con_lb=lo, con_ub=up,
+                var_lb=np.full(n, -2.0), var_ub=np.full(n, 2.0))
+    if with_q:
+        p.Q = CsrMatrix(n, n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32),
+                        rng.uniform(0.05, 1.0, n))
+    return p
+
+
 def diag_qp(seed: int = 4, n: int = 300, m: int = 150) -> Problem:
     p = box_lp(seed, n, m)
     rng = np.random.default_rng(seed + 100)

@@ -72,6 +72,10 @@ CASES = {
     "mixed_cones_lp": (lambda: instances.conic_lp(seed=13, nexp=12, npow=12), {}),
     "mixed_cones_qp": (lambda: instances.conic_lp(seed=14, with_q=True, nexp=10, npow=10), {}),
     "exp_pow_only_qp": (lambda: instances.conic_lp(seed=15, nsoc=0, nrsoc=0, with_q=True, nexp=15, npow=15), {}),
+    # rows and columns longer than the long-row threshold (segment passes before every product)
+    "dense_rows_lp": (lambda: instances.dense_rows_qp(), {}),
+    "dense_rows_qp": (lambda: instances.dense_rows_qp(seed=22, with_q=True), {}),
+    "portfolio_long_rows": (lambda: instances.portfolio(seed=4, scale=0.05), {}),
 }
 
 
@@ -112,7 +116,7 @@ def _solve_gpu_opts(lib, p, params, **opts):
     return d, native.last_stats()
 
 
-@pytest.mark.parametrize("name", ["diag_qp", "conic_qp", "soc_qp_small", "box_lp"])
+@pytest.mark.parametrize("name", ["diag_qp", "conic_qp", "soc_qp_small", "box_lp", "dense_rows_qp"])
 def test_mixed_precision_reaches_fp64_answer(lib, name):
     """FP32 bulk phase + FP64 polish: same status as plain FP64, objective
     within the termination tolerance of the FP64 answer, and the FP32 phase
