@@ -187,10 +187,12 @@ int pdhcg_b200_csr_spmv(int rows, const int *row_ptr, const int *col_ind, const 
 /* Project each cone block of x (scaled space) onto {x : x_i / d_i in K} in the
  * metric sum_i (1 + tau q_i)(x_i - r_i)^2; q may be NULL.  cone_type holds
  * cone_type_t values: SOC and rotated-SOC blocks of at most 256 slots,
- * exponential blocks, and power blocks (exponents in cone_alpha, which may
- * be NULL without power blocks); -3 for a PSD block or a power block
- * without cone_alpha, -2 for a longer block.  Waits for the stream (it reads
- * the block lengths on the host). */
+ * exponential blocks, power blocks (exponents in cone_alpha, which may be
+ * NULL without power blocks) and PSD blocks of order v_dim <= 22 (svec
+ * packing, projected in the plain Frobenius metric as the reference does:
+ * d and q do not enter; 2 v_dim^2 doubles of temporary scratch each); -3
+ * for a power block without cone_alpha or an unknown type, -2 for a longer
+ * block.  Waits for the stream (it reads the block lengths on the host). */
 int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *cone_vdim, const int *cone_type,
                              const double *cone_alpha, double *x, const double *d, const double *q, double tau,
                              void *stream);
@@ -200,7 +202,9 @@ int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *co
  * code whose memory is budgeted up front, or that runs while another
  * component owns the allocator.  No counterpart in the reference.
  * Same arguments, results and error codes as pdhcg_b200_project_cones, plus
- * -4 when num_cones > PDHCG_B200_NOALLOC_MAX_CONES (nothing is launched).
+ * -4 when num_cones > PDHCG_B200_NOALLOC_MAX_CONES (nothing is launched),
+ * except that PSD blocks are refused with -3 (their eigen-decomposition
+ * scratch grows with the order, so it has no fixed bound).
  * Its scratch is one file-scope device array per device
  * ((PDHCG_B200_NOALLOC_MAX_CONES + 2) ints); every call writes it before
  * reading it, so nothing needs to start at zero.
@@ -219,7 +223,9 @@ int pdhcg_b200_project_cones_noalloc(int num_cones, const int *cone_start, const
 
 /* One restarted-Halpern PDHG step (primal prox with diagonal Q or none, cone
  * projection, dual prox, reflection, Halpern averaging) on device arrays;
- * the layout mirrors oracle_step_t of the oracle.  Sizes: n variables, m rows. */
+ * the layout mirrors oracle_step_t of the oracle.  Sizes: n variables, m rows.
+ * -3 with PSD blocks (no scratch is kept for them), -2 for a cone block
+ * longer than 256 slots. */
 typedef struct {
     int n, m;
     const int *A_row_ptr, *A_col_ind;

@@ -9,12 +9,6 @@
 #include <stdio.h>
 #include <stdlib.h>
 
-static void unsupported(const char *what)
-{
-    fprintf(stderr, "[oracle] %s cones are not restated yet\n", what);
-    abort();
-}
-
 /* ---- exponential cone K = cl{(x, y, z) : y > 0, y exp(x / y) <= z} ------
  * Projection of r onto {v : v / d in K} in the unit metric of r's space,
  * restating the reference's point projection (src/kernels/
@@ -187,10 +181,96 @@ void oracle_pow_project(double *x, const double *d, const double *q, double tau,
         x[i] = o[i] * d[i];
 }
 
+/* ---- PSD cone: x holds svec(X) of a symmetric order-n matrix -------------
+ * Slots run down the columns of the lower triangle (col 0: rows 0..n-1,
+ * col 1: rows 1..n-1, ...), off-diagonal entries scaled by sqrt 2, so that
+ * the slot inner product is the trace inner product (reference
+ * src/kernels/pdhcg_psd_cone_kernels.cu:65-91, gather / scatter of the
+ * packed matrices).  The projection is the Frobenius one, taken in the
+ * scaled space as the reference does (:415-475): eigen-decompose X, clip
+ * negative eigenvalues, repack.  Order 1 is max(x, 0).
+ *
+ * The eigen-decomposition is the cyclic Jacobi method with Rutishauser's
+ * rotation (theta = (a_qq - a_pp) / (2 a_pq), t = sign(theta) / (|theta| +
+ * sqrt(theta^2 + 1)), c = 1 / sqrt(t^2 + 1), s = t c), sweeping pairs
+ * p < q in row order until the off-diagonal mass falls below 1e-28 of the
+ * matrix's (at most 100 sweeps; the reference's batched Jacobi uses
+ * tolerance 1e-12 and 100 sweeps).  The device restates the same steps. */
+#define PSD_MAX_SWEEPS 100
+#define PSD_OFF_REL 1e-28
+
+static void psd_jacobi(int n, double *A, double *V)
+{
+    for (int i = 0; i < n * n; ++i) V[i] = 0.0;
+    for (int i = 0; i < n; ++i) V[i * n + i] = 1.0;
+    for (int sweep = 0; sweep < PSD_MAX_SWEEPS; ++sweep) {
+        double off = 0.0, all = 0.0;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                double a2 = A[i * n + j] * A[i * n + j];
+                all += a2;
+                if (i != j) off += a2;
+            }
+        if (!(off > PSD_OFF_REL * all)) break;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                double apq = A[p * n + q];
+                if (apq == 0.0) continue;
+                double theta = (A[q * n + q] - A[p * n + p]) / (2.0 * apq);
+                double t = fabs(theta) > 1e150 ? 0.5 / theta
+                                               : (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+                for (int k = 0; k < n; ++k) { /* columns p, q of A and V */
+                    double akp = A[k * n + p], akq = A[k * n + q];
+                    A[k * n + p] = c * akp - sn * akq;
+                    A[k * n + q] = sn * akp + c * akq;
+                    double vkp = V[k * n + p], vkq = V[k * n + q];
+                    V[k * n + p] = c * vkp - sn * vkq;
+                    V[k * n + q] = sn * vkp + c * vkq;
+                }
+                for (int k = 0; k < n; ++k) { /* rows p, q of A */
+                    double apk = A[p * n + k], aqk = A[q * n + k];
+                    A[p * n + k] = c * apk - sn * aqk;
+                    A[q * n + k] = sn * apk + c * aqk;
+                }
+                A[p * n + q] = A[q * n + p] = 0.0;
+            }
+    }
+}
+
 void oracle_psd_project(int order, double *x)
 {
-    (void)order; (void)x;
-    unsupported("PSD");
+    const int n = order;
+    const double r2 = 1.41421356237309504880, ir2 = 0.70710678118654752440;
+    if (n == 1) {
+        x[0] = fmax(x[0], 0.0);
+        return;
+    }
+    int len = n * (n + 1) / 2, finite = 1;
+    for (int i = 0; i < len; ++i) finite &= isfinite(x[i]) != 0;
+    if (!finite) { /* the reference's failed decomposition: NaN */
+        for (int i = 0; i < len; ++i) x[i] = NAN;
+        return;
+    }
+    double *A = (double *)malloc(sizeof(double) * (size_t)n * n);
+    double *V = (double *)malloc(sizeof(double) * (size_t)n * n);
+    int slot = 0;
+    for (int col = 0; col < n; ++col)
+        for (int row = col; row < n; ++row, ++slot) {
+            double v = row == col ? x[slot] : x[slot] * ir2;
+            A[row * n + col] = A[col * n + row] = v;
+        }
+    psd_jacobi(n, A, V);
+    slot = 0;
+    for (int col = 0; col < n; ++col)
+        for (int row = col; row < n; ++row, ++slot) {
+            double v = 0.0;
+            for (int e = 0; e < n; ++e)
+                v += fmax(A[e * n + e], 0.0) * V[row * n + e] * V[col * n + e];
+            x[slot] = row == col ? v : v * r2;
+        }
+    free(A);
+    free(V);
 }
 
 /* Moreau: the dual residual of rc = c_eff - A^T y is -proj_K(-rc) in the
@@ -214,8 +294,15 @@ void oracle_pow_dual_residual(const double *rc, const double *d, double alpha, d
         out[i] = -o[i];
 }
 
+/* (rc - proj_PSD(rc)) d: the PSD cone is self-dual and the reference
+ * projects rc without a metric (compute_psd_cone_dual_residual,
+ * src/kernels/pdhcg_psd_cone_kernels.cu:477-506) */
 void oracle_psd_dual_residual(int order, const double *rc, const double *d, double *out)
 {
-    (void)order; (void)rc; (void)d; (void)out;
-    unsupported("PSD");
+    int len = order * (order + 1) / 2;
+    double *p = (double *)malloc(sizeof(double) * (size_t)len);
+    for (int i = 0; i < len; ++i) p[i] = rc[i];
+    oracle_psd_project(order, p);
+    for (int i = 0; i < len; ++i) out[i] = (rc[i] - p[i]) * d[i];
+    free(p);
 }

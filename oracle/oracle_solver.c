@@ -1311,8 +1311,13 @@ pdhcg_result_t *oracle_solve(const qp_problem_t *prob, const pdhg_parameters_t *
         S->q_norm = mx;
         S->nonconvexity = mn;
     }
-    /* inner solver (src/solver_state.cu:280-370) */
-    S->use_bb = !(S->qtype == PDHCG_NON_Q || S->qtype == PDHCG_DIAG_Q);
+    /* inner solver (src/solver_state.cu:280-370): diagonal Q with PSD blocks
+     * also takes the BB solve (a nonuniform diagonal metric has no one-EVD
+     * PSD prox), without the Jacobi preconditioner (:307, :323) */
+    int has_psd = 0;
+    for (int b = 0; b < S->P.ncones; ++b)
+        has_psd |= S->P.ctype[b] == CONE_PSD;
+    S->use_bb = !(S->qtype == PDHCG_NON_Q || (S->qtype == PDHCG_DIAG_Q && !has_psd));
     if (S->use_bb) {
         int lim = prm.inner_solver_parameters.iteration_limit;
         double it0 = prm.inner_solver_parameters.initial_tolerance, mt = prm.inner_solver_parameters.min_tolerance;
@@ -1324,7 +1329,7 @@ pdhcg_result_t *oracle_solve(const qp_problem_t *prob, const pdhg_parameters_t *
         S->bb_min_tol = mt;
         S->grad = dvec(n); S->dir = dvec(n); S->pbuf = dvec(n);
         if (cones) S->snap = dvec(n);
-        S->precond = prm.diag_jacobi_precond;
+        S->precond = prm.diag_jacobi_precond && !has_psd;
         if (S->precond) {
             S->diag_h = dvec(n); S->m_diag = dvec(n); S->m_inv = dvec(n); S->Ms = dvec(n);
             S->cached_inv_tau = -1.0;

@@ -52,6 +52,8 @@ struct BBData {
     int n_cones;
     const double *vr;
     double *cone_warm;
+    double *psd_work; // PSD blocks' projection scratch (NULL: none)
+    const long long *psd_off;
     // iterates
     const double *x0;
     double *x, *xp, *xr, *dx;
@@ -217,7 +219,9 @@ struct BBWork {
     int free_tasks, tasks;
     __device__ BBWork(const BBData &D)
     {
-        int nf = D.free_idx ? D.n_free : D.n;
+        // with cone blocks the free variables are exactly the list (possibly
+        // empty, with a NULL list); without, every variable is free
+        int nf = D.n_cones > 0 ? D.n_free : D.n;
         free_tasks = (nf + 32 / G - 1) / (32 / G);
         tasks = free_tasks + D.n_cones;
     }
@@ -282,7 +286,7 @@ __device__ __forceinline__ double bb_cone_block(const BBData &D, const double *d
     __syncwarp();
     bool uni = warp_uniform_unit<S>(sl, L, lane);
     warp_project<S>(type, sl, L, lane, uni, D.cone_warm ? D.cone_warm + cb : nullptr,
-                    D.cone_alpha ? D.cone_alpha[cb] : 0.0);
+                    D.cone_alpha ? D.cone_alpha[cb] : 0.0, D.psd_work ? D.psd_work + D.psd_off[cb] : nullptr);
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         int i = lane + 32 * s;
@@ -313,7 +317,7 @@ __device__ double bb_var_phase(const BBData &D, const double *drx, bool init, do
     for (int task = gwarp; task < W.tasks; task += nwarps) {
         if (task < W.free_tasks) {
             int r = task * (32 / G) + lane / G;
-            int nf = D.free_idx ? D.n_free : D.n;
+            int nf = D.n_cones > 0 ? D.n_free : D.n;
             bool ok = r < nf;
             int j = ok ? (D.free_idx ? D.free_idx[r] : r) : 0;
             double q = 0.0;
@@ -353,7 +357,7 @@ __device__ double bb_var_phase(const BBData &D, const double *drx, bool init, do
             // cone block; 3-slot blocks (exponential, power) take the one-slot
             // instantiation, which alone carries their projection
             const int cb = task - W.free_tasks;
-            if (S > 1 && D.cone_type[cb] >= 2)
+            if (S > 1 && (D.cone_type[cb] == 2 || D.cone_type[cb] == 3))
                 part += bb_cone_block<G, 1>(D, drx, init, alpha, lane, stage, cb);
             else
                 part += bb_cone_block<G, S>(D, drx, init, alpha, lane, stage, cb);

@@ -868,11 +868,146 @@ __device__ __forceinline__ void warp_project3(int type, WarpSlots<S> &sl, int la
 
 // Cone kinds an instantiation carries: SOC / RSOC (any S), and the 3-slot
 // exponential / power cones (S = 1 only; callers route those blocks there).
-enum ConeKinds { CONES_WIDE = 1, CONES_THREE = 2, CONES_ALL = 3 };
+// ---------------------------------------------------------------------------
+// PSD blocks.  The block's L = n (n + 1) / 2 slots hold svec(X): the lower
+// triangle down the columns, off-diagonal entries scaled by sqrt 2 (the
+// reference's packing, src/kernels/pdhcg_psd_cone_kernels.cu:65-91).  The
+// projection is the Frobenius one in the scaled space, as the reference
+// takes it (:415-475; no metric): the warp unpacks X into work[0, n^2)
+// (this block's device scratch, row-major), runs cyclic Jacobi with
+// Rutishauser's rotation on it while accumulating the eigenvectors in
+// work[n^2, 2 n^2), clips the negative eigenvalues and repacks.  Every
+// lane takes the same rotation from the same entries; lane k updates row /
+// column entry k of the two rotated rows and columns, so the arithmetic of
+// each entry is that of the sequential method.  Stops when the
+// off-diagonal mass is below 1e-28 of the whole (at most 100 sweeps).
+// n <= PSD_MAX_ORDER (L <= 256 slots, S <= 8).
+// ---------------------------------------------------------------------------
+constexpr int PSD_MAX_ORDER = 22;
+constexpr int PSD_MAX_SWEEPS = 100;
+constexpr double PSD_OFF_REL = 1e-28;
+
+// (row, col) of svec slot i of an order-n block
+__device__ __forceinline__ void psd_slot_rc(int i, int n, int &row, int &col)
+{
+    int c = 0, first = 0;
+    while (i >= first + (n - c)) {
+        first += n - c;
+        ++c;
+    }
+    col = c;
+    row = c + (i - first);
+}
+
+template <int S>
+__device__ void warp_project_psd(WarpSlots<S> &sl, int L, int lane, double *work)
+{
+    int n = 0;
+    while (n * (n + 1) / 2 < L)
+        ++n;
+    if (n == 1) {
+        if (lane == 0)
+            sl.x[0] = fmax(sl.x[0], 0.0);
+        return;
+    }
+    bool finite = true;
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+        if (lane + 32 * s < L)
+            finite &= isfinite(sl.x[s]) != 0;
+    if (!__all_sync(FULL, finite)) { // the reference's failed decomposition gives NaN
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            if (lane + 32 * s < L)
+                sl.x[s] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
+    const double R2 = 1.41421356237309504880, IR2 = 0.70710678118654752440;
+    double *A = work, *V = work + n * n;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int i = lane + 32 * s;
+        if (i < L) {
+            int row, col;
+            psd_slot_rc(i, n, row, col);
+            const double v = row == col ? sl.x[s] : sl.x[s] * IR2;
+            A[row * n + col] = v;
+            A[col * n + row] = v;
+        }
+    }
+    for (int e = lane; e < n * n; e += 32)
+        V[e] = (e / n == e % n) ? 1.0 : 0.0;
+    __syncwarp();
+    for (int sweep = 0; sweep < PSD_MAX_SWEEPS; ++sweep) {
+        double off = 0.0, all = 0.0;
+        for (int e = lane; e < n * n; e += 32) {
+            const double a2 = A[e] * A[e];
+            all += a2;
+            if (e / n != e % n)
+                off += a2;
+        }
+        off = warp_sum(off);
+        all = warp_sum(all);
+        if (!(off > PSD_OFF_REL * all))
+            break;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                const double apq = A[p * n + q];
+                if (apq == 0.0)
+                    continue;
+                const double theta = (A[q * n + q] - A[p * n + p]) / (2.0 * apq);
+                const double t = fabs(theta) > 1e150
+                                     ? 0.5 / theta
+                                     : (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+                __syncwarp(); // every lane has read a_pp, a_qq, a_pq
+                if (lane < n) { // columns p, q of A and V
+                    const int k = lane;
+                    const double akp = A[k * n + p], akq = A[k * n + q];
+                    A[k * n + p] = c * akp - sn * akq;
+                    A[k * n + q] = sn * akp + c * akq;
+                    const double vkp = V[k * n + p], vkq = V[k * n + q];
+                    V[k * n + p] = c * vkp - sn * vkq;
+                    V[k * n + q] = sn * vkp + c * vkq;
+                }
+                __syncwarp();
+                if (lane < n) { // rows p, q of A
+                    const int k = lane;
+                    const double apk = A[p * n + k], aqk = A[q * n + k];
+                    A[p * n + k] = c * apk - sn * aqk;
+                    A[q * n + k] = sn * apk + c * aqk;
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    A[p * n + q] = 0.0;
+                    A[q * n + p] = 0.0;
+                }
+                __syncwarp();
+            }
+    }
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int i = lane + 32 * s;
+        if (i < L) {
+            int row, col;
+            psd_slot_rc(i, n, row, col);
+            double v = 0.0;
+            for (int e = 0; e < n; ++e)
+                v += fmax(A[e * n + e], 0.0) * V[row * n + e] * V[col * n + e];
+            sl.x[s] = row == col ? v : v * R2;
+        }
+    }
+    __syncwarp(); // the scratch may be reused by this warp's next projection
+}
+
+// Cone kinds an instantiation carries: SOC / RSOC (any S), the 3-slot
+// exponential / power cones (S = 1 only; callers route those blocks there)
+// and PSD blocks (psd: this block's scratch of 2 n^2 doubles).
+enum ConeKinds { CONES_WIDE = 1, CONES_THREE = 2, CONES_PSD = 4, CONES_ALL = 7 };
 
 template <int S, int KINDS = CONES_ALL>
 __device__ __forceinline__ void warp_project(int type, WarpSlots<S> &sl, int L, int lane, bool uniform_unit,
-                                             double *warm, double alpha = 0.0)
+                                             double *warm, double alpha = 0.0, double *psd = nullptr)
 {
     if ((KINDS & CONES_WIDE) && type == 1) // CONE_STANDARD_SOC
         warp_project_soc<S>(sl, L, lane, uniform_unit, warm);
@@ -880,6 +1015,8 @@ __device__ __forceinline__ void warp_project(int type, WarpSlots<S> &sl, int L, 
         warp_project_rsoc<S>(sl, L, lane, uniform_unit, warm);
     else if ((KINDS & CONES_THREE) && S == 1 && (type == 2 || type == 3)) // CONE_EXPONENTIAL, CONE_POWER
         warp_project3<S>(type, sl, lane, alpha);
+    else if ((KINDS & CONES_PSD) && type == 4 && psd != nullptr) // CONE_PSD
+        warp_project_psd<S>(sl, L, lane, psd);
 }
 
 // Is d uniform over the block and w == 1 everywhere?  (warp vote)

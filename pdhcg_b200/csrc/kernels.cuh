@@ -66,6 +66,8 @@ struct StepData {
     T *x0, *x, *xp, *xr, *dx, *dual_slack;
     T *y0, *y, *yp, *dy;
     LongRows A_long, At_long; // long rows of A (pass over x_refl) and of A^T (pass over y)
+    double *psd_work;         // PSD blocks' projection scratch (NULL: no PSD blocks)
+    const long long *psd_off; // per cone block: offset of its scratch in psd_work
 };
 
 // The step kernels are written as warp bodies (one tile or one cone block per
@@ -193,7 +195,7 @@ __device__ __forceinline__ void primal_cone_block(const StepData<T> &D, const St
     }
     bool uni = warp_uniform_unit<S>(sl, L, lane);
     warp_project<S, KINDS>(type, sl, L, lane, uni, D.cone_warm ? D.cone_warm + cb : nullptr,
-                           D.cone_alpha ? D.cone_alpha[cb] : 0.0);
+                           D.cone_alpha ? D.cone_alpha[cb] : 0.0, D.psd_work ? D.psd_work + D.psd_off[cb] : nullptr);
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         const int i = lane + 32 * s;
@@ -213,7 +215,7 @@ __device__ __forceinline__ void primal_cone_block(const StepData<T> &D, const St
 
 // One warp per cone block of the list ids (NULL: blocks 0 .. nids - 1);
 // KINDS = CONES_WIDE for SOC / RSOC blocks, CONES_THREE (S = 1) for the
-// 3-slot exponential and power blocks.
+// 3-slot exponential and power blocks, CONES_PSD for PSD blocks.
 template <int S, typename T, bool HAS_Q, int KINDS>
 __global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<T> D, StepParams P, const int *ids, int nids)
 {

@@ -63,6 +63,8 @@ struct ResidualData {
     double *partials;
     int rows_blocks, free_blocks, cone_blocks;
     LongRows A_long, At_long; // passes over x_pdhg and y_pdhg
+    double *psd_work;         // PSD blocks' projection scratch (NULL: none)
+    const long long *psd_off;
 };
 
 __device__ __forceinline__ double norm_term(double v, int l2) { return l2 ? v * v : abs_or_inf(v); }
@@ -106,9 +108,11 @@ __device__ __forceinline__ void residual_cone_block(const ResidualData<VT> &D, c
     }
     const double alpha = D.cone_alpha ? D.cone_alpha[cb] : 0.0;
     bool uni = warp_uniform_unit<S>(aug, L, lane); // d uniform <=> 1/d uniform
-    if (type == 0 || type == 1) {
+    double *psd = D.psd_work ? D.psd_work + D.psd_off[cb] : nullptr;
+    if (type == 0 || type == 1 || type == 4) {
         // self-dual: projection onto the dual cone in the 1/d metric
-        warp_project<S>(type, dual, L, lane, uni, D.warm_dual ? D.warm_dual + cb : nullptr);
+        // (PSD: without a metric, as the reference projects it)
+        warp_project<S>(type, dual, L, lane, uni, D.warm_dual ? D.warm_dual + cb : nullptr, 0.0, psd);
     } else {
         // Moreau: rc - proj_{K*}(rc) = -proj_K(-rc), in the inverse scaling
         // (exponential) or on rc d in the unit metric (power) (reference
@@ -129,7 +133,7 @@ __device__ __forceinline__ void residual_cone_block(const ResidualData<VT> &D, c
             dual.x[s] = type == 2 ? rc[s] + neg.x[s] : rc[s] + neg.x[s] / vr;
         }
     }
-    warp_project<S>(type, aug, L, lane, uni, D.warm_aug ? D.warm_aug + cb : nullptr, alpha);
+    warp_project<S>(type, aug, L, lane, uni, D.warm_aug ? D.warm_aug + cb : nullptr, alpha, psd);
     if (type == 3 && lane == 0) {
         // power-cone primal violation (reference compute_power_cone_primal_violation_kernel,
         // src/kernels/pdhcg_power_cone_kernels.cu:623-669): lane 0 holds slot 0 and
@@ -280,7 +284,8 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
         for (int cb = b * WARPS + wib; cb < D.n_cones; cb += nwarps) {
             // 3-slot blocks (exponential, power) take the one-slot
             // instantiation, which alone carries their projection
-            if (S > 1 && D.cone_type[cb] >= 2)
+            const int ct = D.cone_type[cb];
+            if (S > 1 && (ct == 2 || ct == 3))
                 residual_cone_block<1, VT>(D, P, cb, lane, stage, acc, ops);
             else
                 residual_cone_block<S, VT>(D, P, cb, lane, stage, acc, ops);

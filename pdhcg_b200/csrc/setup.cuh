@@ -431,7 +431,7 @@ __global__ void dual_start_kernel(int m, const double *start, const double *cr, 
 // warp-per-cone projection of a vector (unit metric, d = rescaling)
 template <int S>
 __device__ __forceinline__ void project_cone_block(int st, int L, int tp, double alpha, double *x, const double *d,
-                                                   const double *q, double tau, int lane)
+                                                   const double *q, double tau, int lane, double *psd)
 {
     WarpSlots<S> sl;
 #pragma unroll
@@ -442,7 +442,7 @@ __device__ __forceinline__ void project_cone_block(int st, int L, int tp, double
         sl.w[s] = (i < L && q) ? 1.0 + tau * q[st + i] : 1.0;
     }
     bool uni = warp_uniform_unit<S>(sl, L, lane);
-    warp_project<S>(tp, sl, L, lane, uni, nullptr, alpha);
+    warp_project<S>(tp, sl, L, lane, uni, nullptr, alpha, psd);
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         int i = lane + 32 * s;
@@ -451,19 +451,23 @@ __device__ __forceinline__ void project_cone_block(int st, int L, int tp, double
     }
 }
 
+// psd_work / psd_off: PSD blocks' scratch and each block's offset in it
+// (NULL: no PSD blocks)
 template <int S>
 __global__ void __launch_bounds__(TPB) project_cones_kernel(int ncones, const int *start, const int *len,
                                                             const int *type, const double *alpha, double *x,
-                                                            const double *d, const double *q, double tau)
+                                                            const double *d, const double *q, double tau,
+                                                            double *psd_work, const long long *psd_off)
 {
     const int lane = threadIdx.x & 31;
     for (int cb = blockIdx.x * WARPS + (threadIdx.x >> 5); cb < ncones; cb += gridDim.x * WARPS) {
         const int st = start[cb], L = len[cb], tp = type[cb];
         const double a = alpha ? alpha[cb] : 0.0;
-        if (S > 1 && tp >= 2) // 3-slot blocks: the one-slot instantiation
-            project_cone_block<1>(st, L, tp, a, x, d, q, tau, lane);
+        double *psd = psd_work ? psd_work + psd_off[cb] : nullptr;
+        if (S > 1 && (tp == 2 || tp == 3)) // 3-slot blocks: the one-slot instantiation
+            project_cone_block<1>(st, L, tp, a, x, d, q, tau, lane, psd);
         else
-            project_cone_block<S>(st, L, tp, a, x, d, q, tau, lane);
+            project_cone_block<S>(st, L, tp, a, x, d, q, tau, lane, psd);
     }
 }
 

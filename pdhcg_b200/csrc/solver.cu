@@ -157,20 +157,43 @@ std::vector<int2> row_tiles(const std::vector<int> &rows)
 // sit in the wide kernels' register allocation.  A list pointer stays null
 // when its launch covers every block (all of one kind).
 struct ConeSplit {
-    std::vector<int> wide, three;
-    int *wide_d = nullptr, *three_d = nullptr;
-    int n_wide = 0, n_three = 0;
+    std::vector<int> wide, three, psd;
+    int *wide_d = nullptr, *three_d = nullptr, *psd_d = nullptr;
+    int n_wide = 0, n_three = 0, n_psd = 0;
 
     void build(const std::vector<int> &types)
     {
         wide.clear();
         three.clear();
-        for (int b = 0; b < (int)types.size(); ++b)
-            (types[b] == CONE_EXPONENTIAL || types[b] == CONE_POWER ? three : wide).push_back(b);
+        psd.clear();
+        for (int b = 0; b < (int)types.size(); ++b) {
+            if (types[b] == CONE_EXPONENTIAL || types[b] == CONE_POWER)
+                three.push_back(b);
+            else if (types[b] == CONE_PSD)
+                psd.push_back(b);
+            else
+                wide.push_back(b);
+        }
         n_wide = (int)wide.size();
         n_three = (int)three.size();
+        n_psd = (int)psd.size();
     }
-    bool mixed() const { return n_wide > 0 && n_three > 0; }
+    // more than one launch: every launch takes its index list
+    bool mixed() const { return (n_wide > 0) + (n_three > 0) + (n_psd > 0) > 1; }
+    // the three lists back to back in one device array of n_wide + n_three + n_psd ints
+    void place(int *ids)
+    {
+        wide_d = ids;
+        three_d = ids + n_wide;
+        psd_d = ids + n_wide + n_three;
+    }
+    std::vector<int> joined() const
+    {
+        std::vector<int> all(wide);
+        all.insert(all.end(), three.begin(), three.end());
+        all.insert(all.end(), psd.begin(), psd.end());
+        return all;
+    }
 };
 
 // lanes per row from the mean row length
@@ -314,7 +337,11 @@ struct DeviceProblem {
     double *c = nullptr, *l = nullptr, *u = nullptr, *lc = nullptr, *uc = nullptr, *g = nullptr;
     int *cst = nullptr, *clen = nullptr, *ctype = nullptr, *cvdim = nullptr, *free_d = nullptr;
     double *calpha = nullptr; // power-cone exponents per cone block
-    ConeSplit split;            // cone blocks by launch (wide / 3-slot)
+    ConeSplit split;            // cone blocks by launch (wide / 3-slot / PSD)
+    bool has_psd = false;
+    std::vector<long long> psd_off; // per cone block: offset of its PSD scratch (2 n^2 doubles)
+    long long psd_total = 0;
+    long long *psd_off_d = nullptr;
     int2 *free_tiles = nullptr; // free variables as tiles of consecutive rows
     int n_free_tiles = 0;
     double *pstart = nullptr, *dstart = nullptr;
@@ -456,8 +483,14 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
             in_cone[j] = 1;
             d.cone_box |= std::isfinite(p->variable_lower_bound[j]) || std::isfinite(p->variable_upper_bound[j]);
         }
-        if (p->cones.type[b] == CONE_PSD)
-            d.unsupported = "PSD cones are not available on the device path yet";
+        d.psd_off.push_back(d.psd_total);
+        if (p->cones.type[b] == CONE_PSD) {
+            const int order = p->cones.v_dim[b];
+            if (order > PSD_MAX_ORDER)
+                d.unsupported = "PSD blocks of order above 22 are not supported yet";
+            d.has_psd = true;
+            d.psd_total += 2LL * order * order;
+        }
         d.cone_alpha.push_back(p->cones.power_alpha ? p->cones.power_alpha[b] : 0.0);
     }
     int nc = (int)d.cone_start.size();
@@ -473,8 +506,12 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
         d.calpha = ar.upload(d.cone_alpha.data(), nc, s);
         d.split.build(d.cone_type);
         if (d.split.mixed()) {
-            d.split.wide_d = ar.upload(d.split.wide.data(), d.split.n_wide, s);
-            d.split.three_d = ar.upload(d.split.three.data(), d.split.n_three, s);
+            std::vector<int> all = d.split.joined();
+            d.split.place(ar.upload(all.data(), all.size(), s));
+            CK(cudaStreamSynchronize(s));
+        }
+        if (d.has_psd) {
+            d.psd_off_d = ar.upload(d.psd_off.data(), nc, s);
             CK(cudaStreamSynchronize(s));
         }
         if (!d.free_idx.empty()) {
@@ -574,6 +611,7 @@ private:
            *g_d_ = nullptr, *cr_d_ = nullptr, *vr_d_ = nullptr;
     int *free_d_ = nullptr, *cst_d_ = nullptr, *clen_d_ = nullptr, *ctype_d_ = nullptr, *cvdim_d_ = nullptr;
     double *cone_warm_ = nullptr, *warm_dual_ = nullptr, *warm_aug_ = nullptr; // per-cone multipliers
+    double *psd_work_ = nullptr; // PSD blocks' eigen-decomposition scratch (2 n^2 doubles each)
     double *x0_, *x_, *xp_, *xr_, *dx_, *dslack_, *y0_, *y_, *yp_, *dy_;
     // FP32 mirrors of the matrices, problem vectors and iterates (mixed precision)
     struct {
@@ -659,6 +697,16 @@ int launch_primal_cones(const StepData<T> &D, const StepParams &P, const ConeSpl
             primal_cone_kernel<1, T, true, CONES_THREE><<<grid, TPB, 0, s>>>(D, P, sp.three_d, sp.n_three);
         else
             primal_cone_kernel<1, T, false, CONES_THREE><<<grid, TPB, 0, s>>>(D, P, sp.three_d, sp.n_three);
+        ++launches;
+    }
+    if (sp.n_psd > 0) { // LP path only: diagonal Q with PSD blocks takes the inner BB solve
+        dispatch_s(S, [&](auto SC) {
+            int grid = grid_for(sp.n_psd, WARPS);
+            if (hasq)
+                primal_cone_kernel<SC.value, T, true, CONES_PSD><<<grid, TPB, 0, s>>>(D, P, sp.psd_d, sp.n_psd);
+            else
+                primal_cone_kernel<SC.value, T, false, CONES_PSD><<<grid, TPB, 0, s>>>(D, P, sp.psd_d, sp.n_psd);
+        });
         ++launches;
     }
     return launches;
@@ -888,9 +936,11 @@ void Solve::init_state()
         warm_aug_ = cone_warm_ + 2 * (size_t)nc;
         CK(cudaMemsetAsync(cone_warm_, 0, 3 * (size_t)nc * sizeof(double), s)); // 0 = no warm start
         cone_aux_init_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(nc, cst_d_, cvdim_d_, ctype_d_, vr_d_, sb_, x0_);
+        if (dp_.has_psd)
+            psd_work_ = ar_.alloc<double>((size_t)dp_.psd_total);
         dispatch_s(S_, [&](auto SC) {
-            project_cones_kernel<SC.value><<<grid_for(nc, WARPS), TPB, 0, s>>>(nc, cst_d_, clen_d_, ctype_d_,
-                                                                             dp_.calpha, x0_, vr_d_, nullptr, 0.0);
+            project_cones_kernel<SC.value><<<grid_for(nc, WARPS), TPB, 0, s>>>(
+                nc, cst_d_, clen_d_, ctype_d_, dp_.calpha, x0_, vr_d_, nullptr, 0.0, psd_work_, dp_.psd_off_d);
         });
     }
     box_clamp_copy_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(n, l_d_, u_d_, x0_, x_, xp_, xr_);
@@ -943,6 +993,8 @@ BBData Solve::bb_data() const
     D.cone_len = clen_d_;
     D.cone_type = ctype_d_;
     D.cone_alpha = dp_.calpha;
+    D.psd_work = psd_work_;
+    D.psd_off = dp_.psd_off_d;
     D.n_cones = (int)cone_start_.size();
     D.vr = vr_d_;
     D.cone_warm = cone_warm_;
@@ -1013,7 +1065,7 @@ void Solve::setup_bb()
     bb_min_tol_ = mt;
     double init[2] = {it0, 1.0};
     CK(cudaMemcpyAsync(bb_tol_, init, sizeof(init), cudaMemcpyHostToDevice, s));
-    if (prm_.diag_jacobi_precond) {
+    if (prm_.diag_jacobi_precond && !dp_.has_psd) { // the reference runs PSD models unpreconditioned
         bb_diag_h_ = ar_.alloc<double>(n);
         bb_m_ = ar_.alloc<double>(n);
         bb_minv_ = ar_.alloc<double>(n);
@@ -1137,6 +1189,8 @@ StepData<T> Solve::step_data()
     D.cone_len = clen_d_;
     D.cone_type = ctype_d_;
     D.cone_alpha = dp_.calpha;
+    D.psd_work = psd_work_;
+    D.psd_off = dp_.psd_off_d;
     D.n_cones = (int)cone_start_.size();
     if constexpr (std::is_same<T, double>::value) {
         D.A_v = A_.v;
@@ -1435,6 +1489,8 @@ void Solve::enqueue_residual_t(bool want_dist)
     D.cone_len = clen_d_;
     D.cone_type = ctype_d_;
     D.cone_alpha = dp_.calpha;
+    D.psd_work = psd_work_;
+    D.psd_off = dp_.psd_off_d;
     D.n_cones = (int)cone_start_.size();
     D.partials = partials_;
     D.rows_blocks = res_rows_blocks_;
@@ -1953,7 +2009,9 @@ pdhcg_result_t *Solve::run()
     init_state();
     step_size();
     CK(cudaStreamSynchronize(st_));
-    bb_ = qtype_ != PDHCG_NON_Q && qtype_ != PDHCG_DIAG_Q;
+    // diagonal Q with PSD blocks takes the inner BB solve, as the reference
+    // does (a nonuniform diagonal metric has no one-decomposition PSD prox)
+    bb_ = qtype_ != PDHCG_NON_Q && (qtype_ != PDHCG_DIAG_Q || dp_.has_psd);
     if (bb_)
         setup_bb();
     if (opt_.precision == PDHCG_B200_MIXED && !bb_) // the inner BB solve runs in FP64 only
@@ -2013,13 +2071,16 @@ int step_impl(StepData<double> D, StepParams P, const pdhcg_b200_step_t *t, cuda
             return -2;
         std::vector<int2> ft = row_tiles(fr);
         split.build(tp);
+        if (split.n_psd > 0) { // the kernel-level step keeps no PSD scratch
+            std::fprintf(stderr, "[pdhcg_b200_pdhg_step] PSD blocks are not supported by the kernel-level step.\n");
+            return -3;
+        }
         if (split.mixed()) {
+            std::vector<int> all = split.joined();
             CK(cudaMallocAsync((void **)&ids_d, nc * sizeof(int), s));
-            CK(cudaMemcpyAsync(ids_d, split.wide.data(), split.n_wide * sizeof(int), cudaMemcpyHostToDevice, s));
-            CK(cudaMemcpyAsync(ids_d + split.n_wide, split.three.data(), split.n_three * sizeof(int),
-                               cudaMemcpyHostToDevice, s));
-            split.wide_d = ids_d;
-            split.three_d = ids_d + split.n_wide;
+            CK(cudaMemcpyAsync(ids_d, all.data(), nc * sizeof(int), cudaMemcpyHostToDevice, s));
+            CK(cudaStreamSynchronize(s)); // all goes out of scope
+            split.place(ids_d);
         }
         CK(cudaMallocAsync((void **)&len_d, nc * sizeof(int), s));
         CK(cudaMallocAsync((void **)&free_d, std::max<size_t>(fr.size(), 1) * sizeof(int), s));
@@ -2320,23 +2381,36 @@ int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *co
     cone_len_kernel<<<grid_for(num_cones, TPB), TPB, 0, s>>>(num_cones, cone_vdim, cone_type, len);
     int maxlen = 0;
     bool types_ok = true;
+    std::vector<long long> psd_off(num_cones, 0);
+    long long psd_total = 0;
     {
-        std::vector<int> h(num_cones), t(num_cones);
+        std::vector<int> h(num_cones), t(num_cones), vd(num_cones);
         cudaMemcpyAsync(h.data(), len, num_cones * sizeof(int), cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(t.data(), cone_type, num_cones * sizeof(int), cudaMemcpyDeviceToHost, s);
         if (cudaStreamSynchronize(s) != cudaSuccess) {
             cudaFreeAsync(len, s);
             return -1;
         }
+        if (cudaMemcpyAsync(vd.data(), cone_vdim, num_cones * sizeof(int), cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            cudaFreeAsync(len, s);
+            return -1;
+        }
         for (int i = 0; i < num_cones; ++i) {
             maxlen = std::max(maxlen, h[i]);
             types_ok = types_ok && (t[i] == CONE_STANDARD_SOC || t[i] == CONE_ROTATED_SOC ||
-                                    t[i] == CONE_EXPONENTIAL || (t[i] == CONE_POWER && cone_alpha));
+                                    t[i] == CONE_EXPONENTIAL || (t[i] == CONE_POWER && cone_alpha) ||
+                                    t[i] == CONE_PSD);
+            if (t[i] == CONE_PSD) {
+                psd_off[i] = psd_total;
+                psd_total += 2LL * vd[i] * vd[i];
+            }
         }
     }
-    if (!types_ok) { // the PSD projection is not built; a power block needs its exponent
-        std::fprintf(stderr, "[pdhcg_b200_project_cones] only SOC, rotated-SOC, exponential and power blocks "
-                             "(with cone_alpha) are supported.\n");
+    if (!types_ok) { // a power block needs its exponent
+        std::fprintf(stderr, "[pdhcg_b200_project_cones] only SOC, rotated-SOC, exponential, power (with "
+                             "cone_alpha) and PSD blocks are supported.\n");
         cudaFreeAsync(len, s);
         return -3;
     }
@@ -2345,12 +2419,28 @@ int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *co
         cudaFreeAsync(len, s);
         return -2;
     }
+    double *psd_work = nullptr;
+    long long *psd_off_d = nullptr;
+    if (psd_total > 0) {
+        if (cudaMallocAsync((void **)&psd_work, psd_total * sizeof(double), s) != cudaSuccess ||
+            cudaMallocAsync((void **)&psd_off_d, num_cones * sizeof(long long), s) != cudaSuccess ||
+            cudaMemcpyAsync(psd_off_d, psd_off.data(), num_cones * sizeof(long long), cudaMemcpyHostToDevice, s) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) { // psd_off goes out of scope
+            cudaFreeAsync(len, s);
+            return -1;
+        }
+    }
     dispatch_s(S, [&](auto SC) {
         project_cones_kernel<SC.value><<<grid_for(num_cones, WARPS), TPB, 0, s>>>(num_cones, cone_start, len,
                                                                                  cone_type, cone_alpha, x, d, q,
-                                                                                 tau);
+                                                                                 tau, psd_work, psd_off_d);
     });
     cudaFreeAsync(len, s);
+    if (psd_work) {
+        cudaFreeAsync(psd_work, s);
+        cudaFreeAsync(psd_off_d, s);
+    }
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -2387,7 +2477,7 @@ int pdhcg_b200_project_cones_noalloc(int num_cones, const int *cone_start, const
     dispatch_s(S, [&](auto SC) {
         project_cones_kernel<SC.value><<<grid_for(num_cones, WARPS), TPB, 0, s>>>(num_cones, cone_start, scratch,
                                                                                  cone_type, cone_alpha, x, d, q,
-                                                                                 tau);
+                                                                                 tau, nullptr, nullptr);
     });
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

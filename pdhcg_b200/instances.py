@@ -20,7 +20,8 @@ from __future__ import annotations
 import numpy as np
 import scipy.sparse as sp
 
-from .capi import CONE_EXPONENTIAL, CONE_POWER, CONE_ROTATED_SOC, CONE_STANDARD_SOC, Cone, CsrMatrix, Problem
+from .capi import (CONE_EXPONENTIAL, CONE_POWER, CONE_PSD, CONE_ROTATED_SOC, CONE_STANDARD_SOC, Cone, CsrMatrix,
+                   Problem)
 
 
 def random_csr(rng: np.random.Generator, m: int, n: int, per_row: int, values: str = "normal") -> CsrMatrix:
@@ -195,6 +196,45 @@ def conic_lp(seed: int = 5, nfree: int = 60, nsoc: int = 10, soc_len: int = 12, 
     if with_q:
         q = rng.uniform(0.1, 1.0, n)
         p.Q = CsrMatrix(n, n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), q)
+    return p
+
+
+def _svec(X: np.ndarray) -> np.ndarray:
+    """Lower triangle down the columns, off-diagonal entries times sqrt 2."""
+    n = X.shape[0]
+    return np.array([X[r, c] if r == c else X[r, c] * np.sqrt(2.0) for c in range(n) for r in range(c, n)])
+
+
+def psd_lp(seed: int = 6, nfree: int = 40, orders=(2, 3, 4, 5, 3, 6), with_q: bool = False) -> Problem:
+    """Box variables plus PSD blocks (svec packing, orders ``orders``),
+    equality rows through a point whose PSD blocks are positive definite,
+    and an objective positive definite on each PSD block (so the problem is
+    feasible and bounded).  with_q adds a diagonal Q (the inner BB solve)."""
+    rng = np.random.default_rng(seed)
+    lens = [k * (k + 1) // 2 for k in orders]
+    n = nfree + sum(lens)
+    m = n // 3
+    A = random_csr(rng, m, n, 5)
+    x0 = np.zeros(n)
+    c = rng.standard_normal(n) * 0.5
+    x0[:nfree] = rng.uniform(-0.5, 0.5, nfree)
+    cones, st = [], nfree
+    for k, L in zip(orders, lens):
+        B = rng.standard_normal((k, k))
+        x0[st:st + L] = _svec(B @ B.T + np.eye(k))
+        C2 = rng.standard_normal((k, k))
+        c[st:st + L] = _svec(C2 @ C2.T / k + 0.5 * np.eye(k))
+        cones.append(Cone(CONE_PSD, st, k))
+        st += L
+    b = A.to_scipy() @ x0
+    lb = np.full(n, -np.inf)
+    ub = np.full(n, np.inf)
+    lb[:nfree] = -1.0
+    ub[:nfree] = 1.0
+    p = Problem(c=c, A=A, con_lb=b, con_ub=b.copy(), var_lb=lb, var_ub=ub, cones=cones)
+    if with_q:
+        p.Q = CsrMatrix(n, n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32),
+                        rng.uniform(0.1, 1.0, n))
     return p
 
 

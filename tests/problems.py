@@ -6,8 +6,8 @@ CUDA solver are both checked against the answers the reference asserts.
 """
 import numpy as np
 
-from pdhcg_b200.capi import (CONE_EXPONENTIAL, CONE_POWER, CONE_ROTATED_SOC, CONE_STANDARD_SOC, NORM_L2, Cone, CsrMatrix,
-                             Problem)
+from pdhcg_b200.capi import (CONE_EXPONENTIAL, CONE_POWER, CONE_PSD, CONE_ROTATED_SOC, CONE_STANDARD_SOC, NORM_L2, Cone,
+                             CsrMatrix, Problem)
 
 BIG = 1e30
 
@@ -115,7 +115,41 @@ def pow_diag_q():
     return p, dict(_POW_PRM), {"x": [3.427365210244501, 0.4816579589566281, -1.902365192823554], "tol": 2e-4}
 
 
+_PSD_PRM = {"use_cone_preserving_scaling": False, "termination_evaluation_frequency": 10,
+            "termination_criteria.eps_optimal_relative": 1e-7, "termination_criteria.eps_feasible_relative": 1e-7,
+            "termination_criteria.iteration_limit": 1000000, "termination_criteria.time_sec_limit": 30.0}
+
+
+def variable_psd():
+    """test/test_psd_cones.c:24-68: min X_22 over svec(X) in PSD (order 2)
+    with 100 X_11 = 100 and 0.01 svec_21 = 0.02 sqrt 2, i.e. X_21 = 2.
+    Expected svec = (1, 2 sqrt 2, 4) (tol 2e-4, 2e-4, 3e-4), relative
+    primal and dual residuals below 2e-6."""
+    r2 = np.sqrt(2.0)
+    A = CsrMatrix(2, 3, np.array([0, 1, 2]), np.array([0, 1]), np.array([100.0, 0.01]))
+    b = np.array([100.0, 0.02 * r2])
+    p = Problem(c=np.array([0.0, 0.0, 1.0]), A=A, con_lb=b, con_ub=b.copy(), var_lb=np.full(3, -np.inf),
+                var_ub=np.full(3, np.inf), cones=[Cone(CONE_PSD, 0, 2)])
+    return p, dict(_PSD_PRM), {"x": [1.0, 2.0 * r2, 4.0], "x_tol": [2e-4, 2e-4, 3e-4], "tol": 3e-4, "res": 2e-6}
+
+
+def diagonal_q_psd():
+    """test/test_psd_cones.c:120-180: min X_22^2 / 2 - 3 X_22 over svec(X) in
+    PSD (order 2) with X_11 = 1, svec_21 = 2 sqrt 2 (diagonal Q: the inner
+    BB solve).  Expected X_22 = 4 (tol 5e-4), relative residuals below
+    3e-6."""
+    r2 = np.sqrt(2.0)
+    A = CsrMatrix(2, 3, np.array([0, 1, 2]), np.array([0, 1]), np.array([1.0, 1.0]))
+    b = np.array([1.0, 2.0 * r2])
+    Q = CsrMatrix(3, 3, np.array([0, 0, 0, 1]), np.array([2]), np.array([1.0]))
+    p = Problem(c=np.array([0.0, 0.0, -3.0]), A=A, con_lb=b, con_ub=b.copy(), var_lb=np.full(3, -np.inf),
+                var_ub=np.full(3, np.inf), Q=Q, cones=[Cone(CONE_PSD, 0, 2)])
+    return p, dict(_PSD_PRM), {"xi": [(2, 4.0)], "tol": 5e-4, "res": 3e-6}
+
+
 KNOWN_ANSWERS = {
+    "variable_psd": variable_psd,
+    "diagonal_q_psd": diagonal_q_psd,
     "exp_cone_linear": exp_cone_linear,
     "pow_full_cone_0.2": lambda: pow_full_cone(0.2),
     "pow_full_cone_0.5": lambda: pow_full_cone(0.5),
@@ -137,7 +171,13 @@ def check_known_answer(res: dict, expect: dict):
     x = res["x"]
     if "x" in expect:
         e = np.asarray(expect["x"], dtype=float)
-        assert np.all(np.abs(np.asarray(x) - e) <= tol * (1 + np.abs(e))), (x, e)
+        t = np.asarray(expect.get("x_tol", [tol] * len(e)), dtype=float)
+        assert np.all(np.abs(np.asarray(x) - e) <= t * (1 + np.abs(e))), (x, e)
+    for i, v in expect.get("xi", []):
+        assert abs(x[i] - v) <= tol * (1 + abs(v)), (i, x[i], v)
+    if "res" in expect:
+        assert res["relative_primal_residual"] < expect["res"], res["relative_primal_residual"]
+        assert res["relative_dual_residual"] < expect["res"], res["relative_dual_residual"]
     if "y" in expect:
         np.testing.assert_allclose(res["y"], expect["y"], atol=tol * 10)
     if "obj" in expect:

@@ -115,13 +115,65 @@ def test_exp_pow_projection_matches_oracle(lib, oracle, weighted):
     np.testing.assert_allclose(got, expect, rtol=1e-9, atol=1e-9 * np.abs(expect).max())
 
 
+def _svec(X):
+    n = X.shape[0]
+    return np.array([X[r, c] if r == c else X[r, c] * np.sqrt(2.0) for c in range(n) for r in range(c, n)])
+
+
+def test_psd_projection_matches_oracle(lib, oracle):
+    """PSD blocks of orders 1..22 (svec packing) among SOC blocks, with
+    spectra of mixed signs, all negative (projection 0) and all positive
+    (projection = input), against the oracle's Jacobi restatement and numpy's
+    eigh.  PSD blocks take no metric (d and q do not enter), as in the
+    reference.  Tolerance 1e-10 relative to the block scale."""
+    import torch
+    rng = np.random.default_rng(31)
+    blocks, parts, st = [], [], 0
+    for k, order in enumerate([1, 2, 3, 4, 5, 7, 9, 12, 16, 22, 1, 2, 6]):
+        M = rng.standard_normal((order, order))
+        M = (M + M.T) / 2
+        if k == 3:
+            M = -M @ M.T - 0.1 * np.eye(order)  # negative definite: projects to 0
+        if k == 4:
+            M = M @ M.T + 0.1 * np.eye(order)  # positive definite: unchanged
+        v = _svec(M)
+        blocks.append((st, order, capi.CONE_PSD, M))
+        parts.append(v)
+        st += len(v)
+        L = int(rng.integers(3, 40))  # an SOC block between PSD blocks
+        blocks.append((st, L - 2, capi.CONE_STANDARD_SOC, None))
+        parts.append(rng.standard_normal(L))
+        st += L
+    x = np.concatenate(parts)
+    d = rng.uniform(0.5, 2.0, st)
+    expect = x.copy()
+    for s0, vd, t, M in blocks:
+        L = vd * (vd + 1) // 2 if t == capi.CONE_PSD else vd + 2
+        blk = expect[s0:s0 + L].copy()
+        dd = d[s0:s0 + L].copy()
+        oracle.oracle_project_cone_block(t, vd, 0.0, blk.ctypes.data_as(_dp), dd.ctypes.data_as(_dp), None, 0.0)
+        expect[s0:s0 + L] = blk
+        if M is not None:  # the oracle itself against eigh
+            w, V = np.linalg.eigh(M)
+            np.testing.assert_allclose(blk, _svec((V * np.maximum(w, 0)) @ V.T), atol=1e-11 * (1 + np.abs(M).max()))
+    starts = _dev([b[0] for b in blocks], np.int32)
+    vdims = _dev([b[1] for b in blocks], np.int32)
+    types = _dev([b[2] for b in blocks], np.int32)
+    xd, dd_ = _dev(x), _dev(d)
+    rc = lib.pdhcg_b200_project_cones(len(blocks), _ptr(starts), _ptr(vdims), _ptr(types), None, _ptr(xd),
+                                      _ptr(dd_), None, 0.0, None)
+    torch.cuda.synchronize()
+    assert rc == 0
+    np.testing.assert_allclose(xd.cpu().numpy(), expect, rtol=1e-10, atol=1e-10 * np.abs(expect).max())
+
+
 def test_cone_projection_rejects_unbuilt_cone_types(lib):
-    """A PSD block is refused (-3) and x is left untouched."""
+    """An unknown cone type is refused (-3) and x is left untouched."""
     import torch
     x = np.arange(8, dtype=np.float64)
     xd = _dev(x)
-    starts, vdims = _dev([0, 3], np.int32), _dev([1, 2], np.int32)
-    types = _dev([capi.CONE_STANDARD_SOC, capi.CONE_PSD], np.int32)
+    starts, vdims = _dev([0, 3], np.int32), _dev([1, 3], np.int32)
+    types = _dev([capi.CONE_STANDARD_SOC, 9], np.int32)
     d = _dev(np.ones(8))
     rc = lib.pdhcg_b200_project_cones(2, _ptr(starts), _ptr(vdims), _ptr(types), None, _ptr(xd), _ptr(d), None,
                                       1.0, None)

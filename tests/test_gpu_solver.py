@@ -10,8 +10,10 @@ import ctypes as C
 
 import numpy as np
 import pytest
+import scipy.sparse as sp
 
 from pdhcg_b200 import capi, instances, native
+from pdhcg_b200.capi import CsrMatrix
 from problems import INFEASIBLE, KNOWN_ANSWERS, check_known_answer
 
 pytestmark = pytest.mark.gpu
@@ -49,6 +51,20 @@ def test_known_answers_on_gpu(lib, name):
     check_known_answer(res, expect)
 
 
+def _all_cones_sparse_q(seed=16):
+    """SOC / RSOC blocks covering every variable, with a tridiagonal Q (the
+    inner BB solve with an empty free-variable list)."""
+    p = instances.conic_lp(seed=seed, nfree=0)
+    n = p.n
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        for j, v in ((i - 1, 0.3), (i, 1.0), (i + 1, 0.3)):
+            if 0 <= j < n:
+                rows.append(i), cols.append(j), vals.append(v)
+    p.Q = CsrMatrix.from_scipy(sp.csr_matrix((vals, (rows, cols)), shape=(n, n)))
+    return p
+
+
 CASES = {
     "box_lp": (lambda: instances.box_lp(), {}),
     "diag_qp": (lambda: instances.diag_qp(), {}),
@@ -76,6 +92,11 @@ CASES = {
     "dense_rows_lp": (lambda: instances.dense_rows_qp(), {}),
     "dense_rows_qp": (lambda: instances.dense_rows_qp(seed=22, with_q=True), {}),
     "portfolio_long_rows": (lambda: instances.portfolio(seed=4, scale=0.05), {}),
+    # PSD blocks: the LP step (own launch) and, with a diagonal Q, the inner BB solve
+    "psd_lp": (lambda: instances.psd_lp(), {}),
+    "psd_lp_mixed_cones": (lambda: instances.psd_lp(seed=7, orders=(2, 4, 1, 3)), {"use_cone_preserving_scaling": False}),
+    "psd_qp": (lambda: instances.psd_lp(seed=8, with_q=True), {}),
+    "all_cones_sparse_q": (_all_cones_sparse_q, {}),
 }
 
 
