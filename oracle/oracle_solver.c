@@ -170,6 +170,7 @@ typedef struct {
     double *calpha;
     int naff;
     int *astart, *avdim, *atype;
+    double *aalpha; /* affine power-cone exponents */
     double *primal_start, *dual_start;
 } oprob;
 
@@ -178,7 +179,7 @@ static void oprob_free(oprob *P)
     csr_free(&P->A); csr_free(&P->Q); csr_free(&P->R); csr_free(&P->D);
     free(P->c); free(P->l); free(P->u); free(P->lc); free(P->uc); free(P->g);
     free(P->cstart); free(P->cvdim); free(P->ctype); free(P->calpha);
-    free(P->astart); free(P->avdim); free(P->atype);
+    free(P->astart); free(P->avdim); free(P->atype); free(P->aalpha);
     free(P->primal_start); free(P->dual_start);
 }
 
@@ -234,10 +235,12 @@ static void oprob_load(oprob *P, const qp_problem_t *prob)
     P->astart = (int *)xcalloc((size_t)P->naff, sizeof(int));
     P->avdim = (int *)xcalloc((size_t)P->naff, sizeof(int));
     P->atype = (int *)xcalloc((size_t)P->naff, sizeof(int));
+    P->aalpha = (double *)xcalloc((size_t)P->naff, sizeof(double));
     for (int i = 0; i < P->naff; ++i) {
         P->astart[i] = prob->affine_cones.start_idx[i];
         P->avdim[i] = prob->affine_cones.v_dim[i];
         P->atype[i] = (int)prob->affine_cones.type[i];
+        P->aalpha[i] = prob->affine_cones.power_alpha ? prob->affine_cones.power_alpha[i] : 0.0;
     }
     if (prob->primal_start)
         P->primal_start = dcopy(prob->primal_start, P->n);
@@ -638,6 +641,9 @@ typedef struct {
     double cum_time;
 } ostate;
 
+static void project_affine(ostate *S, double *v);
+
+
 static void apply_middle(ostate *S)
 {
     int r = S->P.rank;
@@ -832,13 +838,35 @@ static void pdhg_update(ostate *S)
     S->inner_total++;
     spmv(&S->P.A, S->xr, S->Ax);
     int store_dual = S->is_major || store_rule;
+    /* with affine cones the clamped point is projected onto the cones of the
+     * affine rows before the update (reference pdhg_update,
+     * src/pdhg_core_op.cu:810-829, prepare / finish_constraint_dual_update) */
+    double *pr = dvec(m);
+    for (int i = 0; i < m; ++i)
+        pr[i] = clampd(S->P.lc[i], S->Ax[i] + S->P.g[i] - S->y[i] / sigma, S->P.uc[i]);
+    if (S->P.naff > 0) project_affine(S, pr);
     for (int i = 0; i < m; ++i) {
         double cur = S->y[i];
         double v = S->Ax[i] + S->P.g[i];
-        double pr = clampd(S->P.lc[i], v - cur / sigma, S->P.uc[i]);
-        double nx = cur - sigma * v + sigma * pr;
+        double nx = cur - sigma * v + sigma * pr[i];
         if (store_dual) S->yp[i] = nx;
         S->yr[i] = 2.0 * nx - cur;
+    }
+    free(pr);
+}
+
+/* Projection of the affine-cone rows of a row vector v onto their cones in
+ * the unit metric of the scaled space, K defined on v / d with d = 1 / cr
+ * (the reference's affine coordinate rescaling, src/solver_state.cu:625-638;
+ * project_cone_runtime on the affine runtime, src/cone_dispatch.cu:38-57). */
+static void project_affine(ostate *S, double *v)
+{
+    for (int b = 0; b < S->P.naff; ++b) {
+        int st = S->P.astart[b], len = cone_len(S->P.atype[b], S->P.avdim[b]);
+        double *d = dvec(len);
+        for (int i = 0; i < len; ++i) d[i] = 1.0 / S->cr[st + i];
+        oracle_project_cone_block(S->P.atype[b], S->P.avdim[b], S->P.aalpha[b], v + st, d, NULL, 0.0);
+        free(d);
     }
 }
 
@@ -902,8 +930,9 @@ static void augment_projected_gradient(ostate *S, const double *eff)
     }
 }
 
-/* compute_residual, reference src/pdhg_core_op.cu:1037-1294 (no affine or
- * power cones in the oracle) */
+/* compute_residual, reference src/pdhg_core_op.cu:1037-1294 (affine cones:
+ * compute_affine_cone_residuals, :109-212, and
+ * src/kernels/pdhcg_affine_cone_kernels.cu) */
 static void compute_residual(ostate *S, norm_type_t nt)
 {
     int n = S->n, m = S->m;
@@ -911,12 +940,40 @@ static void compute_residual(ostate *S, norm_type_t nt)
     spmv(&S->At, S->yp, S->Aty);
     update_obj_product(S, S->xp);
     int cones = S->P.ncones > 0;
+    double *pp = dvec(m);
     for (int i = 0; i < m; ++i) {
-        double v = S->Ax[i] + S->P.g[i];
-        double p = clampd(S->P.lc[i], v, S->P.uc[i]);
-        S->primal_residual[i] = (v - p) * S->cr[i];
+        pp[i] = clampd(S->P.lc[i], S->Ax[i] + S->P.g[i], S->P.uc[i]);
         S->primal_slack[i] = fmax(S->yp[i], 0.0) * S->lc_fin[i] + fmin(S->yp[i], 0.0) * S->uc_fin[i] -
             S->P.g[i] * S->yp[i];
+    }
+    if (S->P.naff > 0) project_affine(S, pp); /* affine rows: distance to their cone */
+    for (int i = 0; i < m; ++i)
+        S->primal_residual[i] = (S->Ax[i] + S->P.g[i] - pp[i]) * S->cr[i];
+    free(pp);
+    /* affine rows: dual membership proj_K(-y) (zero when y is in the dual
+     * cone) in the 1 / cr scaling, and per-block complementarity
+     * |y . (A x + g)| / sb */
+    double mem_norm = 0.0, compl_norm = 0.0;
+    if (S->P.naff > 0) {
+        double *mv = dvec(m), *cpl = dvec(S->P.naff);
+        for (int b = 0; b < S->P.naff; ++b) {
+            int st = S->P.astart[b], len = cone_len(S->P.atype[b], S->P.avdim[b]);
+            double d = 0.0;
+            for (int i = st; i < st + len; ++i) {
+                mv[i] = -S->yp[i];
+                d += S->yp[i] * (S->Ax[i] + S->P.g[i]);
+            }
+            cpl[b] = fabs(d) / S->sb;
+        }
+        project_affine(S, mv);
+        for (int b = 0; b < S->P.naff; ++b) {
+            int st = S->P.astart[b], len = cone_len(S->P.atype[b], S->P.avdim[b]);
+            for (int i = st; i < st + len; ++i) mv[i] /= S->cr[i];
+        }
+        mem_norm = vnorm(mv, m, nt);
+        compl_norm = vnorm(cpl, S->P.naff, nt);
+        free(mv);
+        free(cpl);
     }
     if (S->is_lp) {
         for (int i = 0; i < n; ++i)
@@ -981,6 +1038,10 @@ static void compute_residual(ostate *S, norm_type_t nt)
     if (cones)
         S->abs_p = nt == NORM_TYPE_L_INF ? fmax(S->abs_p, pv_abs) : hypot(S->abs_p, pv_abs);
     S->abs_d = vnorm(S->dual_residual, n, nt); /* complementarity residual is 0 without fixed sections */
+    if (nt == NORM_TYPE_L_INF)
+        S->abs_d = fmax(S->abs_d, fmax(mem_norm, compl_norm));
+    else
+        S->abs_d = sqrt(S->abs_d * S->abs_d + mem_norm * mem_norm + compl_norm * compl_norm);
     S->abs_d /= S->sc;
     double half_xqx = S->qtype == PDHCG_NON_Q ? 0.0 : 0.5 * dot(S->xp, S->qx, n);
     S->pobj = (dot(S->P.c, S->xp, n) + half_xqx) / (S->sb * S->sc) + S->P.c0;
@@ -1205,8 +1266,8 @@ pdhcg_result_t *oracle_solve(const qp_problem_t *prob, const pdhg_parameters_t *
     if (params_in) prm = *params_in;
     else return NULL;
     if (!prob) return NULL;
-    if (prob->cones.is_fixed || (prob->affine_cones.num_cones > 0) || prob->num_quadratic_constraints > 0) {
-        fprintf(stderr, "[oracle] fixed cone slots, affine cones and quadratic constraints are not restated\n");
+    if (prob->cones.is_fixed || prob->affine_cones.is_fixed || prob->num_quadratic_constraints > 0) {
+        fprintf(stderr, "[oracle] fixed cone slots and quadratic constraints are not restated\n");
         return NULL;
     }
     ostate Sv;
@@ -1384,7 +1445,7 @@ pdhcg_result_t *oracle_solve(const qp_problem_t *prob, const pdhg_parameters_t *
     while (S->k < prm.termination_criteria.iteration_limit) {
         if (S->is_major || S->k == 0 || (S->k % print_frequency(S->k)) == 0) {
             compute_residual(S, prm.optimality_norm);
-            if (!cones && S->is_major && S->k < 3 * freq) infeasibility_info(S);
+            if (!cones && S->P.naff == 0 && S->is_major && S->k < 3 * freq) infeasibility_info(S);
             S->cum_time = now_sec() - t0;
             check_termination(S, &prm.termination_criteria);
             if (S->reason != TERMINATION_REASON_UNSPECIFIED) break;

@@ -229,6 +229,9 @@ class Problem:
     primal_start: Optional[np.ndarray] = None
     dual_start: Optional[np.ndarray] = None
     R_dense: Optional[np.ndarray] = None  # optional dense R (k x n), passed as matrix_dense
+    F: Optional[CsrMatrix] = None  # affine cone rows: F x + g in the affine cones
+    g: Optional[np.ndarray] = None
+    affine_cones: Sequence[Cone] = field(default_factory=list)  # blocks over the rows of F
 
     @property
     def n(self) -> int:
@@ -272,10 +275,19 @@ def build(lib: C.CDLL, p: Problem):
         cones[i].type, cones[i].start_idx, cones[i].v_dim = k.type, k.start, k.v_dim
         cones[i].power_alpha, cones[i].is_fixed = k.alpha, None
     keep.append(cones)
+    acones = (ConeSpec * max(1, len(p.affine_cones)))()
+    for i, k in enumerate(p.affine_cones):
+        acones[i].type, acones[i].start_idx, acones[i].v_dim = k.type, k.start, k.v_dim
+        acones[i].power_alpha, acones[i].is_fixed = k.alpha, None
+    keep.append(acones)
+    g = _f64(p.g) if p.g is not None else None
+    keep.append(g)
     Rd = _dense_desc(p.R_dense, keep) if p.R_dense is not None else _desc(p.R, keep)
     prob = lib.create_qp_problem(_ptr(c), _desc(p.Q, keep), Rd, _desc(p.D, keep), _desc(p.A, keep),
                                  _ptr(arrs[0]), _ptr(arrs[1]), _ptr(arrs[2]), _ptr(arrs[3]), C.byref(oc),
-                                 len(p.cones), cones if p.cones else None, None, None, 0, None)
+                                 len(p.cones), cones if p.cones else None, _desc(p.F, keep),
+                                 _ptr(g) if g is not None else None, len(p.affine_cones),
+                                 acones if p.affine_cones else None)
     if prob and (p.primal_start is not None or p.dual_start is not None):
         ps, ds = _f64(p.primal_start), _f64(p.dual_start)
         keep += [ps, ds]

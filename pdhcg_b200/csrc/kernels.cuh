@@ -68,6 +68,16 @@ struct StepData {
     LongRows A_long, At_long; // long rows of A (pass over x_refl) and of A^T (pass over y)
     double *psd_work;         // PSD blocks' projection scratch (NULL: no PSD blocks)
     const long long *psd_off; // per cone block: offset of its scratch in psd_work
+    // affine cones F x + g in K over blocks of rows: the rows outside them as
+    // tiles of <= 32 consecutive rows {first, count} (NULL: all rows in tiles
+    // of 32), and the blocks themselves (projected with d = 1 / cr)
+    const int2 *row_tiles;
+    int n_row_tiles;
+    const int *aff_start, *aff_len, *aff_type;
+    const double *aff_alpha;
+    const long long *aff_psd_off; // PSD scratch offsets of the affine blocks
+    int n_aff;
+    const double *cr; // constraint rescaling
 };
 
 // The step kernels are written as warp bodies (one tile or one cone block per
@@ -268,10 +278,91 @@ __global__ void __launch_bounds__(TPB) dual_kernel(StepData<T> D, StepParams P)
     __shared__ double stage_all[WARPS][STREAM_CHUNK];
     const int lane = threadIdx.x & 31;
     double *stage = stage_all[threadIdx.x >> 5];
-    const int ntiles = (D.m + 31) / 32;
+    const int ntiles = D.row_tiles ? D.n_row_tiles : (D.m + 31) / 32;
     for (int t = blockIdx.x * WARPS + (threadIdx.x >> 5); t < ntiles; t += gridDim.x * WARPS) {
-        const int r0 = 32 * t;
-        dual_tile<T, EQ_ROWS, HAS_G>(D, P, r0, min(32, D.m - r0), lane, stage);
+        if (D.row_tiles) {
+            const int2 rt = D.row_tiles[t];
+            dual_tile<T, EQ_ROWS, HAS_G>(D, P, rt.x, rt.y, lane, stage);
+        } else {
+            const int r0 = 32 * t;
+            dual_tile<T, EQ_ROWS, HAS_G>(D, P, r0, min(32, D.m - r0), lane, stage);
+        }
+    }
+}
+
+// One affine cone block of rows (reference pdhg_update with affine cones,
+// src/pdhg_core_op.cu:810-829): A x_refl + g over the block's rows, the
+// clamped point v - y / sigma projected onto the cone (unit metric of the
+// scaled space, K on v / d with d = 1 / cr), then the dual update,
+// reflection and Halpern average of the other rows.
+template <int S, typename T>
+__device__ __forceinline__ void dual_cone_block(const StepData<T> &D, const StepParams &P, int ab, int lane,
+                                                double *stage)
+{
+    const int st = D.aff_start[ab], L = D.aff_len[ab], type = D.aff_type[ab];
+    WarpSlots<S> sl;
+    double yi[S], y0[S], gv[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int i = lane + 32 * s;
+        sl.x[s] = 0.0;
+        sl.d[s] = 1.0;
+        sl.w[s] = 1.0;
+        yi[s] = y0[s] = gv[s] = 0.0;
+        if (i < L) {
+            const int j = st + i;
+            yi[s] = D.y[j];
+            y0[s] = D.y0[j];
+            gv[s] = D.g ? (double)D.g[j] : 0.0;
+            sl.d[s] = 1.0 / D.cr[j];
+        }
+    }
+    double axr[S];
+    warp_stream_rows<S>(D.A_rp, D.A_ci, D.A_v, D.xr, st, L, lane, stage, axr, D.A_long);
+    double vv[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int i = lane + 32 * s;
+        vv[s] = axr[s] + gv[s];
+        if (i < L) {
+            const int j = st + i;
+            sl.x[s] = clampd(D.lc[j], vv[s] - yi[s] / P.sigma, D.uc[j]);
+        }
+    }
+    const bool uni = warp_uniform_unit<S>(sl, L, lane);
+    warp_project<S>(type, sl, L, lane, uni, nullptr, D.aff_alpha ? D.aff_alpha[ab] : 0.0,
+                    D.psd_work ? D.psd_work + D.aff_psd_off[ab] : nullptr);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int i = lane + 32 * s;
+        if (i < L) {
+            const int j = st + i;
+            const double yn = yi[s] - P.sigma * vv[s] + P.sigma * sl.x[s];
+            if (P.store_dual)
+                D.yp[j] = (T)yn;
+            const double yr = 2.0 * yn - yi[s];
+            if (P.want_fpe)
+                D.dy[j] = (T)(yr - yi[s]);
+            const double refl = P.rho * yr + (1.0 - P.rho) * yi[s];
+            D.y[j] = (T)(P.w * refl + (1.0 - P.w) * y0[s]);
+        }
+    }
+}
+
+// One warp per affine cone block; 3-slot blocks (exponential, power) take
+// the one-slot instantiation, which alone carries their projection.
+template <int S, typename T>
+__global__ void __launch_bounds__(TPB) dual_cone_kernel(StepData<T> D, StepParams P)
+{
+    __shared__ double stage_all[WARPS][STREAM_CHUNK];
+    const int lane = threadIdx.x & 31;
+    double *stage = stage_all[threadIdx.x >> 5];
+    for (int ab = blockIdx.x * WARPS + (threadIdx.x >> 5); ab < D.n_aff; ab += gridDim.x * WARPS) {
+        const int t = D.aff_type[ab];
+        if (S > 1 && (t == 2 || t == 3))
+            dual_cone_block<1, T>(D, P, ab, lane, stage);
+        else
+            dual_cone_block<S, T>(D, P, ab, lane, stage);
     }
 }
 

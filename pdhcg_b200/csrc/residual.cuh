@@ -27,6 +27,8 @@ enum ResidualScalar {
     RS_DIST_Y,         // |y_pdhg - y_init|^2
     RS_POW_ABS,        // power-cone primal violation (max, or sum of squares)
     RS_POW_REL,        // the same relative to the point's size
+    RS_AFF_MEM,        // affine rows: dual membership proj_K(-y) / cr (max, or sum of squares)
+    RS_AFF_COMPL,      // affine blocks: |y . (A x + g)| / sb (max, or sum of squares)
     RS_COUNT
 };
 
@@ -65,6 +67,13 @@ struct ResidualData {
     LongRows A_long, At_long; // passes over x_pdhg and y_pdhg
     double *psd_work;         // PSD blocks' projection scratch (NULL: none)
     const long long *psd_off;
+    // affine cone blocks of rows and the rows outside them (tiles; NULL: all)
+    const int2 *row_tiles;
+    int n_row_tiles;
+    const int *aff_start, *aff_len, *aff_type;
+    const double *aff_alpha;
+    const long long *aff_psd_off;
+    int n_aff, aff_blocks;
 };
 
 __device__ __forceinline__ double norm_term(double v, int l2) { return l2 ? v * v : abs_or_inf(v); }
@@ -189,12 +198,72 @@ __device__ __forceinline__ void residual_cone_block(const ResidualData<VT> &D, c
     }
 }
 
+// One affine cone block of rows (reference compute_residual with affine
+// cones, src/pdhg_core_op.cu:1037-1294, and compute_affine_cone_residuals,
+// :109-212): v = A x + g; the primal residual is v - proj_K(v) scaled by
+// cr; the dual membership proj_K(-y) / cr (zero when y is in the dual
+// cone); the complementarity |y . v| / sb; the bound terms of the dual
+// objective as for other rows.  Projections as in the dual step (d = 1 / cr).
+template <int S, typename VT>
+__device__ __forceinline__ void residual_affine_block(const ResidualData<VT> &D, const ResidualParams &P, int ab,
+                                                      int lane, double *stage, double (&acc)[RS_COUNT],
+                                                      const int (&ops)[RS_COUNT])
+{
+    auto fold = [&](int s, double v) { acc[s] = ops[s] == RMAX ? fmax(acc[s], v) : acc[s] + v; };
+    const int st = D.aff_start[ab], L = D.aff_len[ab], type = D.aff_type[ab];
+    const double alpha = D.aff_alpha ? D.aff_alpha[ab] : 0.0;
+    double *psd = D.psd_work ? D.psd_work + D.aff_psd_off[ab] : nullptr;
+    double axr[S];
+    warp_stream_rows<S>(D.A_rp, D.A_ci, D.A_v, D.xp, st, L, lane, stage, axr, D.A_long);
+    WarpSlots<S> pv, mv;
+    double vv[S], yv[S];
+    double ydv = 0.0;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int i = lane + 32 * s;
+        pv.x[s] = mv.x[s] = 0.0;
+        pv.d[s] = mv.d[s] = 1.0;
+        pv.w[s] = mv.w[s] = 1.0;
+        vv[s] = yv[s] = 0.0;
+        if (i < L) {
+            const int j = st + i;
+            vv[s] = axr[s] + D.g[j];
+            yv[s] = D.yp[j];
+            pv.x[s] = clampd(D.lc[j], vv[s], D.uc[j]);
+            mv.x[s] = -yv[s];
+            pv.d[s] = mv.d[s] = 1.0 / D.cr[j];
+            ydv += yv[s] * vv[s];
+            const double lcf = isfinite(D.lc[j]) ? D.lc[j] : 0.0, ucf = isfinite(D.uc[j]) ? D.uc[j] : 0.0;
+            fold(RS_PRIMAL_SLACK, fmax(yv[s], 0.0) * lcf + fmin(yv[s], 0.0) * ucf - D.g[j] * yv[s]);
+            if (P.want_dist) {
+                const double d = yv[s] - D.y0[j];
+                fold(RS_DIST_Y, d * d);
+            }
+        }
+    }
+    const bool uni = warp_uniform_unit<S>(pv, L, lane);
+    warp_project<S>(type, pv, L, lane, uni, nullptr, alpha, psd);
+    warp_project<S>(type, mv, L, lane, uni, nullptr, alpha, psd);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int i = lane + 32 * s;
+        if (i < L) {
+            const int j = st + i;
+            fold(RS_PRIMAL_RES, norm_term((vv[s] - pv.x[s]) * D.cr[j], P.l2));
+            fold(RS_AFF_MEM, norm_term(mv.x[s] / D.cr[j], P.l2));
+        }
+    }
+    ydv = warp_sum(ydv);
+    if (lane == 0)
+        fold(RS_AFF_COMPL, norm_term(fabs(ydv) / P.sb, P.l2));
+}
+
 template <int S, typename VT>
 __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, ResidualParams P)
 {
     __shared__ double stage_all[WARPS][STREAM_CHUNK];
     const int NOP = P.l2 ? RSUM : RMAX;
-    const int ops[RS_COUNT] = {NOP, RSUM, NOP, RSUM, RSUM, RSUM, NOP, NOP, RSUM, RSUM, NOP, NOP};
+    const int ops[RS_COUNT] = {NOP, RSUM, NOP, RSUM, RSUM, RSUM, NOP, NOP, RSUM, RSUM, NOP, NOP, NOP, NOP};
     double acc[RS_COUNT];
 #pragma unroll
     for (int s = 0; s < RS_COUNT; ++s)
@@ -206,9 +275,17 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
     int b = blockIdx.x;
     if (b < D.rows_blocks) {
         // constraint rows, one warp per tile of 32
-        const int ntiles = (D.m + 31) / 32;
+        const int ntiles = D.row_tiles ? D.n_row_tiles : (D.m + 31) / 32;
         for (int tile = b * WARPS + wib; tile < ntiles; tile += D.rows_blocks * WARPS) {
-            const int r0 = 32 * tile, nr = min(32, D.m - r0);
+            int r0, nr;
+            if (D.row_tiles) {
+                const int2 rt = D.row_tiles[tile];
+                r0 = rt.x;
+                nr = rt.y;
+            } else {
+                r0 = 32 * tile;
+                nr = min(32, D.m - r0);
+            }
             double axr[1];
             warp_stream_rows<1>(D.A_rp, D.A_ci, D.A_v, D.xp, r0, nr, lane, stage, axr, D.A_long);
             if (lane < nr) {
@@ -278,7 +355,7 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
                 }
             }
         }
-    } else {
+    } else if (b < D.rows_blocks + D.free_blocks + D.cone_blocks) {
         b -= D.rows_blocks + D.free_blocks;
         const int nwarps = D.cone_blocks * WARPS;
         for (int cb = b * WARPS + wib; cb < D.n_cones; cb += nwarps) {
@@ -289,6 +366,16 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
                 residual_cone_block<1, VT>(D, P, cb, lane, stage, acc, ops);
             else
                 residual_cone_block<S, VT>(D, P, cb, lane, stage, acc, ops);
+        }
+    } else {
+        b -= D.rows_blocks + D.free_blocks + D.cone_blocks;
+        const int nwarps = D.aff_blocks * WARPS;
+        for (int ab = b * WARPS + wib; ab < D.n_aff; ab += nwarps) {
+            const int at = D.aff_type[ab];
+            if (S > 1 && (at == 2 || at == 3))
+                residual_affine_block<1, VT>(D, P, ab, lane, stage, acc, ops);
+            else
+                residual_affine_block<S, VT>(D, P, ab, lane, stage, acc, ops);
         }
     }
     block_reduce_store<RS_COUNT>(acc, ops, D.partials);

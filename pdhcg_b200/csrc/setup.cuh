@@ -204,7 +204,9 @@ __global__ void cone_scaling_adjust_kernel(double *s, int ncones, const int *sta
 // Diagonal-congruence projection of the log scaling of a PSD block, used
 // when cone-preserving scaling is off (reference project_psd_log_scaling,
 // src/preconditioner.c:46-92); one thread per block, order <= 64.
-__global__ void psd_scaling_kernel(double *s, int ncones, const int *start, const int *vdim, const int *type)
+// log_space: s already holds log scales (Curtis-Reid) and receives log scales
+__global__ void psd_scaling_kernel(double *s, int ncones, const int *start, const int *vdim, const int *type,
+                                   int log_space)
 {
     const double LIM = 69.07755278982137;
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < ncones; b += gridDim.x * blockDim.x) {
@@ -219,7 +221,7 @@ __global__ void psd_scaling_kernel(double *s, int ncones, const int *start, cons
         int slot = st;
         for (int col = 0; col < order; ++col)
             for (int row = col; row < order; ++row, ++slot) {
-                double v = log(fmax(s[slot], 1e-300));
+                double v = log_space ? s[slot] : log(fmax(s[slot], 1e-300));
                 if (isnan(v))
                     v = 0.0;
                 else if (v > LIM)
@@ -244,7 +246,7 @@ __global__ void psd_scaling_kernel(double *s, int ncones, const int *start, cons
         slot = st;
         for (int col = 0; col < order; ++col)
             for (int row = col; row < order; ++row, ++slot)
-                s[slot] = exp(f[row] + f[col]);
+                s[slot] = log_space ? f[row] + f[col] : exp(f[row] + f[col]);
     }
 }
 

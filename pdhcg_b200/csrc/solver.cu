@@ -360,7 +360,18 @@ struct DeviceProblem {
     int *cst = nullptr, *clen = nullptr, *ctype = nullptr, *cvdim = nullptr, *free_d = nullptr;
     double *calpha = nullptr; // power-cone exponents per cone block
     ConeSplit split;            // cone blocks by launch (wide / 3-slot / PSD)
-    bool has_psd = false;
+    bool has_psd = false;       // PSD blocks among the variable or affine cones (scratch needed)
+    bool var_psd = false;       // PSD blocks among the variable cones
+    // affine cones over blocks of rows (F x + g in K): blocks, their PSD
+    // scratch offsets, and the rows outside them as tiles
+    std::vector<int> aff_start, aff_len, aff_type, aff_vdim;
+    std::vector<double> aff_alpha;
+    std::vector<long long> aff_psd_off;
+    int *ast = nullptr, *alen = nullptr, *atype = nullptr, *avdim = nullptr;
+    double *aalpha = nullptr;
+    long long *apsd_off_d = nullptr;
+    int2 *row_tiles_d = nullptr;
+    int n_row_tiles = 0, S_aff = 1;
     std::vector<long long> psd_off; // per cone block: offset of its PSD scratch (2 n^2 doubles)
     long long psd_total = 0;
     long long *psd_off_d = nullptr;
@@ -511,6 +522,7 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
             if (order > PSD_MAX_ORDER)
                 d.unsupported = "PSD blocks of order above 22 are not supported yet";
             d.has_psd = true;
+            d.var_psd = true;
             d.psd_total += 2LL * order * order;
         }
         d.cone_alpha.push_back(p->cones.power_alpha ? p->cones.power_alpha[b] : 0.0);
@@ -544,12 +556,57 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
             CK(cudaStreamSynchronize(s)); // ft goes out of scope
         }
     }
+    // affine cones (reference initialize_affine_cones, src/pdhcg.c:332-370:
+    // block starts already count the scalar rows before F)
+    const int na = d.dummy ? 0 : p->affine_cones.num_cones;
+    if (na > 0) {
+        std::vector<char> in_aff(d.m, 0);
+        int amax = 0;
+        for (int b = 0; b < na; ++b) {
+            const int t = (int)p->affine_cones.type[b], vd = p->affine_cones.v_dim[b];
+            const int st = p->affine_cones.start_idx[b], len = pdhcg_b200_cone_length(p->affine_cones.type[b], vd);
+            d.aff_start.push_back(st);
+            d.aff_len.push_back(len);
+            d.aff_type.push_back(t);
+            d.aff_vdim.push_back(vd);
+            d.aff_alpha.push_back(p->affine_cones.power_alpha ? p->affine_cones.power_alpha[b] : 0.0);
+            d.aff_psd_off.push_back(d.psd_total);
+            if (t == CONE_PSD) {
+                if (vd > PSD_MAX_ORDER)
+                    d.unsupported = "PSD blocks of order above 22 are not supported yet";
+                d.has_psd = true;
+                d.psd_total += 2LL * vd * vd;
+            }
+            amax = std::max(amax, len);
+            for (int i = st; i < st + len && i < d.m; ++i)
+                in_aff[i] = 1;
+        }
+        std::vector<int> free_rows;
+        for (int i = 0; i < d.m; ++i)
+            if (!in_aff[i])
+                free_rows.push_back(i);
+        std::vector<int2> rt = row_tiles(free_rows);
+        d.n_row_tiles = (int)rt.size();
+        if (rt.empty())
+            rt.push_back(make_int2(0, 0)); // a non-NULL list of no tiles
+        d.row_tiles_d = ar.upload(rt.data(), rt.size(), s);
+        d.S_aff = slots_class(amax);
+        if (d.S_aff < 0) {
+            d.unsupported = "cone blocks longer than 256 slots are not supported yet";
+            d.S_aff = 1;
+        }
+        d.ast = ar.upload(d.aff_start.data(), na, s);
+        d.alen = ar.upload(d.aff_len.data(), na, s);
+        d.atype = ar.upload(d.aff_type.data(), na, s);
+        d.avdim = ar.upload(d.aff_vdim.data(), na, s);
+        d.aalpha = ar.upload(d.aff_alpha.data(), na, s);
+        d.apsd_off_d = ar.upload(d.aff_psd_off.data(), na, s);
+        CK(cudaStreamSynchronize(s)); // host vectors go out of scope
+    }
     if (d.S < 0)
         d.unsupported = "cone blocks longer than 256 slots are not supported yet";
-    if (p->cones.is_fixed)
+    if (p->cones.is_fixed || p->affine_cones.is_fixed)
         d.unsupported = "fixed cone slots are not available on the device path yet";
-    if (p->affine_cones.num_cones > 0)
-        d.unsupported = "affine cones are not available on the device path yet";
     CK(cudaStreamSynchronize(s)); // host sources of the uploads may go away
     return dp;
 }
@@ -653,7 +710,7 @@ private:
     // infeasibility certificates of the last computation (zero until then)
     double p_ray_obj_ = 0.0, d_ray_obj_ = 0.0, max_p_ray_ = 0.0, max_d_ray_ = 0.0;
     void compute_infeasibility();
-    int res_rows_blocks_ = 0, res_free_blocks_ = 0, res_cone_blocks_ = 0;
+    int res_rows_blocks_ = 0, res_free_blocks_ = 0, res_cone_blocks_ = 0, res_aff_blocks_ = 0;
     int fpe_col_blocks_ = 0, fpe_row_blocks_ = 0;
 
     // scaling
@@ -840,7 +897,7 @@ void Solve::upload_and_preprocess()
 void Solve::rescale()
 {
     cudaStream_t s = st_;
-    int n = n_, m = m_, nc = (int)cone_start_.size();
+    int n = n_, m = m_, nc = (int)cone_start_.size(), na = (int)dp_.aff_start.size();
     cr_d_ = ar_.alloc<double>(m);
     vr_d_ = ar_.alloc<double>(n);
     double *fcr = ar_.alloc<double>(m), *fvr = ar_.alloc<double>(n);
@@ -877,21 +934,34 @@ void Solve::rescale()
             if (pres)
                 cone_scaling_adjust_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(fvr, nc, cst_d_, clen_d_, ruiz_phase);
             else
-                psd_scaling_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(fvr, nc, cst_d_, cvdim_d_, ctype_d_);
+                psd_scaling_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(fvr, nc, cst_d_, cvdim_d_, ctype_d_, 0);
+        }
+        if (na > 0) { // affine blocks: the same on the row factors
+            if (pres)
+                cone_scaling_adjust_kernel<<<grid_for(na, TPB), TPB, 0, s>>>(fcr, na, dp_.ast, dp_.alen, ruiz_phase);
+            else
+                psd_scaling_kernel<<<grid_for(na, TPB), TPB, 0, s>>>(fcr, na, dp_.ast, dp_.avdim, dp_.atype, 0);
         }
         apply_scaling();
     };
     if (prm_.curtis_reid_iterations > 0 && m > 0 && n > 0 && A_.nnz > 0) {
         // reference curtis_reid_rescaling, src/preconditioner.c:334-495
         double *rsum = ar_.alloc<double>(m), *csum = ar_.alloc<double>(n), *cs = ar_.alloc<double>(n);
+        double *rs = ar_.alloc<double>(m); // row numerators before the division by the row count
         CK(cudaMemsetAsync(fvr, 0, n * sizeof(double), s)); // column log-scales start at 0
         cr_logsum_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.v, m, rsum);
         cr_logsum_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.v, n, csum);
         for (int it = 0; it < prm_.curtis_reid_iterations; ++it) {
-            cr_average_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.ci, m, rsum, fvr, fcr, nullptr);
+            cr_average_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(A_.rp, A_.ci, m, rsum, fvr, fcr, rs);
+            if (na > 0 && pres) // affine blocks averaged together, as the columns of a cone block
+                cr_cone_average_kernel<<<grid_for(na, TPB), TPB, 0, s>>>(na, dp_.ast, dp_.alen, A_.rp, rs, fcr);
+            else if (na > 0)
+                psd_scaling_kernel<<<grid_for(na, TPB), TPB, 0, s>>>(fcr, na, dp_.ast, dp_.avdim, dp_.atype, 1);
             cr_average_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(At_.rp, At_.ci, n, csum, fcr, fvr, cs);
             if (nc > 0 && pres)
                 cr_cone_average_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(nc, cst_d_, clen_d_, At_.rp, cs, fvr);
+            else if (nc > 0)
+                psd_scaling_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(fvr, nc, cst_d_, cvdim_d_, ctype_d_, 1);
         }
         cr_exp_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(fcr, m);
         cr_exp_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(fvr, n);
@@ -959,14 +1029,14 @@ void Solve::init_state()
         scale_start_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(n, dp_.pstart, vr_d_, sb_, x0_);
     const double *ds = dp_.dstart;
     dual_start_kernel<<<grid_for(m, TPB), TPB, 0, s>>>(m, ds, cr_d_, sc_, y0_, y_, yp_);
+    if (dp_.has_psd) // variable and affine PSD blocks
+        psd_work_ = ar_.alloc<double>((size_t)dp_.psd_total);
     if (nc > 0) {
         cone_warm_ = ar_.alloc<double>(3 * (size_t)nc);
         warm_dual_ = cone_warm_ + nc;
         warm_aug_ = cone_warm_ + 2 * (size_t)nc;
         CK(cudaMemsetAsync(cone_warm_, 0, 3 * (size_t)nc * sizeof(double), s)); // 0 = no warm start
         cone_aux_init_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(nc, cst_d_, cvdim_d_, ctype_d_, vr_d_, sb_, x0_);
-        if (dp_.has_psd)
-            psd_work_ = ar_.alloc<double>((size_t)dp_.psd_total);
         dispatch_s(S_, [&](auto SC) {
             project_cones_kernel<SC.value><<<grid_for(nc, WARPS), TPB, 0, s>>>(
                 nc, cst_d_, clen_d_, ctype_d_, dp_.calpha, x0_, vr_d_, nullptr, 0.0, psd_work_, dp_.psd_off_d);
@@ -1094,7 +1164,7 @@ void Solve::setup_bb()
     bb_min_tol_ = mt;
     double init[2] = {it0, 1.0};
     CK(cudaMemcpyAsync(bb_tol_, init, sizeof(init), cudaMemcpyHostToDevice, s));
-    if (prm_.diag_jacobi_precond && !dp_.has_psd) { // the reference runs PSD models unpreconditioned
+    if (prm_.diag_jacobi_precond && !dp_.var_psd) { // the reference runs PSD models unpreconditioned
         bb_diag_h_ = ar_.alloc<double>(n);
         bb_m_ = ar_.alloc<double>(n);
         bb_minv_ = ar_.alloc<double>(n);
@@ -1201,6 +1271,15 @@ template <typename T>
 StepData<T> Solve::step_data()
 {
     StepData<T> D{};
+    D.row_tiles = dp_.aff_start.empty() ? nullptr : dp_.row_tiles_d; // rows outside the affine blocks
+    D.n_row_tiles = dp_.n_row_tiles;
+    D.aff_start = dp_.ast;
+    D.aff_len = dp_.alen;
+    D.aff_type = dp_.atype;
+    D.aff_alpha = dp_.aalpha;
+    D.aff_psd_off = dp_.apsd_off_d;
+    D.n_aff = (int)dp_.aff_start.size();
+    D.cr = cr_d_;
     D.A_long = A_.lr;
     D.At_long = At_.lr;
     D.cone_warm = cone_warm_;
@@ -1272,7 +1351,15 @@ void Solve::launch_dual(const StepData<T> &D, const StepParams &P)
 {
     cudaStream_t s = st_;
     long_pass(A_, D.A_v, D.xr);
-    int grid = grid_for(((long long)m_ + 31) / 32, WARPS);
+    if (D.n_aff > 0) { // affine cone blocks: one warp each
+        dispatch_s(dp_.S_aff, [&](auto SC) {
+            dual_cone_kernel<SC.value, T><<<grid_for(D.n_aff, WARPS), TPB, 0, s>>>(D, P);
+        });
+        stats_.kernel_launches++;
+        if (D.n_row_tiles == 0)
+            return;
+    }
+    int grid = grid_for(D.row_tiles ? (long long)D.n_row_tiles : ((long long)m_ + 31) / 32, WARPS);
     if (eq_rows_) {
         if (has_g_)
             dual_kernel<T, true, true><<<grid, TPB, 0, s>>>(D, P);
@@ -1525,6 +1612,15 @@ void Solve::enqueue_residual_t(bool want_dist)
     D.rows_blocks = res_rows_blocks_;
     D.free_blocks = res_free_blocks_;
     D.cone_blocks = res_cone_blocks_;
+    D.row_tiles = dp_.aff_start.empty() ? nullptr : dp_.row_tiles_d;
+    D.n_row_tiles = dp_.n_row_tiles;
+    D.aff_start = dp_.ast;
+    D.aff_len = dp_.alen;
+    D.aff_type = dp_.atype;
+    D.aff_alpha = dp_.aalpha;
+    D.aff_psd_off = dp_.apsd_off_d;
+    D.n_aff = (int)dp_.aff_start.size();
+    D.aff_blocks = res_aff_blocks_;
     D.A_long = A_.lr;
     D.At_long = At_.lr;
     long_pass(A_, A_.v, D.xp);
@@ -1547,8 +1643,8 @@ void Solve::enqueue_residual_t(bool want_dist)
         sa = 1.0;
     P.s_aug = sa;
     P.sb = sb_;
-    int nb = D.rows_blocks + D.free_blocks + D.cone_blocks;
-    dispatch_s(S_, [&](auto SC) { residual_kernel<SC.value, VT><<<nb, TPB, 0, s>>>(D, P); });
+    int nb = D.rows_blocks + D.free_blocks + D.cone_blocks + D.aff_blocks;
+    dispatch_s(std::max(S_, dp_.S_aff), [&](auto SC) { residual_kernel<SC.value, VT><<<nb, TPB, 0, s>>>(D, P); });
     fold_partials_kernel<<<1, TPB, 0, s>>>(partials_, nb, RS_COUNT, res_ops_d_, scal_d_);
     stats_.kernel_launches += 2;
     stats_.evaluations++;
@@ -1751,7 +1847,13 @@ void Solve::read_residual()
     auto join = [&](double a, double b) { return l2 ? std::hypot(a, b) : std::fmax(a, b); };
     if (cones)
         abs_p_ = join(abs_p_, pv_abs);
-    abs_d_ = nrm(r[RS_DUAL_RES]) / sc_;
+    // affine cones: dual membership and complementarity join the dual
+    // residual (reference compute_residual, src/pdhg_core_op.cu:1166-1190)
+    if (!dp_.aff_start.empty())
+        abs_d_ = (l2 ? std::sqrt(r[RS_DUAL_RES] + r[RS_AFF_MEM] + r[RS_AFF_COMPL])
+                     : std::fmax(r[RS_DUAL_RES], std::fmax(r[RS_AFF_MEM], r[RS_AFF_COMPL]))) / sc_;
+    else
+        abs_d_ = nrm(r[RS_DUAL_RES]) / sc_;
     double half_xqx = qtype_ == PDHCG_NON_Q ? 0.0 : 0.5 * r[RS_XQX];
     pobj_ = (r[RS_CX] + half_xqx) / (sb_ * sc_) + dp_.obj_const;
     dobj_ = (r[RS_SLACKX] + r[RS_PRIMAL_SLACK] - half_xqx) / (sb_ * sc_) + dp_.obj_const;
@@ -1787,7 +1889,7 @@ void Solve::loop()
             enqueue_residual(restart_check);
             read_residual();
             // reference src/solver.cu:127-131
-            if (cone_start_.empty() && is_major_ && k_ < 3 * freq)
+            if (cone_start_.empty() && dp_.aff_start.empty() && is_major_ && k_ < 3 * freq)
                 compute_infeasibility();
             cum_time_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             // check_termination_criteria (reference src/utils.cu:250-289)
@@ -1987,7 +2089,9 @@ pdhcg_result_t *Solve::run()
     stats_.upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host).count();
     // reduction scratch sized for the widest user
     // residual ranges: one warp per tile of 32 rows / per cone block
-    res_rows_blocks_ = grid_for(((long long)m_ + 31) / 32, WARPS, 148 * 8);
+    res_rows_blocks_ = grid_for(dp_.aff_start.empty() ? ((long long)m_ + 31) / 32 : (long long)dp_.n_row_tiles, WARPS,
+                                148 * 8);
+    res_aff_blocks_ = dp_.aff_start.empty() ? 0 : grid_for((long long)dp_.aff_start.size(), WARPS, 148 * 8);
     res_free_blocks_ = grid_for(cone_start_.empty() ? ((long long)n_ + 31) / 32 : (long long)dp_.n_free_tiles, WARPS,
                                 148 * 8);
     if (!cone_start_.empty() && free_idx_.empty())
@@ -1995,7 +2099,8 @@ pdhcg_result_t *Solve::run()
     res_cone_blocks_ = cone_start_.empty() ? 0 : grid_for((long long)cone_start_.size(), WARPS, 148 * 8);
     fpe_col_blocks_ = grid_for(((long long)n_ + 31) / 32, WARPS, 148 * 8);
     fpe_row_blocks_ = grid_for(m_, TPB, 148 * 4);
-    int maxb = std::max({res_rows_blocks_ + res_free_blocks_ + res_cone_blocks_, fpe_col_blocks_ + fpe_row_blocks_,
+    int maxb = std::max({res_rows_blocks_ + res_free_blocks_ + res_cone_blocks_ + res_aff_blocks_,
+                         fpe_col_blocks_ + fpe_row_blocks_,
                          res_rows_blocks_ + fpe_col_blocks_, 148 * 4});
     partials_ = ar_.alloc<double>((size_t)maxb * RS_COUNT);
     scal_d_ = ar_.alloc<double>(RS_COUNT + 2 * FP_COUNT);
@@ -2003,7 +2108,7 @@ pdhcg_result_t *Solve::run()
     h_scal_ = pinned_scalars();
     {
         int nop = prm_.optimality_norm == NORM_TYPE_L2 ? RSUM : RMAX;
-        int res_ops[RS_COUNT] = {nop, RSUM, nop, RSUM, RSUM, RSUM, nop, nop, RSUM, RSUM, nop, nop};
+        int res_ops[RS_COUNT] = {nop, RSUM, nop, RSUM, RSUM, RSUM, nop, nop, RSUM, RSUM, nop, nop, nop, nop};
         int fpe_ops[FP_COUNT] = {RSUM, RSUM, RSUM};
         int norm_ops[NS_COUNT] = {RSUM, RSUM, RMAX, RMAX};
         res_ops_d_ = ar_.upload(res_ops, RS_COUNT, st_);
@@ -2040,7 +2145,7 @@ pdhcg_result_t *Solve::run()
     CK(cudaStreamSynchronize(st_));
     // diagonal Q with PSD blocks takes the inner BB solve, as the reference
     // does (a nonuniform diagonal metric has no one-decomposition PSD prox)
-    bb_ = qtype_ != PDHCG_NON_Q && (qtype_ != PDHCG_DIAG_Q || dp_.has_psd);
+    bb_ = qtype_ != PDHCG_NON_Q && (qtype_ != PDHCG_DIAG_Q || dp_.var_psd);
     if (bb_)
         setup_bb();
     if (opt_.precision == PDHCG_B200_MIXED && !bb_) // the inner BB solve runs in FP64 only

@@ -238,6 +238,53 @@ def psd_lp(seed: int = 6, nfree: int = 40, orders=(2, 3, 4, 5, 3, 6), with_q: bo
     return p
 
 
+def affine_cone_qp(seed: int = 9, n: int = 80, m_scalar: int = 20,
+                   blocks=((1, 6), (0, 4), (2, 1), (3, 1), (4, 3), (1, 10)), with_q: bool = False) -> Problem:
+    """Box variables, m_scalar equality rows and affine cone rows F x + g in
+    K (blocks of (cone type, v_dim): SOC, RSOC, exponential, power with
+    alpha U(0.2, 0.8), PSD), F with 4 random entries per row; g puts F x0 + g
+    strictly inside each cone at a random x0 inside the box, so the problem
+    is feasible; the box keeps it bounded."""
+    rng = np.random.default_rng(seed)
+    x0 = rng.uniform(-0.5, 0.5, n)
+    A = random_csr(rng, m_scalar, n, 5)
+    b = A.to_scipy() @ x0
+    lens = [3 if t in (2, 3) else (k * (k + 1) // 2 if t == 4 else k + 2) for t, k in blocks]
+    F = random_csr(rng, sum(lens), n, 4)
+    u0, cones, st = [], [], 0
+    for (t, k), L in zip(blocks, lens):
+        if t == 1:  # [v, w, z], |(v, w)| < z
+            v = rng.standard_normal(L - 1)
+            u = np.concatenate([v, [np.linalg.norm(v) + 1.0]])
+        elif t == 0:  # [v, s, t], |v|^2 < 2 s t
+            v = rng.standard_normal(L - 2)
+            s_ = 1.0 + rng.random()
+            u = np.concatenate([v, [s_, (v @ v) / (2 * s_) + 1.0]])
+        elif t == 2:  # y exp(x / y) < z
+            xe, ye = rng.standard_normal(), 1.0 + rng.random()
+            u = np.array([xe, ye, ye * np.exp(xe / ye) + 1.0])
+        elif t == 3:  # x^a y^(1-a) > |z|
+            a = rng.uniform(0.2, 0.8)
+            xp_, yp_ = 1.0 + rng.random(), 1.0 + rng.random()
+            u = np.array([xp_, yp_, 0.5 * xp_ ** a * yp_ ** (1 - a)])
+        else:  # svec of a positive definite matrix
+            B = rng.standard_normal((k, k))
+            u = _svec(B @ B.T + np.eye(k))
+        cones.append(Cone(t, st, k, rng.uniform(0.2, 0.8) if t == 3 else 0.0))
+        if t == 3:  # rebuild the point for the drawn exponent
+            a = cones[-1].alpha
+            u = np.array([u[0], u[1], 0.5 * u[0] ** a * u[1] ** (1 - a)])
+        u0.append(u)
+        st += L
+    g = np.concatenate(u0) - F.to_scipy() @ x0
+    p = Problem(c=rng.standard_normal(n), A=A, con_lb=b, con_ub=b.copy(), var_lb=np.full(n, -1.0),
+                var_ub=np.full(n, 1.0), F=F, g=g, affine_cones=cones)
+    if with_q:
+        p.Q = CsrMatrix(n, n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32),
+                        rng.uniform(0.1, 1.0, n))
+    return p
+
+
 def portfolio(seed: int = 3, scale: float = 1.0, rank: int = 100, sectors: int = 500) -> Problem:
     """Low-rank portfolio QP with a rotated-SOC tracking-error block.
 

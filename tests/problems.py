@@ -147,7 +147,71 @@ def diagonal_q_psd():
     return p, dict(_PSD_PRM), {"xi": [(2, 4.0)], "tol": 5e-4, "res": 3e-6}
 
 
+_AFF_PRM = {"termination_evaluation_frequency": 10, "termination_criteria.eps_optimal_relative": 1e-7,
+            "termination_criteria.eps_feasible_relative": 1e-7, "termination_criteria.iteration_limit": 1000000,
+            "termination_criteria.time_sec_limit": 30.0}
+
+
+def _affine_one_variable(c, q, F_rows, g, cone, norm, preserving):
+    """One variable x, F x + g in one affine cone (test/test_affine_cones.c:
+    make_one_variable_problem / make_one_variable_quadratic_problem)."""
+    m = len(F_rows)
+    rp = np.cumsum([0] + [len(r) for r in F_rows])
+    F = CsrMatrix(m, 1, rp, np.zeros(int(rp[-1]), np.int32), np.array([v for r in F_rows for v in r], float))
+    Q = CsrMatrix(1, 1, np.array([0, 1]), np.array([0]), np.array([q])) if q else \
+        CsrMatrix(1, 1, np.array([0, 0]), np.zeros(0, np.int32), np.zeros(0))
+    p = Problem(c=np.array([c]), Q=Q, F=F, g=np.array(g, float), affine_cones=[cone])
+    prm = dict(_AFF_PRM, optimality_norm=norm, use_cone_preserving_scaling=preserving)
+    return p, prm
+
+
+def affine_soc():
+    """test/test_affine_cones.c:113-137: min x^2/2 - 2x s.t. (10x, 0, x + 9) in
+    the SOC, i.e. 10 |x| <= x + 9.  Expected x = 1 (tol 2e-4), relative
+    residuals below 2e-6 (L-inf norm, no cone-preserving scaling)."""
+    p, prm = _affine_one_variable(-2.0, 1.0, [[10.0], [], [1.0]], [0.0, 0.0, 9.0], Cone(CONE_STANDARD_SOC, 0, 1),
+                                  1, False)
+    return p, prm, {"x": [1.0], "tol": 2e-4, "res": 2e-6}
+
+
+def affine_rsoc():
+    """test/test_affine_cones.c:191-215: max x s.t. (x, 1, 1) in the rotated
+    SOC (x^2 <= 2).  Expected x = sqrt 2 (L2 norm)."""
+    p, prm = _affine_one_variable(-1.0, 0.0, [[1.0], [], []], [0.0, 1.0, 1.0], Cone(CONE_ROTATED_SOC, 0, 1), 0, True)
+    return p, prm, {"x": [np.sqrt(2.0)], "tol": 2e-4, "res": 2e-6}
+
+
+def affine_exp():
+    """test/test_affine_cones.c:139-163: max x s.t. (x, 1, 2) in K_exp
+    (exp(x) <= 2).  Expected x = log 2 (L-inf norm)."""
+    p, prm = _affine_one_variable(-1.0, 0.0, [[1.0], [], []], [0.0, 1.0, 2.0], Cone(CONE_EXPONENTIAL, 0, 1), 1, True)
+    return p, prm, {"x": [np.log(2.0)], "tol": 2e-4, "res": 2e-6}
+
+
+def affine_pow():
+    """test/test_affine_cones.c:165-189: max x s.t. (1, 1, x) in K_0.3
+    (|x| <= 1).  Expected x = 1 (L2 norm)."""
+    p, prm = _affine_one_variable(-1.0, 0.0, [[], [], [1.0]], [1.0, 1.0, 0.0], Cone(CONE_POWER, 0, 1, alpha=0.3),
+                                  0, True)
+    return p, prm, {"x": [1.0], "tol": 2e-4, "res": 2e-6}
+
+
+def affine_psd():
+    """test/test_psd_cones.c:70-118: min x s.t. svec [[x, 1], [1, 1]] =
+    (x, sqrt 2, 1) in PSD (x >= 1).  Expected x = 1 (tol 3e-4), relative
+    residuals below 2e-6."""
+    r2 = np.sqrt(2.0)
+    F = CsrMatrix(3, 1, np.array([0, 1, 1, 1]), np.array([0]), np.array([1.0]))
+    p = Problem(c=np.array([1.0]), F=F, g=np.array([0.0, r2, 1.0]), affine_cones=[Cone(CONE_PSD, 0, 2)])
+    return p, dict(_PSD_PRM), {"x": [1.0], "tol": 3e-4, "res": 2e-6}
+
+
 KNOWN_ANSWERS = {
+    "affine_soc": affine_soc,
+    "affine_rsoc": affine_rsoc,
+    "affine_exp": affine_exp,
+    "affine_pow": affine_pow,
+    "affine_psd": affine_psd,
     "variable_psd": variable_psd,
     "diagonal_q_psd": diagonal_q_psd,
     "exp_cone_linear": exp_cone_linear,

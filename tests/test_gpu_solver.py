@@ -97,6 +97,12 @@ CASES = {
     "psd_lp_mixed_cones": (lambda: instances.psd_lp(seed=7, orders=(2, 4, 1, 3)), {"use_cone_preserving_scaling": False}),
     "psd_qp": (lambda: instances.psd_lp(seed=8, with_q=True), {}),
     "all_cones_sparse_q": (_all_cones_sparse_q, {}),
+    # affine cones F x + g in K over rows: every cone type, with and without Q
+    "affine_lp": (lambda: instances.affine_cone_qp(), {}),
+    "affine_qp": (lambda: instances.affine_cone_qp(seed=10, with_q=True), {}),
+    "affine_lp_l2_np": (lambda: instances.affine_cone_qp(seed=13), {"optimality_norm": capi.NORM_L2,
+                                                                     "use_cone_preserving_scaling": False}),
+    "affine_lp_curtis_reid": (lambda: instances.affine_cone_qp(seed=14), {"curtis_reid_iterations": 5}),
 }
 
 
@@ -137,7 +143,7 @@ def _solve_gpu_opts(lib, p, params, **opts):
     return d, native.last_stats()
 
 
-@pytest.mark.parametrize("name", ["diag_qp", "conic_qp", "soc_qp_small", "box_lp", "dense_rows_qp"])
+@pytest.mark.parametrize("name", ["diag_qp", "conic_qp", "soc_qp_small", "box_lp", "dense_rows_qp", "affine_qp"])
 def test_mixed_precision_reaches_fp64_answer(lib, name):
     """FP32 bulk phase + FP64 polish: same status as plain FP64, objective
     within the termination tolerance of the FP64 answer, and the FP32 phase
