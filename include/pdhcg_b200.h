@@ -173,6 +173,15 @@ int pdhcg_b200_mlp_loss_grad(pdhcg_b200_mlp_t *net, int batch, const float *thet
 int pdhcg_b200_mlp_train(pdhcg_b200_mlp_t *net, int count, const float *theta, const float *target,
                          const float *target_logw, int epochs, int batch, float lr, double *loss);
 
+/* ---- problem files -----------------------------------------------------
+ * MPS / QPS reader, plain or gzip (name ending in .gz): the reference's
+ * read_mps_file (include/mps_parser.h:27, src/mps_parser.c:420-682) with the
+ * same conventions (sections ROWS, COLUMNS, RHS, RANGES, BOUNDS, OBJSENSE,
+ * QUADOBJ, QMATRIX, QCMATRIX; variables default to [0, inf); OBJSENSE MAX
+ * negates the objective).  NULL when the file cannot be read or parsed;
+ * release with qp_problem_free. */
+qp_problem_t *read_mps_file(const char *filename);
+
 /* ---- kernel-level entry points on device pointers ------------------------
  * For parity tests and embedding.  Pointers are device memory of the current
  * device; stream may be NULL (legacy default stream).  They return after

@@ -158,7 +158,41 @@ def bind_api(lib: C.CDLL) -> C.CDLL:
     lib.pdhcg_result_free.argtypes = [P(PdhcgResult)]
     lib.qp_problem_free.restype = None
     lib.qp_problem_free.argtypes = [P(QpProblem)]
+    if hasattr(lib, "read_mps_file"):
+        lib.read_mps_file.restype = P(QpProblem)
+        lib.read_mps_file.argtypes = [C.c_char_p]
     return lib
+
+
+def problem_arrays(prob) -> dict:
+    """Copy the arrays of a qp_problem_t (e.g. from read_mps_file) into numpy:
+    sizes, c, bounds, objective constant, A and Q as (row_ptr, col_ind, val)
+    and the quadratic constraints as (row, (row_ptr, col_ind, val))."""
+    p = prob.contents
+    n, m = p.num_variables, p.num_constraints
+
+    def vec(ptr, k):
+        return np.ctypeslib.as_array(ptr, shape=(k,)).copy() if (ptr and k > 0) else np.zeros(0)
+
+    def csr(M, rows, nnz):
+        if not M:
+            return None
+        M = M.contents
+        rp = np.ctypeslib.as_array(M.row_ptr, shape=(rows + 1,)).copy() if M.row_ptr else None
+        ci = np.ctypeslib.as_array(M.col_ind, shape=(nnz,)).copy() if (M.col_ind and nnz > 0) else np.zeros(0, int)
+        v = np.ctypeslib.as_array(M.val, shape=(nnz,)).copy() if (M.val and nnz > 0) else np.zeros(0)
+        return rp, ci, v
+
+    qcs = []
+    mats = C.cast(p.quadratic_constraint_matrices, C.POINTER(C.POINTER(CsrComponent)))
+    for k in range(p.num_quadratic_constraints):
+        nnz = p.quadratic_constraint_matrix_num_nonzeros[k]
+        qcs.append((p.quadratic_constraint_row_indices[k], csr(mats[k], n, nnz)))
+    return {"n": n, "m": m, "c": vec(p.objective_vector, n), "obj_const": p.objective_constant,
+            "var_lb": vec(p.variable_lower_bound, n), "var_ub": vec(p.variable_upper_bound, n),
+            "con_lb": vec(p.constraint_lower_bound, m), "con_ub": vec(p.constraint_upper_bound, m),
+            "A": csr(p.constraint_matrix, m, p.constraint_matrix_num_nonzeros),
+            "Q": csr(p.objective_sparse_matrix, n, p.objective_sparse_matrix_num_nonzeros), "qc": qcs}
 
 
 # ---- numpy-side problem description -----------------------------------

@@ -77,6 +77,7 @@ EXPORTS = [
     "pdhcg_b200_solve_batch", "pdhcg_b200_batch_autotune", "pdhcg_b200_last_batch_stats",
     "pdhcg_b200_mlp_create", "pdhcg_b200_mlp_free", "pdhcg_b200_mlp_num_params", "pdhcg_b200_mlp_get_params",
     "pdhcg_b200_mlp_set_params", "pdhcg_b200_mlp_predict", "pdhcg_b200_mlp_loss_grad", "pdhcg_b200_mlp_train",
+    "read_mps_file",
 ]
 
 
