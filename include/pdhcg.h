@@ -49,8 +49,11 @@ void set_start_values(qp_problem_t *prob, const double *primal, const double *du
  * Replaces reference set_cone_fixed (include/pdhcg.h:51, src/pdhcg.c:620-666). */
 int set_cone_fixed(qp_problem_t *prob, int cone_idx, int slot, double value);
 
-/* QCQP -> SOCP rewrite.  Problems without quadratic constraints are copied;
- * quadratic constraints are not handled by this library (returns NULL).
+/* QCQP -> SOCP rewrite: each quadratic constraint (diagonal Q_i, one-sided
+ * row) becomes a cone block of type default_type (standard or rotated SOC)
+ * with its auxiliary variables and rows; the same layout as the reference's.
+ * NULL without quadratic constraints, or with a non-diagonal / mixed-sign
+ * Q_i or a two-sided row.  solve_qp_problem applies it by itself.
  * Replaces reference qcqp_to_socp_qp (include/pdhcg.h:53, src/qcqp_transform.c:96). */
 qp_problem_t *qcqp_to_socp_qp(const qp_problem_t *orig_qcqp, cone_type_t default_type);
 

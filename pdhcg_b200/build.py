@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpdhcg_b200.so")
-SOURCES = ["solver.cu", "batch.cu", "mlp.cu", "api.cpp", "mps.cpp"]
+SOURCES = ["solver.cu", "batch.cu", "mlp.cu", "api.cpp", "mps.cpp", "qcqp.cpp"]
 HEADERS = ["device.cuh", "kernels.cuh", "residual.cuh", "setup.cuh", "bb.cuh", "internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -188,7 +188,12 @@ def problem_arrays(prob) -> dict:
     for k in range(p.num_quadratic_constraints):
         nnz = p.quadratic_constraint_matrix_num_nonzeros[k]
         qcs.append((p.quadratic_constraint_row_indices[k], csr(mats[k], n, nnz)))
-    return {"n": n, "m": m, "c": vec(p.objective_vector, n), "obj_const": p.objective_constant,
+    nc = p.cones.num_cones
+    cones = {"start": [p.cones.start_idx[i] for i in range(nc)], "v_dim": [p.cones.v_dim[i] for i in range(nc)],
+             "type": [p.cones.type[i] for i in range(nc)]}
+    fixed = bytes(C.string_at(p.cones.is_fixed, p.cones.fixed_mask_size)) if p.cones.is_fixed else b""
+    return {"n": n, "m": m, "cones": cones, "fixed": fixed, "primal_start": vec(p.primal_start, n),
+            "c": vec(p.objective_vector, n), "obj_const": p.objective_constant,
             "var_lb": vec(p.variable_lower_bound, n), "var_ub": vec(p.variable_upper_bound, n),
             "con_lb": vec(p.constraint_lower_bound, m), "con_ub": vec(p.constraint_upper_bound, m),
             "A": csr(p.constraint_matrix, m, p.constraint_matrix_num_nonzeros),

@@ -807,18 +807,6 @@ int set_cone_fixed(qp_problem_t *prob, int cone_idx, int slot, double value)
     return 0;
 }
 
-qp_problem_t *qcqp_to_socp_qp(const qp_problem_t *orig, cone_type_t default_type)
-{
-    (void)default_type;
-    if (!orig)
-        return nullptr;
-    if (orig->num_quadratic_constraints > 0) {
-        std::fprintf(stderr, "[qcqp_to_socp_qp] quadratic constraints are not supported by this library.\n");
-        return nullptr;
-    }
-    return pdhcg_b200_problem_clone(orig);
-}
-
 void set_default_parameters(pdhg_parameters_t *p)
 {
     std::memset(p, 0, sizeof(*p));

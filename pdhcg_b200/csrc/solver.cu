@@ -607,6 +607,8 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
         d.unsupported = "cone blocks longer than 256 slots are not supported yet";
     if (p->cones.is_fixed || p->affine_cones.is_fixed)
         d.unsupported = "fixed cone slots are not available on the device path yet";
+    if (p->num_quadratic_constraints > 0) // the solve entry points transform them first
+        d.unsupported = "quadratic constraints must be transformed with qcqp_to_socp_qp first";
     CK(cudaStreamSynchronize(s)); // host sources of the uploads may go away
     return dp;
 }
@@ -2366,6 +2368,20 @@ pdhcg_result_t *pdhcg_b200_solve(const qp_problem_t *prob, const pdhg_parameters
         opt = *opts;
     else
         pdhcg_b200_default_options(&opt);
+    if (prob->num_quadratic_constraints > 0) {
+        // quadratic constraints become cone blocks, as the reference's
+        // optimize does (src/solver.cu:43-66, 199), and the result is trimmed
+        // back to the original sizes
+        qp_problem_t *ext = qcqp_to_socp_qp(prob, prm.default_cone_type);
+        if (!ext) {
+            std::fprintf(stderr, "Error: QCQP -> SOCP transformation failed; cannot solve.\n");
+            return nullptr;
+        }
+        pdhcg_result_t *r = pdhcg_b200_solve(ext, &prm, &opt);
+        pdhcg_b200_restore_qcqp_result(r, prob);
+        qp_problem_free(ext);
+        return r;
+    }
     try {
         auto t0 = std::chrono::steady_clock::now();
         pdhcg_result_t *r = nullptr;

@@ -65,3 +65,34 @@ def test_same_answer_as_reference_build(lib, ref, name):
     ob = r["primal_objective_value"]
     tol = 1e-5 if name == "psd_qp" else 1e-8
     assert abs(g["primal_objective_value"] - ob) <= tol * (1 + abs(ob)), (g["primal_objective_value"], ob)
+
+
+@pytest.mark.parametrize("case,form", [(0, capi.CONE_ROTATED_SOC), (1, capi.CONE_STANDARD_SOC),
+                                       (2, capi.CONE_ROTATED_SOC)])
+def test_qcqp_solve_matches_reference_build(tmp_path, lib, ref, case, form):
+    """A QCQP read from an MPS file (each library's own reader), rewritten
+    into cone blocks of the given form and solved: the same status,
+    iteration count and objective as the reference's build, and a result of
+    the original sizes."""
+    import numpy as np
+    from test_qcqp import qcqp_mps
+    path = tmp_path / "qc.mps"
+    path.write_text(qcqp_mps(np.random.default_rng(300 + case), flips=case != 2))
+    out = []
+    for L in (lib, ref):
+        prob = L.read_mps_file(str(path).encode())
+        assert prob
+        n, m = prob.contents.num_variables, prob.contents.num_constraints
+        prm = capi.default_params(L, **{"termination_criteria.iteration_limit": 100000, "default_cone_type": form})
+        r = L.solve_qp_problem(prob, C.byref(prm))
+        assert r
+        rr = r.contents
+        out.append((capi.TERMINATION_REASONS[rr.termination_reason], rr.total_count, rr.primal_objective_value,
+                    rr.num_variables, rr.num_constraints, n, m))
+        L.pdhcg_result_free(r)
+        L.qp_problem_free(prob)
+    (gs, gk, go, gn, gm, n, m), (rs, rk, ro, _, _, _, _) = out
+    assert gs == rs == "OPTIMAL"
+    assert gk == rk, (gk, rk)
+    assert abs(go - ro) <= 1e-8 * (1 + abs(ro)), (go, ro)
+    assert (gn, gm) == (n, m)

@@ -201,6 +201,8 @@ def _same(a, b):
                 assert ra == rb
                 for x, y in zip(ma, mb):
                     np.testing.assert_array_equal(x, y)
+        elif isinstance(a[k], (dict, bytes)):
+            assert a[k] == b[k], k
         else:
             np.testing.assert_array_equal(a[k], b[k], err_msg=k)
 
