@@ -206,6 +206,30 @@ int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *co
                              const double *cone_alpha, double *x, const double *d, const double *q, double tau,
                              void *stream);
 
+/* Projection of cone blocks with fixed slots onto the sections through the
+ * fixed values (set_cone_fixed; reference section projectors,
+ * src/kernels/pdhcg_soc_cone_kernels.cu:23-260,
+ * src/kernels/pdhcg_rsoc_cone_kernels.cu:23-465,
+ * src/kernels/pdhcg_exp_cone_kernels.cu:134-525,
+ * src/kernels/pdhcg_power_cone_kernels.cu:135-434).  Arguments as for
+ * pdhcg_b200_project_cones, plus fixed: device mask over x (nonzero = the
+ * slot keeps its value) and warm: device array of num_cones multipliers
+ * carried from call to call (start at 0; may be NULL).  Every block is
+ * treated as a section block; PSD blocks are refused with -3 (they cannot
+ * be fixed).  Waits for the stream. */
+int pdhcg_b200_project_cone_sections(int num_cones, const int *cone_start, const int *cone_vdim,
+                                     const int *cone_type, const double *cone_alpha, const unsigned char *fixed,
+                                     double *x, const double *d, const double *q, double tau, double *warm,
+                                     void *stream);
+
+/* Checks the fixed slots of a problem's variable cones as solve_qp_problem
+ * does before solving (reference pdhcg_validate_fixed_cone_sections,
+ * src/pdhcg.c:729-892, internal/solver.h:29): the mask has num_variables
+ * entries, fixed values are finite, and each block's section through them is
+ * nonempty.  0 when valid (or nothing is fixed), -1 with a message on stderr
+ * otherwise.  Host only. */
+int pdhcg_b200_validate_fixed_sections(const qp_problem_t *prob);
+
 /* pdhcg_b200_project_cones for callers that must not allocate device memory
  * (no cudaMalloc / cudaMallocAsync / cudaFree, no allocating library): e.g.
  * code whose memory is budgeted up front, or that runs while another

@@ -172,6 +172,7 @@ typedef struct {
     int *astart, *avdim, *atype;
     double *aalpha; /* affine power-cone exponents */
     double *primal_start, *dual_start;
+    char *fixed; /* cones.is_fixed over the n variables, or NULL */
 } oprob;
 
 static void oprob_free(oprob *P)
@@ -181,6 +182,7 @@ static void oprob_free(oprob *P)
     free(P->cstart); free(P->cvdim); free(P->ctype); free(P->calpha);
     free(P->astart); free(P->avdim); free(P->atype); free(P->aalpha);
     free(P->primal_start); free(P->dual_start);
+    free(P->fixed);
 }
 
 /* deepcopy_problem + create_problem_with_dummy_constraint
@@ -244,6 +246,10 @@ static void oprob_load(oprob *P, const qp_problem_t *prob)
     }
     if (prob->primal_start)
         P->primal_start = dcopy(prob->primal_start, P->n);
+    if (prob->cones.is_fixed) {
+        P->fixed = (char *)xmalloc((size_t)(P->n > 0 ? P->n : 1));
+        memcpy(P->fixed, prob->cones.is_fixed, (size_t)P->n);
+    }
     if (dummy) {
         P->dual_start = dvec(1);
     } else if (prob->dual_start) {
@@ -493,8 +499,7 @@ static void bound_obj(oprob *P, double *sb, double *sc)
     }
 }
 
-/* rescale_problem, reference src/preconditioner.c:654-713 (fixed cone slots
- * are not supported by the oracle). */
+/* rescale_problem, reference src/preconditioner.c:654-713 */
 static void rescale(oprob *P, const pdhg_parameters_t *prm, double *cr, double *vr, double *sb, double *sc)
 {
     for (int i = 0; i < P->m; ++i) cr[i] = 1.0;
@@ -505,6 +510,14 @@ static void rescale(oprob *P, const pdhg_parameters_t *prm, double *cr, double *
     if (prm->has_pock_chambolle_alpha) pock_chambolle(P, prm->pock_chambolle_alpha, pres, cr, vr);
     if (prm->bound_objective_rescaling) bound_obj(P, sb, sc);
     else { *sb = 1.0; *sc = 1.0; }
+    /* pin_scaled_fixed_cone_bounds, reference src/preconditioner.c:311-327 */
+    if (P->fixed)
+        for (int j = 0; j < P->n; ++j) {
+            if (!P->fixed[j]) continue;
+            double v = (P->primal_start ? P->primal_start[j] : 0.0) * vr[j] * *sb;
+            P->l[j] = v;
+            P->u[j] = v;
+        }
 }
 
 int oracle_rescale(const qp_problem_t *prob, const pdhg_parameters_t *params, double *con_rescale,
@@ -639,6 +652,10 @@ typedef struct {
     int bb_limit;
     double *snap;
     double cum_time;
+    /* per cone block: warm starts of the section projectors (the step's
+     * projections and those of the residual, reference
+     * projection_warm_start / residual_warm_start), complementarity */
+    double *proj_warm, *res_warm, *compl;
 } ostate;
 
 static void project_affine(ostate *S, double *v);
@@ -702,13 +719,25 @@ static void update_obj_product(ostate *S, const double *x)
         for (int i = 0; i < n; ++i) S->eff[i] = S->P.c[i] + S->qx[i];
 }
 
-static void project_cones(ostate *S, double *vec, const double *q, double tau)
+/* project_cone_runtime (reference src/cone_dispatch.cu:38-58): blocks with
+ * fixed slots take the section projectors, with the warm starts in warm */
+static void project_cones_w(ostate *S, double *vec, const double *q, double tau, double *warm)
 {
     for (int b = 0; b < S->P.ncones; ++b) {
         int st = S->P.cstart[b];
-        oracle_project_cone_block(S->P.ctype[b], S->P.cvdim[b], S->P.calpha[b], vec + st, S->vr + st,
-                                  q ? q + st : NULL, tau);
+        int len = cone_len(S->P.ctype[b], S->P.cvdim[b]);
+        if (S->P.fixed && oracle_block_has_fixed(S->P.fixed + st, len))
+            oracle_section_project(S->P.ctype[b], S->P.cvdim[b], S->P.calpha[b], vec + st, S->vr + st,
+                                   q ? q + st : NULL, tau, S->P.fixed + st, warm + b);
+        else
+            oracle_project_cone_block(S->P.ctype[b], S->P.cvdim[b], S->P.calpha[b], vec + st, S->vr + st,
+                                      q ? q + st : NULL, tau);
     }
+}
+
+static void project_cones(ostate *S, double *vec, const double *q, double tau)
+{
+    project_cones_w(S, vec, q, tau, S->proj_warm);
 }
 
 static void cone_reflection(ostate *S)
@@ -901,14 +930,21 @@ static void fixed_point_error(ostate *S)
 
 /* cone dual residual + projected-gradient augmentation + cone dual slack,
  * reference src/cone_dispatch.cu:88-154 and src/pdhg_core_op.cu:67-90 */
+/* compute_cone_dual_residual, reference src/cone_dispatch.cu:86-108 */
 static void cone_dual_residual(ostate *S, const double *eff)
 {
     for (int b = 0; b < S->P.ncones; ++b) {
         int st = S->P.cstart[b], len = cone_len(S->P.ctype[b], S->P.cvdim[b]);
         double *rc = dvec(len);
         for (int i = 0; i < len; ++i) rc[i] = eff[st + i] - S->Aty[st + i];
-        oracle_cone_dual_residual_block(S->P.ctype[b], S->P.cvdim[b], S->P.calpha[b], rc, S->vr + st,
-                                        S->dual_residual + st);
+        S->compl[b] = 0.0;
+        if (S->P.fixed && oracle_block_has_fixed(S->P.fixed + st, len))
+            S->compl[b] = oracle_section_dual_residual(S->P.ctype[b], S->P.cvdim[b], S->P.calpha[b], S->xp + st, rc,
+                                                       S->vr + st, S->P.fixed + st, S->res_warm + b,
+                                                       S->dual_residual + st);
+        else
+            oracle_cone_dual_residual_block(S->P.ctype[b], S->P.cvdim[b], S->P.calpha[b], rc, S->vr + st,
+                                            S->dual_residual + st);
         free(rc);
     }
 }
@@ -922,7 +958,7 @@ static void augment_projected_gradient(ostate *S, const double *eff)
         double g = eff[i] - S->Aty[i];
         S->dx[i] = clampd(S->P.l[i], S->xp[i] - s * g, S->P.u[i]);
     }
-    project_cones(S, S->dx, NULL, 0.0);
+    project_cones_w(S, S->dx, NULL, 0.0, S->res_warm);
     for (int i = 0; i < n; ++i) {
         double r = (S->xp[i] - S->dx[i]) / s * S->vr[i];
         if (!isfinite(r)) r = copysign(INFINITY, r);
@@ -1037,11 +1073,14 @@ static void compute_residual(ostate *S, norm_type_t nt)
     }
     if (cones)
         S->abs_p = nt == NORM_TYPE_L_INF ? fmax(S->abs_p, pv_abs) : hypot(S->abs_p, pv_abs);
-    S->abs_d = vnorm(S->dual_residual, n, nt); /* complementarity residual is 0 without fixed sections */
+    /* cone complementarity (nonzero only on power blocks with fixed slots),
+     * reference compute_cone_complementarity_norm, src/pdhg_core_op.cu:92-100 */
+    double ccompl = cones ? vnorm(S->compl, S->P.ncones, nt) : 0.0;
+    S->abs_d = vnorm(S->dual_residual, n, nt);
     if (nt == NORM_TYPE_L_INF)
-        S->abs_d = fmax(S->abs_d, fmax(mem_norm, compl_norm));
+        S->abs_d = fmax(fmax(S->abs_d, ccompl), fmax(mem_norm, compl_norm));
     else
-        S->abs_d = sqrt(S->abs_d * S->abs_d + mem_norm * mem_norm + compl_norm * compl_norm);
+        S->abs_d = sqrt(S->abs_d * S->abs_d + ccompl * ccompl + mem_norm * mem_norm + compl_norm * compl_norm);
     S->abs_d /= S->sc;
     double half_xqx = S->qtype == PDHCG_NON_Q ? 0.0 : 0.5 * dot(S->xp, S->qx, n);
     S->pobj = (dot(S->P.c, S->xp, n) + half_xqx) / (S->sb * S->sc) + S->P.c0;
@@ -1253,7 +1292,7 @@ static void state_free(ostate *S)
     double *arrs[] = {S->cr, S->vr, S->lc_fin, S->uc_fin, S->l_fin, S->u_fin, S->qdiag, S->Ddiag, S->Ddense,
                       S->qx, S->Rx, S->Rxbuf, S->eff, S->x0, S->x, S->xp, S->xr, S->Aty, S->y0, S->y, S->yp,
                       S->yr, S->Ax, S->dual_slack, S->primal_slack, S->dual_residual, S->primal_residual, S->dx,
-                      S->dy, S->grad, S->dir, S->pbuf, S->diag_h, S->m_diag, S->m_inv, S->Ms, S->snap};
+                      S->dy, S->grad, S->dir, S->pbuf, S->diag_h, S->m_diag, S->m_inv, S->Ms, S->snap, S->proj_warm, S->res_warm, S->compl};
     for (size_t i = 0; i < sizeof(arrs) / sizeof(arrs[0]); ++i) free(arrs[i]);
 }
 
@@ -1266,8 +1305,8 @@ pdhcg_result_t *oracle_solve(const qp_problem_t *prob, const pdhg_parameters_t *
     if (params_in) prm = *params_in;
     else return NULL;
     if (!prob) return NULL;
-    if (prob->cones.is_fixed || prob->affine_cones.is_fixed || prob->num_quadratic_constraints > 0) {
-        fprintf(stderr, "[oracle] fixed cone slots and quadratic constraints are not restated\n");
+    if (prob->affine_cones.is_fixed || prob->num_quadratic_constraints > 0) {
+        fprintf(stderr, "[oracle] fixed affine slots and quadratic constraints are not restated\n");
         return NULL;
     }
     ostate Sv;
@@ -1339,18 +1378,26 @@ pdhcg_result_t *oracle_solve(const qp_problem_t *prob, const pdhg_parameters_t *
      * (src/solver_state.cu:578-686) */
     int cones = S->P.ncones > 0;
     if (cones && S->qtype != PDHCG_NON_Q) S->eff = dvec(n);
+    S->proj_warm = dvec(S->P.ncones);
+    S->res_warm = dvec(S->P.ncones);
+    S->compl = dvec(S->P.ncones);
     const double INV_SQRT2 = 0.7071067811865475;
     for (int b = 0; b < S->P.ncones; ++b) {
         int aux0 = S->P.cstart[b] + S->P.cvdim[b];
+        const char *fx = S->P.fixed;
         if (S->P.ctype[b] == CONE_STANDARD_SOC) {
             double wv = -INV_SQRT2 * S->sb * S->vr[aux0];
             double zv = INV_SQRT2 * S->sb * S->vr[aux0 + 1];
             double *d4[4] = {S->x0, S->x, S->xp, S->xr};
-            for (int w = 0; w < 4; ++w) { d4[w][aux0] = wv; d4[w][aux0 + 1] = zv; }
+            for (int w = 0; w < 4; ++w) {
+                if (!(fx && fx[aux0])) d4[w][aux0] = wv;
+                if (!(fx && fx[aux0 + 1])) d4[w][aux0 + 1] = zv;
+            }
         } else if (S->P.ctype[b] == CONE_ROTATED_SOC) {
             double tv = S->sb * S->vr[aux0 + 1];
             double *d4[4] = {S->x0, S->x, S->xp, S->xr};
-            for (int w = 0; w < 4; ++w) d4[w][aux0 + 1] = tv;
+            for (int w = 0; w < 4; ++w)
+                if (!(fx && fx[aux0 + 1])) d4[w][aux0 + 1] = tv;
         }
     }
     if (cones) project_cones(S, S->x0, NULL, 0.0);

@@ -57,6 +57,18 @@ void oracle_project_cone_block(int type, int v_dim, double power_alpha, double *
 void oracle_cone_dual_residual_block(int type, int v_dim, double power_alpha, const double *rc,
                                      const double *d, double *out);
 
+/* Blocks with slots fixed by set_cone_fixed (oracle_sections.c): the
+ * weighted projection onto the section through the fixed values (x, d,
+ * q, fx at the block's first slot; warm: the block's multiplier from the
+ * previous call, updated), and the section dual residual (reference
+ * src/kernels/pdhcg_*_cone_kernels.cu, fixed-section branches); the latter
+ * returns the block's complementarity residual. */
+int oracle_block_has_fixed(const char *fx, int len);
+void oracle_section_project(int type, int v_dim, double alpha, double *x, const double *d, const double *q,
+                            double tau, const char *fx, double *warm);
+double oracle_section_dual_residual(int type, int v_dim, double alpha, const double *xp, const double *rc,
+                                    const double *d, const char *fx, double *warm, double *out);
+
 /* One PDHG iteration from a given state, for kernel-level parity tests.
  * Inputs are already-scaled data; see oracle_step_t. */
 typedef struct {

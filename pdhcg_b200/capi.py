@@ -161,6 +161,9 @@ def bind_api(lib: C.CDLL) -> C.CDLL:
     if hasattr(lib, "read_mps_file"):
         lib.read_mps_file.restype = P(QpProblem)
         lib.read_mps_file.argtypes = [C.c_char_p]
+    if hasattr(lib, "pdhcg_b200_validate_fixed_sections"):
+        lib.pdhcg_b200_validate_fixed_sections.restype = C.c_int
+        lib.pdhcg_b200_validate_fixed_sections.argtypes = [P(QpProblem)]
     return lib
 
 
@@ -271,6 +274,7 @@ class Problem:
     F: Optional[CsrMatrix] = None  # affine cone rows: F x + g in the affine cones
     g: Optional[np.ndarray] = None
     affine_cones: Sequence[Cone] = field(default_factory=list)  # blocks over the rows of F
+    fixed: Sequence[tuple] = field(default_factory=list)  # (cone index, slot, value) for set_cone_fixed
 
     @property
     def n(self) -> int:
@@ -331,6 +335,10 @@ def build(lib: C.CDLL, p: Problem):
         ps, ds = _f64(p.primal_start), _f64(p.dual_start)
         keep += [ps, ds]
         lib.set_start_values(prob, _ptr(ps), _ptr(ds))
+    for cone, slot, value in (p.fixed if prob else []):
+        if lib.set_cone_fixed(prob, int(cone), int(slot), float(value)) != 0:
+            lib.qp_problem_free(prob)
+            return None, keep
     return prob, keep
 
 

@@ -6,6 +6,7 @@
 // (reference src/pdhcg.c:35-666, src/cone_utils.c:26-211,
 // src/utils.cu:324-368, 591-833).  The solve itself lives in solver.cu.
 
+#include <cfloat>
 #include <climits>
 #include <cstdint>
 #include <cmath>
@@ -804,6 +805,150 @@ int set_cone_fixed(qp_problem_t *prob, int cone_idx, int slot, double value)
     if (!prob->primal_start)
         prob->primal_start = (double *)xcalloc((size_t)prob->num_variables, sizeof(double));
     prob->primal_start[idx] = value;
+    return 0;
+}
+
+// Is the fixed exponential section {(x, y, z) : y e^{x/y} <= z} closure,
+// with the fixed coordinates at their values, nonempty?  (reference
+// fixed_exp_section_is_nonempty, src/pdhcg.c:682-727)
+static bool exp_section_nonempty(bool fx, bool fy, bool fz, double x, double y, double z)
+{
+    if ((fx && !std::isfinite(x)) || (fy && !std::isfinite(y)) || (fz && !std::isfinite(z)))
+        return false;
+    if (fy) {
+        if (y < 0.0)
+            return false;
+        if (y == 0.0) // only the closure's face {x <= 0, z >= 0}
+            return (!fx || x <= 0.0) && (!fz || z >= 0.0);
+        if (fz && !(z > 0.0))
+            return false;
+        if (fx && fz) {
+            const double lb = std::log(y) + x / y, lz = std::log(z);
+            return lb <= lz + 64.0 * DBL_EPSILON * (1.0 + std::fabs(lb) + std::fabs(lz));
+        }
+        return true;
+    }
+    if (!fz)
+        return true;
+    if (z < 0.0)
+        return false;
+    if (z == 0.0)
+        return !fx || x <= 0.0;
+    if (!fx || x <= 0.0)
+        return true;
+    // the smallest y e^{x/y} over y > 0 is e x for x > 0
+    const double lmin = 1.0 + std::log(x), lz = std::log(z);
+    return lmin <= lz + 64.0 * DBL_EPSILON * (1.0 + std::fabs(lmin) + std::fabs(lz));
+}
+
+// Checks the fixed slots of the variable cones: a mask of the problem's
+// size, finite values, and a nonempty section through them in every block
+// (reference pdhcg_validate_fixed_cone_sections, src/pdhcg.c:729-892, with
+// its messages).  0 when valid or without fixed slots, -1 otherwise.
+int pdhcg_b200_validate_fixed_sections(const qp_problem_t *prob)
+{
+    if (!prob || !prob->cones.is_fixed)
+        return 0;
+    if (prob->cones.fixed_mask_size != prob->num_variables) {
+        std::fprintf(stderr, "[solve_qp_problem] variable cone fixed mask has size %d; expected %d.\n",
+                     prob->cones.fixed_mask_size, prob->num_variables);
+        return -1;
+    }
+    const char *fx = prob->cones.is_fixed;
+    auto val = [&](int j) { return prob->primal_start ? prob->primal_start[j] : 0.0; };
+    for (int c = 0; c < prob->cones.num_cones; ++c) {
+        const int st = prob->cones.start_idx[c], vd = prob->cones.v_dim[c];
+        const int len = cone_block_length(&prob->cones, c);
+        bool any = false;
+        for (int i = 0; i < len; ++i)
+            any |= fx[st + i] != 0;
+        if (!any)
+            continue;
+        const cone_type_t t = prob->cones.type[c];
+        if (t == CONE_EXPONENTIAL) {
+            if (!exp_section_nonempty(fx[st], fx[st + 1], fx[st + 2], val(st), val(st + 1), val(st + 2))) {
+                std::fprintf(stderr,
+                             "[solve_qp_problem] exponential cone %d has an empty or non-finite fixed section.\n", c);
+                return -1;
+            }
+            continue;
+        }
+        if (t == CONE_STANDARD_SOC || t == CONE_ROTATED_SOC) {
+            const bool std_soc = t == CONE_STANDARD_SOC;
+            for (int i = 0; i < vd + 2; ++i)
+                if (fx[st + i] && !std::isfinite(val(st + i))) {
+                    std::fprintf(stderr, "[solve_qp_problem] %s SOC %d has a non-finite fixed value.\n",
+                                 std_soc ? "standard" : "rotated", c);
+                    return -1;
+                }
+            // norm of the fixed vector slots (v and, for the standard cone, w)
+            double fnorm = 0.0;
+            for (int i = 0; i < (std_soc ? vd + 1 : vd); ++i)
+                if (fx[st + i])
+                    fnorm = std::hypot(fnorm, val(st + i));
+            if (std_soc) {
+                const int zi = st + vd + 1;
+                const double z = val(zi);
+                if (fx[zi] && (!(z >= 0.0) || fnorm > z)) {
+                    std::fprintf(stderr,
+                                 "[solve_qp_problem] standard SOC %d has an empty fixed section "
+                                 "(fixed vector norm=%.17g, fixed z=%.17g).\n",
+                                 c, fnorm, z);
+                    return -1;
+                }
+                continue;
+            }
+            const int si = st + vd, ti = si + 1;
+            const bool fs = fx[si] != 0, ft = fx[ti] != 0;
+            const double sv = val(si), tv = val(ti);
+            bool empty = (fs && sv < 0.0) || (ft && tv < 0.0);
+            if (!empty && fs && ft)
+                empty = fnorm > 1.41421356237309504880 * std::sqrt(sv) * std::sqrt(tv);
+            else if (fs && sv == 0.0)
+                empty |= fnorm > 0.0;
+            else if (ft && tv == 0.0)
+                empty |= fnorm > 0.0;
+            if (empty) {
+                std::fprintf(stderr,
+                             "[solve_qp_problem] rotated SOC %d has an empty fixed section "
+                             "(fixed vector norm=%.17g, s=%.17g%s, t=%.17g%s).\n",
+                             c, fnorm, sv, fs ? " fixed" : "", tv, ft ? " fixed" : "");
+                return -1;
+            }
+            continue;
+        }
+        if (t != CONE_POWER)
+            continue;
+        const bool f0 = fx[st] != 0, f1 = fx[st + 1] != 0, f2 = fx[st + 2] != 0;
+        const double x = val(st), y = val(st + 1), z = val(st + 2);
+        if ((f0 && (!std::isfinite(x) || x < 0.0)) || (f1 && (!std::isfinite(y) || y < 0.0)) ||
+            (f2 && !std::isfinite(z))) {
+            std::fprintf(stderr,
+                         "[solve_qp_problem] power cone %d has an invalid fixed value "
+                         "(x=%.17g%s, y=%.17g%s, z=%.17g%s).\n",
+                         c, x, f0 ? " fixed" : "", y, f1 ? " fixed" : "", z, f2 ? " fixed" : "");
+            return -1;
+        }
+        if (f2 && z != 0.0 && ((f0 && x == 0.0) || (f1 && y == 0.0))) {
+            std::fprintf(stderr,
+                         "[solve_qp_problem] power cone %d has an empty fixed section: "
+                         "|z| is positive while a fixed nonnegative axis is zero.\n",
+                         c);
+            return -1;
+        }
+        if (f0 && f1 && f2 && z != 0.0) {
+            const double a = prob->cones.power_alpha[c];
+            const double lb = (x > 0.0 && y > 0.0) ? a * std::log(x) + (1.0 - a) * std::log(y) : -INFINITY;
+            const double lz = std::log(std::fabs(z));
+            if (lb + 64.0 * DBL_EPSILON * (1.0 + std::fabs(lb) + std::fabs(lz)) < lz) {
+                std::fprintf(stderr,
+                             "[solve_qp_problem] power cone %d has an infeasible fully fixed point "
+                             "(x=%.17g, y=%.17g, z=%.17g, alpha=%.17g).\n",
+                             c, x, y, z, a);
+                return -1;
+            }
+        }
+    }
     return 0;
 }
 

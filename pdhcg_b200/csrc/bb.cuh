@@ -52,6 +52,7 @@ struct BBData {
     int n_cones;
     const double *vr;
     double *cone_warm;
+    const unsigned char *fixed, *cone_fixed; // slots fixed by set_cone_fixed, and per block whether any (NULL: none)
     double *psd_work; // PSD blocks' projection scratch (NULL: none)
     const long long *psd_off;
     // iterates
@@ -228,8 +229,9 @@ struct BBWork {
 };
 
 // One cone block of bb_var_phase: the warp computes the candidates,
-// projects, and takes the step from the values before the update.
-template <int G, int S>
+// projects, and takes the step from the values before the update.  SECT:
+// the block holds slots fixed by set_cone_fixed (section projectors).
+template <int G, int S, bool SECT = false>
 __device__ __forceinline__ double bb_cone_block(const BBData &D, const double *drx, bool init, double alpha, int lane,
                                                 double *stage, int cb)
 {
@@ -284,9 +286,15 @@ __device__ __forceinline__ double bb_cone_block(const BBData &D, const double *d
         }
     }
     __syncwarp();
-    bool uni = warp_uniform_unit<S>(sl, L, lane);
-    warp_project<S>(type, sl, L, lane, uni, D.cone_warm ? D.cone_warm + cb : nullptr,
-                    D.cone_alpha ? D.cone_alpha[cb] : 0.0, D.psd_work ? D.psd_work + D.psd_off[cb] : nullptr);
+    if constexpr (SECT) {
+        const unsigned fb = section_bits<S>(D.fixed, st, L, lane);
+        warp_section_project<S>(type, sl, L, lane, fb, D.cone_warm ? D.cone_warm + cb : nullptr,
+                                D.cone_alpha ? D.cone_alpha[cb] : 0.0);
+    } else {
+        bool uni = warp_uniform_unit<S>(sl, L, lane);
+        warp_project<S>(type, sl, L, lane, uni, D.cone_warm ? D.cone_warm + cb : nullptr,
+                        D.cone_alpha ? D.cone_alpha[cb] : 0.0, D.psd_work ? D.psd_work + D.psd_off[cb] : nullptr);
+    }
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         int i = lane + 32 * s;
@@ -306,8 +314,10 @@ __device__ __forceinline__ double bb_cone_block(const BBData &D, const double *d
 // projection that follows, src/pdhg_core_op.cu:531-566)
 // update: alpha from the previous step; x_p = P(x_p - alpha M^-1 grad);
 // dir = x_p(new) - x_p(old) (reference :613-660)
-// Both return the partial of dir' M dir (or dir' dir).
-template <int G, int S>
+// Both return the partial of dir' M dir (or dir' dir).  SECT: the problem
+// has blocks with fixed slots (a kernel of its own, so that the section
+// projectors do not weigh on the registers of the others).
+template <int G, int S, bool SECT>
 __device__ double bb_var_phase(const BBData &D, const double *drx, bool init, double alpha, int lane, int gwarp,
                                int nwarps, double *stage)
 {
@@ -357,7 +367,11 @@ __device__ double bb_var_phase(const BBData &D, const double *drx, bool init, do
             // cone block; 3-slot blocks (exponential, power) take the one-slot
             // instantiation, which alone carries their projection
             const int cb = task - W.free_tasks;
-            if (S > 1 && (D.cone_type[cb] == 2 || D.cone_type[cb] == 3))
+            const bool three = S > 1 && (D.cone_type[cb] == 2 || D.cone_type[cb] == 3);
+            if (SECT && D.cone_fixed[cb])
+                part += three ? bb_cone_block<G, 1, SECT>(D, drx, init, alpha, lane, stage, cb)
+                              : bb_cone_block<G, S, SECT>(D, drx, init, alpha, lane, stage, cb);
+            else if (three)
                 part += bb_cone_block<G, 1>(D, drx, init, alpha, lane, stage, cb);
             else
                 part += bb_cone_block<G, S>(D, drx, init, alpha, lane, stage, cb);
@@ -389,7 +403,7 @@ __device__ double bb_grad_phase(const BBData &D, const double *drx, double inv_t
     return part;
 }
 
-template <int G, int S>
+template <int G, int S, bool SECT>
 __global__ void __launch_bounds__(TPB) bb_kernel(BBData D, BBParams P)
 {
     cgb::grid_group grid = cgb::this_grid();
@@ -416,7 +430,7 @@ __global__ void __launch_bounds__(TPB) bb_kernel(BBData D, BBParams P)
         grid.sync();
         bb_drx_smem(D, drx);
     }
-    double s = bb_var_phase<G, S>(D, drx, true, alpha0, lane, gwarp, nwarps, stage);
+    double s = bb_var_phase<G, S, SECT>(D, drx, true, alpha0, lane, gwarp, nwarps, stage);
     bb_block_partial(s, p_s);
     grid.sync();
     int it = 1;
@@ -437,7 +451,7 @@ __global__ void __launch_bounds__(TPB) bb_kernel(BBData D, BBParams P)
         grid.sync();
         double tmp = bb_fold(p_t, nb);
         double alpha = stMs / tmp; // M-metric BB step (precond: sMs/tmp; plain: |s|^2/tmp)
-        s = bb_var_phase<G, S>(D, drx, false, alpha, lane, gwarp, nwarps, stage);
+        s = bb_var_phase<G, S, SECT>(D, drx, false, alpha, lane, gwarp, nwarps, stage);
         bb_block_partial(s, p_s);
         grid.sync();
         ++it;

@@ -1002,8 +1002,10 @@ __device__ void warp_project_psd(WarpSlots<S> &sl, int L, int lane, double *work
 
 // Cone kinds an instantiation carries: SOC / RSOC (any S), the 3-slot
 // exponential / power cones (S = 1 only; callers route those blocks there)
-// and PSD blocks (psd: this block's scratch of 2 n^2 doubles).
-enum ConeKinds { CONES_WIDE = 1, CONES_THREE = 2, CONES_PSD = 4, CONES_ALL = 7 };
+// and PSD blocks (psd: this block's scratch of 2 n^2 doubles).  Blocks with
+// fixed slots (any type but PSD) are a launch class of their own,
+// CONES_SECTION, projected by section.cuh.
+enum ConeKinds { CONES_WIDE = 1, CONES_THREE = 2, CONES_PSD = 4, CONES_ALL = 7, CONES_SECTION = 8 };
 
 template <int S, int KINDS = CONES_ALL>
 __device__ __forceinline__ void warp_project(int type, WarpSlots<S> &sl, int L, int lane, bool uniform_unit,

@@ -25,6 +25,7 @@
 #pragma once
 
 #include "device.cuh"
+#include "section.cuh"
 
 namespace pdhcg {
 
@@ -63,6 +64,8 @@ struct StepData {
     const double *cone_alpha; // power-cone exponents (NULL: none)
     int n_cones;
     double *cone_warm; // per-cone multiplier warm start (may be NULL)
+    // slots fixed by set_cone_fixed (NULL: none): mask over the variables
+    const unsigned char *fixed;
     T *x0, *x, *xp, *xr, *dx, *dual_slack;
     T *y0, *y, *yp, *dy;
     LongRows A_long, At_long; // long rows of A (pass over x_refl) and of A^T (pass over y)
@@ -203,9 +206,16 @@ __device__ __forceinline__ void primal_cone_block(const StepData<T> &D, const St
                 D.dual_slack[st + i] = (T)((sl.x[s] - tt[s]) / P.tau);
         }
     }
-    bool uni = warp_uniform_unit<S>(sl, L, lane);
-    warp_project<S, KINDS>(type, sl, L, lane, uni, D.cone_warm ? D.cone_warm + cb : nullptr,
-                           D.cone_alpha ? D.cone_alpha[cb] : 0.0, D.psd_work ? D.psd_work + D.psd_off[cb] : nullptr);
+    if constexpr ((KINDS & CONES_SECTION) != 0) { // blocks with fixed slots
+        const unsigned fb = section_bits<S>(D.fixed, st, L, lane);
+        warp_section_project<S>(type, sl, L, lane, fb, D.cone_warm ? D.cone_warm + cb : nullptr,
+                                D.cone_alpha ? D.cone_alpha[cb] : 0.0);
+    } else {
+        bool uni = warp_uniform_unit<S>(sl, L, lane);
+        warp_project<S, KINDS>(type, sl, L, lane, uni, D.cone_warm ? D.cone_warm + cb : nullptr,
+                               D.cone_alpha ? D.cone_alpha[cb] : 0.0,
+                               D.psd_work ? D.psd_work + D.psd_off[cb] : nullptr);
+    }
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         const int i = lane + 32 * s;

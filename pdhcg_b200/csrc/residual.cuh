@@ -29,6 +29,7 @@ enum ResidualScalar {
     RS_POW_REL,        // the same relative to the point's size
     RS_AFF_MEM,        // affine rows: dual membership proj_K(-y) / cr (max, or sum of squares)
     RS_AFF_COMPL,      // affine blocks: |y . (A x + g)| / sb (max, or sum of squares)
+    RS_CONE_COMPL,     // variable cone blocks with fixed slots: complementarity (max, or sum of squares)
     RS_COUNT
 };
 
@@ -62,6 +63,7 @@ struct ResidualData {
     const int *cone_start, *cone_len, *cone_type; int n_cones;
     const double *cone_alpha;     // power-cone exponents (NULL: none)
     double *warm_dual, *warm_aug; // per-cone warm starts of the two projections
+    const unsigned char *fixed, *cone_fixed; // slots fixed by set_cone_fixed, per block whether any (NULL: none)
     double *partials;
     int rows_blocks, free_blocks, cone_blocks;
     LongRows A_long, At_long; // passes over x_pdhg and y_pdhg
@@ -79,8 +81,9 @@ struct ResidualData {
 __device__ __forceinline__ double norm_term(double v, int l2) { return l2 ? v * v : abs_or_inf(v); }
 
 // One cone block of the residual: A^T y over the block, the dual-cone
-// residual and the augmented projected gradient, folded into acc.
-template <int S, typename VT>
+// residual and the augmented projected gradient, folded into acc.  SECT:
+// the block holds slots fixed by set_cone_fixed (section projectors).
+template <int S, typename VT, bool SECT = false>
 __device__ __forceinline__ void residual_cone_block(const ResidualData<VT> &D, const ResidualParams &P, int cb,
                                                     int lane, double *stage, double (&acc)[RS_COUNT],
                                                     const int (&ops)[RS_COUNT])
@@ -116,6 +119,22 @@ __device__ __forceinline__ void residual_cone_block(const ResidualData<VT> &D, c
         }
     }
     const double alpha = D.cone_alpha ? D.cone_alpha[cb] : 0.0;
+    double dres[S]; // the block's dual residual, scaled (before the augmentation)
+    if constexpr (SECT) {
+        // fixed slots: x - P_section(x - rc) in the d metric, and the
+        // projected gradient on the section; both projections share the
+        // block's residual warm start, as in the reference
+        const unsigned fb = section_bits<S>(D.fixed, st, L, lane);
+        double vrs[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            vrs[s] = aug.d[s];
+        double *wa = D.warm_aug ? D.warm_aug + cb : nullptr;
+        const double cplx = warp_section_dual<S>(type, L, lane, fb, xv, rc, vrs, alpha, wa, dres);
+        warp_section_project<S>(type, aug, L, lane, fb, wa, alpha);
+        if (lane == 0)
+            fold(RS_CONE_COMPL, norm_term(cplx, P.l2));
+    } else {
     bool uni = warp_uniform_unit<S>(aug, L, lane); // d uniform <=> 1/d uniform
     double *psd = D.psd_work ? D.psd_work + D.psd_off[cb] : nullptr;
     if (type == 0 || type == 1 || type == 4) {
@@ -143,6 +162,10 @@ __device__ __forceinline__ void residual_cone_block(const ResidualData<VT> &D, c
         }
     }
     warp_project<S>(type, aug, L, lane, uni, D.warm_aug ? D.warm_aug + cb : nullptr, alpha, psd);
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+        dres[s] = (rc[s] - dual.x[s]) * aug.d[s];
+    }
     if (type == 3 && lane == 0) {
         // power-cone primal violation (reference compute_power_cone_primal_violation_kernel,
         // src/kernels/pdhcg_power_cone_kernels.cu:623-669): lane 0 holds slot 0 and
@@ -178,7 +201,7 @@ __device__ __forceinline__ void residual_cone_block(const ResidualData<VT> &D, c
         if (i < L) {
             int j = st + i;
             double vr = D.vr[j];
-            double dr = (rc[s] - dual.x[s]) * vr;
+            double dr = dres[s];
             double rr = (xv[s] - aug.x[s]) / P.s_aug * vr;
             if (!isfinite(rr))
                 rr = copysign(INFINITY, rr);
@@ -258,12 +281,15 @@ __device__ __forceinline__ void residual_affine_block(const ResidualData<VT> &D,
         fold(RS_AFF_COMPL, norm_term(fabs(ydv) / P.sb, P.l2));
 }
 
-template <int S, typename VT>
+// SECT: the problem has blocks with fixed slots (an instantiation of its
+// own, so that the section projectors do not weigh on the registers of the
+// others)
+template <int S, typename VT, bool SECT>
 __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, ResidualParams P)
 {
     __shared__ double stage_all[WARPS][STREAM_CHUNK];
     const int NOP = P.l2 ? RSUM : RMAX;
-    const int ops[RS_COUNT] = {NOP, RSUM, NOP, RSUM, RSUM, RSUM, NOP, NOP, RSUM, RSUM, NOP, NOP, NOP, NOP};
+    const int ops[RS_COUNT] = {NOP, RSUM, NOP, RSUM, RSUM, RSUM, NOP, NOP, RSUM, RSUM, NOP, NOP, NOP, NOP, NOP};
     double acc[RS_COUNT];
 #pragma unroll
     for (int s = 0; s < RS_COUNT; ++s)
@@ -362,10 +388,16 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
             // 3-slot blocks (exponential, power) take the one-slot
             // instantiation, which alone carries their projection
             const int ct = D.cone_type[cb];
-            if (S > 1 && (ct == 2 || ct == 3))
+            if (SECT && D.cone_fixed[cb]) {
+                if (S > 1 && (ct == 2 || ct == 3))
+                    residual_cone_block<1, VT, true>(D, P, cb, lane, stage, acc, ops);
+                else
+                    residual_cone_block<S, VT, true>(D, P, cb, lane, stage, acc, ops);
+            } else if (S > 1 && (ct == 2 || ct == 3)) {
                 residual_cone_block<1, VT>(D, P, cb, lane, stage, acc, ops);
-            else
+            } else {
                 residual_cone_block<S, VT>(D, P, cb, lane, stage, acc, ops);
+            }
         }
     } else {
         b -= D.rows_blocks + D.free_blocks + D.cone_blocks;

@@ -392,18 +392,35 @@ __global__ void scale_start_kernel(int n, const double *start, const double *vr,
         x0[i] = start[i] * vr[i] * sb;
 }
 
+// fixed: slots fixed by set_cone_fixed (NULL: none), which keep their value
 __global__ void cone_aux_init_kernel(int ncones, const int *start, const int *vdim, const int *type,
-                                     const double *vr, double sb, double *x0)
+                                     const double *vr, double sb, double *x0, const unsigned char *fixed)
 {
     const double INV_SQRT2 = 0.7071067811865475;
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < ncones; b += gridDim.x * blockDim.x) {
         int aux0 = start[b] + vdim[b];
         if (type[b] == 1) { // standard SOC: w, z
-            x0[aux0] = -INV_SQRT2 * sb * vr[aux0];
-            x0[aux0 + 1] = INV_SQRT2 * sb * vr[aux0 + 1];
+            if (!(fixed && fixed[aux0]))
+                x0[aux0] = -INV_SQRT2 * sb * vr[aux0];
+            if (!(fixed && fixed[aux0 + 1]))
+                x0[aux0 + 1] = INV_SQRT2 * sb * vr[aux0 + 1];
         } else if (type[b] == 0) { // rotated SOC: t
-            x0[aux0 + 1] = sb * vr[aux0 + 1];
+            if (!(fixed && fixed[aux0 + 1]))
+                x0[aux0 + 1] = sb * vr[aux0 + 1];
         }
+    }
+}
+
+// fixed cone slots: the scaled bounds pinned at value * vr * sb (reference
+// pin_scaled_fixed_cone_bounds, src/preconditioner.c:311-327)
+__global__ void pin_fixed_kernel(int nfix, const int *idx, const double *val, const double *vr, double sb, double *l,
+                                 double *u)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nfix; k += gridDim.x * blockDim.x) {
+        const int j = idx[k];
+        const double v = val[k] * vr[j] * sb;
+        l[j] = v;
+        u[j] = v;
     }
 }
 
@@ -430,10 +447,14 @@ __global__ void dual_start_kernel(int m, const double *start, const double *cr, 
     }
 }
 
-// warp-per-cone projection of a vector (unit metric, d = rescaling)
+// warp-per-cone projection of a vector (unit metric, d = rescaling);
+// fixed: slots fixed by set_cone_fixed (NULL: none), sect: whether this
+// block holds any (then the section projector, with warm start warm)
 template <int S>
 __device__ __forceinline__ void project_cone_block(int st, int L, int tp, double alpha, double *x, const double *d,
-                                                   const double *q, double tau, int lane, double *psd)
+                                                   const double *q, double tau, int lane, double *psd,
+                                                   const unsigned char *fixed = nullptr, bool sect = false,
+                                                   double *warm = nullptr)
 {
     WarpSlots<S> sl;
 #pragma unroll
@@ -443,8 +464,12 @@ __device__ __forceinline__ void project_cone_block(int st, int L, int tp, double
         sl.d[s] = i < L ? d[st + i] : 1.0;
         sl.w[s] = (i < L && q) ? 1.0 + tau * q[st + i] : 1.0;
     }
-    bool uni = warp_uniform_unit<S>(sl, L, lane);
-    warp_project<S>(tp, sl, L, lane, uni, nullptr, alpha, psd);
+    if (sect) {
+        warp_section_project<S>(tp, sl, L, lane, section_bits<S>(fixed, st, L, lane), warm, alpha);
+    } else {
+        bool uni = warp_uniform_unit<S>(sl, L, lane);
+        warp_project<S>(tp, sl, L, lane, uni, nullptr, alpha, psd);
+    }
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         int i = lane + 32 * s;
@@ -459,17 +484,41 @@ template <int S>
 __global__ void __launch_bounds__(TPB) project_cones_kernel(int ncones, const int *start, const int *len,
                                                             const int *type, const double *alpha, double *x,
                                                             const double *d, const double *q, double tau,
-                                                            double *psd_work, const long long *psd_off)
+                                                            double *psd_work, const long long *psd_off,
+                                                            const unsigned char *fixed = nullptr,
+                                                            const unsigned char *cone_fixed = nullptr,
+                                                            double *warm = nullptr)
 {
     const int lane = threadIdx.x & 31;
     for (int cb = blockIdx.x * WARPS + (threadIdx.x >> 5); cb < ncones; cb += gridDim.x * WARPS) {
         const int st = start[cb], L = len[cb], tp = type[cb];
         const double a = alpha ? alpha[cb] : 0.0;
         double *psd = psd_work ? psd_work + psd_off[cb] : nullptr;
+        const bool sect = cone_fixed && cone_fixed[cb];
+        double *wb = warm ? warm + cb : nullptr;
         if (S > 1 && (tp == 2 || tp == 3)) // 3-slot blocks: the one-slot instantiation
-            project_cone_block<1>(st, L, tp, a, x, d, q, tau, lane, psd);
+            project_cone_block<1>(st, L, tp, a, x, d, q, tau, lane, psd, fixed, sect, wb);
         else
-            project_cone_block<S>(st, L, tp, a, x, d, q, tau, lane, psd);
+            project_cone_block<S>(st, L, tp, a, x, d, q, tau, lane, psd, fixed, sect, wb);
+    }
+}
+
+// every block a section block (pdhcg_b200_project_cone_sections)
+template <int S>
+__global__ void __launch_bounds__(TPB) project_sections_kernel(int ncones, const int *start, const int *len,
+                                                               const int *type, const double *alpha, double *x,
+                                                               const double *d, const double *q, double tau,
+                                                               const unsigned char *fixed, double *warm)
+{
+    const int lane = threadIdx.x & 31;
+    for (int cb = blockIdx.x * WARPS + (threadIdx.x >> 5); cb < ncones; cb += gridDim.x * WARPS) {
+        const int st = start[cb], L = len[cb], tp = type[cb];
+        const double a = alpha ? alpha[cb] : 0.0;
+        double *wb = warm ? warm + cb : nullptr;
+        if (S > 1 && (tp == 2 || tp == 3))
+            project_cone_block<1>(st, L, tp, a, x, d, q, tau, lane, nullptr, fixed, true, wb);
+        else
+            project_cone_block<S>(st, L, tp, a, x, d, q, tau, lane, nullptr, fixed, true, wb);
     }
 }
 

@@ -179,17 +179,22 @@ std::vector<int2> row_tiles(const std::vector<int> &rows)
 // sit in the wide kernels' register allocation.  A list pointer stays null
 // when its launch covers every block (all of one kind).
 struct ConeSplit {
-    std::vector<int> wide, three, psd;
-    int *wide_d = nullptr, *three_d = nullptr, *psd_d = nullptr;
-    int n_wide = 0, n_three = 0, n_psd = 0;
+    std::vector<int> wide, three, psd, sect;
+    int *wide_d = nullptr, *three_d = nullptr, *psd_d = nullptr, *sect_d = nullptr;
+    int n_wide = 0, n_three = 0, n_psd = 0, n_sect = 0;
 
-    void build(const std::vector<int> &types)
+    // fixed (may be empty): per block, does it hold slots fixed by
+    // set_cone_fixed?  Those blocks take the section projectors.
+    void build(const std::vector<int> &types, const std::vector<char> &fixed = {})
     {
         wide.clear();
         three.clear();
         psd.clear();
+        sect.clear();
         for (int b = 0; b < (int)types.size(); ++b) {
-            if (types[b] == CONE_EXPONENTIAL || types[b] == CONE_POWER)
+            if (!fixed.empty() && fixed[b])
+                sect.push_back(b);
+            else if (types[b] == CONE_EXPONENTIAL || types[b] == CONE_POWER)
                 three.push_back(b);
             else if (types[b] == CONE_PSD)
                 psd.push_back(b);
@@ -199,21 +204,24 @@ struct ConeSplit {
         n_wide = (int)wide.size();
         n_three = (int)three.size();
         n_psd = (int)psd.size();
+        n_sect = (int)sect.size();
     }
     // more than one launch: every launch takes its index list
-    bool mixed() const { return (n_wide > 0) + (n_three > 0) + (n_psd > 0) > 1; }
-    // the three lists back to back in one device array of n_wide + n_three + n_psd ints
+    bool mixed() const { return (n_wide > 0) + (n_three > 0) + (n_psd > 0) + (n_sect > 0) > 1; }
+    // the lists back to back in one device array of n_wide + n_three + n_psd + n_sect ints
     void place(int *ids)
     {
         wide_d = ids;
         three_d = ids + n_wide;
         psd_d = ids + n_wide + n_three;
+        sect_d = ids + n_wide + n_three + n_psd;
     }
     std::vector<int> joined() const
     {
         std::vector<int> all(wide);
         all.insert(all.end(), three.begin(), three.end());
         all.insert(all.end(), psd.begin(), psd.end());
+        all.insert(all.end(), sect.begin(), sect.end());
         return all;
     }
 };
@@ -378,6 +386,15 @@ struct DeviceProblem {
     int2 *free_tiles = nullptr; // free variables as tiles of consecutive rows
     int n_free_tiles = 0;
     double *pstart = nullptr, *dstart = nullptr;
+    // slots fixed by set_cone_fixed: the mask over the variables, per block
+    // whether it holds any, and the fixed slots with their values (pinned
+    // into the scaled bounds after rescaling)
+    bool has_fixed = false;
+    std::vector<char> cone_fixed;
+    unsigned char *fixed_d = nullptr, *cfix_d = nullptr;
+    int n_fix = 0;
+    int *fix_idx = nullptr;
+    double *fix_val = nullptr;
     // solution kept on the device when a solve is asked to leave it there
     double *x_out = nullptr, *y_out = nullptr, *rc_out = nullptr;
 };
@@ -504,8 +521,15 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
 
     int maxlen = 0;
     std::vector<char> in_cone(d.n, 0);
+    d.has_fixed = p->cones.is_fixed != nullptr && p->cones.num_cones > 0;
     for (int b = 0; b < p->cones.num_cones; ++b) {
         int len = pdhcg_b200_cone_length(p->cones.type[b], p->cones.v_dim[b]);
+        if (d.has_fixed) {
+            char any = 0;
+            for (int i = 0; i < len; ++i)
+                any |= p->cones.is_fixed[p->cones.start_idx[b] + i] != 0;
+            d.cone_fixed.push_back(any);
+        }
         d.cone_start.push_back(p->cones.start_idx[b]);
         d.cone_len.push_back(len);
         d.cone_type.push_back((int)p->cones.type[b]);
@@ -538,7 +562,29 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
         d.ctype = ar.upload(d.cone_type.data(), nc, s);
         d.cvdim = ar.upload(d.cone_vdim.data(), nc, s);
         d.calpha = ar.upload(d.cone_alpha.data(), nc, s);
-        d.split.build(d.cone_type);
+        d.split.build(d.cone_type, d.cone_fixed);
+        if (d.has_fixed) {
+            // fixed slots: bounds pinned after scaling, so the box step holds
+            // them (reference pin_scaled_fixed_cone_bounds, src/preconditioner.c:311-327)
+            d.cone_box = true;
+            std::vector<unsigned char> mask(p->cones.is_fixed, p->cones.is_fixed + d.n);
+            std::vector<unsigned char> cf(d.cone_fixed.begin(), d.cone_fixed.end());
+            std::vector<int> fi;
+            std::vector<double> fv;
+            for (int j = 0; j < d.n; ++j)
+                if (mask[j]) {
+                    fi.push_back(j);
+                    fv.push_back(p->primal_start ? p->primal_start[j] : 0.0);
+                }
+            d.n_fix = (int)fi.size();
+            d.fixed_d = ar.upload(mask.data(), mask.size(), s);
+            d.cfix_d = ar.upload(cf.data(), cf.size(), s);
+            if (d.n_fix > 0) {
+                d.fix_idx = ar.upload(fi.data(), fi.size(), s);
+                d.fix_val = ar.upload(fv.data(), fv.size(), s);
+            }
+            CK(cudaStreamSynchronize(s));
+        }
         if (d.split.mixed()) {
             std::vector<int> all = d.split.joined();
             d.split.place(ar.upload(all.data(), all.size(), s));
@@ -605,8 +651,8 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
     }
     if (d.S < 0)
         d.unsupported = "cone blocks longer than 256 slots are not supported yet";
-    if (p->cones.is_fixed || p->affine_cones.is_fixed)
-        d.unsupported = "fixed cone slots are not available on the device path yet";
+    if (p->affine_cones.is_fixed)
+        d.unsupported = "fixed slots of affine cones are not supported (the reference refuses them too)";
     if (p->num_quadratic_constraints > 0) // the solve entry points transform them first
         d.unsupported = "quadratic constraints must be transformed with qcqp_to_socp_qp first";
     CK(cudaStreamSynchronize(s)); // host sources of the uploads may go away
@@ -794,6 +840,17 @@ int launch_primal_cones(const StepData<T> &D, const StepParams &P, const ConeSpl
                 primal_cone_kernel<SC.value, T, true, CONES_PSD><<<grid, TPB, 0, s>>>(D, P, sp.psd_d, sp.n_psd);
             else
                 primal_cone_kernel<SC.value, T, false, CONES_PSD><<<grid, TPB, 0, s>>>(D, P, sp.psd_d, sp.n_psd);
+        });
+        ++launches;
+    }
+    if (sp.n_sect > 0) { // blocks with fixed slots: section projectors
+        dispatch_s(S, [&](auto SC) {
+            int grid = grid_for(sp.n_sect, WARPS);
+            if (hasq)
+                primal_cone_kernel<SC.value, T, true, CONES_SECTION><<<grid, TPB, 0, s>>>(D, P, sp.sect_d, sp.n_sect);
+            else
+                primal_cone_kernel<SC.value, T, false, CONES_SECTION><<<grid, TPB, 0, s>>>(D, P, sp.sect_d,
+                                                                                           sp.n_sect);
         });
         ++launches;
     }
@@ -1008,6 +1065,9 @@ void Solve::rescale()
                 mul_scalar_kernel<<<grid_for(Rt_.nnz, TPB), TPB, 0, s>>>(Rt_.v, Rt_.nnz, f);
         }
     }
+    if (dp_.n_fix > 0) // fixed cone slots: scaled bounds pinned at the scaled value
+        pin_fixed_kernel<<<grid_for(dp_.n_fix, TPB), TPB, 0, s>>>(dp_.n_fix, dp_.fix_idx, dp_.fix_val, vr_d_, sb_,
+                                                                  l_d_, u_d_);
     CK(cudaGetLastError());
 }
 
@@ -1038,10 +1098,12 @@ void Solve::init_state()
         warm_dual_ = cone_warm_ + nc;
         warm_aug_ = cone_warm_ + 2 * (size_t)nc;
         CK(cudaMemsetAsync(cone_warm_, 0, 3 * (size_t)nc * sizeof(double), s)); // 0 = no warm start
-        cone_aux_init_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(nc, cst_d_, cvdim_d_, ctype_d_, vr_d_, sb_, x0_);
+        cone_aux_init_kernel<<<grid_for(nc, TPB), TPB, 0, s>>>(nc, cst_d_, cvdim_d_, ctype_d_, vr_d_, sb_, x0_,
+                                                               dp_.fixed_d);
         dispatch_s(S_, [&](auto SC) {
             project_cones_kernel<SC.value><<<grid_for(nc, WARPS), TPB, 0, s>>>(
-                nc, cst_d_, clen_d_, ctype_d_, dp_.calpha, x0_, vr_d_, nullptr, 0.0, psd_work_, dp_.psd_off_d);
+                nc, cst_d_, clen_d_, ctype_d_, dp_.calpha, x0_, vr_d_, nullptr, 0.0, psd_work_, dp_.psd_off_d,
+                dp_.fixed_d, dp_.cfix_d, cone_warm_);
         });
     }
     box_clamp_copy_kernel<<<grid_for(n, TPB), TPB, 0, s>>>(n, l_d_, u_d_, x0_, x_, xp_, xr_);
@@ -1099,6 +1161,8 @@ BBData Solve::bb_data() const
     D.n_cones = (int)cone_start_.size();
     D.vr = vr_d_;
     D.cone_warm = cone_warm_;
+    D.fixed = dp_.fixed_d;
+    D.cone_fixed = dp_.cfix_d;
     D.x0 = x0_;
     D.x = x_;
     D.xp = xp_;
@@ -1129,7 +1193,11 @@ void Solve::setup_bb()
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     dispatch_rg(GQ_, [&](auto GC) {
         dispatch_s(S_, [&](auto SC) {
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bb_kernel<GC.value, SC.value>, TPB, 0));
+            if (dp_.has_fixed)
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bb_kernel<GC.value, SC.value, true>, TPB, 0));
+            else
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bb_kernel<GC.value, SC.value, false>, TPB,
+                                                                 0));
         });
     });
     int q_per_sm = 0;
@@ -1285,6 +1353,7 @@ StepData<T> Solve::step_data()
     D.A_long = A_.lr;
     D.At_long = At_.lr;
     D.cone_warm = cone_warm_;
+    D.fixed = dp_.fixed_d;
     D.n = n_;
     D.m = m_;
     D.A_rp = A_.rp;
@@ -1413,7 +1482,9 @@ void Solve::enqueue_step_bb(bool store_dual, bool want_fpe, double w)
     dispatch_rg(GQ_, [&](auto GC) {
         dispatch_s(S_, [&](auto SC) {
             void *args[] = {&D, &BP};
-            CK(cudaLaunchCooperativeKernel((void *)bb_kernel<GC.value, SC.value>, bb_grid_, TPB, args, 0, s));
+            void *k = dp_.has_fixed ? (void *)bb_kernel<GC.value, SC.value, true>
+                                    : (void *)bb_kernel<GC.value, SC.value, false>;
+            CK(cudaLaunchCooperativeKernel(k, bb_grid_, TPB, args, 0, s));
         });
     });
     StepParams P{};
@@ -1568,6 +1639,8 @@ void Solve::enqueue_residual_t(bool want_dist)
     ResidualData<VT> D{};
     D.warm_dual = warm_dual_;
     D.warm_aug = warm_aug_;
+    D.fixed = dp_.fixed_d;
+    D.cone_fixed = dp_.cfix_d;
     D.n = n_;
     D.m = m_;
     D.A_rp = A_.rp;
@@ -1646,7 +1719,12 @@ void Solve::enqueue_residual_t(bool want_dist)
     P.s_aug = sa;
     P.sb = sb_;
     int nb = D.rows_blocks + D.free_blocks + D.cone_blocks + D.aff_blocks;
-    dispatch_s(std::max(S_, dp_.S_aff), [&](auto SC) { residual_kernel<SC.value, VT><<<nb, TPB, 0, s>>>(D, P); });
+    dispatch_s(std::max(S_, dp_.S_aff), [&](auto SC) {
+        if (dp_.has_fixed)
+            residual_kernel<SC.value, VT, true><<<nb, TPB, 0, s>>>(D, P);
+        else
+            residual_kernel<SC.value, VT, false><<<nb, TPB, 0, s>>>(D, P);
+    });
     fold_partials_kernel<<<1, TPB, 0, s>>>(partials_, nb, RS_COUNT, res_ops_d_, scal_d_);
     stats_.kernel_launches += 2;
     stats_.evaluations++;
@@ -1849,13 +1927,14 @@ void Solve::read_residual()
     auto join = [&](double a, double b) { return l2 ? std::hypot(a, b) : std::fmax(a, b); };
     if (cones)
         abs_p_ = join(abs_p_, pv_abs);
-    // affine cones: dual membership and complementarity join the dual
-    // residual (reference compute_residual, src/pdhg_core_op.cu:1166-1190)
-    if (!dp_.aff_start.empty())
-        abs_d_ = (l2 ? std::sqrt(r[RS_DUAL_RES] + r[RS_AFF_MEM] + r[RS_AFF_COMPL])
-                     : std::fmax(r[RS_DUAL_RES], std::fmax(r[RS_AFF_MEM], r[RS_AFF_COMPL]))) / sc_;
-    else
-        abs_d_ = nrm(r[RS_DUAL_RES]) / sc_;
+    // the cone complementarity (nonzero on power blocks with fixed slots
+    // only, reference compute_cone_complementarity_norm,
+    // src/pdhg_core_op.cu:92-100) and, with affine cones, their dual
+    // membership and complementarity join the dual residual (reference
+    // compute_residual, src/pdhg_core_op.cu:1166-1190); all are 0 when absent
+    abs_d_ = (l2 ? std::sqrt(r[RS_DUAL_RES] + r[RS_CONE_COMPL] + r[RS_AFF_MEM] + r[RS_AFF_COMPL])
+                 : std::fmax(std::fmax(r[RS_DUAL_RES], r[RS_CONE_COMPL]), std::fmax(r[RS_AFF_MEM], r[RS_AFF_COMPL]))) /
+             sc_;
     double half_xqx = qtype_ == PDHCG_NON_Q ? 0.0 : 0.5 * r[RS_XQX];
     pobj_ = (r[RS_CX] + half_xqx) / (sb_ * sc_) + dp_.obj_const;
     dobj_ = (r[RS_SLACKX] + r[RS_PRIMAL_SLACK] - half_xqx) / (sb_ * sc_) + dp_.obj_const;
@@ -2110,7 +2189,7 @@ pdhcg_result_t *Solve::run()
     h_scal_ = pinned_scalars();
     {
         int nop = prm_.optimality_norm == NORM_TYPE_L2 ? RSUM : RMAX;
-        int res_ops[RS_COUNT] = {nop, RSUM, nop, RSUM, RSUM, RSUM, nop, nop, RSUM, RSUM, nop, nop, nop, nop};
+        int res_ops[RS_COUNT] = {nop, RSUM, nop, RSUM, RSUM, RSUM, nop, nop, RSUM, RSUM, nop, nop, nop, nop, nop};
         int fpe_ops[FP_COUNT] = {RSUM, RSUM, RSUM};
         int norm_ops[NS_COUNT] = {RSUM, RSUM, RMAX, RMAX};
         res_ops_d_ = ar_.upload(res_ops, RS_COUNT, st_);
@@ -2351,6 +2430,9 @@ void pdhcg_b200_default_options(pdhcg_b200_options_t *o)
     o->polish_threshold = 1e-5;
 }
 
+static pdhcg_result_t *solve_on_device(const qp_problem_t *prob, const pdhg_parameters_t &prm,
+                                       pdhcg_b200_options_t opt);
+
 pdhcg_result_t *pdhcg_b200_solve(const qp_problem_t *prob, const pdhg_parameters_t *params,
                                  const pdhcg_b200_options_t *opts)
 {
@@ -2358,6 +2440,10 @@ pdhcg_result_t *pdhcg_b200_solve(const qp_problem_t *prob, const pdhg_parameters
         std::fprintf(stderr, "[interface] solve_qp_problem: invalid arguments.\n");
         return nullptr;
     }
+    // fixed cone slots are checked on the problem as given, before any
+    // rewrite (reference solve_qp_problem, src/pdhcg.c:894-902)
+    if (pdhcg_b200_validate_fixed_sections(prob) != 0)
+        return nullptr;
     pdhg_parameters_t prm;
     if (params)
         prm = *params;
@@ -2377,11 +2463,17 @@ pdhcg_result_t *pdhcg_b200_solve(const qp_problem_t *prob, const pdhg_parameters
             std::fprintf(stderr, "Error: QCQP -> SOCP transformation failed; cannot solve.\n");
             return nullptr;
         }
-        pdhcg_result_t *r = pdhcg_b200_solve(ext, &prm, &opt);
+        pdhcg_result_t *r = solve_on_device(ext, prm, opt);
         pdhcg_b200_restore_qcqp_result(r, prob);
         qp_problem_free(ext);
         return r;
     }
+    return solve_on_device(prob, prm, opt);
+}
+
+static pdhcg_result_t *solve_on_device(const qp_problem_t *prob, const pdhg_parameters_t &prm,
+                                       pdhcg_b200_options_t opt)
+{
     try {
         auto t0 = std::chrono::steady_clock::now();
         pdhcg_result_t *r = nullptr;
@@ -2429,6 +2521,8 @@ pdhcg_b200_device_problem_t *pdhcg_b200_upload(const qp_problem_t *prob)
         std::fprintf(stderr, "[pdhcg_b200_upload] prob is NULL\n");
         return nullptr;
     }
+    if (pdhcg_b200_validate_fixed_sections(prob) != 0)
+        return nullptr;
     cudaStream_t us = nullptr;
     try {
         CK(cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking));
@@ -2591,6 +2685,53 @@ int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *co
         cudaFreeAsync(psd_work, s);
         cudaFreeAsync(psd_off_d, s);
     }
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int pdhcg_b200_project_cone_sections(int num_cones, const int *cone_start, const int *cone_vdim,
+                                     const int *cone_type, const double *cone_alpha, const unsigned char *fixed,
+                                     double *x, const double *d, const double *q, double tau, double *warm,
+                                     void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    if (num_cones <= 0)
+        return 0;
+    if (!fixed)
+        return -3;
+    int *len = nullptr;
+    if (cudaMallocAsync((void **)&len, num_cones * sizeof(int), s) != cudaSuccess)
+        return -1;
+    cone_len_kernel<<<grid_for(num_cones, TPB), TPB, 0, s>>>(num_cones, cone_vdim, cone_type, len);
+    std::vector<int> h(num_cones), t(num_cones);
+    if (cudaMemcpyAsync(h.data(), len, num_cones * sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(t.data(), cone_type, num_cones * sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaFreeAsync(len, s);
+        return -1;
+    }
+    int maxlen = 0;
+    bool types_ok = true;
+    for (int i = 0; i < num_cones; ++i) {
+        maxlen = std::max(maxlen, h[i]);
+        types_ok = types_ok && (t[i] == CONE_STANDARD_SOC || t[i] == CONE_ROTATED_SOC || t[i] == CONE_EXPONENTIAL ||
+                                (t[i] == CONE_POWER && cone_alpha));
+    }
+    if (!types_ok) {
+        std::fprintf(stderr, "[pdhcg_b200_project_cone_sections] only SOC, rotated-SOC, exponential and power "
+                             "(with cone_alpha) blocks have fixed sections.\n");
+        cudaFreeAsync(len, s);
+        return -3;
+    }
+    int S = slots_class(maxlen);
+    if (S < 0) {
+        cudaFreeAsync(len, s);
+        return -2;
+    }
+    dispatch_s(S, [&](auto SC) {
+        project_sections_kernel<SC.value><<<grid_for(num_cones, WARPS), TPB, 0, s>>>(
+            num_cones, cone_start, len, cone_type, cone_alpha, x, d, q, tau, fixed, warm);
+    });
+    cudaFreeAsync(len, s);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -135,6 +135,56 @@ def conic_lp(seed: int = 5, nfree: int = 60, nsoc: int = 10, soc_len: int = 12, 
     blocks (exponents U(0.2, 0.8)), equality rows through a strictly
     feasible point (so the problem is feasible) and an objective inside the
     dual cone on the cone slots (so it is bounded)."""
+    return _conic_lp_point(seed, nfree, nsoc, soc_len, nrsoc, rsoc_len, with_q, nexp, npow)[0]
+
+
+def fixed_cone_qp(seed: int = 21, with_q: bool = False, sparse_q: bool = False, nexp: int = 6, npow: int = 6,
+                  soc_len: int = 12, nsoc: int = 10) -> Problem:
+    """conic_lp with slots of about half the cone blocks fixed by
+    set_cone_fixed at the strictly feasible point the rows pass through, so
+    every section is nonempty and the problem stays feasible and bounded.
+    The fixed slots cover every kind the section projectors handle: the SOC
+    apex, w or a vector slot; the rotated-SOC s, t, both, or a vector slot;
+    one or two axes of exponential and power blocks.  sparse_q couples
+    neighbouring free variables in Q (the inner BB solve)."""
+    p, x0 = _conic_lp_point(seed, 60, nsoc, soc_len, 4, 8, with_q or sparse_q, nexp, npow)
+    rng = np.random.default_rng(seed + 1000)
+    fixed = []
+    for ci, k in enumerate(p.cones):
+        if rng.random() < 0.45:
+            continue
+        L = k.v_dim + 2
+        if k.type == CONE_STANDARD_SOC:
+            slots = [[L - 1], [L - 2], [0], [0, L - 1]][rng.integers(4)]
+        elif k.type == CONE_ROTATED_SOC:
+            slots = [[L - 2], [L - 1], [L - 2, L - 1], [0]][rng.integers(4)]
+        else:
+            slots = [[0], [1], [2], [0, 1], [1, 2], [0, 2]][rng.integers(6)]
+        for sl in slots:
+            fixed.append((ci, sl, float(x0[k.start + sl])))
+    p.fixed = fixed
+    if sparse_q:
+        n = p.n
+        q = p.Q.val.copy()
+        rows = [[] for _ in range(n)]
+        for i in range(n):
+            rows[i].append((i, q[i]))
+        for i in range(0, 59, 2):  # pairs of free variables, diagonally dominant
+            w = 0.3 * min(q[i], q[i + 1])
+            rows[i].append((i + 1, w))
+            rows[i + 1].append((i, w))
+        rp = np.zeros(n + 1, np.int32)
+        ci_, v_ = [], []
+        for i in range(n):
+            for j, w in sorted(rows[i]):
+                ci_.append(j)
+                v_.append(w)
+            rp[i + 1] = len(ci_)
+        p.Q = CsrMatrix(n, n, rp, np.array(ci_, np.int32), np.array(v_))
+    return p
+
+
+def _conic_lp_point(seed, nfree, nsoc, soc_len, nrsoc, rsoc_len, with_q, nexp, npow):
     rng = np.random.default_rng(seed)
     n = nfree + nsoc * soc_len + nrsoc * rsoc_len + 3 * (nexp + npow)
     m = n // 3
@@ -196,7 +246,7 @@ def conic_lp(seed: int = 5, nfree: int = 60, nsoc: int = 10, soc_len: int = 12, 
     if with_q:
         q = rng.uniform(0.1, 1.0, n)
         p.Q = CsrMatrix(n, n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), q)
-    return p
+    return p, x0
 
 
 def _svec(X: np.ndarray) -> np.ndarray:

@@ -73,7 +73,8 @@ EXPORTS = [
     "pdhcg_b200_default_options", "pdhcg_b200_solve", "pdhcg_b200_last_stats", "pdhcg_b200_csr_spmv",
     "pdhcg_b200_project_cones", "pdhcg_b200_pdhg_step", "pdhcg_b200_upload", "pdhcg_b200_solve_device",
     "pdhcg_b200_device_solution", "pdhcg_b200_device_problem_free", "pdhcg_b200_request_cancel",
-    "cone_block_length", "pdhcg_b200_project_cones_noalloc", "pdhcg_b200_default_batch_options",
+    "cone_block_length", "pdhcg_b200_project_cones_noalloc", "pdhcg_b200_project_cone_sections",
+    "pdhcg_b200_validate_fixed_sections", "pdhcg_b200_default_batch_options",
     "pdhcg_b200_solve_batch", "pdhcg_b200_batch_autotune", "pdhcg_b200_last_batch_stats",
     "pdhcg_b200_mlp_create", "pdhcg_b200_mlp_free", "pdhcg_b200_mlp_num_params", "pdhcg_b200_mlp_get_params",
     "pdhcg_b200_mlp_set_params", "pdhcg_b200_mlp_predict", "pdhcg_b200_mlp_loss_grad", "pdhcg_b200_mlp_train",

@@ -67,17 +67,44 @@ def test_same_answer_as_reference_build(lib, ref, name):
     assert abs(g["primal_objective_value"] - ob) <= tol * (1 + abs(ob)), (g["primal_objective_value"], ob)
 
 
+FIXED = {
+    "fixed_lp": lambda: instances.fixed_cone_qp(seed=21),
+    "fixed_diag_qp": lambda: instances.fixed_cone_qp(seed=22, with_q=True),
+    "fixed_soc_only": lambda: instances.fixed_cone_qp(seed=24, nexp=0, npow=0),
+}
+
+
+@pytest.mark.parametrize("name", sorted(FIXED))
+def test_fixed_sections_match_reference_build(lib, ref, name):
+    """Cone blocks with slots fixed by set_cone_fixed: the same status, the
+    iteration count within 2 % (+200: the section projectors bisect their
+    multipliers to 1e-13 relative, so the two builds differ in the last
+    bits and a run may cross the tolerance at a neighbouring evaluation),
+    objectives within 1e-6 relative."""
+    p = FIXED[name]()
+    g, r = _solve(lib, p), _solve(ref, p)
+    assert g["status"] == r["status"] == "OPTIMAL", (g["status"], r["status"])
+    assert abs(g["total_count"] - r["total_count"]) <= 0.02 * r["total_count"] + 200, (g["total_count"],
+                                                                                      r["total_count"])
+    ob = r["primal_objective_value"]
+    assert abs(g["primal_objective_value"] - ob) <= 1e-6 * (1 + abs(ob)), (g["primal_objective_value"], ob)
+
+
 @pytest.mark.parametrize("case,form", [(0, capi.CONE_ROTATED_SOC), (1, capi.CONE_STANDARD_SOC),
-                                       (2, capi.CONE_ROTATED_SOC)])
+                                       (2, capi.CONE_ROTATED_SOC), (3, capi.CONE_ROTATED_SOC),
+                                       (4, capi.CONE_STANDARD_SOC)])
 def test_qcqp_solve_matches_reference_build(tmp_path, lib, ref, case, form):
     """A QCQP read from an MPS file (each library's own reader), rewritten
     into cone blocks of the given form and solved: the same status,
-    iteration count and objective as the reference's build, and a result of
-    the original sizes."""
+    iteration count (within 2 % + 200 when the rewrite fixed slots) and
+    objective as the reference's build, and a result of the original
+    sizes."""
     import numpy as np
     from test_qcqp import qcqp_mps
     path = tmp_path / "qc.mps"
-    path.write_text(qcqp_mps(np.random.default_rng(300 + case), flips=case != 2))
+    # cases 3 and 4: the first quadratic row has no linear part, so the
+    # rewrite fixes its s, t slots (set_cone_fixed semantics)
+    path.write_text(qcqp_mps(np.random.default_rng(300 + case), pinned=case >= 3, flips=case != 2))
     out = []
     for L in (lib, ref):
         prob = L.read_mps_file(str(path).encode())
@@ -93,6 +120,10 @@ def test_qcqp_solve_matches_reference_build(tmp_path, lib, ref, case, form):
         L.qp_problem_free(prob)
     (gs, gk, go, gn, gm, n, m), (rs, rk, ro, _, _, _, _) = out
     assert gs == rs == "OPTIMAL"
-    assert gk == rk, (gk, rk)
-    assert abs(go - ro) <= 1e-8 * (1 + abs(ro)), (go, ro)
+    if case >= 3:
+        assert abs(gk - rk) <= 0.02 * rk + 200, (gk, rk)
+        assert abs(go - ro) <= 1e-6 * (1 + abs(ro)), (go, ro)
+    else:
+        assert gk == rk, (gk, rk)
+        assert abs(go - ro) <= 1e-8 * (1 + abs(ro)), (go, ro)
     assert (gn, gm) == (n, m)

@@ -1,0 +1,463 @@
+"""Fixed cone sections: slots fixed by set_cone_fixed (reference
+src/pdhcg.c:620-666) keep their values, and the free slots of the block are
+projected onto the section of the cone through them.
+
+CPU (the oracle and the host library):
+- the oracle's section projectors give the nearest point of the section:
+  feasible, fixed slots untouched, and no farther (weighted distance) than
+  any sampled feasible point of the same section, for every cone type and
+  every kind of fixed-slot pattern (the reference's own check,
+  test/test_fixed_cone_sections.cu:124-334, enumerates candidates the same
+  way);
+- the solve-time validation accepts and refuses the sections the
+  reference's test/test_conic_kkt_termination.c:48-107 accepts and refuses;
+- the oracle reproduces the answers that test asserts for whole solves
+  with fixed slots (:109-560).
+GPU: the same known answers through solve_qp_problem, the device section
+projectors against the oracle's, and seeded instances with fixed slots
+against the oracle (status, iterations, objective).
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from pdhcg_b200 import capi, instances
+from pdhcg_b200.capi import (CONE_EXPONENTIAL, CONE_POWER, CONE_ROTATED_SOC, CONE_STANDARD_SOC, NORM_L2, NORM_LINF,
+                             Cone, CsrMatrix, Problem)
+
+_dp = C.POINTER(C.c_double)
+
+
+# ---------------- the oracle's section projectors ----------------
+
+def _bind_sections(oracle):
+    oracle.oracle_section_project.restype = None
+    oracle.oracle_section_project.argtypes = [C.c_int, C.c_int, C.c_double, _dp, _dp, _dp, C.c_double, C.c_char_p,
+                                              _dp]
+    return oracle
+
+
+def _oracle_project(oracle, t, vd, alpha, x, d, fx, q=None, tau=0.0, warm=0.0):
+    xx = np.array(x, dtype=np.float64)
+    dd = np.array(d, dtype=np.float64)
+    qq = None if q is None else np.array(q, dtype=np.float64)
+    w = C.c_double(warm)
+    _bind_sections(oracle).oracle_section_project(t, vd, alpha, xx.ctypes.data_as(_dp), dd.ctypes.data_as(_dp),
+                                                  None if qq is None else qq.ctypes.data_as(_dp), tau,
+                                                  bytes(bytearray(int(f) for f in fx)), C.byref(w))
+    return xx
+
+
+def _in_cone(t, u, alpha, tol=1e-9):
+    """u in actual coordinates"""
+    if t == CONE_STANDARD_SOC:
+        return np.linalg.norm(u[:-1]) <= u[-1] + tol * (1 + abs(u[-1]))
+    if t == CONE_ROTATED_SOC:
+        s, tt = u[-2], u[-1]
+        return s >= -tol and tt >= -tol and u[:-2] @ u[:-2] <= 2 * s * tt + tol * (1 + abs(s * tt))
+    if t == CONE_EXPONENTIAL:
+        x, y, z = u
+        if y > tol and z > 0:
+            return math.log(y) + x / y <= math.log(z) + 1e-7 * (1 + abs(math.log(z)))
+        return abs(y) <= tol and x <= tol and z >= -tol
+    x, y, z = u
+    if x < -tol or y < -tol:
+        return False
+    return abs(z) <= max(x, 0.0) ** alpha * max(y, 0.0) ** (1 - alpha) + tol * (1 + abs(z))
+
+
+def _candidate(rng, t, L, alpha, fx, fv):
+    """A random feasible point of the section (actual coordinates), or None."""
+    u = np.where(fx, fv, 0.0).astype(float)
+    free = ~fx
+    if t == CONE_STANDARD_SOC:
+        nv = L - 1
+        u[:nv][free[:nv]] = rng.standard_normal(free[:nv].sum()) * rng.uniform(0.1, 3.0)
+        if fx[-1]:
+            fixed2 = np.sum(u[:nv][fx[:nv]] ** 2)
+            r2 = u[-1] ** 2 - fixed2
+            f2 = np.sum(u[:nv][free[:nv]] ** 2)
+            if f2 > 0:
+                u[:nv][free[:nv]] *= math.sqrt(max(r2, 0.0) / f2) * rng.uniform(0, 1)
+        else:
+            u[-1] = np.linalg.norm(u[:nv]) + rng.exponential(0.5)
+        return u
+    if t == CONE_ROTATED_SOC:
+        nv = L - 2
+        u[:nv][free[:nv]] = rng.standard_normal(free[:nv].sum()) * rng.uniform(0.1, 3.0)
+        n2 = u[:nv] @ u[:nv]
+        if fx[-2] and fx[-1]:
+            r2 = 2 * u[-2] * u[-1] - np.sum(u[:nv][fx[:nv]] ** 2)
+            f2 = np.sum(u[:nv][free[:nv]] ** 2)
+            if f2 > 0:
+                u[:nv][free[:nv]] *= math.sqrt(max(r2, 0.0) / f2) * rng.uniform(0, 1)
+        elif fx[-2]:
+            if u[-2] <= 0:
+                u[:nv][free[:nv]] = 0.0
+                u[-1] = rng.exponential(1.0)
+            else:
+                u[-1] = n2 / (2 * u[-2]) + rng.exponential(0.5)
+        elif fx[-1]:
+            if u[-1] <= 0:
+                u[:nv][free[:nv]] = 0.0
+                u[-2] = rng.exponential(1.0)
+            else:
+                u[-2] = n2 / (2 * u[-1]) + rng.exponential(0.5)
+        else:
+            u[-2] = rng.exponential(1.0) + 1e-3
+            u[-1] = n2 / (2 * u[-2]) + rng.exponential(0.5)
+        return u
+    if t == CONE_EXPONENTIAL:
+        x, y, z = u
+        if not fx[1]:
+            y = rng.exponential(1.0) + 1e-3
+        if fx[0] and fx[2]:  # y in an interval: search a feasible one
+            ys = np.exp(rng.uniform(-6, 6, 64))
+            ok = [yy for yy in ys if math.log(yy) + x / yy <= math.log(z)] if z > 0 else []
+            if not ok:
+                return None
+            y = float(rng.choice(ok))
+        elif fx[2]:
+            if z <= 0:
+                return None
+            x = y * (math.log(z) - math.log(y)) - rng.exponential(0.5) if y > 0 else -rng.exponential(1.0)
+        else:
+            if not fx[0]:
+                x = rng.standard_normal()
+            z = y * math.exp(x / y) + rng.exponential(0.5) if y > 0 else rng.exponential(1.0)
+        u[:] = x, y, z
+        return u
+    x, y, z = u
+    if not fx[0]:
+        x = rng.exponential(1.0)
+    if not fx[1]:
+        y = rng.exponential(1.0)
+    if fx[2]:
+        need = abs(z)
+        if not fx[0]:
+            x = (need / max(y, 1e-300) ** (1 - alpha)) ** (1 / alpha) + rng.exponential(0.5) if need > 0 else x
+        elif not fx[1]:
+            y = (need / max(x, 1e-300) ** alpha) ** (1 / (1 - alpha)) + rng.exponential(0.5) if need > 0 else y
+    else:
+        z = rng.uniform(-1, 1) * x ** alpha * y ** (1 - alpha)
+    u[:] = x, y, z
+    return u
+
+
+def _patterns(t, L):
+    if t in (CONE_EXPONENTIAL, CONE_POWER):
+        return [[i] for i in range(3)] + [[0, 1], [1, 2], [0, 2]]
+    if t == CONE_STANDARD_SOC:
+        return [[L - 1], [L - 2], [0], [0, L - 1], [0, 1, L - 2]]
+    return [[L - 2], [L - 1], [L - 2, L - 1], [0], [0, L - 1], [0, L - 2]]
+
+
+def _section_point(rng, t, L, alpha, pattern):
+    """Fixed values from a strictly feasible point of moderate size, so the
+    section is nonempty; returns (fx mask, the point, actual coordinates).
+    Exponential points keep |x / y| <= 2: far outside the cone the
+    objective of the reference's golden-section slices (fixed x or fixed z)
+    can have two local minima in y, and like the reference the oracle may
+    return the farther one there."""
+    fx = np.zeros(L, dtype=bool)
+    fx[pattern] = True
+    if t == CONE_EXPONENTIAL:
+        x, y = rng.uniform(-1, 1), rng.uniform(0.5, 2.0)
+        base = np.array([x, y, y * math.exp(x / y) + rng.uniform(0.1, 1.0)])
+    else:
+        base = _candidate(rng, t, L, alpha, np.zeros(L, bool), np.zeros(L))
+    return fx, base
+
+
+CONE_KINDS = [(CONE_STANDARD_SOC, 6, 0.0), (CONE_STANDARD_SOC, 2, 0.0), (CONE_ROTATED_SOC, 5, 0.0),
+              (CONE_ROTATED_SOC, 1, 0.0), (CONE_EXPONENTIAL, 1, 0.0), (CONE_POWER, 1, 0.35), (CONE_POWER, 1, 0.7)]
+
+
+@pytest.mark.parametrize("kind", range(len(CONE_KINDS)))
+def test_oracle_section_projection_is_nearest(oracle, kind):
+    t, vd, alpha = CONE_KINDS[kind]
+    L = 3 if t in (CONE_EXPONENTIAL, CONE_POWER) else vd + 2
+    rng = np.random.default_rng(500 + kind)
+    checked = 0
+    for pattern in _patterns(t, L):
+        for trial in range(12):
+            fx, base = _section_point(rng, t, L, alpha, pattern)
+            d = rng.uniform(0.5, 2.0, L)
+            q = rng.uniform(0.0, 2.0, L) if trial % 3 == 2 else None
+            tau = 0.7 if q is not None else 0.0
+            a = np.where(fx, base, base + rng.standard_normal(L) * rng.choice([0.3, 1.0, 1.8]))
+            x_in = a * d
+            p = _oracle_project(oracle, t, vd, alpha, x_in, d, fx, q, tau)
+            u = p / d
+            assert np.array_equal(p[fx], x_in[fx]), "a fixed slot moved"
+            assert _in_cone(t, u, alpha, 1e-7), (t, pattern, u)
+            om = (1.0 + (tau * q if q is not None else 0.0)) * d * d
+            dist = np.sum(om * (u - a) ** 2)
+            for _ in range(40):
+                cand = _candidate(rng, t, L, alpha, fx, np.where(fx, a, 0.0))
+                if cand is None or not _in_cone(t, cand, alpha, 1e-12):
+                    continue
+                cd = np.sum(om * (cand - a) ** 2)
+                assert dist <= cd * (1 + 1e-6) + 1e-9, (t, pattern, dist, cd)
+                checked += 1
+    assert checked > 100
+
+
+# ---------------- validation and known answers ----------------
+
+def _empty_cone_problem(t):
+    """test/test_conic_kkt_termination.c:8-26: three variables in one block
+    (v_dim 1), no rows, zero objective."""
+    return Problem(c=np.zeros(3), A=CsrMatrix(0, 3, np.array([0]), np.zeros(0, np.int32), np.zeros(0)),
+                   cones=[Cone(t, 0, 1, 0.5 if t == CONE_POWER else 0.0)])
+
+
+VALIDATION = [  # (cone, fixed slots, accepted) -- test/test_conic_kkt_termination.c:48-107
+    (CONE_STANDARD_SOC, [(1, 1.0)], True),
+    (CONE_EXPONENTIAL, [(0, 0.0)], True),
+    (CONE_ROTATED_SOC, [(1, 1.0)], True),
+    (CONE_STANDARD_SOC, [(0, 2.0), (2, 1.0)], False),
+    (CONE_EXPONENTIAL, [(0, 1.0), (2, 1.0)], False),
+    (CONE_ROTATED_SOC, [(0, 1.0), (1, 0.0)], False),
+    # the remaining rules of the reference's pdhcg_validate_fixed_cone_sections (src/pdhcg.c:729-892)
+    (CONE_EXPONENTIAL, [(1, -1.0)], False),
+    (CONE_EXPONENTIAL, [(0, 1.0), (2, math.e + 1e-9)], True),
+    (CONE_POWER, [(0, -1.0)], False),
+    (CONE_POWER, [(0, 0.0), (2, 1.0)], False),
+    (CONE_POWER, [(0, 1.0), (1, 1.0), (2, 1.5)], False),
+    (CONE_POWER, [(0, 1.0), (1, 4.0), (2, 1.5)], True),
+    (CONE_ROTATED_SOC, [(1, 2.0), (2, -0.5)], False),
+    (CONE_ROTATED_SOC, [(0, 2.0), (1, 1.0), (2, 2.0)], True),
+    (CONE_ROTATED_SOC, [(0, 2.0), (1, 1.0), (2, 1.9)], False),
+]
+
+
+@pytest.mark.parametrize("case", range(len(VALIDATION)))
+def test_fixed_section_validation(lib, case):
+    t, fixes, ok = VALIDATION[case]
+    p = _empty_cone_problem(t)
+    p.fixed = [(0, s, v) for s, v in fixes]
+    prob, keep = capi.build(lib, p)
+    assert prob
+    assert (lib.pdhcg_b200_validate_fixed_sections(prob) == 0) == ok
+    lib.qp_problem_free(prob)
+
+
+def test_set_cone_fixed_rules(lib):
+    """set_cone_fixed refuses PSD blocks, slots out of range and non-finite
+    values; clearing warm starts keeps fixed values (reference
+    test/test_conic_kkt_termination.c:28-46, src/pdhcg.c:620-666)."""
+    p = _empty_cone_problem(CONE_STANDARD_SOC)
+    prob, keep = capi.build(lib, p)
+    assert lib.set_cone_fixed(prob, 0, 3, 1.0) != 0
+    assert lib.set_cone_fixed(prob, 1, 0, 1.0) != 0
+    assert lib.set_cone_fixed(prob, 0, 0, float("nan")) != 0
+    assert lib.set_cone_fixed(prob, 0, 1, 1.25) == 0
+    start = np.array([2.0, 1.25, 3.0])
+    lib.set_start_values(prob, start.ctypes.data_as(_dp), None)
+    lib.set_start_values(prob, None, None)
+    ps = prob.contents.primal_start
+    assert [ps[0], ps[1], ps[2]] == [0.0, 1.25, 0.0]
+    lib.qp_problem_free(prob)
+
+
+def _one_row(t, col, coef, rhs, c, start, fixes, alpha=0.0):
+    p = Problem(c=np.array(c, float), A=CsrMatrix(1, 3, np.array([0, 1]), np.array([col], np.int32),
+                                                  np.array([coef])),
+                con_lb=np.array([rhs]), con_ub=np.array([rhs]), cones=[Cone(t, 0, 1, alpha)],
+                primal_start=np.array(start, float), dual_start=np.array([0.0]))
+    p.fixed = [(0, s, v) for s, v in fixes]
+    return p
+
+
+def _kkt_params(norm, limit=1, freq=1):
+    return {"optimality_norm": norm, "l_inf_ruiz_iterations": 0, "has_pock_chambolle_alpha": False,
+            "bound_objective_rescaling": False, "termination_evaluation_frequency": freq,
+            "termination_criteria.eps_optimal_relative": 1e-8, "termination_criteria.eps_feasible_relative": 1e-8,
+            "termination_criteria.iteration_limit": limit}
+
+
+def _soc_w_zero(vd):
+    """test/test_conic_kkt_termination.c:172-236: min w with only w = 0 fixed,
+    zero start: optimal at iteration 0."""
+    c = np.zeros(vd + 2)
+    c[vd] = 1.0
+    p = Problem(c=c, A=CsrMatrix(0, vd + 2, np.array([0]), np.zeros(0, np.int32), np.zeros(0)),
+                cones=[Cone(CONE_STANDARD_SOC, 0, vd)], primal_start=np.zeros(vd + 2))
+    p.fixed = [(0, vd, 0.0)]
+    return p
+
+
+# name -> (problem, params, expected status, expected count or None for > 0, checks)
+def _known(norm):
+    return {
+        "soc_w_zero_1": (lambda: _soc_w_zero(1), _kkt_params(norm), "OPTIMAL", 0),
+        "soc_w_zero_32": (lambda: _soc_w_zero(32), _kkt_params(norm), "OPTIMAL", 0),
+        # :238-304 s = t = 1 fixed: |x| <= sqrt 2, a tiny row makes the first step large
+        "rsoc_large_step": (lambda: _one_row(CONE_ROTATED_SOC, 1, 1e-9, 1e-9, [-1, 0, 0], [0.5, 1, 1],
+                                             [(1, 1.0), (2, 1.0)]), _kkt_params(norm), "ITERATION_LIMIT", 1),
+        # :306-370 z = 1 fixed
+        "soc_large_step": (lambda: _one_row(CONE_STANDARD_SOC, 2, 1e-9, 1e-9, [-1, 0, 0], [0.5, 0, 1],
+                                            [(2, 1.0)]), _kkt_params(norm), "ITERATION_LIMIT", 1),
+        # :379-444 x = y = 1 fixed, alpha 0.5: |z| <= 1
+        "pow_large_step": (lambda: _one_row(CONE_POWER, 0, 1e-9, 1e-9, [0, 0, -1], [1, 1, 0.5],
+                                            [(0, 1.0), (1, 1.0)], 0.5), _kkt_params(norm), "ITERATION_LIMIT", 1),
+        # :446-512 y = 1 fixed, min z over z >= exp(x)
+        "exp_large_step": (lambda: _one_row(CONE_EXPONENTIAL, 0, 1e-10, 0.0, [0, 0, 1], [0, 1, 2], [(1, 1.0)]),
+                           _kkt_params(norm), "ITERATION_LIMIT", 1),
+    }
+
+
+KNOWN_FIXED = {f"{k}_{'l2' if norm == NORM_L2 else 'linf'}": v for norm in (NORM_LINF, NORM_L2)
+               for k, v in _known(norm).items()}
+
+
+def exp_log2():
+    """test/test_conic_kkt_termination.c:515-560: min -x s.t. z = 2 (a row of
+    coefficient 1e-12), y = 1 fixed: x = log 2 after more than 0 iterations."""
+    p = _one_row(CONE_EXPONENTIAL, 2, 1e-12, 2e-12, [-1, 0, 0], [0, 1, 2], [(1, 1.0)])
+    prm = _kkt_params(NORM_L2, limit=1000000, freq=200)
+    del prm["optimality_norm"]
+    return p, prm
+
+
+def _solve(solver, lib, p, params, oracle=False):
+    prob, keep = capi.build(lib, p)
+    assert prob
+    prm = capi.default_params(lib, **params)
+    r = (solver.oracle_solve if oracle else solver.solve_qp_problem)(prob, C.byref(prm))
+    assert r
+    m = p.A.m if p.A is not None else 0
+    d = capi.result_dict(r, p.n, max(m, 1))
+    (solver.oracle_result_free if oracle else solver.pdhcg_result_free)(r)
+    lib.qp_problem_free(prob)
+    return d
+
+
+def _check_known(d, status, count):
+    assert d["status"] == status, (d["status"], d["total_count"])
+    assert d["total_count"] == count, d["total_count"]
+
+
+@pytest.mark.parametrize("name", sorted(KNOWN_FIXED))
+def test_oracle_fixed_known_answers(oracle, lib, name):
+    mk, prm, status, count = KNOWN_FIXED[name]
+    _check_known(_solve(oracle, lib, mk(), prm, oracle=True), status, count)
+
+
+def test_oracle_fixed_exp_log2(oracle, lib):
+    p, prm = exp_log2()
+    d = _solve(oracle, lib, p, prm, oracle=True)
+    assert d["status"] == "OPTIMAL" and d["total_count"] > 0
+    assert abs(d["x"][0] - math.log(2.0)) <= 1e-7
+    assert d["x"][1] == 1.0
+
+
+# ---------------- GPU ----------------
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(KNOWN_FIXED))
+def test_gpu_fixed_known_answers(lib, name):
+    mk, prm, status, count = KNOWN_FIXED[name]
+    _check_known(_solve(lib, lib, mk(), prm), status, count)
+
+
+@pytest.mark.gpu
+def test_gpu_fixed_exp_log2(lib):
+    p, prm = exp_log2()
+    d = _solve(lib, lib, p, prm)
+    assert d["status"] == "OPTIMAL" and d["total_count"] > 0
+    assert abs(d["x"][0] - math.log(2.0)) <= 1e-7
+    assert d["x"][1] == 1.0
+
+
+@pytest.mark.gpu
+def test_gpu_refuses_empty_sections(lib):
+    p = _empty_cone_problem(CONE_STANDARD_SOC)
+    p.fixed = [(0, 0, 2.0), (0, 2, 1.0)]
+    prob, keep = capi.build(lib, p)
+    prm = capi.default_params(lib)
+    assert not lib.solve_qp_problem(prob, C.byref(prm))
+    lib.qp_problem_free(prob)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", range(len(CONE_KINDS)))
+def test_gpu_section_projection_matches_oracle(lib, oracle, kind):
+    """pdhcg_b200_project_cone_sections against the oracle, many blocks of
+    one kind (every fixed-slot pattern), with and without a diagonal
+    metric; a second call reuses the multipliers of the first."""
+    import torch
+    t, vd, alpha = CONE_KINDS[kind]
+    L = 3 if t in (CONE_EXPONENTIAL, CONE_POWER) else vd + 2
+    rng = np.random.default_rng(900 + kind)
+    blocks = []
+    for pattern in _patterns(t, L):
+        for trial in range(20):
+            fx, base = _section_point(rng, t, L, alpha, pattern)
+            d = rng.uniform(0.5, 2.0, L)
+            a = np.where(fx, base, base + rng.standard_normal(L) * rng.choice([0.3, 2.0, 6.0]))
+            blocks.append((fx, a * d, d))
+    nb = len(blocks)
+    x = np.concatenate([b[1] for b in blocks])
+    d = np.concatenate([b[2] for b in blocks])
+    fx = np.concatenate([b[0] for b in blocks]).astype(np.uint8)
+    q = rng.uniform(0.0, 2.0, len(x))
+    starts = np.arange(nb, dtype=np.int32) * L
+    for tau, qq in ((0.0, None), (0.7, q)):
+        def dev(a, dt):
+            return torch.tensor(a, dtype=dt, device="cuda")
+        # every device array stays referenced until the call has finished
+        xd = dev(x, torch.float64)
+        warm = torch.zeros(nb, dtype=torch.float64, device="cuda")
+        st_d, vd_d = dev(starts, torch.int32), dev(np.full(nb, vd, np.int32), torch.int32)
+        tp_d, al_d = dev(np.full(nb, t, np.int32), torch.int32), dev(np.full(nb, alpha), torch.float64)
+        fx_d, d_d = dev(fx, torch.uint8), dev(d, torch.float64)
+        q_d = dev(qq, torch.float64) if qq is not None else None
+        ptr = lambda a: C.c_void_p(a.data_ptr()) if a is not None else None
+        lib.pdhcg_b200_project_cone_sections.restype = C.c_int
+        rc = lib.pdhcg_b200_project_cone_sections(nb, ptr(st_d), ptr(vd_d), ptr(tp_d), ptr(al_d), ptr(fx_d), ptr(xd),
+                                                  ptr(d_d), ptr(q_d), C.c_double(tau), ptr(warm), None)
+        assert rc == 0
+        torch.cuda.synchronize()
+        got = xd.cpu().numpy()
+        for b in range(nb):
+            sl = slice(b * L, (b + 1) * L)
+            want = _oracle_project(oracle, t, vd, alpha, x[sl], d[sl], fx[sl].astype(bool),
+                                   None if qq is None else qq[sl], tau)
+            np.testing.assert_allclose(got[sl], want, rtol=1e-7, atol=1e-9, err_msg=f"block {b}")
+
+
+FIXED_CASES = {
+    "fixed_lp": lambda: instances.fixed_cone_qp(seed=21),
+    "fixed_diag_qp": lambda: instances.fixed_cone_qp(seed=22, with_q=True),
+    "fixed_sparse_qp": lambda: instances.fixed_cone_qp(seed=23, sparse_q=True, nexp=3, npow=3),
+}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(FIXED_CASES))
+def test_gpu_fixed_instances_match_oracle(lib, oracle, name):
+    """Seeded instances with fixed slots: the same status, iterations within
+    2 % (+200), the objective within 1e-5 and the fixed slots exact.  The
+    sparse-Q instance (inner BB solve) is compared after 3000 iterations:
+    with or without fixed slots its dual residual levels off near 5e-2, so
+    it does not reach the tolerance; the reference's own build does the
+    same (60000 iterations: the same dual residual and objective)."""
+    p = FIXED_CASES[name]()
+    sparse = name == "fixed_sparse_qp"
+    prm = {"termination_criteria.eps_optimal_relative": 1e-6, "termination_criteria.eps_feasible_relative": 1e-6,
+           "termination_criteria.iteration_limit": 3000 if sparse else 60000}
+    g = _solve(lib, lib, p, prm)
+    o = _solve(oracle, lib, p, prm, oracle=True)
+    want = "ITERATION_LIMIT" if sparse else "OPTIMAL"
+    assert g["status"] == o["status"] == want, (g["status"], o["status"])
+    assert abs(g["total_count"] - o["total_count"]) <= 0.02 * o["total_count"] + 200, (g["total_count"],
+                                                                                      o["total_count"])
+    ob = o["primal_objective_value"]
+    assert abs(g["primal_objective_value"] - ob) <= 1e-5 * (1 + abs(ob))
+    x = np.asarray(g["x"])
+    for ci, sl, v in p.fixed:
+        assert x[p.cones[ci].start + sl] == pytest.approx(v, rel=1e-12, abs=1e-12)
