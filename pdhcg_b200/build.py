@@ -12,13 +12,14 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpdhcg_b200.so")
 SOURCES = ["solver.cu", "batch.cu", "mlp.cu", "api.cpp", "mps.cpp", "qcqp.cpp"]
-HEADERS = ["device.cuh", "kernels.cuh", "residual.cuh", "setup.cuh", "bb.cuh", "internal.h"]
+HEADERS = ["device.cuh", "kernels.cuh", "residual.cuh", "setup.cuh", "bb.cuh", "section.cuh", "internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -41,7 +42,7 @@ def _stale() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
-    objs = []
+    objs, cmds = [], []
     nvcc = _nvcc()
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include")]
     for src in SOURCES:
@@ -54,8 +55,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
                    "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
-        subprocess.check_call(cmd)
+        cmds.append(cmd)
         objs.append(obj)
+    # the translation units compile side by side (solver.cu dominates)
+    with ThreadPoolExecutor(max_workers=len(cmds)) as pool:
+        for f in [pool.submit(subprocess.check_call, c) for c in cmds]:
+            f.result()
     tmp = LIB + ".tmp"
     cmd = [nvcc, *ARCH, "-shared", *objs, "-o", tmp, "-Xlinker", "-Bsymbolic", "-lz"]  # zlib: gzip MPS files
     if verbose:

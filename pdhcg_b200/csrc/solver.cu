@@ -843,15 +843,12 @@ int launch_primal_cones(const StepData<T> &D, const StepParams &P, const ConeSpl
         });
         ++launches;
     }
-    if (sp.n_sect > 0) { // blocks with fixed slots: section projectors
-        dispatch_s(S, [&](auto SC) {
-            int grid = grid_for(sp.n_sect, WARPS);
-            if (hasq)
-                primal_cone_kernel<SC.value, T, true, CONES_SECTION><<<grid, TPB, 0, s>>>(D, P, sp.sect_d, sp.n_sect);
-            else
-                primal_cone_kernel<SC.value, T, false, CONES_SECTION><<<grid, TPB, 0, s>>>(D, P, sp.sect_d,
-                                                                                           sp.n_sect);
-        });
+    if (sp.n_sect > 0) { // blocks with fixed slots: section projectors, one slot class (any block length)
+        int grid = grid_for(sp.n_sect, WARPS);
+        if (hasq)
+            primal_cone_kernel<8, T, true, CONES_SECTION><<<grid, TPB, 0, s>>>(D, P, sp.sect_d, sp.n_sect);
+        else
+            primal_cone_kernel<8, T, false, CONES_SECTION><<<grid, TPB, 0, s>>>(D, P, sp.sect_d, sp.n_sect);
         ++launches;
     }
     return launches;
@@ -1191,14 +1188,16 @@ void Solve::setup_bb()
     int dev = 0, nsm = 0, per_sm = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    // problems with fixed cone slots take the widest slot class (one
+    // instantiation per row group serves every block length)
     dispatch_rg(GQ_, [&](auto GC) {
-        dispatch_s(S_, [&](auto SC) {
-            if (dp_.has_fixed)
-                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bb_kernel<GC.value, SC.value, true>, TPB, 0));
-            else
+        if (dp_.has_fixed)
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bb_kernel<GC.value, 8, true>, TPB, 0));
+        else
+            dispatch_s(S_, [&](auto SC) {
                 CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bb_kernel<GC.value, SC.value, false>, TPB,
                                                                  0));
-        });
+            });
     });
     int q_per_sm = 0;
     dispatch_rg(GQ_, [&](auto GC) {
@@ -1482,8 +1481,7 @@ void Solve::enqueue_step_bb(bool store_dual, bool want_fpe, double w)
     dispatch_rg(GQ_, [&](auto GC) {
         dispatch_s(S_, [&](auto SC) {
             void *args[] = {&D, &BP};
-            void *k = dp_.has_fixed ? (void *)bb_kernel<GC.value, SC.value, true>
-                                    : (void *)bb_kernel<GC.value, SC.value, false>;
+            void *k = dp_.has_fixed ? (void *)bb_kernel<GC.value, 8, true> : (void *)bb_kernel<GC.value, SC.value, false>;
             CK(cudaLaunchCooperativeKernel(k, bb_grid_, TPB, args, 0, s));
         });
     });
@@ -1719,12 +1717,10 @@ void Solve::enqueue_residual_t(bool want_dist)
     P.s_aug = sa;
     P.sb = sb_;
     int nb = D.rows_blocks + D.free_blocks + D.cone_blocks + D.aff_blocks;
-    dispatch_s(std::max(S_, dp_.S_aff), [&](auto SC) {
-        if (dp_.has_fixed)
-            residual_kernel<SC.value, VT, true><<<nb, TPB, 0, s>>>(D, P);
-        else
-            residual_kernel<SC.value, VT, false><<<nb, TPB, 0, s>>>(D, P);
-    });
+    if (dp_.has_fixed) // one slot class for problems with fixed cone slots
+        residual_kernel<8, VT, true><<<nb, TPB, 0, s>>>(D, P);
+    else
+        dispatch_s(std::max(S_, dp_.S_aff), [&](auto SC) { residual_kernel<SC.value, VT, false><<<nb, TPB, 0, s>>>(D, P); });
     fold_partials_kernel<<<1, TPB, 0, s>>>(partials_, nb, RS_COUNT, res_ops_d_, scal_d_);
     stats_.kernel_launches += 2;
     stats_.evaluations++;

@@ -461,3 +461,33 @@ def test_gpu_fixed_instances_match_oracle(lib, oracle, name):
     x = np.asarray(g["x"])
     for ci, sl, v in p.fixed:
         assert x[p.cones[ci].start + sl] == pytest.approx(v, rel=1e-12, abs=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["fixed_lp", "fixed_diag_qp"])
+def test_gpu_fixed_mixed_precision(lib, name):
+    """FP32 bulk phase + FP64 polish with fixed slots: the FP32 copies of
+    the pinned bounds round the fixed values, the FP64 polish restores
+    them; same status and objective as plain FP64, fixed slots exact."""
+    from pdhcg_b200 import native
+    p = FIXED_CASES[name]()
+    params = {"termination_criteria.eps_optimal_relative": 1e-6, "termination_criteria.eps_feasible_relative": 1e-6,
+              "termination_criteria.iteration_limit": 60000}
+    out = []
+    for precision in (0, 1):
+        prob, keep = capi.build(lib, p)
+        prm = capi.default_params(lib, **params)
+        o = native.default_options(precision=precision)
+        r = lib.pdhcg_b200_solve(prob, C.byref(prm), C.byref(o))
+        assert r
+        out.append((capi.result_dict(r, p.n, p.A.m), native.last_stats()))
+        lib.pdhcg_result_free(r)
+        lib.qp_problem_free(prob)
+    (f64, _), (mix, st) = out
+    assert f64["status"] == mix["status"] == "OPTIMAL"
+    assert st["fp32_iterations"] > 0
+    ob = f64["primal_objective_value"]
+    assert abs(mix["primal_objective_value"] - ob) <= 1e-5 * (1 + abs(ob))
+    x = np.asarray(mix["x"])
+    for ci, sl, v in p.fixed:
+        assert x[p.cones[ci].start + sl] == pytest.approx(v, rel=1e-12, abs=1e-12)
