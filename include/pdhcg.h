@@ -45,7 +45,11 @@ qp_problem_t *create_qp_problem(const double *objective_c,
  * Replaces reference set_start_values (include/pdhcg.h:49, src/pdhcg.c:569-618). */
 void set_start_values(qp_problem_t *prob, const double *primal, const double *dual);
 
-/* Pin one slot of a variable cone to a value; returns 0 or -1.
+/* Pin one slot of a variable cone (SOC, rotated SOC, exponential or power;
+ * not PSD) to a finite value; returns 0 or -1.  The value also becomes that
+ * slot's primal start.  solve_qp_problem keeps the slot at the value and
+ * projects the block's free slots onto the cone's section through the
+ * fixed values; it returns NULL (with a message) when a section is empty.
  * Replaces reference set_cone_fixed (include/pdhcg.h:51, src/pdhcg.c:620-666). */
 int set_cone_fixed(qp_problem_t *prob, int cone_idx, int slot, double value);
 
