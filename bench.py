@@ -51,6 +51,10 @@ WORKLOADS = {
                           "Q diag U(1e-4, 1e-2), budget + 500 sector + 100 exposure rows, RSOC tracking-error "
                           "block, x in [0, 0.02], eps 1e-6",
                   "mixed": False, "l2": "working set (A, R and R^T, >700 MB) larger than L2"},
+    "fixed_soc": {"make": lambda scale, r: instances.fixed_cone_qp(seed=21 + r, nsoc=400, soc_len=50),
+                  "desc": "fixed_soc: conic LP with 400 SOC blocks of 50, 4 RSOC, 6 EXP and 6 POW blocks and "
+                          "slots of about half the blocks fixed by set_cone_fixed (n=20128), eps 1e-6",
+                  "mixed": False, "l2": "L2-resident working set: time to tolerance"},
 }
 
 
@@ -549,7 +553,7 @@ def main():
     ap.add_argument("--iters", type=int, default=None, help="iteration cap (profiling only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="soc_qp",
-                    choices=["soc_qp", "sparse_qp", "portfolio", "mpc_batch", "warm_start"],
+                    choices=["soc_qp", "sparse_qp", "portfolio", "fixed_soc", "mpc_batch", "warm_start"],
                     help="soc_qp: the headline single-instance workload; sparse_qp: sparse-Q QP (inner BB "
                          "solve); portfolio: low-rank portfolio QP; mpc_batch: the batched workload; "
                          "warm_start: the learned warm start on the parametric family")
