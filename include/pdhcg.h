@@ -62,6 +62,9 @@ int set_cone_fixed(qp_problem_t *prob, int cone_idx, int slot, double value);
 qp_problem_t *qcqp_to_socp_qp(const qp_problem_t *orig_qcqp, cone_type_t default_type);
 
 /* Solve on the current CUDA device; params == NULL means defaults.
+ * A NaN anywhere in c, the bounds or the matrix values, or an infinite
+ * entry of c or of a matrix, gives NULL with a message instead of a run
+ * that would iterate on NaN until a limit.
  * Replaces reference solve_qp_problem (include/pdhcg.h:56, src/pdhcg.c:894-922). */
 pdhcg_result_t *solve_qp_problem(const qp_problem_t *prob, const pdhg_parameters_t *params);
 

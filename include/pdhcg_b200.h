@@ -88,6 +88,17 @@ typedef struct {
 
 int pdhcg_b200_last_stats(pdhcg_b200_stats_t *out);
 
+/* The rescaling a solve would apply to prob under params, computed on the
+ * device (Curtis-Reid, Ruiz, Pock-Chambolle, bound/objective scaling and
+ * the cone-preserving adjustment; reference rescale_problem,
+ * src/preconditioner.c:654-713) and copied out: con_rescale[num_constraints]
+ * and var_rescale[num_variables] are the cumulative row and column factors
+ * (the reference's rescale_info_t con_rescale / var_rescale), bound_obj[0]
+ * the bound rescaling and bound_obj[1] the objective rescaling.  Returns 0,
+ * or -1 (NULL arguments, a problem the solver refuses, a device error). */
+int pdhcg_b200_rescaling(const qp_problem_t *prob, const pdhg_parameters_t *params, double *con_rescale,
+                         double *var_rescale, double *bound_obj);
+
 /* Cancellation.  g_pdhcg_cancel_request is the reference's flag (reference
  * src/pdhcg.c:31), exported under the same name so that its Python binding
  * (which declares it extern and sets it from a SIGINT handler, reference
@@ -242,8 +253,11 @@ int pdhcg_b200_validate_fixed_sections(const qp_problem_t *prob);
  * ((PDHCG_B200_NOALLOC_MAX_CONES + 2) ints); every call writes it before
  * reading it, so nothing needs to start at zero.
  * - The first call on each device looks up that array's address
- *   (cudaGetSymbolAddress with the device current); make that first call
- *   before any stream capture.
+ *   (cudaGetSymbolAddress with the device current) and keeps it for the
+ *   life of the process; make that first call before any stream capture.
+ *   The kept address belongs to the device's context at that time: after a
+ *   cudaDeviceReset of that device, do not call this entry point again in
+ *   the same process.
  * - Calls on the same device share the scratch: two calls that overlap in
  *   time (other threads, or other streams before the first has finished)
  *   race.  Serialise them.

@@ -472,6 +472,14 @@ __device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform
                 break;
             }
             double nx = lam - f / df;
+            // a Newton step below the resolution of lam cannot improve it:
+            // stop there (without this, rounding that keeps |f| above its
+            // tolerance sent the search into ~40 bisections of the bracket,
+            // and the warp holding that block set the length of the launch)
+            if (isfinite(nx) && fabs(nx - lam) <= 2.0 * DBL_EPSILON * fabs(lam)) {
+                done = true;
+                break;
+            }
             if (!isfinite(nx) || !(nx > lo && nx < hi))
                 nx = isfinite(hi) ? 0.5 * (lo + hi) : 2.0 * lam;
             lam = nx;
@@ -640,6 +648,8 @@ __device__ void warp_project_rsoc(WarpSlots<S> &sl, int L, int lane, bool unifor
                                 (isfinite(hi) && hi - lo <= 1e-13 * (1.0 + hi + lo))))
                 break;
             double nx = lam - f / df;
+            if (isfinite(f) && isfinite(nx) && fabs(nx - lam) <= 2.0 * DBL_EPSILON * fabs(lam))
+                break; // step below the resolution of lam (as for the SOC)
             if (!isfinite(nx) || !(nx > lo && nx < hi))
                 nx = isfinite(hi) ? 0.5 * (lo + hi) : 2.0 * lam;
             lam = nx;

@@ -84,6 +84,19 @@ __global__ void dense_rows_check_kernel(int rows, int cols, const int *rp, const
         atomicOr(bad, 1);
 }
 
+// *flag = 1 when an entry of v[0, n) is NaN (strict = 0: bounds, where
+// +-inf means "no bound") or not finite (strict = 1: objective, matrices)
+__global__ void nonfinite_kernel(const double *v, long long n, int strict, int *flag)
+{
+    bool bad = false;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double x = v[i];
+        bad |= strict ? !isfinite(x) : isnan(x);
+    }
+    if (__any_sync(FULL, bad) && (threadIdx.x & 31) == 0)
+        atomicOr(flag, 1);
+}
+
 __global__ void iota_kernel(int *v, int n)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)

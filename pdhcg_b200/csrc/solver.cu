@@ -677,9 +677,15 @@ public:
         }
     }
     pdhcg_result_t *run();
+    // the device rescaling only (upload, transpose, rescale), factors copied
+    // to the host: con_rescale[orig rows], var_rescale[n], bound_obj[2]
+    void rescaling(double *con_rescale, double *var_rescale, double *bound_obj);
 
 private:
     void build_host();
+    void setup_scratch();
+    void check_finite();
+    int *nonfinite_ = nullptr;
     void upload_and_preprocess();
     void rescale();
     void init_state();
@@ -2150,20 +2156,10 @@ pdhcg_result_t *Solve::make_result()
     return r;
 }
 
-pdhcg_result_t *Solve::run()
+// Reduction scratch (block partials sized for the widest user, folded
+// scalars, the pinned host mirror) and the fold operators.
+void Solve::setup_scratch()
 {
-    auto t_setup = std::chrono::steady_clock::now();
-    CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
-    ar_.s = st_;
-    dp_.ar.s = st_; // outputs kept with the device problem are allocated in this solve's order
-    build_host();
-    auto t_host = std::chrono::steady_clock::now();
-    stats_.host_copy_ms = std::chrono::duration<double, std::milli>(t_host - t_setup).count();
-    if (!dp_.unsupported.empty())
-        throw CudaError(dp_.unsupported);
-    upload_and_preprocess();
-    CK(cudaStreamSynchronize(st_));
-    stats_.upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host).count();
     // reduction scratch sized for the widest user
     // residual ranges: one warp per tile of 32 rows / per cone block
     res_rows_blocks_ = grid_for(dp_.aff_start.empty() ? ((long long)m_ + 31) / 32 : (long long)dp_.n_row_tiles, WARPS,
@@ -2198,6 +2194,69 @@ pdhcg_result_t *Solve::run()
         ray_d_ = ar_.alloc<double>(RN_COUNT + RY_COUNT);
         CK(cudaStreamSynchronize(st_)); // the uploads above read stack arrays
     }
+}
+
+// A NaN in c, the bounds or the matrix values, or an infinite entry of c
+// or of a matrix, would only be noticed as a NaN residual at the first
+// evaluation and then iterated on until a limit: refuse the problem.
+void Solve::check_finite()
+{
+    cudaStream_t s = st_;
+    nonfinite_ = ar_.alloc<int>(1);
+    CK(cudaMemsetAsync(nonfinite_, 0, sizeof(int), s));
+    nonfinite_kernel<<<grid_for(n_, TPB, 148 * 4), TPB, 0, s>>>(c_d_, n_, 1, nonfinite_);
+    nonfinite_kernel<<<grid_for(n_, TPB, 148 * 4), TPB, 0, s>>>(l_d_, n_, 0, nonfinite_);
+    nonfinite_kernel<<<grid_for(n_, TPB, 148 * 4), TPB, 0, s>>>(u_d_, n_, 0, nonfinite_);
+    nonfinite_kernel<<<grid_for(m_, TPB, 148 * 4), TPB, 0, s>>>(lc_d_, m_, 0, nonfinite_);
+    nonfinite_kernel<<<grid_for(m_, TPB, 148 * 4), TPB, 0, s>>>(uc_d_, m_, 0, nonfinite_);
+    nonfinite_kernel<<<grid_for(A_.nnz, TPB, 148 * 8), TPB, 0, s>>>(A_.v, A_.nnz, 1, nonfinite_);
+    if (Q_.nnz > 0)
+        nonfinite_kernel<<<grid_for(Q_.nnz, TPB, 148 * 8), TPB, 0, s>>>(Q_.v, Q_.nnz, 1, nonfinite_);
+    if (R_.nnz > 0)
+        nonfinite_kernel<<<grid_for(R_.nnz, TPB, 148 * 8), TPB, 0, s>>>(R_.v, R_.nnz, 1, nonfinite_);
+    int bad = 0;
+    CK(cudaMemcpyAsync(&bad, nonfinite_, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (bad)
+        throw CudaError("the problem holds NaN values, or infinite objective or matrix entries");
+}
+
+void Solve::rescaling(double *con_rescale, double *var_rescale, double *bound_obj)
+{
+    CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    ar_.s = st_;
+    dp_.ar.s = st_;
+    build_host();
+    if (!dp_.unsupported.empty())
+        throw CudaError(dp_.unsupported);
+    upload_and_preprocess();
+    check_finite();
+    setup_scratch();
+    rescale();
+    const int rows = dp_.dummy ? 0 : m_;
+    if (rows > 0)
+        CK(cudaMemcpyAsync(con_rescale, cr_d_, rows * sizeof(double), cudaMemcpyDeviceToHost, st_));
+    CK(cudaMemcpyAsync(var_rescale, vr_d_, n_ * sizeof(double), cudaMemcpyDeviceToHost, st_));
+    CK(cudaStreamSynchronize(st_));
+    bound_obj[0] = sb_;
+    bound_obj[1] = sc_;
+}
+
+pdhcg_result_t *Solve::run()
+{
+    auto t_setup = std::chrono::steady_clock::now();
+    CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    ar_.s = st_;
+    dp_.ar.s = st_; // outputs kept with the device problem are allocated in this solve's order
+    build_host();
+    auto t_host = std::chrono::steady_clock::now();
+    stats_.host_copy_ms = std::chrono::duration<double, std::milli>(t_host - t_setup).count();
+    if (!dp_.unsupported.empty())
+        throw CudaError(dp_.unsupported);
+    upload_and_preprocess();
+    check_finite();
+    stats_.upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host).count();
+    setup_scratch();
     // unscaled norms for the relative errors (reference src/solver_state.cu:854-934)
     {
         int nb = grid_for((long long)n_ + m_, TPB, 148 * 4);
@@ -2598,6 +2657,40 @@ int pdhcg_b200_last_stats(pdhcg_b200_stats_t *out)
     return 0;
 }
 
+int pdhcg_b200_rescaling(const qp_problem_t *prob, const pdhg_parameters_t *params, double *con_rescale,
+                         double *var_rescale, double *bound_obj)
+{
+    if (!prob || !var_rescale || !bound_obj || (prob->num_constraints > 0 && !con_rescale)) {
+        std::fprintf(stderr, "[pdhcg_b200_rescaling] invalid arguments\n");
+        return -1;
+    }
+    pdhg_parameters_t prm;
+    if (params)
+        prm = *params;
+    else
+        set_default_parameters(&prm);
+    try {
+        cudaStream_t us = nullptr;
+        CK(cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking));
+        std::unique_ptr<DeviceProblem> dp;
+        try {
+            dp = make_device_problem(prob, us);
+        } catch (...) {
+            cudaStreamDestroy(us);
+            throw;
+        }
+        cudaStreamDestroy(us);
+        pdhcg_b200_options_t opt;
+        pdhcg_b200_default_options(&opt);
+        Solve s(*dp, true, prm, opt);
+        s.rescaling(con_rescale, var_rescale, bound_obj);
+        return 0;
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "[pdhcg_b200_rescaling] %s\n", e.what());
+        return -1;
+    }
+}
+
 int pdhcg_b200_csr_spmv(int rows, const int *row_ptr, const int *col_ind, const double *val, const double *x,
                         double *y, void *stream)
 {
@@ -2625,9 +2718,12 @@ int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *co
     long long psd_total = 0;
     {
         std::vector<int> h(num_cones), t(num_cones), vd(num_cones);
-        cudaMemcpyAsync(h.data(), len, num_cones * sizeof(int), cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(t.data(), cone_type, num_cones * sizeof(int), cudaMemcpyDeviceToHost, s);
-        if (cudaStreamSynchronize(s) != cudaSuccess) {
+        // a failed enqueue would leave h and t unset: check every call
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(h.data(), len, num_cones * sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaMemcpyAsync(t.data(), cone_type, num_cones * sizeof(int), cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
             cudaFreeAsync(len, s);
             return -1;
         }
