@@ -70,7 +70,8 @@ EXPORTS = [
     "create_qp_problem", "set_start_values", "set_cone_fixed", "qcqp_to_socp_qp", "solve_qp_problem",
     "solve_qp_problem_distributed", "set_default_parameters", "pdhcg_result_free", "qp_problem_free",
     # additive entry points (include/pdhcg_b200.h)
-    "pdhcg_b200_default_options", "pdhcg_b200_solve", "pdhcg_b200_last_stats", "pdhcg_b200_csr_spmv",
+    "pdhcg_b200_default_options", "pdhcg_b200_solve", "pdhcg_b200_last_stats", "pdhcg_b200_rescaling",
+    "pdhcg_b200_csr_spmv",
     "pdhcg_b200_project_cones", "pdhcg_b200_pdhg_step", "pdhcg_b200_upload", "pdhcg_b200_solve_device",
     "pdhcg_b200_device_solution", "pdhcg_b200_device_problem_free", "pdhcg_b200_request_cancel",
     "cone_block_length", "pdhcg_b200_project_cones_noalloc", "pdhcg_b200_project_cone_sections",
@@ -104,6 +105,9 @@ def load(build: bool = True) -> C.CDLL:
     lib.pdhcg_b200_solve.argtypes = [P(capi.QpProblem), P(capi.PdhgParameters), P(Options)]
     lib.pdhcg_b200_last_stats.restype = C.c_int
     lib.pdhcg_b200_last_stats.argtypes = [P(Stats)]
+    dp = P(C.c_double)
+    lib.pdhcg_b200_rescaling.restype = C.c_int
+    lib.pdhcg_b200_rescaling.argtypes = [P(capi.QpProblem), P(capi.PdhgParameters), dp, dp, dp]
     lib.pdhcg_b200_csr_spmv.restype = C.c_int
     lib.pdhcg_b200_csr_spmv.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p]

@@ -28,7 +28,9 @@ def test_batch_matches_single_solves(lib, shape):
             1 + abs(ref["primal_objective_value"]))
         assert g["relative_primal_residual"] < EPS and g["relative_dual_residual"] < EPS
         assert g["relative_objective_gap"] < EPS
-        np.testing.assert_allclose(g["x"], ref["x"], atol=1e-2 * (1 + np.abs(ref["x"]).max()))
+        # FP32 storage against FP64: ~5e-6 relative measured against the reference build
+        np.testing.assert_allclose(g["x"], ref["x"], rtol=0, atol=1e-4 * (1 + np.abs(ref["x"]).max()))
+        np.testing.assert_allclose(g["y"], ref["y"], rtol=0, atol=1e-4 * (1 + np.abs(ref["y"]).max()))
 
 
 def test_batch_mixed_sizes_and_fallback(lib):

@@ -173,6 +173,10 @@ def _section_point(rng, t, L, alpha, pattern):
 
 CONE_KINDS = [(CONE_STANDARD_SOC, 6, 0.0), (CONE_STANDARD_SOC, 2, 0.0), (CONE_ROTATED_SOC, 5, 0.0),
               (CONE_ROTATED_SOC, 1, 0.0), (CONE_EXPONENTIAL, 1, 0.0), (CONE_POWER, 1, 0.35), (CONE_POWER, 1, 0.7)]
+# long blocks: 50 and 102 slots put slots in a lane's second and later
+# registers (several slots per lane in the warp-wide section projectors)
+LONG_KINDS = [(CONE_STANDARD_SOC, 48, 0.0), (CONE_STANDARD_SOC, 100, 0.0), (CONE_ROTATED_SOC, 48, 0.0),
+              (CONE_ROTATED_SOC, 100, 0.0)]
 
 
 @pytest.mark.parametrize("kind", range(len(CONE_KINDS)))
@@ -384,13 +388,14 @@ def test_gpu_refuses_empty_sections(lib):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", range(len(CONE_KINDS)))
+@pytest.mark.parametrize("kind", range(len(CONE_KINDS) + len(LONG_KINDS)))
 def test_gpu_section_projection_matches_oracle(lib, oracle, kind):
     """pdhcg_b200_project_cone_sections against the oracle, many blocks of
     one kind (every fixed-slot pattern), with and without a diagonal
-    metric; a second call reuses the multipliers of the first."""
+    metric; a second call reuses the multipliers of the first.  The kinds
+    include SOC and rotated-SOC blocks of 50 and 102 slots."""
     import torch
-    t, vd, alpha = CONE_KINDS[kind]
+    t, vd, alpha = (CONE_KINDS + LONG_KINDS)[kind]
     L = 3 if t in (CONE_EXPONENTIAL, CONE_POWER) else vd + 2
     rng = np.random.default_rng(900 + kind)
     blocks = []
@@ -434,6 +439,9 @@ FIXED_CASES = {
     "fixed_lp": lambda: instances.fixed_cone_qp(seed=21),
     "fixed_diag_qp": lambda: instances.fixed_cone_qp(seed=22, with_q=True),
     "fixed_sparse_qp": lambda: instances.fixed_cone_qp(seed=23, sparse_q=True, nexp=3, npow=3),
+    # SOC blocks of 50 slots: 48 vector slots, where the section dual
+    # residual of the block is 0 (the reference's block method)
+    "fixed_soc50": lambda: instances.fixed_cone_qp(seed=25, soc_len=50, nexp=0, npow=0),
 }
 
 
