@@ -7,13 +7,18 @@
 //   o  = U z + bu                     (out_dim = n + m: x then y, normalised)
 //   lw = wp . h2 + bp                 (log primal weight)
 //
-// Weights W are [out_features x in_features] row-major.  The products use
-// BF16 copies of the weights with FP32 accumulation; FP32 master copies take
-// the Adam updates.  Activations and gradients are FP32.  Every kernel here
-// (products, bias/ReLU, loss, column sums, Adam) is written for this file;
-// the products are tiled FP32-accumulate CUDA-core kernels: at these shapes
-// (a batch of 64 against 512-wide layers and a rank-64 head) a step is a few
-// microseconds of arithmetic and is bound by launch latency.
+// Weights W are [out_features x in_features] row-major.  Every product runs
+// on the tensor cores (mma.sync m16n8k16, BF16 operands, FP32
+// accumulation).  The weights enter as their BF16 copy; FP32 master copies
+// take the Adam updates.  Activations and gradients stay FP32: each such
+// operand is staged as a BF16 pair hi = bf16(v), lo = bf16(v - hi) (16
+// significant bits, ~8e-6 relative) and the products add hi.hi, hi.lo and
+// lo.hi, so the network is the BF16-weight, FP32-activation one.  Products with a long reduction and few output tiles (the
+// output head's dZ = dO U reduces over all n + m outputs) split K over the
+// grid and fold the partial tiles in a fixed order.  The loss of a training
+// run is accumulated on the device and read once at the end.  Every kernel
+// here (products, bias/ReLU, loss, column sums, Adam) is written for this
+// file.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -21,6 +26,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "pdhcg_b200.h"
@@ -41,62 +47,179 @@ using bf16 = __nv_bfloat16;
 __device__ __forceinline__ float ld(const float *p) { return *p; }
 __device__ __forceinline__ float ld(const bf16 *p) { return __bfloat162float(*p); }
 
-// C[M x N] = alpha * op(A)[M x K] * op(B)[K x N] + beta * C, FP32 accumulation.
-// op(A)(i, k) = TA ? A[k * lda + i] : A[i * lda + k]; op(B)(k, j) = TB ? B[j * ldb + k] : B[k * ldb + j].
-// 64 x 64 tiles, 256 threads, 4 x 4 outputs per thread, K in steps of 16.
-constexpr int GT = 64, GK = 16;
-template <bool TA, bool TB, typename AT, typename BT>
-__global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const AT *A, int lda, const BT *B, int ldb,
-                                                   float *C, int ldc, float alpha, float beta)
+// C[M x N] = alpha * op(A)[M x K] * op(B)[K x N] + beta * C on the tensor
+// cores.  op(A)(i, k) = TA ? A[k * lda + i] : A[i * lda + k];
+// op(B)(k, j) = TB ? B[j * ldb + k] : B[k * ldb + j].  A CTA of 4 warps owns
+// a 64 x 64 tile and walks K in steps of 32 (its K range is
+// [z kchunk, (z + 1) kchunk) for grid index z); each warp owns 32 x 32 as
+// 2 x 4 mma tiles of 16 x 8.  Operands are staged in shared memory as BF16,
+// FP32 ones as hi / lo pairs; rows of 32 + 8 elements (80 bytes: the
+// fragment loads of a warp hit 32 different banks).  With part != NULL the
+// CTA writes its FP32 tile to part[z] for splitk_fold_kernel instead of C.
+constexpr int TM = 64, TN = 64, TK = 32, TKP = TK + 8;
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2])
 {
-    __shared__ float As[GK][GT + 1];
-    __shared__ float Bs[GK][GT + 1];
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    const int i0 = blockIdx.y * GT, j0 = blockIdx.x * GT;
-    float acc[4][4] = {};
-    for (int k0 = 0; k0 < K; k0 += GK) {
-        for (int e = threadIdx.x; e < GK * GT; e += 256) {
-            int kk = e / GT, ii = e % GT;
-            int i = i0 + ii, k = k0 + kk;
-            As[kk][ii] = (i < M && k < K) ? ld(TA ? A + (size_t)k * lda + i : A + (size_t)i * lda + k) : 0.0f;
-            int j = j0 + ii;
-            Bs[kk][ii] = (j < N && k < K) ? ld(TB ? B + (size_t)j * ldb + k : B + (size_t)k * ldb + j) : 0.0f;
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+                 "{%8, %9}, {%0, %1, %2, %3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// v into its BF16 pair (hi, lo); a BF16 source is exact in hi alone
+__device__ __forceinline__ void split_bf16(float v, bf16 &hi, bf16 &lo)
+{
+    hi = __float2bfloat16_rn(v);
+    lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
+
+template <bool TA, bool TB, typename AT, typename BT>
+__global__ void __launch_bounds__(128) mma_gemm_kernel(int M, int N, int K, int kchunk, const AT *A, int lda,
+                                                       const BT *B, int ldb, float *C, int ldc, float alpha,
+                                                       float beta, float *part)
+{
+    constexpr bool SA = !std::is_same<AT, bf16>::value, SB = !std::is_same<BT, bf16>::value; // FP32: hi / lo
+    __shared__ __align__(16) bf16 As[SA ? 2 : 1][TM][TKP];
+    __shared__ __align__(16) bf16 Bs[SB ? 2 : 1][TN][TKP];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int i0 = blockIdx.y * TM, j0 = blockIdx.x * TN;
+    const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
+    float acc[2][4][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                acc[mt][nt][q] = 0.0f;
+    for (int k0 = kb; k0 < ke; k0 += TK) {
+        // stage op(A) and op(B)^T, the contiguous index of each source
+        // varying fastest across the threads
+        for (int e = threadIdx.x; e < TM * TK; e += 128) {
+            const int ii = TA ? e % TM : e / TK, kk = TA ? e / TM : e % TK;
+            const int i = i0 + ii, k = k0 + kk;
+            const float v = (i < M && k < ke) ? ld(TA ? A + (size_t)k * lda + i : A + (size_t)i * lda + k) : 0.0f;
+            bf16 hi, lo;
+            split_bf16(v, hi, lo);
+            As[0][ii][kk] = hi;
+            if (SA)
+                As[SA ? 1 : 0][ii][kk] = lo;
+            const int jj = TB ? e / TK : e % TN, kb2 = TB ? e % TK : e / TN;
+            const int j = j0 + jj, k2 = k0 + kb2;
+            const float w = (j < N && k2 < ke) ? ld(TB ? B + (size_t)j * ldb + k2 : B + (size_t)k2 * ldb + j) : 0.0f;
+            split_bf16(w, hi, lo);
+            Bs[0][jj][kb2] = hi;
+            if (SB)
+                Bs[SB ? 1 : 0][jj][kb2] = lo;
         }
         __syncthreads();
 #pragma unroll
-        for (int kk = 0; kk < GK; ++kk) {
-            float a[4], b[4];
+        for (int ks = 0; ks < TK; ks += 16) {
+            unsigned a[2][2][4], b[2][4][2]; // [hi / lo][tile][register]
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                a[r] = As[kk][ty * 4 + r];
-                b[r] = Bs[kk][tx * 4 + r];
-            }
+            for (int h = 0; h < (SA ? 2 : 1); ++h)
 #pragma unroll
-            for (int r = 0; r < 4; ++r)
+                for (int mt = 0; mt < 2; ++mt) {
+                    const int r = wm + mt * 16 + g;
+                    a[h][mt][0] = *(const unsigned *)&As[h][r][ks + 2 * t];
+                    a[h][mt][1] = *(const unsigned *)&As[h][r + 8][ks + 2 * t];
+                    a[h][mt][2] = *(const unsigned *)&As[h][r][ks + 2 * t + 8];
+                    a[h][mt][3] = *(const unsigned *)&As[h][r + 8][ks + 2 * t + 8];
+                }
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    acc[r][q] = fmaf(a[r], b[q], acc[r][q]);
+            for (int h = 0; h < (SB ? 2 : 1); ++h)
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) {
+                    const int c = wn + nt * 8 + g;
+                    b[h][nt][0] = *(const unsigned *)&Bs[h][c][ks + 2 * t];
+                    b[h][nt][1] = *(const unsigned *)&Bs[h][c][ks + 2 * t + 8];
+                }
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) {
+                    if (SA) // the small terms first
+                        mma_bf16(acc[mt][nt], a[1][mt], b[0][nt]);
+                    if (SB)
+                        mma_bf16(acc[mt][nt], a[0][mt], b[1][nt]);
+                    mma_bf16(acc[mt][nt], a[0][mt], b[0][nt]);
+                }
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
+    for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            int i = i0 + ty * 4 + r, j = j0 + tx * 4 + q;
-            if (i < M && j < N) {
-                float v = alpha * acc[r][q];
-                C[(size_t)i * ldc + j] = beta == 0.0f ? v : v + beta * C[(size_t)i * ldc + j];
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int i = i0 + wm + mt * 16 + g + 8 * (q >> 1), j = j0 + wn + nt * 8 + 2 * t + (q & 1);
+                if (i < M && j < N) {
+                    const float v = acc[mt][nt][q];
+                    if (part)
+                        part[((size_t)blockIdx.z * M + i) * N + j] = v;
+                    else
+                        C[(size_t)i * ldc + j] = beta == 0.0f ? alpha * v : alpha * v + beta * C[(size_t)i * ldc + j];
+                }
             }
-        }
 }
 
-template <bool TA, bool TB, typename AT, typename BT>
-void gemm(int M, int N, int K, const AT *A, int lda, const BT *B, int ldb, float *C, int ldc, float alpha, float beta,
-          cudaStream_t s)
+// C = alpha * sum_z part[z] + beta * C, the K slices added in order
+__global__ void splitk_fold_kernel(int M, int N, int splits, const float *part, float *C, int ldc, float alpha,
+                                   float beta)
 {
-    dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT);
-    gemm_kernel<TA, TB, AT, BT><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta);
+    const long long MN = (long long)M * N;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < MN; e += (long long)gridDim.x * blockDim.x) {
+        float s = 0.0f;
+        for (int z = 0; z < splits; ++z)
+            s += part[z * MN + e];
+        const int i = (int)(e / N), j = (int)(e % N);
+        float *c = C + (size_t)i * ldc + j;
+        *c = beta == 0.0f ? alpha * s : alpha * s + beta * *c;
+    }
+}
+
+// split-K workspace of the products (grown on demand, kept with the stream's owner)
+struct SplitWs {
+    float *p = nullptr;
+    size_t cap = 0;
+};
+
+template <bool TA, bool TB, typename AT, typename BT>
+int gemm(int M, int N, int K, const AT *A, int lda, const BT *B, int ldb, float *C, int ldc, float alpha, float beta,
+         cudaStream_t s, SplitWs &ws)
+{
+    const int gm = (M + TM - 1) / TM, gn = (N + TN - 1) / TN;
+    // few output tiles and a long reduction: split K so every SM has a slice
+    int splits = 1;
+    if (gm * gn < 74 && K >= 4 * TK * 8)
+        splits = std::max(1, std::min(148 / (gm * gn), (K + 255) / 256));
+    int kchunk = (K + splits - 1) / splits;
+    kchunk = (kchunk + TK - 1) / TK * TK;
+    splits = (K + kchunk - 1) / kchunk;
+    if (splits > 1) {
+        const size_t need = (size_t)splits * M * N;
+        if (need > ws.cap) {
+            if (ws.p)
+                cudaFree(ws.p);
+            ws.p = nullptr;
+            ws.cap = 0;
+            if (cudaMalloc((void **)&ws.p, need * sizeof(float)) != cudaSuccess)
+                return -1;
+            ws.cap = need;
+        }
+        mma_gemm_kernel<TA, TB, AT, BT><<<dim3(gn, gm, splits), 128, 0, s>>>(M, N, K, kchunk, A, lda, B, ldb, C, ldc,
+                                                                            alpha, beta, ws.p);
+        const long long MN = (long long)M * N;
+        splitk_fold_kernel<<<(int)std::min<long long>((MN + 255) / 256, 148 * 8), 256, 0, s>>>(M, N, splits, ws.p, C,
+                                                                                              ldc, alpha, beta);
+    } else {
+        mma_gemm_kernel<TA, TB, AT, BT><<<dim3(gn, gm, 1), 128, 0, s>>>(M, N, K, K, A, lda, B, ldb, C, ldc, alpha,
+                                                                       beta, nullptr);
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 // Y[B x N] += bias, then ReLU if asked
@@ -147,6 +270,24 @@ __global__ void mse_kernel(long long n, const float *o, const float *t, float sc
     }
     if (threadIdx.x == 0)
         part[blockIdx.x] = sh[0];
+}
+
+// acc += (sum of the nb block partials, in order) / tot + the head's loss
+__global__ void loss_fold_kernel(const double *part, int nb, double tot, const double *hloss, double *acc)
+{
+    __shared__ double sh[256];
+    double a = 0.0;
+    for (int b = threadIdx.x; b < nb; b += 256)
+        a += part[b];
+    sh[threadIdx.x] = a;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        acc[0] += sh[0] / tot + hloss[0];
 }
 
 // log-weight head: lw[b] = wp . h2[b] + bp; dlw = 2 (lw - tl) / B; loss partial
@@ -232,6 +373,8 @@ struct pdhcg_b200_mlp_s {
     float *X = nullptr, *H1 = nullptr, *H2 = nullptr, *Z = nullptr, *O = nullptr, *LW = nullptr;
     float *T = nullptr, *TL = nullptr, *dO = nullptr, *dZ = nullptr, *dH2 = nullptr, *dH1 = nullptr, *dLW = nullptr;
     double *part = nullptr, *hloss = nullptr;
+    double *acc = nullptr; // loss accumulated over the minibatches of a run (device)
+    SplitWs ws;
     cudaStream_t s = nullptr;
 };
 
@@ -249,7 +392,9 @@ void free_acts(pdhcg_b200_mlp_s *n)
         cudaFree(n->part);
     if (n->hloss)
         cudaFree(n->hloss);
-    n->part = n->hloss = nullptr;
+    if (n->acc)
+        cudaFree(n->acc);
+    n->part = n->hloss = n->acc = nullptr;
     n->cap = 0;
 }
 
@@ -264,7 +409,8 @@ int ensure_acts(pdhcg_b200_mlp_s *n, int B)
         al(&n->T, (long long)B * n->out) || al(&n->TL, B) || al(&n->dO, (long long)B * n->out) ||
         al(&n->dZ, (long long)B * n->rank) || al(&n->dH2, (long long)B * n->hid) ||
         al(&n->dH1, (long long)B * n->hid) || al(&n->dLW, B) ||
-        cudaMalloc((void **)&n->part, 148 * 8 * sizeof(double)) || cudaMalloc((void **)&n->hloss, sizeof(double))) {
+        cudaMalloc((void **)&n->part, 148 * 8 * sizeof(double)) || cudaMalloc((void **)&n->hloss, sizeof(double)) ||
+        cudaMalloc((void **)&n->acc, sizeof(double))) {
         std::fprintf(stderr, "[pdhcg_b200_mlp] activation allocation failed.\n");
         return -1;
     }
@@ -273,34 +419,31 @@ int ensure_acts(pdhcg_b200_mlp_s *n, int B)
 }
 
 // forward of B rows already in n->X; with targets (T, TL) also the loss and dO, dLW
-int forward(pdhcg_b200_mlp_s *n, int B, bool with_loss, double *loss)
+int forward(pdhcg_b200_mlp_s *n, int B, bool with_loss)
 {
     cudaStream_t s = n->s;
     const bf16 *W1 = n->wb + n->off[P_W1], *W2 = n->wb + n->off[P_W2], *W3 = n->wb + n->off[P_W3],
                *U = n->wb + n->off[P_U];
     const float *b1 = n->w + n->off[P_B1], *b2 = n->w + n->off[P_B2], *b3 = n->w + n->off[P_B3],
                 *bu = n->w + n->off[P_BU], *wp = n->w + n->off[P_WP], *bp = n->w + n->off[P_BP];
-    gemm<false, true>(B, n->hid, n->in, n->X, n->in, W1, n->in, n->H1, n->hid, 1.0f, 0.0f, s);
+    if (gemm<false, true>(B, n->hid, n->in, n->X, n->in, W1, n->in, n->H1, n->hid, 1.0f, 0.0f, s, n->ws))
+        return -1;
     bias_act_kernel<<<blocks_for((long long)B * n->hid), 256, 0, s>>>(B, n->hid, n->H1, b1, 1);
-    gemm<false, true>(B, n->hid, n->hid, n->H1, n->hid, W2, n->hid, n->H2, n->hid, 1.0f, 0.0f, s);
+    if (gemm<false, true>(B, n->hid, n->hid, n->H1, n->hid, W2, n->hid, n->H2, n->hid, 1.0f, 0.0f, s, n->ws))
+        return -1;
     bias_act_kernel<<<blocks_for((long long)B * n->hid), 256, 0, s>>>(B, n->hid, n->H2, b2, 1);
-    gemm<false, true>(B, n->rank, n->hid, n->H2, n->hid, W3, n->hid, n->Z, n->rank, 1.0f, 0.0f, s);
+    if (gemm<false, true>(B, n->rank, n->hid, n->H2, n->hid, W3, n->hid, n->Z, n->rank, 1.0f, 0.0f, s, n->ws))
+        return -1;
     bias_act_kernel<<<blocks_for((long long)B * n->rank), 256, 0, s>>>(B, n->rank, n->Z, b3, 0);
-    gemm<false, true>(B, n->out, n->rank, n->Z, n->rank, U, n->rank, n->O, n->out, 1.0f, 0.0f, s);
+    if (gemm<false, true>(B, n->out, n->rank, n->Z, n->rank, U, n->rank, n->O, n->out, 1.0f, 0.0f, s, n->ws))
+        return -1;
     bias_act_kernel<<<blocks_for((long long)B * n->out), 256, 0, s>>>(B, n->out, n->O, bu, 0);
     head_kernel<<<1, 256, 0, s>>>(B, n->hid, n->H2, wp, bp, with_loss ? n->TL : nullptr, n->LW, n->dLW, n->hloss);
-    if (with_loss) {
+    if (with_loss) { // the minibatch's loss is added to n->acc on the device (no host wait)
         long long tot = (long long)B * n->out;
         int nb = blocks_for(tot);
         mse_kernel<<<nb, 256, 0, s>>>(tot, n->O, n->T, 1.0f / (float)tot, n->dO, n->part);
-        std::vector<double> h(nb + 1);
-        MCK(cudaMemcpyAsync(h.data(), n->part, nb * sizeof(double), cudaMemcpyDeviceToHost, s));
-        MCK(cudaMemcpyAsync(h.data() + nb, n->hloss, sizeof(double), cudaMemcpyDeviceToHost, s));
-        MCK(cudaStreamSynchronize(s));
-        double a = 0.0;
-        for (int b = 0; b < nb; ++b)
-            a += h[b];
-        *loss = a / (double)tot + h[nb];
+        loss_fold_kernel<<<1, 256, 0, s>>>(n->part, nb, (double)tot, n->hloss, n->acc);
     }
     MCK(cudaGetLastError());
     return 0;
@@ -314,24 +457,31 @@ int backward(pdhcg_b200_mlp_s *n, int B)
     const float *wp = n->w + n->off[P_WP];
     float *g = n->g;
     // output head: dU = dO^T Z, dbu = colsum dO, dZ = dO U
-    gemm<true, false>(n->out, n->rank, B, n->dO, n->out, n->Z, n->rank, g + n->off[P_U], n->rank, 1.0f, 0.0f, s);
+    if (gemm<true, false>(n->out, n->rank, B, n->dO, n->out, n->Z, n->rank, g + n->off[P_U], n->rank, 1.0f, 0.0f, s, n->ws))
+        return -1;
     colsum_kernel<<<blocks_for(n->out), 256, 0, s>>>(B, n->out, n->dO, g + n->off[P_BU]);
-    gemm<false, false>(B, n->rank, n->out, n->dO, n->out, U, n->rank, n->dZ, n->rank, 1.0f, 0.0f, s);
+    if (gemm<false, false>(B, n->rank, n->out, n->dO, n->out, U, n->rank, n->dZ, n->rank, 1.0f, 0.0f, s, n->ws))
+        return -1;
     // z = W3 h2 + b3
-    gemm<true, false>(n->rank, n->hid, B, n->dZ, n->rank, n->H2, n->hid, g + n->off[P_W3], n->hid, 1.0f, 0.0f, s);
+    if (gemm<true, false>(n->rank, n->hid, B, n->dZ, n->rank, n->H2, n->hid, g + n->off[P_W3], n->hid, 1.0f, 0.0f, s, n->ws))
+        return -1;
     colsum_kernel<<<blocks_for(n->rank), 256, 0, s>>>(B, n->rank, n->dZ, g + n->off[P_B3]);
-    gemm<false, false>(B, n->hid, n->rank, n->dZ, n->rank, W3, n->hid, n->dH2, n->hid, 1.0f, 0.0f, s);
+    if (gemm<false, false>(B, n->hid, n->rank, n->dZ, n->rank, W3, n->hid, n->dH2, n->hid, 1.0f, 0.0f, s, n->ws))
+        return -1;
     // log-weight head
     head_back_kernel<<<blocks_for(n->hid), 256, 0, s>>>(B, n->hid, n->H2, wp, n->dLW, n->dH2, g + n->off[P_WP],
                                                          g + n->off[P_BP]);
     relu_back_kernel<<<blocks_for((long long)B * n->hid), 256, 0, s>>>((long long)B * n->hid, n->dH2, n->H2);
     // h2 = relu(W2 h1 + b2)
-    gemm<true, false>(n->hid, n->hid, B, n->dH2, n->hid, n->H1, n->hid, g + n->off[P_W2], n->hid, 1.0f, 0.0f, s);
+    if (gemm<true, false>(n->hid, n->hid, B, n->dH2, n->hid, n->H1, n->hid, g + n->off[P_W2], n->hid, 1.0f, 0.0f, s, n->ws))
+        return -1;
     colsum_kernel<<<blocks_for(n->hid), 256, 0, s>>>(B, n->hid, n->dH2, g + n->off[P_B2]);
-    gemm<false, false>(B, n->hid, n->hid, n->dH2, n->hid, W2, n->hid, n->dH1, n->hid, 1.0f, 0.0f, s);
+    if (gemm<false, false>(B, n->hid, n->hid, n->dH2, n->hid, W2, n->hid, n->dH1, n->hid, 1.0f, 0.0f, s, n->ws))
+        return -1;
     relu_back_kernel<<<blocks_for((long long)B * n->hid), 256, 0, s>>>((long long)B * n->hid, n->dH1, n->H1);
     // h1 = relu(W1 x + b1)
-    gemm<true, false>(n->hid, n->in, B, n->dH1, n->hid, n->X, n->in, g + n->off[P_W1], n->in, 1.0f, 0.0f, s);
+    if (gemm<true, false>(n->hid, n->in, B, n->dH1, n->hid, n->X, n->in, g + n->off[P_W1], n->in, 1.0f, 0.0f, s, n->ws))
+        return -1;
     colsum_kernel<<<blocks_for(n->hid), 256, 0, s>>>(B, n->hid, n->dH1, g + n->off[P_B1]);
     MCK(cudaGetLastError());
     return 0;
@@ -412,6 +562,8 @@ void pdhcg_b200_mlp_free(pdhcg_b200_mlp_t *n)
     if (!n)
         return;
     free_acts(n);
+    if (n->ws.p)
+        cudaFree(n->ws.p);
     for (void *p : {(void *)n->w, (void *)n->g, (void *)n->mom, (void *)n->vel, (void *)n->wb})
         if (p)
             cudaFree(p);
@@ -448,7 +600,7 @@ int pdhcg_b200_mlp_predict(pdhcg_b200_mlp_t *n, int batch, const float *theta, f
     if (ensure_acts(n, batch))
         return -1;
     MCK(cudaMemcpyAsync(n->X, theta, (size_t)batch * n->in * sizeof(float), cudaMemcpyHostToDevice, n->s));
-    if (forward(n, batch, false, nullptr))
+    if (forward(n, batch, false))
         return -1;
     MCK(cudaMemcpyAsync(out, n->O, (size_t)batch * n->out * sizeof(float), cudaMemcpyDeviceToHost, n->s));
     if (logw)
@@ -467,10 +619,12 @@ int pdhcg_b200_mlp_loss_grad(pdhcg_b200_mlp_t *n, int batch, const float *theta,
     MCK(cudaMemcpyAsync(n->X, theta, (size_t)batch * n->in * sizeof(float), cudaMemcpyHostToDevice, n->s));
     MCK(cudaMemcpyAsync(n->T, target, (size_t)batch * n->out * sizeof(float), cudaMemcpyHostToDevice, n->s));
     MCK(cudaMemcpyAsync(n->TL, target_logw, batch * sizeof(float), cudaMemcpyHostToDevice, n->s));
-    if (forward(n, batch, true, loss) || backward(n, batch))
+    MCK(cudaMemsetAsync(n->acc, 0, sizeof(double), n->s));
+    if (forward(n, batch, true) || backward(n, batch))
         return -1;
     if (grad)
         MCK(cudaMemcpyAsync(grad, n->g, n->total * sizeof(float), cudaMemcpyDeviceToHost, n->s));
+    MCK(cudaMemcpyAsync(loss, n->acc, sizeof(double), cudaMemcpyDeviceToHost, n->s));
     MCK(cudaStreamSynchronize(n->s));
     return 0;
 }
@@ -492,19 +646,19 @@ int pdhcg_b200_mlp_train(pdhcg_b200_mlp_t *n, int count, const float *theta, con
     MCK(cudaMemcpy(dt, target, (size_t)count * n->out * sizeof(float), cudaMemcpyHostToDevice));
     MCK(cudaMemcpy(dtl, target_logw, count * sizeof(float), cudaMemcpyHostToDevice));
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-    double epoch_loss = 0.0;
-    int rc = 0;
+    int rc = 0, nbat = 0;
     for (int ep = 0; ep < epochs && rc == 0; ++ep) {
-        epoch_loss = 0.0;
-        int nbat = 0;
+        // the last epoch's mean minibatch loss is read once, after the run
+        if (cudaMemsetAsync(n->acc, 0, sizeof(double), n->s) != cudaSuccess)
+            rc = -1;
+        nbat = 0;
         for (int b0 = 0; b0 + batch <= count && rc == 0; b0 += batch, ++nbat) { // full minibatches in order
             cudaMemcpyAsync(n->X, dth + (size_t)b0 * n->in, (size_t)batch * n->in * sizeof(float),
                             cudaMemcpyDeviceToDevice, n->s);
             cudaMemcpyAsync(n->T, dt + (size_t)b0 * n->out, (size_t)batch * n->out * sizeof(float),
                             cudaMemcpyDeviceToDevice, n->s);
             cudaMemcpyAsync(n->TL, dtl + b0, batch * sizeof(float), cudaMemcpyDeviceToDevice, n->s);
-            double l = 0.0;
-            rc = forward(n, batch, true, &l);
+            rc = forward(n, batch, true);
             if (rc == 0)
                 rc = backward(n, batch);
             if (rc == 0) {
@@ -514,17 +668,18 @@ int pdhcg_b200_mlp_train(pdhcg_b200_mlp_t *n, int count, const float *theta, con
                                                                     c1, c2, eps);
                 rc = refresh_bf16(n);
             }
-            epoch_loss += l;
         }
-        if (nbat > 0)
-            epoch_loss /= nbat;
     }
+    double acc = 0.0;
+    const cudaError_t e1 = cudaMemcpyAsync(&acc, n->acc, sizeof(double), cudaMemcpyDeviceToHost, n->s);
+    const cudaError_t e2 = cudaStreamSynchronize(n->s);
     cudaFree(dth);
     cudaFree(dt);
     cudaFree(dtl);
+    if (e1 != cudaSuccess || e2 != cudaSuccess)
+        rc = -1;
     if (loss)
-        *loss = epoch_loss;
-    MCK(cudaStreamSynchronize(n->s));
+        *loss = nbat > 0 ? acc / nbat : 0.0;
     return rc;
 }
 

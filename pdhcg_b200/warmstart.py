@@ -14,6 +14,7 @@ reference: a warm solve must meet the same termination tolerance.
 from __future__ import annotations
 
 import ctypes as C
+import time
 
 import numpy as np
 
@@ -67,6 +68,7 @@ class WarmStart:
         if not self.net:
             raise RuntimeError("pdhcg_b200_mlp_create failed")
         self.mean = np.zeros(self.out_dim)
+        self.mean_log_weight = 0.0
         self.scale = np.ones(self.out_dim)
         # 0.998 / sigma_max of the scaled A, shared by the whole family (A and
         # the scaling parameters are fixed), recorded by the first cold solve
@@ -84,22 +86,41 @@ class WarmStart:
             pass
 
     # ---- data -------------------------------------------------------------
-    def solve(self, theta, params: dict, warm: bool = False) -> dict:
-        """One solve of the instance theta (cold, or from the predicted point)."""
+    def solve(self, theta, params: dict, warm: bool = False, start: str | None = None) -> dict:
+        """One solve of the instance theta from one of three starts:
+
+        - ``"cold"``: x = 0, y = 0 and the solver's own primal weight;
+        - ``"mean"``: the mean of the training targets (x, y) and their mean
+          log primal weight, the same for every instance (what a start
+          without the network gets from the training data);
+        - ``"net"`` (``warm=True``): the network's prediction for theta.
+
+        Once a cold solve has recorded the family's step size (0.998 /
+        sigma_max of the scaled A, shared by the family: A and the scaling
+        parameters are fixed), every form reuses it and skips the power
+        method, so the forms differ only in their start.  ``wall_s`` is the
+        wall time of the whole call, the network's prediction included."""
+        start = start or ("net" if warm else "cold")
         lib = self.lib
+        t0 = time.perf_counter()
         p = self.family.problem(theta)
         prob, keep = capi.build(lib, p)
         opts = native.default_options()
-        if warm:
-            x, y, w = self.predict(theta[None, :])
-            xs, ys = np.ascontiguousarray(x[0], np.float64), np.ascontiguousarray(y[0], np.float64)
+        if start in ("net", "mean"):
+            if start == "net":
+                x, y, w = self.predict(theta[None, :])
+                x, y, w = x[0], y[0], float(w[0])
+            else:
+                x, y = self.mean[:self.family.n], self.mean[self.family.n:]
+                w = float(np.exp(self.mean_log_weight))
+            xs, ys = np.ascontiguousarray(x, np.float64), np.ascontiguousarray(y, np.float64)
             dp = C.POINTER(C.c_double)
             lib.set_start_values(prob, xs.ctypes.data_as(dp), ys.ctypes.data_as(dp))
             opts.has_initial_primal_weight = 1
-            opts.initial_primal_weight = float(w[0])
-            if self.step_size:
-                opts.has_initial_step_size = 1
-                opts.initial_step_size = self.step_size
+            opts.initial_primal_weight = w
+        if self.step_size:
+            opts.has_initial_step_size = 1
+            opts.initial_step_size = self.step_size
         prm = capi.default_params(lib, **params)
         r = lib.pdhcg_b200_solve(prob, C.byref(prm), C.byref(opts))
         if not r:
@@ -108,10 +129,12 @@ class WarmStart:
         d = capi.result_dict(r, p.n, p.A.m)
         st = native.last_stats()
         d["final_primal_weight"] = st["primal_weight"]
-        if not warm and self.step_size is None:
+        if self.step_size is None:
             self.step_size = st["step_size"]
         lib.pdhcg_result_free(r)
         lib.qp_problem_free(prob)
+        d["wall_s"] = time.perf_counter() - t0
+        d["stats"] = st
         return d
 
     def collect(self, thetas: np.ndarray, params: dict):
@@ -132,6 +155,7 @@ class WarmStart:
             lr: float = 1e-3) -> float:
         """Normalise the targets per output (mean, scale) and train on the GPU."""
         self.mean = X.mean(0).astype(np.float64)
+        self.mean_log_weight = float(np.mean(lw))
         sd = X.std(0).astype(np.float64)
         self.scale = np.where(sd > 1e-8, sd, 1.0)
         T = ((X - self.mean) / self.scale).astype(np.float32)
