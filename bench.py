@@ -168,11 +168,14 @@ def run_ours(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     if world > 1:
+        import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", init_method="env://")
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
     lib = native.load()
     W = WORKLOADS[args.workload]
-    problem = W["make"](args.scale, rank)
+    # one instance does not shard (its products would need an exchange each
+    # step): with several ranks every rank solves the same instance, a replica
+    problem = W["make"](args.scale, 0)
     prob, keep = capi.build(lib, problem)
     prm = _params(lib, args.iters)
     forms = {"fp64": 0, "mixed": 1} if W["mixed"] else {"fp64": 0}
@@ -256,7 +259,8 @@ def run_ours(args):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_solve * 1e3,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64" if W["mixed"] else "f64", "data": "synthetic",
-        "config": {"workload": W["desc"], "parallelism": "replicas" if world > 1 else "single",
+        "config": {"workload": W["desc"],
+                   "parallelism": "replicas: every rank solves the same instance" if world > 1 else "single",
                    "eps": EPS, "form": "mixed: FP32 bulk, FP64 polish below 1e-5" if W["mixed"] else "FP64",
                    "l2_flush": W["l2"],
                    "inputs": "value: problem resident in HBM (pdhcg_b200_upload once), solution left on device; "
@@ -287,6 +291,15 @@ def run_ours(args):
         line["inner_iterations"] = res.get("total_inner_count")
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(problem, res["total_count"])
+    if world == 1 and not args.no_extras and args.workload == "soc_qp":
+        # the other patterns and workloads on the same line (one GPU): the
+        # batched solver on the full 4096-instance batch, the learned warm
+        # start at a reduced training count, and the inner-BB workloads
+        # beside the reference's own build
+        line["batched"] = measure_batch(4096, steps=3, warmup=1)
+        line["warm_start"] = measure_warm_start(50000, train=256, epochs=60, heldout=24)
+        for name in ("sparse_qp", "portfolio"):
+            line[name] = measure_single(name)
     print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -304,118 +317,139 @@ def _batch_params(lib):
                                        "termination_criteria.time_sec_limit": 600.0})
 
 
-def run_batch(args):
-    """The batched workload: all instances in pdhcg_b200_solve_batch (value:
-    kernel time, problem arrays already uploaded; e2e: the whole call from
-    host problems), against one solve_qp_problem per instance on a sample."""
+def measure_batch(count: int, steps: int, warmup: int, rank: int = 0, world: int = 1, seq_sample: int = 16) -> dict:
+    """One batch of ``count`` MPC instances split across the ranks by
+    nonzero count (pdhcg_b200.shard): every rank builds only its bin and
+    solves it with pdhcg_b200_solve_batch on its own GPU; the results come
+    back to rank 0 once at the end.  Times are the max over ranks; the
+    throughputs are the whole batch over that time (strong scaling: the
+    batch is the same for every rank count).  Rank 0 also times one
+    solve_qp_problem per instance on a sample, the way the reference would
+    solve them."""
     import torch
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", init_method="env://")
+    from pdhcg_b200 import shard
     lib = native.load()
-    count = max(1, int(4096 * args.scale))
-    # instances partition across ranks: rank r solves its own seeded share
-    probs = instances.mpc_batch(seed=4 + rank, count=count)
+    weights = [instances.mpc_nnz(int(t)) for t in instances.mpc_horizons(4, count)]
+    mine = shard.partition(weights, world)[rank]
+    probs = instances.mpc_batch(seed=4, count=count, indices=mine)
     built = [capi.build(lib, p) for p in probs]
-    arr = (C.POINTER(capi.QpProblem) * count)(*[b[0] for b in built])
+    k = len(built)
+    arr = (C.POINTER(capi.QpProblem) * max(k, 1))(*[b[0] for b in built])
     prm = _batch_params(lib)
     opts = native.BatchOptions()
     lib.pdhcg_b200_default_batch_options(C.byref(opts))
     shape_ms = (C.c_double * native.BATCH_SHAPES)()
-    tune = min(count, 512)
-    if lib.pdhcg_b200_batch_autotune(tune, arr, C.byref(prm), C.byref(opts), shape_ms) != 0:
+    if k and lib.pdhcg_b200_batch_autotune(min(k, 512), arr, C.byref(prm), C.byref(opts), shape_ms) != 0:
         raise RuntimeError("batch autotune failed")
-    res = (C.POINTER(capi.PdhcgResult) * count)()
+    res = (C.POINTER(capi.PdhcgResult) * max(k, 1))()
     launches = [0]
 
     def solve():
+        if not k:
+            return 0.0, 0.0, {}
         t0 = time.perf_counter()
-        if lib.pdhcg_b200_solve_batch(count, arr, C.byref(prm), C.byref(opts), res) != 0:
+        if lib.pdhcg_b200_solve_batch(k, arr, C.byref(prm), C.byref(opts), res) != 0:
             raise RuntimeError("batch solve failed")
         wall = time.perf_counter() - t0
         bst = native.BatchStats()
         lib.pdhcg_b200_last_batch_stats(C.byref(bst))
-        kern = bst.kernel_ms * 1e-3
         launches[0] += bst.launches
-        stat = {}
-        iters = 0
-        for r in res:
-            st = capi.TERMINATION_REASONS[r.contents.termination_reason]
-            stat[st] = stat.get(st, 0) + 1
-            iters += r.contents.total_count
+        out = {}
+        for i, r in zip(mine, res[:k]):
+            out[i] = (capi.TERMINATION_REASONS[r.contents.termination_reason], r.contents.total_count)
             lib.pdhcg_result_free(r)
-        return wall, kern, stat, iters / count
+        return wall, bst.kernel_ms * 1e-3, out
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         solve()
     launches[0] = 0
-    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
-    sampler.start()
-    walls, kerns = [], []
-    for _ in range(args.steps):
+    walls, kerns, last = [], [], {}
+    for _ in range(steps):
         if world > 1:
             torch.distributed.barrier()
-        w, k, stat, mean_it = solve()
+        w, kt, last = solve()
         walls.append(w)
-        kerns.append(k)
-    clocks = sampler.stop()
+        kerns.append(kt)
     wall, kern = max(walls), max(kerns)
     if world > 1:
         t = torch.tensor([wall, kern], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         wall, kern = t[0].item(), t[1].item()
-    # sequential plain solves (the reference's way: one solve_qp_problem per instance)
-    k_seq = min(16, count)
-    t0 = time.perf_counter()
-    for i in range(k_seq):
-        r = lib.solve_qp_problem(arr[i], C.byref(prm))
-        lib.pdhcg_result_free(r)
-    seq = k_seq / (time.perf_counter() - t0)
-    if rank != 0:
-        if world > 1:
-            torch.distributed.destroy_process_group()
-        return
-    total = count * world
-    nnz = sum(p.A.nnz for p in probs)
-    line = {
-        "metric": BATCH_METRIC, "value": total / kern, "unit": "instances/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": kern * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": BATCH_WORKLOAD, "instances_per_gpu": count, "parallelism":
-                   "instances partitioned across ranks" if world > 1 else "single",
-                   "shape": int(opts.shape), "autotune_ms": list(shape_ms),
-                   "l2_flush": "not needed: each instance lives in shared memory for its whole solve",
-                   "inputs": "value: kernel time, problem arrays already on the device; e2e: the whole "
-                             "pdhcg_b200_solve_batch call from host problems"},
-        "statuses": stat, "mean_iterations": mean_it, "nnz_per_gpu": int(nnz),
-        "e2e": {"value": total / wall, "unit": "instances/s",
-                "h2d_bytes_per_step": int(sum(p.A.nnz * 24 + (p.A.m + 1) * 4 + (p.n + 1) * 4 + p.n * 32 +
-                                              p.A.m * 16 for p in probs)),
-                "d2h_bytes_per_step": int(sum(8 * (p.n + p.A.m) for p in probs))},
-        "sequential_plain_solves": {"value": seq, "unit": "instances/s", "sample": k_seq,
-                                    "call": "solve_qp_problem per instance"},
-        "speedup_vs_sequential": (total / wall) / (seq * world),
-        "gpu_launches": launches[0],
-        "clocks": clocks,
-    }
-    if not args.no_cpu_baseline:
-        oracle = C.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
-        oracle.oracle_solve.restype = C.POINTER(capi.PdhcgResult)
-        oracle.oracle_solve.argtypes = [C.POINTER(capi.QpProblem), C.POINTER(capi.PdhgParameters)]
-        t0, done = time.perf_counter(), 0
-        while done < count and time.perf_counter() - t0 < 10.0:
-            r = oracle.oracle_solve(arr[done], C.byref(prm))
-            oracle.oracle_result_free(r)
-            done += 1
-        dt = time.perf_counter() - t0
-        line["cpu_baseline"] = {"value": done / dt, "unit": "instances/s", "cores": 1, "kind": "port",
-                                "sample": f"oracle FP64 on the first {done} instances ({dt:.1f}s)"}
-    print(json.dumps(line))
+    allres = shard.gather_results(last, rank, world, count)
+    nnz_mine = int(sum(weights[i] for i in mine))
+    out = None
+    if rank == 0:
+        stat = {}
+        for st, _ in allres:
+            stat[st] = stat.get(st, 0) + 1
+        t0 = time.perf_counter()
+        for i in range(min(seq_sample, k)):
+            r = lib.solve_qp_problem(arr[i], C.byref(prm))
+            lib.pdhcg_result_free(r)
+        seq = min(seq_sample, k) / (time.perf_counter() - t0)
+        out = {"value": count / kern, "unit": "instances/s", "ms_per_step": kern * 1e3, "instances": count,
+               "statuses": stat, "mean_iterations": float(np.mean([it for _, it in allres])),
+               "e2e": {"value": count / wall, "unit": "instances/s",
+                       "h2d_bytes_per_step": int(sum(p.A.nnz * 24 + (p.A.m + 1) * 4 + (p.n + 1) * 4 + p.n * 32 +
+                                                     p.A.m * 16 for p in probs)),
+                       "d2h_bytes_per_step": int(sum(8 * (p.n + p.A.m) for p in probs))},
+               "sequential_plain_solves": {"value": seq, "unit": "instances/s", "sample": min(seq_sample, k),
+                                           "call": "solve_qp_problem per instance, one GPU"},
+               "speedup_vs_sequential": (count / wall) / seq,
+               "shape": int(opts.shape), "autotune_ms": list(shape_ms), "gpu_launches": launches[0],
+               "partition": {"ranks": world, "instances_on_rank0": k, "nnz_on_rank0": nnz_mine,
+                             "nnz_total": int(sum(weights))}}
     for b in built:
         lib.qp_problem_free(b[0])
+    return out
+
+
+def run_batch(args):
+    """The batched workload on its own line (--workload mpc_batch)."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
+    count = max(1, int(4096 * args.scale))
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    m = measure_batch(count, args.steps, args.warmup, rank, world)
+    clocks = sampler.stop()
+    if rank == 0:
+        line = {"metric": BATCH_METRIC, "value": m["value"], "unit": "instances/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms_per_step"],
+                "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+                "dtype": "f32+f64", "data": "synthetic",
+                "config": {"workload": BATCH_WORKLOAD, "instances": count,
+                           "parallelism": "one batch partitioned across ranks by nonzeros" if world > 1 else "single",
+                           "l2_flush": "not needed: each instance lives in shared memory for its whole solve",
+                           "inputs": "value: kernel time, problem arrays already on the device; e2e: the whole "
+                                     "pdhcg_b200_solve_batch call from host problems"},
+                **{k: v for k, v in m.items() if k not in ("value", "unit", "ms_per_step")},
+                "clocks": clocks}
+        if not args.no_cpu_baseline:
+            lib = native.load()
+            oracle = C.CDLL(os.path.join(ROOT, "oracle", "liboracle.so"))
+            oracle.oracle_solve.restype = C.POINTER(capi.PdhcgResult)
+            oracle.oracle_solve.argtypes = [C.POINTER(capi.QpProblem), C.POINTER(capi.PdhgParameters)]
+            prm = _batch_params(lib)
+            t0, done = time.perf_counter(), 0
+            for p in instances.mpc_batch(seed=4, count=count, indices=range(min(count, 2000))):
+                if time.perf_counter() - t0 >= 10.0:
+                    break
+                prob, keep = capi.build(lib, p)
+                r = oracle.oracle_solve(prob, C.byref(prm))
+                oracle.oracle_result_free(r)
+                lib.qp_problem_free(prob)
+                done += 1
+            dt = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": done / dt, "unit": "instances/s", "cores": 1, "kind": "port",
+                                    "sample": f"oracle FP64 on the first {done} instances ({dt:.1f}s)"}
+        print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
 
@@ -424,76 +458,143 @@ WS_METRIC = "learned warm start: time-to-1e-6 KKT (s) per held-out instance, war
 WS_EPS = 1e-6
 
 
-def run_warm_start(args):
-    """The parametric family: cold solves of the training parameters, the MLP
-    trained on the GPU, then held-out instances solved cold and warm (each
-    warm answer must meet the same tolerance).  value = mean warm time per
-    held-out solve; the cold mean is the comparison."""
-    import torch
+def measure_warm_start(n: int, train: int, epochs: int, heldout: int, warmup: int = 2) -> dict:
+    """The parametric family: cold solves of ``train`` parameters, the MLP
+    trained on the GPU, then ``heldout`` new instances solved three ways --
+    cold, from the training targets' mean, and from the network's
+    prediction -- all with the family's cached step size (no power method in
+    any of them), each timed as a whole call (the prediction included).
+    Every answer must meet the same tolerance."""
     from pdhcg_b200 import warmstart
+    fam = warmstart.ParametricQP(seed=5, n=n)
+    params = {"termination_criteria.eps_optimal_relative": WS_EPS,
+              "termination_criteria.eps_feasible_relative": WS_EPS, "termination_criteria.time_sec_limit": 600.0}
+    ws = warmstart.WarmStart(fam, hidden=512, rank=64, seed=1)
+    try:
+        t0 = time.perf_counter()
+        thetas = fam.thetas(train, seed=1)
+        X, lw, train_its = ws.collect(thetas, params)
+        t_collect = time.perf_counter() - t0
+        batch = min(64, train)
+        t0 = time.perf_counter()
+        loss = ws.fit(thetas, X, lw, epochs=epochs, batch=batch, lr=1e-3)
+        t_fit = time.perf_counter() - t0
+        held = fam.thetas(heldout + warmup, seed=2)
+        for th in held[:warmup]:
+            for f in ("cold", "mean", "net"):
+                ws.solve(th, params, start=f)
+        forms = {f: {"t": [], "it": [], "ok": 0} for f in ("cold", "mean", "net")}
+        for th in held[warmup:]:
+            res = {f: ws.solve(th, params, start=f) for f in forms}
+            ref = res["cold"]["primal_objective_value"]
+            for f, d in res.items():
+                forms[f]["t"].append(d["wall_s"])
+                forms[f]["it"].append(d["total_count"])
+                forms[f]["ok"] += int(d["status"] == "OPTIMAL" and
+                                      abs(d["primal_objective_value"] - ref) <= 10 * WS_EPS * (1 + abs(ref)))
+    finally:
+        ws.close()
+    summ = {f: {"value": float(np.mean(v["t"])), "unit": "s", "mean_iterations": float(np.mean(v["it"])),
+                "passing_same_tolerance": f"{v['ok']}/{heldout}"} for f, v in forms.items()}
+    steps = epochs * (train // batch)
+    return {"value": summ["net"]["value"], "unit": "s", "forms": summ,
+            "speedup_net_vs_cold": summ["cold"]["value"] / summ["net"]["value"],
+            "speedup_net_vs_mean": summ["mean"]["value"] / summ["net"]["value"],
+            "iterations_cold_over_net": summ["cold"]["mean_iterations"] / summ["net"]["mean_iterations"],
+            "iterations_mean_over_net": summ["mean"]["mean_iterations"] / summ["net"]["mean_iterations"],
+            "equal_setup": "every form reuses the family's cached step size (no power method); times are whole "
+                           "calls, the network's prediction included",
+            "training": {"solves": train, "epochs": epochs, "collect_s": t_collect, "fit_s": t_fit,
+                         "fit_ms_per_step": t_fit / max(1, steps) * 1e3, "final_loss": loss,
+                         "mean_training_iterations": float(np.mean(train_its))},
+            "config": {"workload": f"parametric QP family: n={n}, m={n // 2}, A 6 nnz/row, diag Q, theta in R^32, "
+                                   f"c = c0 + C theta, row bounds + L theta, eps 1e-6",
+                       "network": "32-512-512 MLP, rank-64 output head to n + m, log primal-weight head; "
+                                  "BF16 tensor-core products, FP32 accumulation"}}
+
+
+def run_warm_start(args):
+    """The learned warm start on its own line (--workload warm_start)."""
+    import torch
     rank = int(os.environ.get("RANK", "0"))
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     if rank != 0:  # one family, one GPU: the other ranks idle
         return
     n = max(1000, int(50000 * args.scale))
-    fam = warmstart.ParametricQP(seed=5, n=n)
-    params = {"termination_criteria.eps_optimal_relative": WS_EPS,
-              "termination_criteria.eps_feasible_relative": WS_EPS, "termination_criteria.time_sec_limit": 600.0}
-    ws = warmstart.WarmStart(fam, hidden=512, rank=64, seed=1)
-    t0 = time.perf_counter()
-    train = fam.thetas(args.train, seed=1)
-    X, lw, train_its = ws.collect(train, params)
-    t_collect = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    loss = ws.fit(train, X, lw, epochs=args.epochs, batch=64, lr=1e-3)
-    t_fit = time.perf_counter() - t0
-    held = fam.thetas(args.heldout + args.warmup, seed=2)
-    for th in held[:args.warmup]:
-        ws.solve(th, params)
-        ws.solve(th, params, warm=True)
     sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     sampler.start()
-    cold_t, warm_t, cold_it, warm_it, ok = [], [], [], [], 0
-    cold_st, warm_st = [], []
-    keys = ("setup_ms", "loop_ms", "result_ms", "upload_ms", "evaluations", "restarts")
-    for th in held[args.warmup:]:
-        c = ws.solve(th, params)
-        st = native.last_stats()
-        cold_t.append(st["total_ms"] * 1e-3)
-        cold_st.append([st[k] for k in keys])
-        w = ws.solve(th, params, warm=True)
-        st = native.last_stats()
-        warm_t.append(st["total_ms"] * 1e-3)
-        warm_st.append([st[k] for k in keys])
-        cold_it.append(c["total_count"])
-        warm_it.append(w["total_count"])
-        ok += int(c["status"] == w["status"] == "OPTIMAL" and abs(c["primal_objective_value"] - w[
-            "primal_objective_value"]) <= 10 * WS_EPS * (1 + abs(c["primal_objective_value"])))
+    m = measure_warm_start(n, args.train, args.epochs, args.heldout, args.warmup)
     clocks = sampler.stop()
-    ws.close()
-    line = {
-        "metric": WS_METRIC, "value": float(np.mean(warm_t)), "unit": "s", "n_gpus": 1, "steps": args.heldout,
-        "warmup": args.warmup, "ms_per_step": float(np.mean(warm_t)) * 1e3, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64 solve, bf16/f32 network", "data": "synthetic",
-        "config": {"workload": f"parametric QP family: n={n}, m={n // 2}, A 6 nnz/row, diag Q, theta in R^32, "
-                               f"c = c0 + C theta, row bounds + L theta, eps 1e-6",
-                   "network": "32-512-512 MLP, rank-64 output head to n + m, log primal-weight head",
-                   "training_solves": args.train, "heldout_solves": args.heldout, "epochs": args.epochs},
-        "cold": {"value": float(np.mean(cold_t)), "unit": "s", "mean_iterations": float(np.mean(cold_it)),
-                 "mean_breakdown": dict(zip(keys, np.mean(cold_st, 0).tolist()))},
-        "warm": {"value": float(np.mean(warm_t)), "unit": "s", "mean_iterations": float(np.mean(warm_it)),
-                 "mean_breakdown": dict(zip(keys, np.mean(warm_st, 0).tolist()))},
-        "speedup_warm_vs_cold": float(np.mean(cold_t) / np.mean(warm_t)),
-        "iteration_ratio_cold_over_warm": float(np.mean(cold_it) / np.mean(warm_it)),
-        "heldout_passing_same_tolerance": f"{ok}/{args.heldout}",
-        "training": {"collect_s": t_collect, "fit_s": t_fit, "final_loss": loss,
-                     "mean_training_iterations": float(np.mean(train_its))},
-        "e2e": {"value": float(np.mean(warm_t)), "unit": "s",
-                "h2d_bytes_per_step": int(fam.A.nnz * 12 + n * 8 * 6 + (n // 2) * 8 * 3),
-                "d2h_bytes_per_step": int(8 * (2 * n + n // 2))},
-        "clocks": clocks,
-    }
+    line = {"metric": WS_METRIC, "value": m["value"], "unit": "s", "n_gpus": 1, "steps": args.heldout,
+            "warmup": args.warmup, "ms_per_step": m["value"] * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 solve, bf16/f32 network", "data": "synthetic",
+            "config": {**m["config"], "training_solves": args.train, "heldout_solves": args.heldout,
+                       "epochs": args.epochs},
+            **{k: v for k, v in m.items() if k not in ("value", "unit", "config")},
+            "e2e": {"value": m["value"], "unit": "s",
+                    "h2d_bytes_per_step": int(n // 2 * 6 * 12 + n * 8 * 6 + (n // 2) * 8 * 3),
+                    "d2h_bytes_per_step": int(8 * (2 * n + n // 2))},
+            "clocks": clocks}
     print(json.dumps(line))
+
+
+def measure_single(name: str, steps: int = 2, warmup: int = 1) -> dict:
+    """Time to 1e-6 of one single-instance workload: the problem resident
+    (pdhcg_b200_upload, then solves) and from host buffers, beside the
+    reference's own build on the same instance when it is present."""
+    import torch
+    lib = native.load()
+    W = WORKLOADS[name]
+    problem = W["make"](1.0, 0)
+    prob, keep = capi.build(lib, problem)
+    prm = _params(lib)
+    handle = lib.pdhcg_b200_upload(prob)
+    res = {}
+    for device in (True, False):
+        ts = []
+        for i in range(warmup + steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = lib.pdhcg_b200_solve_device(handle, C.byref(prm), None) if device else \
+                lib.pdhcg_b200_solve(prob, C.byref(prm), None)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            d = capi.result_dict(r, problem.n, problem.A.m) if not device else {
+                "status": capi.TERMINATION_REASONS[r.contents.termination_reason],
+                "total_count": r.contents.total_count, "primal_objective_value": r.contents.primal_objective_value,
+                "total_inner_count": r.contents.total_inner_count}
+            lib.pdhcg_result_free(r)
+            if i >= warmup:
+                ts.append(dt)
+        res["device" if device else "host"] = (float(np.mean(ts)), d)
+    lib.pdhcg_b200_device_problem_free(handle)
+    lib.qp_problem_free(prob)
+    (tv, d), (te, _) = res["device"], res["host"]
+    out = {"value": tv, "unit": "s", "e2e": te, "status": d["status"], "iterations": d["total_count"],
+           "inner_iterations": d.get("total_inner_count"), "objective": d["primal_objective_value"],
+           "workload": W["desc"]}
+    path = os.path.join(ROOT, "oracle", "_ref", "libpdhcg_ref.so")
+    if os.path.exists(path):
+        ref = capi.bind_api(C.CDLL(path))
+        rprob, rkeep = capi.build(ref, problem)
+        rprm = _params(ref)
+        ts = []
+        for i in range(1 + 1):
+            t0 = time.perf_counter()
+            r = ref.solve_qp_problem(rprob, C.byref(rprm))
+            dt = time.perf_counter() - t0
+            rd = capi.result_dict(r, problem.n, problem.A.m)
+            ref.pdhcg_result_free(r)
+            if i >= 1:
+                ts.append(dt)
+        ref.qp_problem_free(rprob)
+        out["reference"] = {"value": float(np.mean(ts)), "unit": "s", "status": rd["status"],
+                            "iterations": rd["total_count"],
+                            "objective_rel_diff": abs(d["primal_objective_value"] - rd["primal_objective_value"]) /
+                                                  (1 + abs(rd["primal_objective_value"])),
+                            "call": "the reference's own build, solve_qp_problem from host buffers"}
+        out["speedup_e2e_vs_reference"] = out["reference"]["value"] / te
+    return out
 
 
 def run_reference(args):
@@ -560,7 +661,18 @@ def main():
     ap.add_argument("--train", type=int, default=2000, help="warm_start: training solves")
     ap.add_argument("--heldout", type=int, default=200, help="warm_start: held-out solves")
     ap.add_argument("--epochs", type=int, default=100, help="warm_start: training epochs")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="soc_qp: leave out the batched, warm-start, sparse_qp and portfolio measurements")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: start them (the driver launches torchrun itself)
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+        sys.exit(subprocess.call(cmd))
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "mpc_batch":

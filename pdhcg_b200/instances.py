@@ -408,37 +408,59 @@ def mpc_qp(seed: int, horizon: int, nx: int = 8, nu: int = 4) -> Problem:
     nxT, nuT = nx * T, nu * T
     n = nxT + nuT
     m = nxT
-    rows, cols, vals = [], [], []
-    b = np.zeros(m)
     x0 = rng.standard_normal(nx)
+    # the draws in their stage order (E_0, B_0, E_1, B_1, ...), then the
+    # stages' arithmetic on the stacks
+    E = np.empty((T, nx, nx))
+    Bs = np.empty((T, nx, nu))
     for t in range(T):
-        At = np.eye(nx) + rng.standard_normal((nx, nx)) * (0.3 / np.sqrt(nx))
-        rad = np.max(np.abs(np.linalg.eigvals(At)))
-        if rad > 1.0:
-            At /= rad
-        Bt = rng.standard_normal((nx, nu)) * 0.3
-        r0 = t * nx
-        # + x_{t+1}
-        rows.append(r0 + np.arange(nx)); cols.append(t * nx + np.arange(nx)); vals.append(np.ones(nx))
-        if t == 0:
-            b[:nx] = At @ x0
-        else:
-            rr, cc = np.meshgrid(np.arange(nx), np.arange(nx), indexing="ij")
-            rows.append((r0 + rr).ravel()); cols.append(((t - 1) * nx + cc).ravel()); vals.append(-At.ravel())
-        rr, cc = np.meshgrid(np.arange(nx), np.arange(nu), indexing="ij")
-        rows.append((r0 + rr).ravel()); cols.append((nxT + t * nu + cc).ravel()); vals.append(-Bt.ravel())
-    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(m, n))
-    A.sort_indices()
+        E[t] = rng.standard_normal((nx, nx))
+        Bs[t] = rng.standard_normal((nx, nu))
+    At = np.eye(nx) + E * (0.3 / np.sqrt(nx))
+    rad = np.max(np.abs(np.linalg.eigvals(At)), axis=1)
+    At[rad > 1.0] /= rad[rad > 1.0][:, None, None]
+    Bt = Bs * 0.3
+    b = np.zeros(m)
+    b[:nx] = At[0] @ x0
+    # CSR rows in column order: -A_t (from stage 1 on), the identity of
+    # x_{t+1}, -B_t; stage 0 rows have 1 + nu entries, the others nx + 1 + nu
+    i = np.arange(nx)
+    c0 = np.concatenate([i[:, None], nxT + np.broadcast_to(np.arange(nu), (nx, nu))], axis=1)
+    v0 = np.concatenate([np.ones((nx, 1)), -Bt[0]], axis=1)
+    t = np.arange(1, T)[:, None, None]
+    ca = np.broadcast_to((t - 1) * nx + np.arange(nx)[None, None, :], (T - 1, nx, nx))
+    ci = np.broadcast_to(t * nx + i[None, :, None], (T - 1, nx, 1))
+    cb = np.broadcast_to(nxT + t * nu + np.arange(nu)[None, None, :], (T - 1, nx, nu))
+    c1 = np.concatenate([ca, ci, cb], axis=2)
+    v1 = np.concatenate([-At[1:], np.ones((T - 1, nx, 1)), -Bt[1:]], axis=2)
+    col = np.concatenate([c0.ravel(), c1.ravel()])
+    val = np.concatenate([v0.ravel(), v1.ravel()])
+    per = np.full(m, 1 + nu, dtype=np.int64)
+    per[nx:] += nx
+    row_ptr = np.concatenate([[0], np.cumsum(per)])
+    A = CsrMatrix(m, n, row_ptr.astype(np.int32), col.astype(np.int32), val)
     q = rng.uniform(0.1, 1.0, n)
     lb = np.concatenate([np.full(nxT, -np.inf), np.full(nuT, -1.0)])
     ub = np.concatenate([np.full(nxT, np.inf), np.full(nuT, 1.0)])
     Q = CsrMatrix(n, n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), q)
-    return Problem(c=np.zeros(n), A=CsrMatrix.from_scipy(A), con_lb=b, con_ub=b.copy(), var_lb=lb, var_ub=ub, Q=Q)
+    return Problem(c=np.zeros(n), A=A, con_lb=b, con_ub=b.copy(), var_lb=lb, var_ub=ub, Q=Q)
 
 
-def mpc_batch(seed: int = 4, count: int = 4096, tmin: int = 10, tmax: int = 100) -> list:
+def mpc_horizons(seed: int = 4, count: int = 4096, tmin: int = 10, tmax: int = 100) -> np.ndarray:
+    """The horizons of mpc_batch(seed, count), without building the instances."""
+    return np.random.default_rng(seed).integers(tmin, tmax + 1, size=count)
+
+
+def mpc_nnz(horizon: int, nx: int = 8, nu: int = 4) -> int:
+    """Nonzeros of mpc_qp(., horizon)'s constraint matrix: per stage the
+    identity of x_{t+1}, A_t (except the first stage, whose A_0 x_0 is the
+    right-hand side) and B_t."""
+    return int(horizon * (nx + nx * nu) + (horizon - 1) * nx * nx)
+
+
+def mpc_batch(seed: int = 4, count: int = 4096, tmin: int = 10, tmax: int = 100, indices=None) -> list:
     """`count` MPC QPs of uneven horizons T ~ U{tmin..tmax}, instance i seeded
-    by (seed, i)."""
-    rng = np.random.default_rng(seed)
-    horizons = rng.integers(tmin, tmax + 1, size=count)
-    return [mpc_qp(seed * 1000003 + i, int(horizons[i])) for i in range(count)]
+    by (seed, i); ``indices`` builds only those instances of the batch."""
+    horizons = mpc_horizons(seed, count, tmin, tmax)
+    idx = range(count) if indices is None else indices
+    return [mpc_qp(seed * 1000003 + i, int(horizons[i])) for i in idx]
