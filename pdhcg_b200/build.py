@@ -48,10 +48,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for src in SOURCES:
         obj = os.path.join(CSRC, os.path.splitext(src)[0] + ".o")
         if src.endswith(".cu"):
-            # --split-compile: the device optimiser and ptxas work on the
-            # kernels of one translation unit in parallel (solver.cu: 10 -> 3.5 min)
-            cmd = [nvcc, *ARCH, "-lineinfo", "-Xptxas", "-warn-spills", "--split-compile=8", *common, "-c",
-                   os.path.join(CSRC, src), "-o", obj]
+            # (no --split-compile: it cut the build from 10 to 3.5 min but
+            # changed the register allocation of the step kernels -- 80 -> 101
+            # registers on the cone kernel, spills in the FP32 dual kernel --
+            # and cost ~8 % of the step)
+            cmd = [nvcc, *ARCH, "-lineinfo", "-Xptxas", "-warn-spills", *common, "-c", os.path.join(CSRC, src),
+                   "-o", obj]
         else:
             cmd = [os.environ.get("CXX", "g++"), "-O3", "-std=c++17", "-fPIC", "-I" + os.path.join(ROOT, "include"),
                    "-c", os.path.join(CSRC, src), "-o", obj]

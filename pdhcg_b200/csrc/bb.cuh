@@ -309,6 +309,53 @@ __device__ __forceinline__ double bb_cone_block(const BBData &D, const double *d
     return part;
 }
 
+// A PSD block longer than the warp's registers hold: the same step, slot by
+// slot, with the candidate staged in the block's scratch and projected in
+// memory.
+template <int G>
+__device__ __noinline__ double bb_psd_long_block(const BBData &D, const double *drx, bool init, double alpha,
+                                                 int lane, int cb)
+{
+    const int st = D.cone_start[cb], L = D.cone_len[cb];
+    const int n = psd_order(L);
+    double *work = D.psd_work + D.psd_off[cb];
+    double *sv = work + 2LL * n * n, *xo_s = sv + L; // candidates, then the values before the step
+    for (int i = lane; i < L; i += 32) {
+        const int j = st + i;
+        const double mi = D.m_inv ? D.m_inv[j] : 1.0;
+        double g, xo;
+        if (init) {
+            double q = 0.0; // (Q x)_j, one lane per slot
+            if (D.sparse)
+                for (int t = D.Q_rp[j]; t < D.Q_rp[j + 1]; ++t)
+                    q += D.Q_v[t] * D.x[D.Q_ci[t]];
+            if (D.k > 0)
+                q += bb_rt_part<1>(D, drx, j, 0);
+            g = q + D.c[j] - D.aty[j];
+            xo = D.x[j];
+            D.grad[j] = g;
+            D.qx[j] = q;
+        } else {
+            g = D.grad[j];
+            xo = D.xp[j];
+        }
+        sv[i] = clampd(D.l[j], xo - alpha * mi * g, D.u[j]);
+        xo_s[i] = xo;
+    }
+    __syncwarp();
+    warp_project_psd_mem(sv, sv, L, lane, work);
+    double part = 0.0;
+    for (int i = lane; i < L; i += 32) {
+        const int j = st + i;
+        D.xp[j] = sv[i];
+        const double dd = sv[i] - xo_s[i];
+        D.dir[j] = dd;
+        part += D.m_diag ? dd * D.m_diag[j] * dd : dd * dd;
+    }
+    __syncwarp();
+    return part;
+}
+
 // init: grad = Qx + c - A^T y; x_p = P(x - alpha0 M^-1 grad); dir = x_p - x
 // (reference primal_gradient_descent_kernel_bb_init[_precond] and the cone
 // projection that follows, src/pdhg_core_op.cu:531-566)
@@ -368,7 +415,9 @@ __device__ double bb_var_phase(const BBData &D, const double *drx, bool init, do
             // instantiation, which alone carries their projection
             const int cb = task - W.free_tasks;
             const bool three = S > 1 && (D.cone_type[cb] == 2 || D.cone_type[cb] == 3);
-            if (SECT && D.cone_fixed[cb])
+            if (D.cone_type[cb] == 4 && D.cone_len[cb] > 32 * S)
+                part += bb_psd_long_block<G>(D, drx, init, alpha, lane, cb);
+            else if (SECT && D.cone_fixed[cb])
                 part += three ? bb_cone_block<G, 1, SECT>(D, drx, init, alpha, lane, stage, cb)
                               : bb_cone_block<G, S, SECT>(D, drx, init, alpha, lane, stage, cb);
             else if (three)

@@ -396,6 +396,14 @@ __device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform
     // 1/(omega_i + lam) (reused for the output).
     double b[S], om[S], inv[S];
     double n2 = 0.0, p2 = 0.0;
+    // d uniform over the block (what cone-preserving scaling gives): one
+    // reciprocal serves every slot (the same value each slot would compute)
+    bool dsame = true;
+#pragma unroll
+    for (int s = 0; s < S; ++s)
+        if (lane + 32 * s < apex)
+            dsame = dsame && sl.d[s] == dz;
+    const double rdz = __all_sync(FULL, dsame) ? __drcp_rn(dz) : 0.0;
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         int i = lane + 32 * s;
@@ -403,7 +411,7 @@ __device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform
         om[s] = 1.0;
         inv[s] = 1.0;
         if (i < apex) {
-            double rd = __drcp_rn(sl.d[s]);
+            double rd = rdz != 0.0 ? rdz : __drcp_rn(sl.d[s]);
             double a = sl.x[s] * rd;
             om[s] = fmax(sl.w[s] * sl.d[s] * sl.d[s], DBL_MIN);
             b[s] = sl.w[s] * sl.d[s] * sl.x[s];
@@ -448,21 +456,18 @@ __device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform
         double izl = 0.0;
         bool done = false;
         for (int it = 0; it < ROOT_ITERS; ++it) {
-            double t2 = 0.0, dt2 = 0.0;
+            double t2 = 0.0;
 #pragma unroll
             for (int s = 0; s < S; ++s)
                 if (lane + 32 * s < apex) {
                     inv[s] = __drcp_rn(om[s] + lam);
                     double t = b[s] * inv[s];
                     t2 += t * t;
-                    dt2 += t * t * inv[s];
                 }
             t2 = warp_sum(t2);
-            dt2 = warp_sum(dt2);
             izl = __drcp_rn(omz - lam);
             double z = bz * izl;
             double f = t2 - z * z;
-            double df = -2.0 * dt2 - 2.0 * z * z * izl;
             if ((lower && f > 0.0) || (!lower && f < 0.0))
                 lo = lam;
             else
@@ -471,6 +476,17 @@ __device__ void warp_project_soc(WarpSlots<S> &sl, int L, int lane, bool uniform
                 done = true;
                 break;
             }
+            // f' only when a Newton step follows (a warm-started search
+            // usually stops at its first evaluation)
+            double dt2 = 0.0;
+#pragma unroll
+            for (int s = 0; s < S; ++s)
+                if (lane + 32 * s < apex) {
+                    double t = b[s] * inv[s];
+                    dt2 += t * t * inv[s];
+                }
+            dt2 = warp_sum(dt2);
+            double df = -2.0 * dt2 - 2.0 * z * z * izl;
             double nx = lam - f / df;
             // a Newton step below the resolution of lam cannot improve it:
             // stop there (without this, rounding that keeps |f| above its
@@ -1008,6 +1024,116 @@ __device__ void warp_project_psd(WarpSlots<S> &sl, int L, int lane, double *work
         }
     }
     __syncwarp(); // the scratch may be reused by this warp's next projection
+}
+
+// PSD blocks of any order ("long" blocks: more slots than a warp's
+// registers hold, L > 32 S).  The svec lies in memory (in, L doubles; out
+// may alias it); the warp unpacks it into work[0, n^2), runs the same
+// cyclic Jacobi as warp_project_psd with every row / column loop strided
+// over the lanes, clips and repacks into out.  Callers stage the block's
+// candidate in its scratch (after the 2 n^2 doubles of the decomposition)
+// and call this instead of the register form.
+__device__ __forceinline__ int psd_order(int L)
+{
+    int n = (int)floor(sqrt(2.0 * L));
+    while (n * (n + 1) / 2 < L)
+        ++n;
+    while (n > 1 && (n - 1) * n / 2 >= L)
+        --n;
+    return n;
+}
+
+// L doubles of candidate staging per long block, after its 2 n^2 doubles
+// (the residual stages three vectors, so 3 L are kept)
+__host__ __device__ inline long long psd_scratch_doubles(int order, bool is_long)
+{
+    const long long L = (long long)order * (order + 1) / 2;
+    return 2LL * order * order + (is_long ? 3 * L : 0);
+}
+
+__device__ void warp_project_psd_mem(const double *in, double *out, int L, int lane, double *work)
+{
+    const int n = psd_order(L);
+    if (n == 1) {
+        if (lane == 0)
+            out[0] = fmax(in[0], 0.0);
+        __syncwarp();
+        return;
+    }
+    bool finite = true;
+    for (int i = lane; i < L; i += 32)
+        finite &= isfinite(in[i]) != 0;
+    if (!__all_sync(FULL, finite)) { // the reference's failed decomposition gives NaN
+        for (int i = lane; i < L; i += 32)
+            out[i] = __longlong_as_double(0x7ff8000000000000LL);
+        __syncwarp();
+        return;
+    }
+    const double R2 = 1.41421356237309504880, IR2 = 0.70710678118654752440;
+    double *A = work, *V = work + (size_t)n * n;
+    for (int col = 0, first = 0; col < n; first += n - col, ++col)
+        for (int row = col + lane; row < n; row += 32) {
+            const double x = in[first + row - col];
+            const double v = row == col ? x : x * IR2;
+            A[(size_t)row * n + col] = v;
+            A[(size_t)col * n + row] = v;
+        }
+    for (long long e = lane; e < (long long)n * n; e += 32)
+        V[e] = (e / n == e % n) ? 1.0 : 0.0;
+    __syncwarp();
+    for (int sweep = 0; sweep < PSD_MAX_SWEEPS; ++sweep) {
+        double off = 0.0, all = 0.0;
+        for (long long e = lane; e < (long long)n * n; e += 32) {
+            const double a2 = A[e] * A[e];
+            all += a2;
+            if (e / n != e % n)
+                off += a2;
+        }
+        off = warp_sum(off);
+        all = warp_sum(all);
+        if (!(off > PSD_OFF_REL * all))
+            break;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                const double apq = A[(size_t)p * n + q];
+                if (apq == 0.0)
+                    continue;
+                const double theta = (A[(size_t)q * n + q] - A[(size_t)p * n + p]) / (2.0 * apq);
+                const double t = fabs(theta) > 1e150
+                                     ? 0.5 / theta
+                                     : (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+                __syncwarp(); // every lane has read a_pp, a_qq, a_pq
+                for (int k = lane; k < n; k += 32) { // columns p, q of A and V
+                    const double akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+                    A[(size_t)k * n + p] = c * akp - sn * akq;
+                    A[(size_t)k * n + q] = sn * akp + c * akq;
+                    const double vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
+                    V[(size_t)k * n + p] = c * vkp - sn * vkq;
+                    V[(size_t)k * n + q] = sn * vkp + c * vkq;
+                }
+                __syncwarp();
+                for (int k = lane; k < n; k += 32) { // rows p, q of A
+                    const double apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+                    A[(size_t)p * n + k] = c * apk - sn * aqk;
+                    A[(size_t)q * n + k] = sn * apk + c * aqk;
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    A[(size_t)p * n + q] = 0.0;
+                    A[(size_t)q * n + p] = 0.0;
+                }
+                __syncwarp();
+            }
+    }
+    for (int col = 0, first = 0; col < n; first += n - col, ++col)
+        for (int row = col + lane; row < n; row += 32) {
+            double v = 0.0;
+            for (int e = 0; e < n; ++e)
+                v += fmax(A[(size_t)e * n + e], 0.0) * V[(size_t)row * n + e] * V[(size_t)col * n + e];
+            out[first + row - col] = row == col ? v : v * R2;
+        }
+    __syncwarp(); // the scratch and out may be read by other lanes next
 }
 
 // Cone kinds an instantiation carries: SOC / RSOC (any S), the 3-slot

@@ -233,9 +233,57 @@ __device__ __forceinline__ void primal_cone_block(const StepData<T> &D, const St
     }
 }
 
+// A PSD block longer than the warp's registers hold (L > 32 S): the same
+// step with the candidate staged in the block's scratch.  Chunks of 32 S
+// rows of A^T y and prox, the projection in memory, then the reflection and
+// Halpern average slot by slot.
+template <int S, typename T, bool HAS_Q>
+__device__ __noinline__ void primal_psd_long_block(const StepData<T> &D, const StepParams &P, int cb, int lane,
+                                                   double *stage)
+{
+    const int st = D.cone_start[cb], L = D.cone_len[cb];
+    const int n = psd_order(L);
+    double *work = D.psd_work + D.psd_off[cb];
+    double *sv = work + 2LL * n * n;
+    for (int c0 = 0; c0 < L; c0 += 32 * S) {
+        const int nr = min(32 * S, L - c0);
+        double aty[S];
+        warp_stream_rows<S>(D.At_rp, D.At_ci, D.At_v, D.y, st + c0, nr, lane, stage, aty, D.At_long);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const int i = lane + 32 * s;
+            if (i < nr) {
+                const int j = st + c0 + i;
+                double t = (double)D.x[j] - P.tau * ((double)D.c[j] - aty[s]);
+                if (HAS_Q)
+                    t /= 1.0 + P.tau * (double)D.q[j];
+                const double xc = P.cone_box ? clampd(D.l[j], t, D.u[j]) : t;
+                if (P.lp_slack)
+                    D.dual_slack[j] = (T)((xc - t) / P.tau);
+                sv[c0 + i] = xc;
+            }
+        }
+    }
+    __syncwarp();
+    warp_project_psd_mem(sv, sv, L, lane, work);
+    for (int i = lane; i < L; i += 32) {
+        const int j = st + i;
+        const double xi = D.x[j], p = sv[i];
+        const double xr = 2.0 * p - xi;
+        D.xr[j] = (T)xr;
+        D.xp[j] = (T)p;
+        if (P.want_fpe)
+            D.dx[j] = (T)(xr - xi);
+        const double refl = P.rho * xr + (1.0 - P.rho) * xi;
+        D.x[j] = (T)(P.w * refl + (1.0 - P.w) * (double)D.x0[j]);
+    }
+    __syncwarp();
+}
+
 // One warp per cone block of the list ids (NULL: blocks 0 .. nids - 1);
 // KINDS = CONES_WIDE for SOC / RSOC blocks, CONES_THREE (S = 1) for the
-// 3-slot exponential and power blocks, CONES_PSD for PSD blocks.
+// 3-slot exponential and power blocks, CONES_PSD for PSD blocks (those
+// longer than 32 S slots through their scratch).
 template <int S, typename T, bool HAS_Q, int KINDS>
 __global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<T> D, StepParams P, const int *ids, int nids)
 {
@@ -244,8 +292,16 @@ __global__ void __launch_bounds__(TPB) primal_cone_kernel(StepData<T> D, StepPar
     const int warp = blockIdx.x * WARPS + (threadIdx.x >> 5);
     const int nwarps = gridDim.x * WARPS;
     double *stage = stage_all[threadIdx.x >> 5];
-    for (int i = warp; i < nids; i += nwarps)
-        primal_cone_block<S, T, HAS_Q, KINDS>(D, P, ids ? ids[i] : i, lane, stage);
+    for (int i = warp; i < nids; i += nwarps) {
+        const int cb = ids ? ids[i] : i;
+        if constexpr ((KINDS & CONES_PSD) != 0) {
+            if (D.cone_len[cb] > 32 * S) {
+                primal_psd_long_block<S, T, HAS_Q>(D, P, cb, lane, stage);
+                continue;
+            }
+        }
+        primal_cone_block<S, T, HAS_Q, KINDS>(D, P, cb, lane, stage);
+    }
 }
 
 // One tile of 32 consecutive rows of A: A x_refl by stream-mode products,

@@ -221,6 +221,70 @@ __device__ __forceinline__ void residual_cone_block(const ResidualData<VT> &D, c
     }
 }
 
+// A PSD block longer than the warp's registers hold: the terms of
+// residual_cone_block slot by slot, with rc, the augmented point and A^T y
+// staged in the block's scratch and the two projections (no metric, as for
+// every PSD block) taken in memory.
+template <int S, typename VT>
+__device__ __noinline__ void residual_psd_long_block(const ResidualData<VT> &D, const ResidualParams &P, int cb,
+                                                     int lane, double *stage, double (&acc)[RS_COUNT],
+                                                     const int (&ops)[RS_COUNT])
+{
+    auto fold = [&](int s, double v) { acc[s] = ops[s] == RMAX ? fmax(acc[s], v) : acc[s] + v; };
+    const int st = D.cone_start[cb], L = D.cone_len[cb];
+    const int n = psd_order(L);
+    double *work = D.psd_work + D.psd_off[cb];
+    double *rcv = work + 2LL * n * n, *augv = rcv + L, *atyv = augv + L;
+    auto qx_of = [&](int j, double x) {
+        return P.qmode == 1 ? D.q[j] * x : (P.qmode == 2 ? D.qx[j] : 0.0);
+    };
+    for (int c0 = 0; c0 < L; c0 += 32 * S) {
+        const int nr = min(32 * S, L - c0);
+        double atys[S];
+        warp_stream_rows<S>(D.At_rp, D.At_ci, D.At_v, D.yp, st + c0, nr, lane, stage, atys, D.At_long);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const int i = lane + 32 * s;
+            if (i < nr) {
+                const int j = st + c0 + i;
+                const double x = D.xp[j];
+                const double eff = P.qmode ? D.c[j] + qx_of(j, x) : D.c[j];
+                const double rc = eff - atys[s];
+                rcv[c0 + i] = rc;
+                augv[c0 + i] = clampd(D.l[j], x - P.s_aug * rc, D.u[j]);
+                atyv[c0 + i] = atys[s];
+            }
+        }
+    }
+    __syncwarp();
+    double *psd = D.psd_work + D.psd_off[cb];
+    warp_project_psd_mem(rcv, rcv, L, lane, psd);   // the dual cone (self-dual) of rc
+    warp_project_psd_mem(augv, augv, L, lane, psd); // the augmented point
+    for (int i = lane; i < L; i += 32) {
+        const int j = st + i;
+        const double x = D.xp[j], qx = qx_of(j, x), aty = atyv[i];
+        const double eff = P.qmode ? D.c[j] + qx : D.c[j];
+        const double rc = eff - aty, vr = D.vr[j];
+        double dr = (rc - rcv[i]) * vr;
+        double rr = (x - augv[i]) / P.s_aug * vr;
+        if (!isfinite(rr))
+            rr = copysign(INFINITY, rr);
+        if (fabs(rr) > fabs(dr))
+            dr = rr;
+        fold(RS_DUAL_RES, norm_term(dr, P.l2));
+        fold(RS_CX, D.c[j] * x);
+        fold(RS_XQX, x * qx);
+        fold(RS_SLACKX, rc * x);
+        fold(RS_QX_NORM, norm_term(qx * vr, P.l2));
+        fold(RS_ATY_NORM, norm_term(aty * vr, P.l2));
+        if (P.want_dist) {
+            const double d = x - (double)D.x0[j];
+            fold(RS_DIST_X, d * d);
+        }
+    }
+    __syncwarp();
+}
+
 // One affine cone block of rows (reference compute_residual with affine
 // cones, src/pdhg_core_op.cu:1037-1294, and compute_affine_cone_residuals,
 // :109-212): v = A x + g; the primal residual is v - proj_K(v) scaled by
@@ -395,6 +459,8 @@ __global__ void __launch_bounds__(TPB) residual_kernel(ResidualData<VT> D, Resid
                     residual_cone_block<S, VT, true>(D, P, cb, lane, stage, acc, ops);
             } else if (S > 1 && (ct == 2 || ct == 3)) {
                 residual_cone_block<1, VT>(D, P, cb, lane, stage, acc, ops);
+            } else if (ct == 4 && D.cone_len[cb] > 32 * S) {
+                residual_psd_long_block<S, VT>(D, P, cb, lane, stage, acc, ops);
             } else {
                 residual_cone_block<S, VT>(D, P, cb, lane, stage, acc, ops);
             }

@@ -511,7 +511,10 @@ __global__ void __launch_bounds__(TPB) project_cones_kernel(int ncones, const in
         double *wb = warm ? warm + cb : nullptr;
         if (S > 1 && (tp == 2 || tp == 3)) // 3-slot blocks: the one-slot instantiation
             project_cone_block<1>(st, L, tp, a, x, d, q, tau, lane, psd, fixed, sect, wb);
-        else
+        else if (tp == 4 && L > 32 * S) { // a long PSD block: in place, in memory (no metric)
+            if (psd)
+                warp_project_psd_mem(x + st, x + st, L, lane, psd);
+        } else
             project_cone_block<S>(st, L, tp, a, x, d, q, tau, lane, psd, fixed, sect, wb);
     }
 }

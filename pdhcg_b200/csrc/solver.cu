@@ -534,7 +534,10 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
         d.cone_len.push_back(len);
         d.cone_type.push_back((int)p->cones.type[b]);
         d.cone_vdim.push_back(p->cones.v_dim[b]);
-        maxlen = std::max(maxlen, len);
+        // PSD blocks beyond the widest slot class take the memory path
+        // (their length does not set the class)
+        if (!(p->cones.type[b] == CONE_PSD && len > 32 * 8))
+            maxlen = std::max(maxlen, len);
         for (int i = 0; i < len; ++i) {
             int j = p->cones.start_idx[b] + i;
             in_cone[j] = 1;
@@ -542,12 +545,11 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
         }
         d.psd_off.push_back(d.psd_total);
         if (p->cones.type[b] == CONE_PSD) {
-            const int order = p->cones.v_dim[b];
-            if (order > PSD_MAX_ORDER)
-                d.unsupported = "PSD blocks of order above 22 are not supported yet";
+            // decomposition scratch, plus candidate staging for blocks the
+            // registers of a warp do not hold (any order)
             d.has_psd = true;
             d.var_psd = true;
-            d.psd_total += 2LL * order * order;
+            d.psd_total += psd_scratch_doubles(p->cones.v_dim[b], len > 32);
         }
         d.cone_alpha.push_back(p->cones.power_alpha ? p->cones.power_alpha[b] : 0.0);
     }
@@ -619,7 +621,7 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
             d.aff_psd_off.push_back(d.psd_total);
             if (t == CONE_PSD) {
                 if (vd > PSD_MAX_ORDER)
-                    d.unsupported = "PSD blocks of order above 22 are not supported yet";
+                    d.unsupported = "affine PSD blocks of order above 22 are not supported yet";
                 d.has_psd = true;
                 d.psd_total += 2LL * vd * vd;
             }
@@ -2734,7 +2736,8 @@ int pdhcg_b200_project_cones(int num_cones, const int *cone_start, const int *co
             return -1;
         }
         for (int i = 0; i < num_cones; ++i) {
-            maxlen = std::max(maxlen, h[i]);
+            if (!(t[i] == CONE_PSD && h[i] > 32 * 8)) // long PSD blocks: projected in memory, in place
+                maxlen = std::max(maxlen, h[i]);
             types_ok = types_ok && (t[i] == CONE_STANDARD_SOC || t[i] == CONE_ROTATED_SOC ||
                                     t[i] == CONE_EXPONENTIAL || (t[i] == CONE_POWER && cone_alpha) ||
                                     t[i] == CONE_PSD);

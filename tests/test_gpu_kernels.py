@@ -167,6 +167,49 @@ def test_psd_projection_matches_oracle(lib, oracle):
     np.testing.assert_allclose(xd.cpu().numpy(), expect, rtol=1e-10, atol=1e-10 * np.abs(expect).max())
 
 
+@pytest.mark.parametrize("orders", [(23, 32), (64,), (100,)])
+def test_psd_projection_of_large_orders(lib, oracle, orders):
+    """PSD blocks of orders 23 .. 100 (more svec slots than a warp's
+    registers hold: projected through device scratch) among SOC blocks,
+    spectra of mixed signs, against the oracle's Jacobi restatement and
+    numpy's eigh: 1e-10 relative to the block scale."""
+    import torch
+    rng = np.random.default_rng(sum(orders))
+    blocks, parts, st = [], [], 0
+    for order in orders:
+        M = rng.standard_normal((order, order))
+        M = (M + M.T) / 2
+        v = _svec(M)
+        blocks.append((st, order, capi.CONE_PSD, M))
+        parts.append(v)
+        st += len(v)
+        L = int(rng.integers(3, 40))
+        blocks.append((st, L - 2, capi.CONE_STANDARD_SOC, None))
+        parts.append(rng.standard_normal(L))
+        st += L
+    x = np.concatenate(parts)
+    d = rng.uniform(0.5, 2.0, st)
+    expect = x.copy()
+    for s0, vd, t, M in blocks:
+        L = vd * (vd + 1) // 2 if t == capi.CONE_PSD else vd + 2
+        blk = expect[s0:s0 + L].copy()
+        dd = d[s0:s0 + L].copy()
+        oracle.oracle_project_cone_block(t, vd, 0.0, blk.ctypes.data_as(_dp), dd.ctypes.data_as(_dp), None, 0.0)
+        expect[s0:s0 + L] = blk
+        if M is not None:
+            w, V = np.linalg.eigh(M)
+            np.testing.assert_allclose(blk, _svec((V * np.maximum(w, 0)) @ V.T), atol=1e-10 * (1 + np.abs(M).max()))
+    starts = _dev([b[0] for b in blocks], np.int32)
+    vdims = _dev([b[1] for b in blocks], np.int32)
+    types = _dev([b[2] for b in blocks], np.int32)
+    xd, dd_ = _dev(x), _dev(d)
+    rc = lib.pdhcg_b200_project_cones(len(blocks), _ptr(starts), _ptr(vdims), _ptr(types), None, _ptr(xd),
+                                      _ptr(dd_), None, 0.0, None)
+    torch.cuda.synchronize()
+    assert rc == 0
+    np.testing.assert_allclose(xd.cpu().numpy(), expect, rtol=1e-10, atol=1e-10 * np.abs(expect).max())
+
+
 def test_cone_projection_rejects_unbuilt_cone_types(lib):
     """An unknown cone type is refused (-3) and x is left untouched."""
     import torch

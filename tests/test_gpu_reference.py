@@ -34,6 +34,8 @@ CASES = {
     "mixed_cones_lp": lambda: instances.conic_lp(seed=13, nexp=12, npow=12),
     "psd_lp": lambda: instances.psd_lp(),
     "psd_qp": lambda: instances.psd_lp(seed=8, with_q=True),
+    # PSD blocks of orders 24 and 30 (more slots than a warp's registers hold)
+    "psd_large_lp": lambda: instances.psd_lp(seed=12, orders=(24, 3, 30)),
     "sparse_qp_small": lambda: instances.sparse_qp(scale=0.05),
     "portfolio_small": lambda: instances.portfolio(scale=0.01),
     "dense_rows_lp": lambda: instances.dense_rows_qp(),

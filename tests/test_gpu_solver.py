@@ -96,6 +96,7 @@ CASES = {
     "psd_lp": (lambda: instances.psd_lp(), {}),
     "psd_lp_mixed_cones": (lambda: instances.psd_lp(seed=7, orders=(2, 4, 1, 3)), {"use_cone_preserving_scaling": False}),
     "psd_qp": (lambda: instances.psd_lp(seed=8, with_q=True), {}),
+    "psd_large_lp": (lambda: instances.psd_lp(seed=12, orders=(24, 3, 30)), {}),
     "all_cones_sparse_q": (_all_cones_sparse_q, {}),
     # affine cones F x + g in K over rows: every cone type, with and without Q
     "affine_lp": (lambda: instances.affine_cone_qp(), {}),
