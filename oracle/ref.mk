@@ -5,7 +5,10 @@
 # solve is run beside ours on a GPU host).  It is never linked into the
 # product.
 #
-#   make -f oracle/ref.mk REF=/root/reference -j8
+#   make -f oracle/ref.mk REF=<reference source tree> -j8
+#
+# REF defaults to $(PDHCG_REFERENCE_SRC), else a "reference" directory
+# beside the repository.
 #
 # The reference's own CMake build is not used.  The source list mirrors
 # what that build puts in its core library for a single-GPU build: every
@@ -13,7 +16,7 @@
 # distributed stubs.  It links the CUDA toolkit's cuSPARSE, cuBLAS and
 # cuSOLVER and zlib, all present in the image.
 
-REF ?= /root/reference
+REF ?= $(if $(PDHCG_REFERENCE_SRC),$(PDHCG_REFERENCE_SRC),$(abspath ../reference))
 OUT := oracle/_ref
 NVCC ?= nvcc
 CC ?= gcc

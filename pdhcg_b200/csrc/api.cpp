@@ -49,6 +49,44 @@ void csr_release(CsrComponent *c)
 }
 
 // ---- matrix descriptor checks (reference src/pdhcg.c:35-168) -------------
+// The two compressed formats are one check over a view: a pointer array
+// over the major dimension spanning [0, nnz], and minor indices in range.
+// The messages are the reference's (callers match on them).
+struct CompressedView {
+    const char *fmt;        // "CSR" / "CSC"
+    const char *ptrs;       // "row pointers" / "column pointers"
+    const char *major;      // "row" / "column"
+    const char *minor;      // "column" / "row"
+    int nmajor, nminor, nnz;
+    const int *ptr, *idx;
+    const double *vals;
+};
+
+int check_compressed(const CompressedView &v, const char *name)
+{
+    if (v.nnz < 0 || !v.ptr || (v.nnz > 0 && (!v.idx || !v.vals))) {
+        std::fprintf(stderr, "[create_qp_problem] %s %s storage is incomplete.\n", name, v.fmt);
+        return -1;
+    }
+    if (v.ptr[0] != 0 || v.ptr[v.nmajor] != v.nnz) {
+        std::fprintf(stderr, "[create_qp_problem] %s %s %s do not span [0, nnz].\n", name, v.fmt, v.ptrs);
+        return -1;
+    }
+    for (int r = 0; r < v.nmajor; ++r)
+        if (v.ptr[r] > v.ptr[r + 1] || v.ptr[r] < 0 || v.ptr[r + 1] > v.nnz) {
+            std::fprintf(stderr, "[create_qp_problem] %s %s %s are invalid at %s %d.\n", name, v.fmt, v.ptrs,
+                         v.major, r);
+            return -1;
+        }
+    for (int k = 0; k < v.nnz; ++k)
+        if (v.idx[k] < 0 || v.idx[k] >= v.nminor) {
+            std::fprintf(stderr, "[create_qp_problem] %s %s %s index %d is out of range [0, %d).\n", name, v.fmt,
+                         v.minor, v.idx[k], v.nminor);
+            return -1;
+        }
+    return 0;
+}
+
 int check_descriptor(const matrix_desc_t *d, const char *name)
 {
     if (!d)
@@ -58,6 +96,18 @@ int check_descriptor(const matrix_desc_t *d, const char *name)
         return -1;
     }
     switch (d->fmt) {
+    case matrix_csr: {
+        const auto &c = d->data.csr;
+        return check_compressed({"CSR", "row pointers", "row", "column", d->m, d->n, c.nnz, c.row_ptr, c.col_ind,
+                                 c.vals},
+                                name);
+    }
+    case matrix_csc: {
+        const auto &c = d->data.csc;
+        return check_compressed({"CSC", "column pointers", "column", "row", d->n, d->m, c.nnz, c.col_ptr, c.row_ind,
+                                 c.vals},
+                                name);
+    }
     case matrix_dense:
         if (d->m > 0 && d->n > INT_MAX / d->m) {
             std::fprintf(stderr, "[create_qp_problem] %s dense matrix is too large to index with int.\n", name);
@@ -68,74 +118,19 @@ int check_descriptor(const matrix_desc_t *d, const char *name)
             return -1;
         }
         return 0;
-    case matrix_csr: {
-        int nnz = d->data.csr.nnz;
-        const int *rp = d->data.csr.row_ptr;
-        if (nnz < 0 || !rp || (nnz > 0 && (!d->data.csr.col_ind || !d->data.csr.vals))) {
-            std::fprintf(stderr, "[create_qp_problem] %s CSR storage is incomplete.\n", name);
-            return -1;
-        }
-        if (rp[0] != 0 || rp[d->m] != nnz) {
-            std::fprintf(stderr, "[create_qp_problem] %s CSR row pointers do not span [0, nnz].\n", name);
-            return -1;
-        }
-        for (int r = 0; r < d->m; ++r)
-            if (rp[r] > rp[r + 1] || rp[r] < 0 || rp[r + 1] > nnz) {
-                std::fprintf(stderr, "[create_qp_problem] %s CSR row pointers are invalid at row %d.\n", name, r);
-                return -1;
-            }
-        for (int k = 0; k < nnz; ++k) {
-            int c = d->data.csr.col_ind[k];
-            if (c < 0 || c >= d->n) {
-                std::fprintf(stderr, "[create_qp_problem] %s CSR column index %d is out of range [0, %d).\n", name, c,
-                             d->n);
-                return -1;
-            }
-        }
-        return 0;
-    }
-    case matrix_csc: {
-        int nnz = d->data.csc.nnz;
-        const int *cp = d->data.csc.col_ptr;
-        if (nnz < 0 || !cp || (nnz > 0 && (!d->data.csc.row_ind || !d->data.csc.vals))) {
-            std::fprintf(stderr, "[create_qp_problem] %s CSC storage is incomplete.\n", name);
-            return -1;
-        }
-        if (cp[0] != 0 || cp[d->n] != nnz) {
-            std::fprintf(stderr, "[create_qp_problem] %s CSC column pointers do not span [0, nnz].\n", name);
-            return -1;
-        }
-        for (int c = 0; c < d->n; ++c)
-            if (cp[c] > cp[c + 1] || cp[c] < 0 || cp[c + 1] > nnz) {
-                std::fprintf(stderr, "[create_qp_problem] %s CSC column pointers are invalid at column %d.\n", name,
-                             c);
-                return -1;
-            }
-        for (int k = 0; k < nnz; ++k) {
-            int r = d->data.csc.row_ind[k];
-            if (r < 0 || r >= d->m) {
-                std::fprintf(stderr, "[create_qp_problem] %s CSC row index %d is out of range [0, %d).\n", name, r,
-                             d->m);
-                return -1;
-            }
-        }
-        return 0;
-    }
     case matrix_coo: {
-        int nnz = d->data.coo.nnz;
-        if (nnz < 0 || (nnz > 0 && (!d->data.coo.row_ind || !d->data.coo.col_ind || !d->data.coo.vals))) {
+        const auto &c = d->data.coo;
+        if (c.nnz < 0 || (c.nnz > 0 && (!c.row_ind || !c.col_ind || !c.vals))) {
             std::fprintf(stderr, "[create_qp_problem] %s COO storage is incomplete.\n", name);
             return -1;
         }
-        for (int k = 0; k < nnz; ++k) {
-            int r = d->data.coo.row_ind[k], c = d->data.coo.col_ind[k];
-            if (r < 0 || r >= d->m || c < 0 || c >= d->n) {
+        for (int k = 0; k < c.nnz; ++k)
+            if (c.row_ind[k] < 0 || c.row_ind[k] >= d->m || c.col_ind[k] < 0 || c.col_ind[k] >= d->n) {
                 std::fprintf(stderr,
                              "[create_qp_problem] %s COO index (%d, %d) is out of range for shape (%d, %d).\n", name,
-                             r, c, d->m, d->n);
+                             c.row_ind[k], c.col_ind[k], d->m, d->n);
                 return -1;
             }
-        }
         return 0;
     }
     default:
