@@ -39,6 +39,13 @@ WORKLOAD = "soc_qp: n=1e6 (20000 SOC blocks x 50), m=5e5 eq rows, 10 nnz/row, di
 # Single-instance workloads: the generator, the forms the solver has for the
 # problem class (the inner BB solve of sparse / low-rank Q runs in FP64
 # only) and what keeps the timed solves out of L2.
+# DRAM read + write bytes of one step of the SOC-QP workload (both
+# kernels), measured by ncu (profiles/step_kernels_soc_qp_n1e6.md)
+STEP_TRAFFIC = {"f64": 202.5e6, "f32": 121.4e6}
+# random 4- / 8-byte gathers per second of one B200 through L1TEX
+# (profiles/spmv_gather_ceiling_b200.md)
+GATHER_RATE = 1.95e11
+
 WORKLOADS = {
     "soc_qp": {"make": lambda scale, r: instances.soc_qp(seed=2 + r, scale=scale), "desc": WORKLOAD,
                "mixed": True, "l2": "working set (>=134 MB) larger than L2"},
@@ -131,6 +138,17 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def _cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(problem, n_iter_ref: int, budget_s: float = 20.0) -> dict:
     """The oracle (single-threaded FP64 port of the same iteration) timed on
     a bounded sample: a fixed number of iterations on the full workload,
@@ -155,7 +173,7 @@ def cpu_baseline(problem, n_iter_ref: int, budget_s: float = 20.0) -> dict:
     per_iter = (dt2 - dt) / (sample2 - sample_iters)
     setup = max(dt - per_iter * sample_iters, 0.0)
     est = setup + per_iter * n_iter_ref
-    return {"value": est, "unit": "s", "cores": 1, "kind": "port",
+    return {"value": est, "unit": "s", "cores": 1, "kind": "port", "cpu_model": _cpu_model(),
             "sample": f"oracle FP64 on the full workload: {sample_iters} and {sample2} iterations "
                       f"({dt:.1f}s, {dt2:.1f}s), extrapolated to {n_iter_ref} iterations "
                       f"(setup {setup:.2f}s + {per_iter * 1e3:.1f} ms/iter)"}
@@ -245,9 +263,24 @@ def run_ours(args):
     def roof(tstats):
         step_ms = tstats["step_kernel_ms"] / max(1, tstats["step_kernel_launches"])
         ach = tstats["step_bytes"] / (step_ms * 1e-3) / 1e9 if step_ms > 0 else None
+        # DRAM bytes (read + write) of one step's kernels, from the ncu capture of
+        # profiles/step_kernels_soc_qp_n1e6.md, weighted like the timed steps
+        traffic = None
+        if args.workload == "soc_qp" and args.scale == 1.0 and tstats["step_kernel_launches"] > 0:
+            f32 = tstats["fp32_iterations"] / tstats["step_kernel_launches"]
+            traffic = f32 * STEP_TRAFFIC["f32"] + (1.0 - f32) * STEP_TRAFFIC["f64"]
         return {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                "frac": (ach / peak) if ach else None, "traffic": None, "peak_kind": peak_kind,
-                "bytes_per_step": tstats["step_bytes"], "step_kernel_ms": step_ms}
+                "frac": (ach / peak) if ach else None, "traffic": traffic, "peak_kind": peak_kind,
+                "bytes_per_step": tstats["step_bytes"], "step_kernel_ms": step_ms,
+                "kernels": "the two launches of a step: primal_cone_kernel (A^T y, prox, SOC projection, "
+                           "Halpern) and dual_kernel (A x_refl, dual prox, Halpern)",
+                # each product gathers one vector entry per nonzero; the B200's
+                # random-gather rate bounds the step below HBM speed
+                "gather_bound": {"gathers_per_step": 2 * problem.A.nnz, "measured_ceiling_per_s": GATHER_RATE,
+                                 "floor_ms": 2 * problem.A.nnz / GATHER_RATE * 1e3,
+                                 "frac_of_floor": (2 * problem.A.nnz / GATHER_RATE * 1e3) / step_ms
+                                 if step_ms > 0 else None,
+                                 "source": "profiles/spmv_gather_ceiling_b200.md"}}
 
     head = out["mixed"] if W["mixed"] else out["fp64"]
     fp64 = out["fp64"]
@@ -343,6 +376,7 @@ def measure_batch(count: int, steps: int, warmup: int, rank: int = 0, world: int
         raise RuntimeError("batch autotune failed")
     res = (C.POINTER(capi.PdhcgResult) * max(k, 1))()
     launches = [0]
+    copies = [(0, 0, 0.0)]
 
     def solve():
         if not k:
@@ -354,6 +388,7 @@ def measure_batch(count: int, steps: int, warmup: int, rank: int = 0, world: int
         bst = native.BatchStats()
         lib.pdhcg_b200_last_batch_stats(C.byref(bst))
         launches[0] += bst.launches
+        copies[0] = (int(bst.h2d_bytes), int(bst.d2h_bytes), bst.pack_ms)
         out = {}
         for i, r in zip(mine, res[:k]):
             out[i] = (capi.TERMINATION_REASONS[r.contents.termination_reason], r.contents.total_count)
@@ -375,6 +410,9 @@ def measure_batch(count: int, steps: int, warmup: int, rank: int = 0, world: int
         t = torch.tensor([wall, kern], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         wall, kern = t[0].item(), t[1].item()
+        b = torch.tensor([float(copies[0][0]), float(copies[0][1])], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(b)  # copies of all ranks
+        copies[0] = (int(b[0].item()), int(b[1].item()), copies[0][2])
     allres = shard.gather_results(last, rank, world, count)
     nnz_mine = int(sum(weights[i] for i in mine))
     out = None
@@ -389,10 +427,8 @@ def measure_batch(count: int, steps: int, warmup: int, rank: int = 0, world: int
         seq = min(seq_sample, k) / (time.perf_counter() - t0)
         out = {"value": count / kern, "unit": "instances/s", "ms_per_step": kern * 1e3, "instances": count,
                "statuses": stat, "mean_iterations": float(np.mean([it for _, it in allres])),
-               "e2e": {"value": count / wall, "unit": "instances/s",
-                       "h2d_bytes_per_step": int(sum(p.A.nnz * 24 + (p.A.m + 1) * 4 + (p.n + 1) * 4 + p.n * 32 +
-                                                     p.A.m * 16 for p in probs)),
-                       "d2h_bytes_per_step": int(sum(8 * (p.n + p.A.m) for p in probs))},
+               "e2e": {"value": count / wall, "unit": "instances/s", "h2d_bytes_per_step": copies[0][0],
+                       "d2h_bytes_per_step": copies[0][1], "pack_ms_rank0": copies[0][2]},
                "sequential_plain_solves": {"value": seq, "unit": "instances/s", "sample": min(seq_sample, k),
                                            "call": "solve_qp_problem per instance, one GPU"},
                "speedup_vs_sequential": (count / wall) / seq,

@@ -139,14 +139,20 @@ int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *probs, const pd
                            const pdhcg_b200_batch_options_t *opts, pdhcg_result_t **results);
 /* Figures of the last pdhcg_b200_solve_batch on the calling thread. */
 typedef struct {
-    double kernel_ms;   /* the batch kernels, first launch to last (CUDA events) */
+    double kernel_ms;   /* device work: the A^T build and the batch kernels, first launch to last (CUDA events) */
     double total_ms;    /* the whole call, wall clock */
-    int launches;       /* kernel launches (one per size class) */
+    double pack_ms;     /* sizing and packing the instances into page-locked staging memory, wall clock */
+    double h2d_bytes;   /* bytes copied host to device (one copy of the packed inputs) */
+    double d2h_bytes;   /* bytes copied device to host (one copy of the packed outputs) */
+    int launches;       /* kernel launches (the A^T build, then one per size class) */
     int batched;        /* instances solved by the batch kernels */
     int fallback;       /* instances handed to solve_qp_problem */
     int reserved[5];
 } pdhcg_b200_batch_stats_t;
 int pdhcg_b200_last_batch_stats(pdhcg_b200_batch_stats_t *out);
+/* Batch solves keep their page-locked staging buffer and device buffer
+ * (sized for the largest batch so far) between calls; this frees both. */
+void pdhcg_b200_batch_release(void);
 
 /* Times every launch shape on the given instances (solving them each time)
  * and stores the fastest in opts->shape; shape_ms (may be NULL) receives

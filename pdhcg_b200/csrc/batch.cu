@@ -27,6 +27,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <optional>
 #include <thread>
 #include <vector>
 
@@ -47,6 +50,8 @@ struct BInst {            // one instance, offsets into the packed arrays
     long long k_off;      // entries of A (and of A^T, same count)
     long long x_off;      // x-side vectors (n)
     long long y_off;      // y-side vectors (m)
+    long long so_off;     // slice tables: A's (m/32 + 2 ints), then A^T's (n/32 + 2 ints)
+    int sell_a, sell_at;  // entries of A and A^T in the sliced layout (padding included)
     int smem;             // bytes of shared memory the instance needs
     int qmode;            // 0 LP, 1 diagonal Q
     double obj_const;
@@ -74,6 +79,7 @@ struct BData {               // packed inputs and outputs of the whole batch
     const double *c, *l, *u, *q;     // x side (q: diagonal, 0 for LP)
     const double *lc, *uc;           // y side
     const double *v0;                // power-method start vector (rand_r(1234) in [-1, 1])
+    const int *S_tab;                // slice tables of the sliced layout
     const BInst *inst;
     const int *order;                // instance indices, largest first
     int count;
@@ -95,24 +101,34 @@ __host__ __device__ inline int print_freq(int it)
     return step;
 }
 
+// Matrices in shared memory are sliced (SELL-32): rows in slices of 32,
+// slice s holding (max row length in s) x 32 entries, entry k of the slice's
+// row r at so[s] + 32 k + (r mod 32), rows shorter than the slice's longest
+// padded with (column 0, value 0).  The 32 lanes of a warp own the 32 rows
+// of one slice, so a product reads indices and values without bank
+// conflicts, every lane of the warp runs the same trip count, and the
+// padding adds exact zeros after a row's entries (the sums are those of the
+// plain CSR loop).  so[] has one entry per slice plus the end.
+__host__ __device__ inline int slices(int rows) { return (rows + 31) >> 5; }
+
 // Shared-memory layout of one instance (byte offsets; every array 16-byte aligned).
 struct Layout {
-    int arp, atrp, aci, atci, av, atv;                 // matrices
+    int arp, atrp, aci, atci, av, atv;                 // matrices: slice tables, indices, values
     int c, l, u, q, x0, x, xp, xr, dx, ds;             // x side, float
     int lc, uc, y0, y, yp, dy;                         // y side, float
     int vr, cr;                                        // scaling, double
     int red;                                           // reduction scratch, double[32]
     int total;
     __host__ __device__ static int al(int b) { return (b + 15) & ~15; }
-    __host__ __device__ Layout(int n, int m, int nnz)
+    __host__ __device__ Layout(int n, int m, int sell_a, int sell_at)
     {
         int o = 0;
-        arp = o; o += al(4 * (m + 1));
-        atrp = o; o += al(4 * (n + 1));
-        aci = o; o += al(2 * nnz);
-        atci = o; o += al(2 * nnz);
-        av = o; o += al(4 * nnz);
-        atv = o; o += al(4 * nnz);
+        arp = o; o += al(4 * (slices(m) + 1));
+        atrp = o; o += al(4 * (slices(n) + 1));
+        aci = o; o += al(2 * sell_a);
+        atci = o; o += al(2 * sell_at);
+        av = o; o += al(4 * sell_a);
+        atv = o; o += al(4 * sell_at);
         c = o; o += al(4 * n);
         l = o; o += al(4 * n);
         u = o; o += al(4 * n);
@@ -181,6 +197,20 @@ __device__ __forceinline__ double gtimer_ns()
 }
 __device__ __forceinline__ double nterm(double v, int l2) { return l2 ? v * v : (isfinite(v) ? fabs(v) : INFINITY); }
 
+// row r of a sliced matrix times v, FP64 accumulation in entry order
+__device__ __forceinline__ double sell_dot(const int *so, const unsigned short *ci, const float *va, const float *v,
+                                           int r)
+{
+    const int sl = r >> 5, ln = r & 31;
+    const int o = so[sl], len = (so[sl + 1] - o) >> 5;
+    double acc = 0.0;
+    for (int k = 0; k < len; ++k) {
+        const int e = o + (k << 5) + ln;
+        acc += (double)va[e] * (double)v[ci[e]];
+    }
+    return acc;
+}
+
 template <int BT, int GROUP>
 __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *sm, const Grp<BT, GROUP> &g)
 {
@@ -192,7 +222,9 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
     const double *Av = D.A_v + I.k_off, *Atv = D.At_v + I.k_off;
     const double *gc = D.c + I.x_off, *gl = D.l + I.x_off, *gu = D.u + I.x_off, *gq = D.q + I.x_off;
     const double *glc = D.lc + I.y_off, *guc = D.uc + I.y_off;
-    Layout Lo(n, m, nnz);
+    const int nsa = slices(m), nsat = slices(n);
+    const int *gsa = D.S_tab + I.so_off, *gsat = gsa + nsa + 1;
+    Layout Lo(n, m, I.sell_a, I.sell_at);
     int *arp = (int *)(sm + Lo.arp), *atrp = (int *)(sm + Lo.atrp);
     unsigned short *aci = (unsigned short *)(sm + Lo.aci), *atci = (unsigned short *)(sm + Lo.atci);
     float *av = (float *)(sm + Lo.av), *atv = (float *)(sm + Lo.atv);
@@ -290,22 +322,30 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
         sb = 1.0 / (sqrt(bb2) + 1.0);
         sc = 1.0 / (sqrt(cc2) + 1.0);
     }
-    // ---- scaled data in shared memory --------------------------------------
-    for (int i = t; i <= m; i += GROUP)
-        arp[i] = Arp[i];
-    for (int j = t; j <= n; j += GROUP)
-        atrp[j] = Atrp[j];
-    for (int k = t; k < nnz; k += GROUP) {
-        aci[k] = (unsigned short)Aci[k];
-        atci[k] = (unsigned short)Atci[k];
-    }
+    // ---- scaled data in shared memory (sliced matrices) --------------------
+    for (int s = t; s <= nsa; s += GROUP)
+        arp[s] = gsa[s];
+    for (int s = t; s <= nsat; s += GROUP)
+        atrp[s] = gsat[s];
     g.sync();
-    for (int i = t; i < m; i += GROUP)
-        for (int k = arp[i]; k < arp[i + 1]; ++k)
-            av[k] = (float)(Av[k] / (cr[i] * vr[aci[k]]));
-    for (int j = t; j < n; j += GROUP)
-        for (int k = atrp[j]; k < atrp[j + 1]; ++k)
-            atv[k] = (float)(Atv[k] / (vr[j] * cr[atci[k]]));
+    for (int i = t; i < m; i += GROUP) {
+        const int o = arp[i >> 5] + (i & 31), len = (arp[(i >> 5) + 1] - arp[i >> 5]) >> 5;
+        const int k0 = Arp[i], rl = Arp[i + 1] - k0;
+        for (int k = 0; k < len; ++k) {
+            const int col = k < rl ? Aci[k0 + k] : 0;
+            aci[o + 32 * k] = (unsigned short)col;
+            av[o + 32 * k] = k < rl ? (float)(Av[k0 + k] / (cr[i] * vr[col])) : 0.0f;
+        }
+    }
+    for (int j = t; j < n; j += GROUP) {
+        const int o = atrp[j >> 5] + (j & 31), len = (atrp[(j >> 5) + 1] - atrp[j >> 5]) >> 5;
+        const int k0 = Atrp[j], cl = Atrp[j + 1] - k0;
+        for (int k = 0; k < len; ++k) {
+            const int row = k < cl ? Atci[k0 + k] : 0;
+            atci[o + 32 * k] = (unsigned short)row;
+            atv[o + 32 * k] = k < cl ? (float)(Atv[k0 + k] / (vr[j] * cr[row])) : 0.0f;
+        }
+    }
     for (int j = t; j < n; j += GROUP) {
         const double vj = vr[j];
         c[j] = (float)(gc[j] / vj * sc);
@@ -340,18 +380,12 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
         g.sync();
         double s2 = 1.0;
         for (int it = 0; it < P.sv_max_iter; ++it) {
-            for (int j = t; j < n; j += GROUP) {
-                double s = 0.0;
-                for (int k = atrp[j]; k < atrp[j + 1]; ++k)
-                    s += (double)atv[k] * (double)v[atci[k]];
-                dp[j] = (float)s;
-            }
+            for (int j = t; j < n; j += GROUP)
+                dp[j] = (float)sell_dot(atrp, atci, atv, v, j);
             g.sync();
             a = 0.0;
             for (int i = t; i < m; i += GROUP) {
-                double s = 0.0;
-                for (int k = arp[i]; k < arp[i + 1]; ++k)
-                    s += (double)av[k] * (double)dp[aci[k]];
+                const double s = sell_dot(arp, aci, av, dp, i);
                 nv[i] = (float)s;
                 a += s * (double)v[i];
             }
@@ -394,9 +428,7 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
         const double tau = step / omega;
         double pr = 0.0, pslack = 0.0, dy2 = 0.0;
         for (int i = t; i < m; i += GROUP) {
-            double s = 0.0;
-            for (int kk = arp[i]; kk < arp[i + 1]; ++kk)
-                s += (double)av[kk] * (double)xp[aci[kk]];
+            const double s = sell_dot(arp, aci, av, xp, i);
             double proj = clampd((double)lc[i], s, (double)uc[i]);
             pr = P.l2 ? pr + nterm((s - proj) * cr[i], 1) : fmax(pr, nterm((s - proj) * cr[i], 0));
             double yv = yp[i];
@@ -409,9 +441,7 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
         }
         double dr = 0.0, cx = 0.0, xqx = 0.0, sx = 0.0, qn = 0.0, an = 0.0, dx2 = 0.0;
         for (int j = t; j < n; j += GROUP) {
-            double s = 0.0;
-            for (int kk = atrp[j]; kk < atrp[j + 1]; ++kk)
-                s += (double)atv[kk] * (double)yp[atci[kk]];
+            const double s = sell_dot(atrp, atci, atv, yp, j);
             double xv = xp[j], qx = hasq ? (double)q[j] * xv : 0.0;
             double dsl, drr;
             if (!hasq) {
@@ -465,9 +495,7 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
     auto fixed_point_error = [&]() {
         double p2 = 0.0, d2 = 0.0, cross = 0.0;
         for (int j = t; j < n; j += GROUP) {
-            double s = 0.0;
-            for (int kk = atrp[j]; kk < atrp[j + 1]; ++kk)
-                s += (double)atv[kk] * (double)dy[atci[kk]];
+            const double s = sell_dot(atrp, atci, atv, dy, j);
             double d = dx[j];
             p2 += d * d;
             cross += s * d;
@@ -543,9 +571,7 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
         const double tau = step / omega, sigma = step * omega;
         // primal step (reference pdhg_update + halpern_update)
         for (int j = t; j < n; j += GROUP) {
-            double s = 0.0;
-            for (int kk = atrp[j]; kk < atrp[j + 1]; ++kk)
-                s += (double)atv[kk] * (double)y[atci[kk]];
+            const double s = sell_dot(atrp, atci, atv, y, j);
             double xi = x[j];
             double tt = xi - tau * ((double)c[j] - s);
             if (hasq)
@@ -562,9 +588,7 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
         }
         g.sync();
         for (int i = t; i < m; i += GROUP) {
-            double s = 0.0;
-            for (int kk = arp[i]; kk < arp[i + 1]; ++kk)
-                s += (double)av[kk] * (double)xr[aci[kk]];
+            const double s = sell_dot(arp, aci, av, xr, i);
             double yi = y[i];
             double pr = clampd((double)lc[i], s - yi / sigma, (double)uc[i]);
             double yn = yi - sigma * s + sigma * pr;
@@ -629,6 +653,87 @@ __global__ void __launch_bounds__(BT) batch_kernel(BData D, BParams P, int smem_
     }
 }
 
+// A^T of every instance, one warp per instance, entries of each column in
+// increasing row order (what a counting sort over the rows gives, so the
+// batch kernel sums A^T y in the same order as with a host transpose):
+// column counts by atomics, a warp scan into the row pointers of A^T, then
+// the entries scattered in entry order, 32 at a time; the lanes of a chunk
+// that share a column rank themselves with __match_any_sync and the
+// column's first lane advances its cursor.  cur: n ints of scratch per
+// instance.
+__global__ void __launch_bounds__(256) transpose_kernel(const int *A_rp, const int *A_ci, const double *A_v,
+                                                        int *At_rp, int *At_ci, double *At_v, int *cur,
+                                                        const BInst *inst, int count)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int warps = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); w < count; w += warps) {
+        const BInst b = inst[w];
+        const int n = b.n, m = b.m;
+        const int *rp = A_rp + b.rp_off;
+        const int *ci = A_ci + b.k_off;
+        const double *av = A_v + b.k_off;
+        int *trp = At_rp + b.trp_off;
+        int *cu = cur + b.x_off;
+        int *tci = At_ci + b.k_off;
+        double *tv = At_v + b.k_off;
+        const int nnz = rp[m];
+        for (int j = lane; j <= n; j += 32)
+            trp[j] = 0;
+        __syncwarp();
+        for (int k = lane; k < nnz; k += 32)
+            atomicAdd(&trp[ci[k] + 1], 1);
+        __syncwarp();
+        int carry = 0; // inclusive scan of trp[1..n]
+        for (int j0 = 1; j0 <= n; j0 += 32) {
+            const int j = j0 + lane;
+            int v = j <= n ? trp[j] : 0;
+            for (int d = 1; d < 32; d <<= 1) {
+                const int t = __shfl_up_sync(FULL, v, d);
+                if (lane >= d)
+                    v += t;
+            }
+            v += carry;
+            if (j <= n)
+                trp[j] = v;
+            carry = __shfl_sync(FULL, v, 31);
+        }
+        __syncwarp();
+        for (int j = lane; j < n; j += 32)
+            cu[j] = trp[j];
+        __syncwarp();
+        for (int k0 = 0; k0 < nnz; k0 += 32) {
+            const int k = k0 + lane;
+            const bool ok = k < nnz;
+            const int col = ok ? ci[k] : -1 - lane;
+            int row = 0;
+            if (ok) { // rp[lo] <= k < rp[hi]
+                int lo = 0, hi = m;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (rp[mid] <= k)
+                        lo = mid;
+                    else
+                        hi = mid;
+                }
+                row = lo;
+            }
+            const unsigned same = __match_any_sync(FULL, col);
+            const int rank = __popc(same & ((1u << lane) - 1u));
+            const int base = ok ? cu[col] : 0;
+            __syncwarp();
+            if (ok) {
+                tci[base + rank] = row;
+                tv[base + rank] = av[k];
+                if (rank == 0)
+                    cu[col] = base + __popc(same);
+            }
+            __syncwarp();
+        }
+    }
+}
+
 } // namespace
 
 // ---------------------------------------------------------------------------
@@ -669,35 +774,95 @@ void parallel_for(int count, F &&f)
         }                                                                                                              \
     } while (0)
 
-struct DevBuf { // device allocations of one batch solve
-    std::vector<void *> p;
-    template <typename T>
-    T *up(const std::vector<T> &h)
-    {
-        void *d = nullptr;
-        if (cudaMalloc(&d, std::max<size_t>(h.size(), 1) * sizeof(T)) != cudaSuccess)
+// Page-locked staging memory and device memory that batch solves keep
+// between calls (one host buffer, one device buffer per device), grown on
+// demand (with 1/8 headroom) and freed by pdhcg_b200_batch_release.  A call
+// holds g_arena_mu from packing to the copy of the results, so concurrent
+// batch solves in one process take turns.
+struct Arena {
+    char *p = nullptr;
+    size_t cap = 0;
+};
+std::mutex g_arena_mu;
+Arena g_host_arena;
+std::map<int, Arena> g_dev_arena;
+
+char *host_arena(size_t need)
+{
+    Arena &a = g_host_arena;
+    if (a.cap < need) {
+        if (a.p)
+            cudaFreeHost(a.p);
+        a = Arena{};
+        void *p = nullptr;
+        const size_t want = need + need / 8;
+        if (cudaHostAlloc(&p, want, cudaHostAllocPortable) != cudaSuccess)
             return nullptr;
-        p.push_back(d);
-        if (!h.empty() && cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
-            return nullptr;
-        return (T *)d;
+        a.p = (char *)p;
+        a.cap = want;
     }
-    template <typename T>
-    T *zeros(size_t k)
-    {
-        void *d = nullptr;
-        if (cudaMalloc(&d, std::max<size_t>(k, 1) * sizeof(T)) != cudaSuccess)
+    return a.p;
+}
+
+char *dev_arena(int dev, size_t need)
+{
+    Arena &a = g_dev_arena[dev];
+    if (a.cap < need) {
+        if (a.p)
+            cudaFree(a.p);
+        a = Arena{};
+        void *p = nullptr;
+        const size_t want = need + need / 8;
+        if (cudaMalloc(&p, want) != cudaSuccess)
             return nullptr;
-        p.push_back(d);
-        if (cudaMemset(d, 0, std::max<size_t>(k, 1) * sizeof(T)) != cudaSuccess)
-            return nullptr;
-        return (T *)d;
+        a.p = (char *)p;
+        a.cap = want;
     }
-    ~DevBuf()
+    return a.p;
+}
+
+// Byte offsets of the packed arrays (each 256-byte aligned): the inputs
+// first, copied host to device in one piece; then A^T and the scratch
+// (device only); then the outputs, copied back in one piece.  The staging
+// buffer holds the inputs and, after them (at in_end), the outputs.
+struct Pack {
+    size_t A_rp, A_ci, A_v, c, l, u, q, lc, uc, v0, S, inst, order, in_end;
+    size_t At_rp, At_ci, At_v, cur, next, out, x_out, y_out, stats, end;
+    Pack(long long rp, long long trp, long long k, long long x, long long y, long long s, int max_m, int nb,
+         int classes)
     {
-        for (void *q : p)
-            cudaFree(q);
+        size_t o = 0;
+        auto put = [&o](long long bytes) {
+            const size_t at = o;
+            o += ((size_t)std::max(bytes, 1LL) + 255) & ~(size_t)255;
+            return at;
+        };
+        A_rp = put(rp * 4);
+        A_ci = put(k * 4);
+        A_v = put(k * 8);
+        c = put(x * 8);
+        l = put(x * 8);
+        u = put(x * 8);
+        q = put(x * 8);
+        lc = put(y * 8);
+        uc = put(y * 8);
+        v0 = put((long long)max_m * 8);
+        S = put(s * 4);
+        inst = put((long long)nb * (long long)sizeof(BInst));
+        order = put((long long)nb * 4);
+        in_end = o;
+        At_rp = put(trp * 4);
+        At_ci = put(k * 4);
+        At_v = put(k * 8);
+        cur = put(x * 4);
+        next = put((long long)classes * 4);
+        out = o;
+        x_out = put(x * 8);
+        y_out = put(y * 8);
+        stats = put((long long)nb * BS_COUNT * 8);
+        end = o;
     }
+    size_t host_bytes() const { return in_end + (end - out); }
 };
 
 // A launch shape: threads per CTA, threads per instance group.
@@ -807,9 +972,14 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
     // by a pool of host threads into its slot of the packed arrays ----------
     std::vector<int> batched, fallback;
     std::vector<BInst> inst;
-    long long tot_rp = 0, tot_trp = 0, tot_k = 0, tot_x = 0, tot_y = 0;
+    long long tot_rp = 0, tot_trp = 0, tot_k = 0, tot_x = 0, tot_y = 0, tot_s = 0;
     int max_m = 1;
+    std::vector<std::vector<int>> tab(count); // slice tables of the candidates
     {
+        // cheap checks here; the matrix checks and the slice tables of the
+        // sliced layout (max row length of A and of A^T per 32 rows) on the
+        // thread pool
+        std::vector<char> cand(count, 0), valid(count, 1);
         std::vector<double> qd;
         for (int i = 0; i < count; ++i) {
             const qp_problem_t *p = probs[i];
@@ -818,13 +988,67 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
                 return -1;
             }
             const int n = p->num_variables, m = p->num_constraints;
-            bool ok = n > 0 && m > 0 && n < 65536 && m < 65536 && p->cones.num_cones == 0 &&
+            cand[i] = n > 0 && m > 0 && n < 65536 && m < 65536 && p->cones.num_cones == 0 &&
                       p->affine_cones.num_cones == 0 && p->constraint_matrix && diag_q(p, qd);
+        }
+        parallel_for(count, [&](int i) {
+            if (!cand[i])
+                return;
+            const qp_problem_t *p = probs[i];
+            const int n = p->num_variables, m = p->num_constraints;
+            const int *rp = p->constraint_matrix->row_ptr, *ci = p->constraint_matrix->col_ind;
+            bool ok = rp[0] == 0;
+            for (int r = 0; ok && r < m; ++r)
+                ok = rp[r] <= rp[r + 1];
+            const int nnz = ok ? rp[m] : 0;
+            for (int k = 0; ok && k < nnz; ++k)
+                ok = ci[k] >= 0 && ci[k] < n;
+            if (!ok) {
+                valid[i] = 0;
+                return;
+            }
+            const int sa = slices(m), sat = slices(n);
+            std::vector<int> &T = tab[i];
+            T.resize(sa + 1 + sat + 1);
+            int o = 0;
+            for (int s = 0; s < sa; ++s) {
+                int mx = 0;
+                for (int r = 32 * s; r < std::min(32 * s + 32, m); ++r)
+                    mx = std::max(mx, rp[r + 1] - rp[r]);
+                T[s] = o;
+                o += 32 * mx;
+            }
+            T[sa] = o;
+            std::vector<int> cnt(n, 0);
+            for (int k = 0; k < nnz; ++k)
+                cnt[ci[k]]++;
+            int *Tt = T.data() + sa + 1;
+            o = 0;
+            for (int s = 0; s < sat; ++s) {
+                int mx = 0;
+                for (int j = 32 * s; j < std::min(32 * s + 32, n); ++j)
+                    mx = std::max(mx, cnt[j]);
+                Tt[s] = o;
+                o += 32 * mx;
+            }
+            Tt[sat] = o;
+        });
+        for (int i = 0; i < count; ++i)
+            if (cand[i] && !valid[i]) {
+                std::fprintf(stderr, "[pdhcg_b200_solve_batch] problem %d: the constraint matrix is not valid CSR "
+                                     "(row pointers must start at 0 and not decrease, columns must lie in [0, n)).\n",
+                             i);
+                return -1;
+            }
+        for (int i = 0; i < count; ++i) {
+            const qp_problem_t *p = probs[i];
+            const int n = p->num_variables, m = p->num_constraints;
             BInst b{};
-            int nnz = 0;
+            bool ok = cand[i];
             if (ok) {
-                nnz = p->constraint_matrix->row_ptr[m];
-                Layout Lo(n, m, nnz);
+                b.sell_a = tab[i][slices(m)];
+                b.sell_at = tab[i].back();
+                const Layout Lo(n, m, b.sell_a, b.sell_at);
                 ok = Lo.total <= SMEM_CAP;
                 b.smem = Lo.total;
             }
@@ -832,6 +1056,7 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
                 fallback.push_back(i);
                 continue;
             }
+            const int nnz = p->constraint_matrix->row_ptr[m];
             b.n = n;
             b.m = m;
             b.rp_off = tot_rp;
@@ -839,6 +1064,7 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
             b.k_off = tot_k;
             b.x_off = tot_x;
             b.y_off = tot_y;
+            b.so_off = tot_s;
             b.qmode = (p->objective_sparse_matrix && p->objective_sparse_matrix_num_nonzeros > 0) ? 1 : 0;
             b.obj_const = p->objective_constant;
             tot_rp += m + 1;
@@ -846,48 +1072,12 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
             tot_k += nnz;
             tot_x += n;
             tot_y += m;
+            tot_s += (long long)tab[i].size();
             max_m = std::max(max_m, m);
             inst.push_back(b);
             batched.push_back(i);
         }
     }
-    std::vector<int> A_rp(tot_rp), A_ci(tot_k), At_rp(tot_trp), At_ci(tot_k);
-    std::vector<double> A_v(tot_k), At_v(tot_k), c(tot_x), l(tot_x), u(tot_x), q(tot_x), lc(tot_y), uc(tot_y);
-    auto fill = [&](int bi) {
-        const qp_problem_t *p = probs[batched[bi]];
-        const BInst &b = inst[bi];
-        const int n = b.n, m = b.m;
-        const CsrComponent *A = p->constraint_matrix;
-        const int nnz = A->row_ptr[m];
-        std::memcpy(&A_rp[b.rp_off], A->row_ptr, (m + 1) * sizeof(int));
-        std::memcpy(&A_ci[b.k_off], A->col_ind, nnz * sizeof(int));
-        std::memcpy(&A_v[b.k_off], A->val, nnz * sizeof(double));
-        // A^T by counting sort (entries of each column in increasing row order)
-        int *trp = &At_rp[b.trp_off];
-        std::fill(trp, trp + n + 1, 0);
-        for (int k = 0; k < nnz; ++k)
-            trp[A->col_ind[k] + 1]++;
-        for (int j = 0; j < n; ++j)
-            trp[j + 1] += trp[j];
-        std::vector<int> pos(trp, trp + n);
-        for (int r = 0; r < m; ++r)
-            for (int k = A->row_ptr[r]; k < A->row_ptr[r + 1]; ++k) {
-                int d = pos[A->col_ind[k]]++;
-                At_ci[b.k_off + d] = r;
-                At_v[b.k_off + d] = A->val[k];
-            }
-        std::vector<double> qd;
-        diag_q(p, qd);
-        for (int j = 0; j < n; ++j) {
-            c[b.x_off + j] = p->objective_vector ? p->objective_vector[j] : 0.0;
-            l[b.x_off + j] = p->variable_lower_bound[j];
-            u[b.x_off + j] = p->variable_upper_bound[j];
-            q[b.x_off + j] = qd[j];
-        }
-        std::memcpy(&lc[b.y_off], p->constraint_lower_bound, m * sizeof(double));
-        std::memcpy(&uc[b.y_off], p->constraint_upper_bound, m * sizeof(double));
-    };
-    parallel_for((int)inst.size(), fill);
     const int nb = (int)inst.size();
     // power-method start vector (reference: rand_r with seed 1234 in [-1, 1])
     std::vector<double> v0(max_m);
@@ -916,44 +1106,19 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
     P.k_i = prm.restart_params.k_i;
     P.k_d = prm.restart_params.k_d;
 
-    std::vector<double> xo(c.size()), yo(lc.size()), st((size_t)std::max(nb, 1) * BS_COUNT);
-    double kernel_ms = 0.0;
+    double kernel_ms = 0.0, pack_ms = 0.0;
+    size_t h2d = 0, d2h = 0;
     int launches = 0;
+    std::unique_lock<std::mutex> lock(g_arena_mu, std::defer_lock);
+    std::optional<Pack> pk;
     if (nb > 0) {
-        // classes by size: instances sorted by shared-memory need, largest first;
-        // one launch per class of similar size
+        // classes by size: instances sorted by shared-memory need, largest
+        // first; one launch per class of similar size (a new class starts
+        // when the need drops below half)
         std::vector<int> order(nb);
         for (int i = 0; i < nb; ++i)
             order[i] = i;
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return inst[a].smem > inst[b].smem; });
-        DevBuf B;
-        BData D{};
-        D.A_rp = B.up(A_rp);
-        D.A_ci = B.up(A_ci);
-        D.A_v = B.up(A_v);
-        D.At_rp = B.up(At_rp);
-        D.At_ci = B.up(At_ci);
-        D.At_v = B.up(At_v);
-        D.c = B.up(c);
-        D.l = B.up(l);
-        D.u = B.up(u);
-        D.q = B.up(q);
-        D.lc = B.up(lc);
-        D.uc = B.up(uc);
-        D.v0 = B.up(v0);
-        D.inst = B.up(inst);
-        D.x_out = B.zeros<double>(xo.size());
-        D.y_out = B.zeros<double>(yo.size());
-        D.stats = B.zeros<double>(st.size());
-        if (!D.A_rp || !D.A_ci || !D.A_v || !D.At_rp || !D.At_ci || !D.At_v || !D.c || !D.l || !D.u || !D.q ||
-            !D.lc || !D.uc || !D.v0 || !D.inst || !D.x_out || !D.y_out || !D.stats) {
-            std::fprintf(stderr, "[pdhcg_b200_solve_batch] device allocation or upload failed.\n");
-            return -1;
-        }
-        int dev = 0, sms = 0;
-        BCK(cudaGetDevice(&dev));
-        BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        // size classes: a new class starts when the need drops below half
         std::vector<std::pair<int, int>> classes; // [begin, end) in order
         for (int b = 0; b < nb;) {
             int e = b + 1;
@@ -962,14 +1127,91 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
             classes.push_back({b, e});
             b = e;
         }
-        int *d_order = B.up(order);
-        int *d_next = B.zeros<int>(classes.size());
-        if (!d_order || !d_next)
+        pk.emplace(tot_rp, tot_trp, tot_k, tot_x, tot_y, tot_s, max_m, nb, (int)classes.size());
+        const Pack &L = *pk;
+        int dev = 0, sms = 0;
+        BCK(cudaGetDevice(&dev));
+        BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        lock.lock();
+        char *H = host_arena(L.host_bytes());
+        char *G = dev_arena(dev, L.end);
+        if (!H || !G) {
+            std::fprintf(stderr, "[pdhcg_b200_solve_batch] cannot allocate %zu bytes of page-locked or %zu bytes of "
+                                 "device memory.\n", L.host_bytes(), L.end);
             return -1;
+        }
+        int *hA_rp = (int *)(H + L.A_rp), *hA_ci = (int *)(H + L.A_ci);
+        double *hA_v = (double *)(H + L.A_v), *hc = (double *)(H + L.c), *hl = (double *)(H + L.l);
+        double *hu = (double *)(H + L.u), *hq = (double *)(H + L.q), *hlc = (double *)(H + L.lc);
+        double *huc = (double *)(H + L.uc);
+        int *hS = (int *)(H + L.S);
+        // pack: every instance copied by a pool of host threads into its slot
+        // of the staging buffer (A^T is built on the device)
+        parallel_for(nb, [&](int bi) {
+            const qp_problem_t *p = probs[batched[bi]];
+            const BInst &b = inst[bi];
+            const int n = b.n, m = b.m;
+            const CsrComponent *A = p->constraint_matrix;
+            const int nnz = A->row_ptr[m];
+            const std::vector<int> &T = tab[batched[bi]];
+            std::memcpy(hS + b.so_off, T.data(), T.size() * sizeof(int));
+            std::memcpy(hA_rp + b.rp_off, A->row_ptr, (m + 1) * sizeof(int));
+            std::memcpy(hA_ci + b.k_off, A->col_ind, nnz * sizeof(int));
+            std::memcpy(hA_v + b.k_off, A->val, nnz * sizeof(double));
+            std::vector<double> qd;
+            diag_q(p, qd);
+            for (int j = 0; j < n; ++j)
+                hc[b.x_off + j] = p->objective_vector ? p->objective_vector[j] : 0.0;
+            std::memcpy(hl + b.x_off, p->variable_lower_bound, n * sizeof(double));
+            std::memcpy(hu + b.x_off, p->variable_upper_bound, n * sizeof(double));
+            std::memcpy(hq + b.x_off, qd.data(), n * sizeof(double));
+            std::memcpy(hlc + b.y_off, p->constraint_lower_bound, m * sizeof(double));
+            std::memcpy(huc + b.y_off, p->constraint_upper_bound, m * sizeof(double));
+        });
+        std::memcpy(H + L.v0, v0.data(), v0.size() * sizeof(double));
+        std::memcpy(H + L.inst, inst.data(), inst.size() * sizeof(BInst));
+        std::memcpy(H + L.order, order.data(), order.size() * sizeof(int));
+        pack_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+
+        BData D{};
+        D.A_rp = (const int *)(G + L.A_rp);
+        D.A_ci = (const int *)(G + L.A_ci);
+        D.A_v = (const double *)(G + L.A_v);
+        D.At_rp = (const int *)(G + L.At_rp);
+        D.At_ci = (const int *)(G + L.At_ci);
+        D.At_v = (const double *)(G + L.At_v);
+        D.c = (const double *)(G + L.c);
+        D.l = (const double *)(G + L.l);
+        D.u = (const double *)(G + L.u);
+        D.q = (const double *)(G + L.q);
+        D.lc = (const double *)(G + L.lc);
+        D.uc = (const double *)(G + L.uc);
+        D.v0 = (const double *)(G + L.v0);
+        D.S_tab = (const int *)(G + L.S);
+        D.inst = (const BInst *)(G + L.inst);
+        D.x_out = (double *)(G + L.x_out);
+        D.y_out = (double *)(G + L.y_out);
+        D.stats = (double *)(G + L.stats);
+        const int *d_order = (const int *)(G + L.order);
+        int *d_next = (int *)(G + L.next);
+        h2d = L.in_end;
+        d2h = L.end - L.out;
+        BCK(cudaMemcpyAsync(G, H, h2d, cudaMemcpyHostToDevice, 0));
+        BCK(cudaMemsetAsync(G + L.next, 0, L.out - L.next, 0));
+        BCK(cudaMemsetAsync(G + L.out, 0, d2h, 0));
         cudaEvent_t e0, e1;
         BCK(cudaEventCreate(&e0));
         BCK(cudaEventCreate(&e1));
         BCK(cudaEventRecord(e0, 0));
+        {
+            const int warps_per_cta = 8;
+            const int grid = std::max(1, std::min((nb + warps_per_cta - 1) / warps_per_cta, sms * 8));
+            transpose_kernel<<<grid, 32 * warps_per_cta, 0, 0>>>(D.A_rp, D.A_ci, D.A_v, (int *)(G + L.At_rp),
+                                                                 (int *)(G + L.At_ci), (double *)(G + L.At_v),
+                                                                 (int *)(G + L.cur), D.inst, nb);
+            ++launches;
+            BCK(cudaGetLastError());
+        }
         for (size_t ci = 0; ci < classes.size(); ++ci) {
             const int b = classes[ci].first, e = classes[ci].second;
             int max_smem = 0, max_dim = 0;
@@ -992,23 +1234,29 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
             }
         }
         BCK(cudaEventRecord(e1, 0));
-        BCK(cudaEventSynchronize(e1));
+        BCK(cudaMemcpyAsync(H + L.in_end, G + L.out, d2h, cudaMemcpyDeviceToHost, 0));
+        BCK(cudaStreamSynchronize(0));
         float ms = 0.0f;
         BCK(cudaEventElapsedTime(&ms, e0, e1));
         kernel_ms = ms;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        BCK(cudaMemcpy(xo.data(), D.x_out, xo.size() * sizeof(double), cudaMemcpyDeviceToHost));
-        BCK(cudaMemcpy(yo.data(), D.y_out, yo.size() * sizeof(double), cudaMemcpyDeviceToHost));
-        BCK(cudaMemcpy(st.data(), D.stats, st.size() * sizeof(double), cudaMemcpyDeviceToHost));
     }
-    // ---- results ----------------------------------------------------------
+    // ---- results (from the staging buffer, still held) -------------------
     std::atomic<int> alloc_failed{0};
     parallel_for(nb, [&](int bi) {
+        const Pack &L = *pk;
+        const char *H = g_host_arena.p;
         const int i = batched[bi];
         const qp_problem_t *p = probs[i];
         const BInst &b = inst[bi];
-        const double *s = st.data() + (size_t)bi * BS_COUNT;
+        const double *xo = (const double *)(H + L.in_end + (L.x_out - L.out));
+        const double *yo = (const double *)(H + L.in_end + (L.y_out - L.out));
+        const double *s = (const double *)(H + L.in_end + (L.stats - L.out)) + (size_t)bi * BS_COUNT;
+        const int *arp = (const int *)(H + L.A_rp) + b.rp_off;
+        const int *aci = (const int *)(H + L.A_ci) + b.k_off;
+        const double *av = (const double *)(H + L.A_v) + b.k_off;
+        const double *q = (const double *)(H + L.q) + b.x_off;
         pdhcg_result_t *r = (pdhcg_result_t *)std::calloc(1, sizeof(pdhcg_result_t));
         if (!r) {
             alloc_failed = 1;
@@ -1019,16 +1267,20 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
         r->primal_solution = (double *)std::malloc(b.n * sizeof(double));
         r->dual_solution = (double *)std::malloc(b.m * sizeof(double));
         r->reduced_cost = (double *)std::malloc(b.n * sizeof(double));
-        std::memcpy(r->primal_solution, xo.data() + b.x_off, b.n * sizeof(double));
-        std::memcpy(r->dual_solution, yo.data() + b.y_off, b.m * sizeof(double));
+        results[i] = r;
+        if (!r->primal_solution || !r->dual_solution || !r->reduced_cost) {
+            alloc_failed = 1;
+            return;
+        }
+        std::memcpy(r->primal_solution, xo + b.x_off, b.n * sizeof(double));
+        std::memcpy(r->dual_solution, yo + b.y_off, b.m * sizeof(double));
         // reduced cost c + Qx - A^T y, clamped on infinite bounds (reference
         // compute_and_rescale_reduced_cost_qp_kernel)
         for (int j = 0; j < b.n; ++j)
-            r->reduced_cost[j] = (p->objective_vector ? p->objective_vector[j] : 0.0) + q[b.x_off + j] * r->primal_solution[j];
-        const int *arp = A_rp.data() + b.rp_off;
+            r->reduced_cost[j] = (p->objective_vector ? p->objective_vector[j] : 0.0) + q[j] * r->primal_solution[j];
         for (int row = 0; row < b.m; ++row)
             for (int k = arp[row]; k < arp[row + 1]; ++k)
-                r->reduced_cost[A_ci[b.k_off + k]] -= A_v[b.k_off + k] * r->dual_solution[row];
+                r->reduced_cost[aci[k]] -= av[k] * r->dual_solution[row];
         for (int j = 0; j < b.n; ++j) {
             if (!std::isfinite(p->variable_lower_bound[j]))
                 r->reduced_cost[j] = std::fmin(r->reduced_cost[j], 0.0);
@@ -1046,8 +1298,9 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
         r->objective_gap = s[BS_GAP];
         r->relative_objective_gap = s[BS_REL_GAP];
         r->cumulative_time_sec = kernel_ms * 1e-3;
-        results[i] = r;
     });
+    if (lock.owns_lock())
+        lock.unlock();
     if (alloc_failed) {
         for (int i = 0; i < count; ++i)
             if (results[i]) {
@@ -1064,6 +1317,9 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
     std::memset(&g_batch_stats, 0, sizeof(g_batch_stats));
     g_batch_stats.kernel_ms = kernel_ms;
     g_batch_stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    g_batch_stats.pack_ms = pack_ms;
+    g_batch_stats.h2d_bytes = (double)h2d;
+    g_batch_stats.d2h_bytes = (double)d2h;
     g_batch_stats.launches = launches;
     g_batch_stats.batched = nb;
     g_batch_stats.fallback = (int)fallback.size();
@@ -1076,6 +1332,25 @@ extern "C" int pdhcg_b200_last_batch_stats(pdhcg_b200_batch_stats_t *out)
         return -1;
     *out = g_batch_stats;
     return 0;
+}
+
+extern "C" void pdhcg_b200_batch_release(void)
+{
+    std::lock_guard<std::mutex> lock(g_arena_mu);
+    if (g_host_arena.p)
+        cudaFreeHost(g_host_arena.p);
+    g_host_arena = Arena{};
+    int cur = 0;
+    const bool have = cudaGetDevice(&cur) == cudaSuccess;
+    for (auto &kv : g_dev_arena) {
+        if (!kv.second.p)
+            continue;
+        cudaSetDevice(kv.first);
+        cudaFree(kv.second.p);
+    }
+    g_dev_arena.clear();
+    if (have)
+        cudaSetDevice(cur);
 }
 
 extern "C" int pdhcg_b200_batch_autotune(int count, const qp_problem_t *const *probs, const pdhg_parameters_t *params,

@@ -226,7 +226,7 @@ __device__ __forceinline__ void residual_cone_block(const ResidualData<VT> &D, c
 // staged in the block's scratch and the two projections (no metric, as for
 // every PSD block) taken in memory.
 template <int S, typename VT>
-__device__ __noinline__ void residual_psd_long_block(const ResidualData<VT> &D, const ResidualParams &P, int cb,
+__device__ __forceinline__ void residual_psd_long_block(const ResidualData<VT> &D, const ResidualParams &P, int cb,
                                                      int lane, double *stage, double (&acc)[RS_COUNT],
                                                      const int (&ops)[RS_COUNT])
 {

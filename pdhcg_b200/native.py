@@ -44,7 +44,8 @@ BATCH_SHAPES = 5
 
 class BatchStats(C.Structure):
     """pdhcg_b200_batch_stats_t (include/pdhcg_b200.h)."""
-    _fields_ = [("kernel_ms", C.c_double), ("total_ms", C.c_double), ("launches", C.c_int), ("batched", C.c_int),
+    _fields_ = [("kernel_ms", C.c_double), ("total_ms", C.c_double), ("pack_ms", C.c_double),
+                ("h2d_bytes", C.c_double), ("d2h_bytes", C.c_double), ("launches", C.c_int), ("batched", C.c_int),
                 ("fallback", C.c_int), ("reserved", C.c_int * 5)]
 
 
@@ -76,7 +77,7 @@ EXPORTS = [
     "pdhcg_b200_device_solution", "pdhcg_b200_device_problem_free", "pdhcg_b200_request_cancel",
     "cone_block_length", "pdhcg_b200_project_cones_noalloc", "pdhcg_b200_project_cone_sections",
     "pdhcg_b200_validate_fixed_sections", "pdhcg_b200_default_batch_options",
-    "pdhcg_b200_solve_batch", "pdhcg_b200_batch_autotune", "pdhcg_b200_last_batch_stats",
+    "pdhcg_b200_solve_batch", "pdhcg_b200_batch_autotune", "pdhcg_b200_last_batch_stats", "pdhcg_b200_batch_release",
     "pdhcg_b200_mlp_create", "pdhcg_b200_mlp_free", "pdhcg_b200_mlp_num_params", "pdhcg_b200_mlp_get_params",
     "pdhcg_b200_mlp_set_params", "pdhcg_b200_mlp_predict", "pdhcg_b200_mlp_loss_grad", "pdhcg_b200_mlp_train",
     "read_mps_file",
@@ -136,6 +137,8 @@ def load(build: bool = True) -> C.CDLL:
                                               P(BatchOptions), P(C.c_double)]
     lib.pdhcg_b200_last_batch_stats.restype = C.c_int
     lib.pdhcg_b200_last_batch_stats.argtypes = [P(BatchStats)]
+    lib.pdhcg_b200_batch_release.restype = None
+    lib.pdhcg_b200_batch_release.argtypes = []
     fp = P(C.c_float)
     lib.pdhcg_b200_mlp_create.restype = C.c_void_p
     lib.pdhcg_b200_mlp_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong]

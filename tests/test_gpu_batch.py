@@ -62,3 +62,84 @@ def test_batch_autotune_picks_a_shape(lib):
     assert all(v > 0 for v in ms)
     for b in built:
         lib.qp_problem_free(b[0])
+
+
+def _solve_raw(lib, built, prm, shape):
+    import ctypes as C
+    from pdhcg_b200 import capi
+    arr = (C.POINTER(capi.QpProblem) * len(built))(*[b[0] for b in built])
+    opts = native.BatchOptions()
+    lib.pdhcg_b200_default_batch_options(C.byref(opts))
+    opts.shape = shape
+    res = (C.POINTER(capi.PdhcgResult) * len(built))()
+    rc = lib.pdhcg_b200_solve_batch(len(built), arr, C.byref(prm), C.byref(opts), res)
+    out = []
+    if rc == 0:
+        for b, r in zip(built, res):
+            n, m = r.contents.num_variables, r.contents.num_constraints
+            out.append((np.ctypeslib.as_array(r.contents.primal_solution, (n,)).copy(),
+                        np.ctypeslib.as_array(r.contents.dual_solution, (m,)).copy(),
+                        np.ctypeslib.as_array(r.contents.reduced_cost, (n,)).copy(), r.contents.total_count))
+            lib.pdhcg_result_free(r)
+    st = native.BatchStats()
+    lib.pdhcg_b200_last_batch_stats(C.byref(st))
+    return rc, out, st
+
+
+def test_batch_buffers_kept_between_calls(lib):
+    """The staging and device buffers outlive a call and grow on demand: an
+    instance gives bit-identical x, y, reduced cost and iteration count
+    alone, in a small batch, in a larger one (the buffers grow), after
+    pdhcg_b200_batch_release, and the transposes built on the device give
+    the same iterates as the host-side counting sort did (checked through
+    the single solves in test_batch_matches_single_solves)."""
+    import ctypes as C
+    from pdhcg_b200 import capi
+    probs = instances.mpc_batch(seed=8, count=40, tmin=5, tmax=80)
+    built = [capi.build(lib, p) for p in probs]
+    prm = capi.default_params(lib, **PRM)
+    try:
+        rc, alone, st = _solve_raw(lib, built[:1], prm, 0)
+        assert rc == 0 and st.batched == 1 and st.launches == 2  # A^T build + one class
+        assert st.h2d_bytes > 0 and st.d2h_bytes >= 8 * (probs[0].n + probs[0].A.m)
+        rc, small, _ = _solve_raw(lib, built[:8], prm, 0)
+        assert rc == 0
+        rc, large, st = _solve_raw(lib, built, prm, 0)
+        assert rc == 0 and st.batched == 40
+        lib.pdhcg_b200_batch_release()
+        rc, again, _ = _solve_raw(lib, built[:8], prm, 0)
+        assert rc == 0
+        for got in (small[0], large[0], again[0]):
+            for a, b in zip(alone[0][:3], got[:3]):
+                assert np.array_equal(a, b)
+            assert alone[0][3] == got[3]
+        for i in range(8):
+            for a, b in zip(small[i][:3], large[i][:3]):
+                assert np.array_equal(a, b)
+            for a, b in zip(small[i][:3], again[i][:3]):
+                assert np.array_equal(a, b)
+    finally:
+        for b in built:
+            lib.qp_problem_free(b[0])
+
+
+def test_batch_rejects_bad_column_index_on_host(lib):
+    """A column index outside [0, n) written into a built problem is caught
+    while packing, before anything reaches the device."""
+    import ctypes as C
+    from pdhcg_b200 import capi
+    probs = instances.mpc_batch(seed=9, count=3, tmin=5, tmax=10)
+    built = [capi.build(lib, p) for p in probs]
+    prm = capi.default_params(lib, **PRM)
+    try:
+        A = built[1][0].contents.constraint_matrix.contents
+        saved = A.col_ind[2]
+        A.col_ind[2] = probs[1].n + 7
+        rc, out, _ = _solve_raw(lib, built, prm, -1)
+        A.col_ind[2] = saved
+        assert rc == -1 and out == []
+        rc, out, _ = _solve_raw(lib, built, prm, -1)  # the same problems, repaired
+        assert rc == 0 and len(out) == 3
+    finally:
+        for b in built:
+            lib.qp_problem_free(b[0])
