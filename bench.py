@@ -36,9 +36,8 @@ EPS = 1e-6
 METRIC = "time-to-1e-6 KKT (s) & SpMV GB/s: mixed/warm-start vs plain FP64, 1 B200"
 WORKLOAD = "soc_qp: n=1e6 (20000 SOC blocks x 50), m=5e5 eq rows, 10 nnz/row, diag Q, eps 1e-6"
 
-# Single-instance workloads: the generator, the forms the solver has for the
-# problem class (the inner BB solve of sparse / low-rank Q runs in FP64
-# only) and what keeps the timed solves out of L2.
+# Single-instance workloads: the generator, whether the mixed form is timed
+# beside FP64, and what keeps the timed solves out of L2.
 # DRAM read + write bytes of one step of the SOC-QP workload (both
 # kernels), measured by ncu (profiles/step_kernels_soc_qp_n1e6.md)
 STEP_TRAFFIC = {"f64": 202.5e6, "f32": 121.4e6}
@@ -52,12 +51,12 @@ WORKLOADS = {
     "sparse_qp": {"make": lambda scale, r: instances.sparse_qp(seed=1 + r, scale=scale),
                   "desc": "sparse_qp: n=1e4, m=5e3, 8 nnz/row, Q = B'B + 0.1 I (B 2000 x 1e4, 4 nnz/row; "
                           "sparse Q, inner BB solve), box [-10, 10], eps 1e-6",
-                  "mixed": False, "l2": "L2-resident working set (< 3 MB): latency-bound, time to tolerance"},
+                  "mixed": True, "l2": "L2-resident working set (< 3 MB): latency-bound, time to tolerance"},
     "portfolio": {"make": lambda scale, r: instances.portfolio(seed=3 + r, scale=scale),
                   "desc": "portfolio: n=2e5 assets, R 100 x 2e5 dense N(0, 1/sqrt n), D diag U(0.5, 2), "
                           "Q diag U(1e-4, 1e-2), budget + 500 sector + 100 exposure rows, RSOC tracking-error "
                           "block, x in [0, 0.02], eps 1e-6",
-                  "mixed": False, "l2": "working set (A, R and R^T, >700 MB) larger than L2"},
+                  "mixed": True, "l2": "working set (A, R and R^T, >700 MB) larger than L2"},
     "fixed_soc": {"make": lambda scale, r: instances.fixed_cone_qp(seed=21 + r, nsoc=400, soc_len=50),
                   "desc": "fixed_soc: conic LP with 400 SOC blocks of 50, 4 RSOC, 6 EXP and 6 POW blocks and "
                           "slots of about half the blocks fixed by set_cone_fixed (n=20128), eps 1e-6",
@@ -576,8 +575,10 @@ def run_warm_start(args):
 
 def measure_single(name: str, steps: int = 2, warmup: int = 1) -> dict:
     """Time to 1e-6 of one single-instance workload: the problem resident
-    (pdhcg_b200_upload, then solves) and from host buffers, beside the
-    reference's own build on the same instance when it is present."""
+    (pdhcg_b200_upload, then solves) and from host buffers, in FP64 and,
+    where the workload has one, the mixed form (FP32 bulk phase, FP64
+    polish), beside the reference's own build on the same instance when it
+    is present."""
     import torch
     lib = native.load()
     W = WORKLOADS[name]
@@ -585,30 +586,46 @@ def measure_single(name: str, steps: int = 2, warmup: int = 1) -> dict:
     prob, keep = capi.build(lib, problem)
     prm = _params(lib)
     handle = lib.pdhcg_b200_upload(prob)
+    forms = {"fp64": 0, "mixed": 1} if W["mixed"] else {"fp64": 0}
     res = {}
-    for device in (True, False):
-        ts = []
-        for i in range(warmup + steps):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            r = lib.pdhcg_b200_solve_device(handle, C.byref(prm), None) if device else \
-                lib.pdhcg_b200_solve(prob, C.byref(prm), None)
-            torch.cuda.synchronize()
-            dt = time.perf_counter() - t0
-            d = capi.result_dict(r, problem.n, problem.A.m) if not device else {
-                "status": capi.TERMINATION_REASONS[r.contents.termination_reason],
-                "total_count": r.contents.total_count, "primal_objective_value": r.contents.primal_objective_value,
-                "total_inner_count": r.contents.total_inner_count}
-            lib.pdhcg_result_free(r)
-            if i >= warmup:
-                ts.append(dt)
-        res["device" if device else "host"] = (float(np.mean(ts)), d)
+    for form, precision in forms.items():
+        for device in (True, False):
+            opts = native.default_options(precision=precision, solution_on_device=int(device))
+            ts = []
+            for i in range(warmup + steps):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                r = lib.pdhcg_b200_solve_device(handle, C.byref(prm), C.byref(opts)) if device else \
+                    lib.pdhcg_b200_solve(prob, C.byref(prm), C.byref(opts))
+                torch.cuda.synchronize()
+                dt = time.perf_counter() - t0
+                rr = r.contents
+                d = {"status": capi.TERMINATION_REASONS[rr.termination_reason], "total_count": rr.total_count,
+                     "primal_objective_value": rr.primal_objective_value,
+                     "total_inner_count": rr.total_inner_count,
+                     "rel_kkt": max(rr.relative_primal_residual, rr.relative_dual_residual,
+                                    rr.relative_objective_gap),
+                     "fp32_iterations": native.last_stats()["fp32_iterations"]}
+                lib.pdhcg_result_free(r)
+                if i >= warmup:
+                    ts.append(dt)
+            res[(form, device)] = (float(np.mean(ts)), d)
     lib.pdhcg_b200_device_problem_free(handle)
     lib.qp_problem_free(prob)
-    (tv, d), (te, _) = res["device"], res["host"]
+    (tv, d), (te, _) = res[("fp64", True)], res[("fp64", False)]
     out = {"value": tv, "unit": "s", "e2e": te, "status": d["status"], "iterations": d["total_count"],
            "inner_iterations": d.get("total_inner_count"), "objective": d["primal_objective_value"],
-           "workload": W["desc"]}
+           "rel_kkt": d["rel_kkt"], "form": "FP64", "workload": W["desc"]}
+    if "mixed" in forms:
+        (mv, md), (me, _) = res[("mixed", True)], res[("mixed", False)]
+        out["mixed"] = {"value": mv, "unit": "s", "e2e": me, "status": md["status"], "iterations": md["total_count"],
+                        "fp32_iterations": md["fp32_iterations"], "inner_iterations": md.get("total_inner_count"),
+                        "objective": md["primal_objective_value"], "rel_kkt": md["rel_kkt"],
+                        "objective_rel_diff_vs_fp64": abs(md["primal_objective_value"] - d["primal_objective_value"]) /
+                                                      (1 + abs(d["primal_objective_value"])),
+                        "form": "FP32 values of Q, R, R^T and of A's long rows with FP64 iterates and accumulation "
+                                "until the relative KKT error is below 1e-5, then FP64"}
+        out["speedup_mixed_vs_fp64"] = tv / mv
     path = os.path.join(ROOT, "oracle", "_ref", "libpdhcg_ref.so")
     if os.path.exists(path):
         ref = capi.bind_api(C.CDLL(path))

@@ -21,7 +21,10 @@ extern "C" {
 typedef enum {
     PDHCG_B200_FP64 = 0,       /* every vector and matrix value in double */
     PDHCG_B200_MIXED = 1       /* FP32 matrix values and iterates with FP64 accumulation and FP64
-                                  residuals/restarts, then an FP64 polish phase */
+                                  residuals/restarts, then an FP64 polish phase.  Problems that take
+                                  the inner BB solve (sparse or low-rank Q, PSD blocks) read FP32
+                                  values of Q, R, R^T and of A's long rows in the bulk phase, with
+                                  FP64 iterates. */
 } pdhcg_b200_precision_t;
 
 typedef struct {

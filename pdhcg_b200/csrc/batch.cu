@@ -117,7 +117,7 @@ struct Layout {
     int c, l, u, q, x0, x, xp, xr, dx, ds;             // x side, float
     int lc, uc, y0, y, yp, dy;                         // y side, float
     int vr, cr;                                        // scaling, double
-    int red;                                           // reduction scratch, double[32]
+    int red;                                           // reduction scratch, double[320]
     int total;
     __host__ __device__ static int al(int b) { return (b + 15) & ~15; }
     __host__ __device__ Layout(int n, int m, int sell_a, int sell_at)
@@ -147,7 +147,7 @@ struct Layout {
         dy = o; o += al(4 * m);
         vr = o; o += al(8 * n);
         cr = o; o += al(8 * m);
-        red = o; o += al(8 * 64);
+        red = o; o += al(8 * 10 * 32); // reduce_n of up to 10 values over up to 32 warps
         total = o;
     }
 };
@@ -185,6 +185,40 @@ struct Grp {
             r = is_max ? fmax(r, red[i]) : r + red[i];
         sync();
         return r;
+    }
+    // K values at once (bit k of is_max: maximum instead of sum), each in the
+    // order reduce() uses, with two barriers for all of them; red holds
+    // K x GROUP / 32 doubles
+    template <int K>
+    __device__ void reduce_n(double (&v)[K], unsigned is_max, double *red) const
+    {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const bool mx = (is_max >> k) & 1u;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double w = __shfl_xor_sync(0xffffffffu, v[k], o);
+                v[k] = mx ? fmax(v[k], w) : v[k] + w;
+            }
+        }
+        if (GROUP == 32)
+            return;
+        constexpr int NW = GROUP / 32;
+        if ((t & 31) == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+                red[k * NW + (t >> 5)] = v[k];
+        }
+        sync();
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const bool mx = (is_max >> k) & 1u;
+            double r = red[k * NW];
+            for (int i = 1; i < NW; ++i)
+                r = mx ? fmax(r, red[k * NW + i]) : r + red[k * NW + i];
+            v[k] = r;
+        }
+        sync();
     }
 };
 
@@ -259,10 +293,14 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
         b2 += bb;
         bmax = fmax(bmax, bm);
     }
-    c2 = g.reduce(c2, false, red);
-    cmax = g.reduce(cmax, true, red);
-    b2 = g.reduce(b2, false, red);
-    bmax = g.reduce(bmax, true, red);
+    {
+        double rv[4] = {c2, cmax, b2, bmax};
+        g.reduce_n(rv, 0xau, red);
+        c2 = rv[0];
+        cmax = rv[1];
+        b2 = rv[2];
+        bmax = rv[3];
+    }
     const double cnorm = P.l2 ? sqrt(c2) : cmax, bnorm = P.l2 ? sqrt(b2) : bmax;
 
     // ---- rescaling (reference rescale_problem, src/preconditioner.c:654-713):
@@ -317,8 +355,10 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
             double v = gc[j] / vr[j];
             cc2 += v * v;
         }
-        bb2 = g.reduce(bb2, false, red);
-        cc2 = g.reduce(cc2, false, red);
+        double rv[2] = {bb2, cc2};
+        g.reduce_n(rv, 0u, red);
+        bb2 = rv[0];
+        cc2 = rv[1];
         sb = 1.0 / (sqrt(bb2) + 1.0);
         sc = 1.0 / (sqrt(cc2) + 1.0);
     }
@@ -466,16 +506,18 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
             }
         }
         const bool L2 = P.l2 != 0;
-        pr = g.reduce(pr, !L2, red);
-        dr = g.reduce(dr, !L2, red);
-        qn = g.reduce(qn, !L2, red);
-        an = g.reduce(an, !L2, red);
-        pslack = g.reduce(pslack, false, red);
-        cx = g.reduce(cx, false, red);
-        xqx = g.reduce(xqx, false, red);
-        sx = g.reduce(sx, false, red);
-        dx2 = g.reduce(dx2, false, red);
-        dy2 = g.reduce(dy2, false, red);
+        double rv[10] = {pr, dr, qn, an, pslack, cx, xqx, sx, dx2, dy2};
+        g.reduce_n(rv, L2 ? 0u : 0xfu, red);
+        pr = rv[0];
+        dr = rv[1];
+        qn = rv[2];
+        an = rv[3];
+        pslack = rv[4];
+        cx = rv[5];
+        xqx = rv[6];
+        sx = rv[7];
+        dx2 = rv[8];
+        dy2 = rv[9];
         auto nrm = [&](double v) { return L2 ? sqrt(v) : v; };
         abs_p = nrm(pr) / sb;
         abs_d = nrm(dr) / sc;
@@ -504,9 +546,11 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
             double d = dy[i];
             d2 += d * d;
         }
-        p2 = g.reduce(p2, false, red);
-        d2 = g.reduce(d2, false, red);
-        cross = g.reduce(cross, false, red);
+        double rv[3] = {p2, d2, cross};
+        g.reduce_n(rv, 0u, red);
+        p2 = rv[0];
+        d2 = rv[1];
+        cross = rv[2];
         double mv = p2 * omega + d2 / omega;
         return sqrt(mv + 2.0 * step * cross);
     };
@@ -569,6 +613,7 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
         const bool want_fpe = is_major || do_restart;
         const double w = (double)(inner + 1) / (double)(inner + 2);
         const double tau = step / omega, sigma = step * omega;
+        const double inv_tau = 1.0 / tau, inv_sigma = 1.0 / sigma;
         // primal step (reference pdhg_update + halpern_update)
         for (int j = t; j < n; j += GROUP) {
             const double s = sell_dot(atrp, atci, atv, y, j);
@@ -581,7 +626,7 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
             xp[j] = (float)p;
             xr[j] = (float)xrr;
             if (!hasq)
-                ds[j] = (float)((p - tt) / tau);
+                ds[j] = (float)((p - tt) * inv_tau);
             dx[j] = (float)(xrr - xi);
             double refl = P.rho * xrr + (1.0 - P.rho) * xi;
             x[j] = (float)(w * refl + (1.0 - w) * (double)x0[j]);
@@ -590,7 +635,7 @@ __device__ void solve_instance(const BData &D, const BParams &P, int idx, char *
         for (int i = t; i < m; i += GROUP) {
             const double s = sell_dot(arp, aci, av, xr, i);
             double yi = y[i];
-            double pr = clampd((double)lc[i], s - yi / sigma, (double)uc[i]);
+            double pr = clampd((double)lc[i], s - yi * inv_sigma, (double)uc[i]);
             double yn = yi - sigma * s + sigma * pr;
             double yrr = 2.0 * yn - yi;
             yp[i] = (float)yn;
@@ -863,6 +908,23 @@ struct Pack {
         end = o;
     }
     size_t host_bytes() const { return in_end + (end - out); }
+};
+
+// The streams and events of one call's class launches (released on every
+// exit path).
+struct ClassStreams {
+    cudaEvent_t ready = nullptr;
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> done;
+    ~ClassStreams()
+    {
+        for (cudaStream_t st : streams)
+            cudaStreamDestroy(st);
+        for (cudaEvent_t ev : done)
+            cudaEventDestroy(ev);
+        if (ready)
+            cudaEventDestroy(ready);
+    }
 };
 
 // A launch shape: threads per CTA, threads per instance group.
@@ -1212,6 +1274,22 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
             ++launches;
             BCK(cudaGetLastError());
         }
+        // every class on a stream of its own, all queued at once: a class's
+        // CTAs take the SMs that the previous class's CTAs leave when its
+        // instances run out, so the classes' tails overlap instead of adding
+        // up (each class still runs its instances largest first)
+        ClassStreams cs;
+        BCK(cudaEventCreateWithFlags(&cs.ready, cudaEventDisableTiming));
+        BCK(cudaEventRecord(cs.ready, 0));
+        for (size_t ci = 0; ci < classes.size(); ++ci) {
+            cudaStream_t st = nullptr;
+            cudaEvent_t done = nullptr;
+            BCK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            cs.streams.push_back(st);
+            BCK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+            cs.done.push_back(done);
+            BCK(cudaStreamWaitEvent(st, cs.ready, 0));
+        }
         for (size_t ci = 0; ci < classes.size(); ++ci) {
             const int b = classes[ci].first, e = classes[ci].second;
             int max_smem = 0, max_dim = 0;
@@ -1226,12 +1304,14 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
             Dc.order = d_order + b;
             Dc.count = e - b;
             Dc.next = d_next + ci;
-            cudaError_t err = launch(sh, Dc, P, max_smem, sms, 0);
+            cudaError_t err = launch(sh, Dc, P, max_smem, sms, cs.streams[ci]);
             ++launches;
             if (err != cudaSuccess) {
                 std::fprintf(stderr, "[pdhcg_b200_solve_batch] launch: %s\n", cudaGetErrorString(err));
                 return -1;
             }
+            BCK(cudaEventRecord(cs.done[ci], cs.streams[ci]));
+            BCK(cudaStreamWaitEvent(0, cs.done[ci], 0));
         }
         BCK(cudaEventRecord(e1, 0));
         BCK(cudaMemcpyAsync(H + L.in_end, G + L.out, d2h, cudaMemcpyDeviceToHost, 0));

@@ -41,6 +41,9 @@ struct BBData {
                               // row-major k x r_width (R^T not built); 0: R and R^T as CSR
     int dkind;               // 0 none (D = I), 1 diagonal, 2 dense (row-major, upper triangle used)
     const double *Ddiag, *Ddense;
+    // FP32 copies of Q's, R's and R^T's values for the mixed-precision bulk
+    // phase (NULL: the FP64 values); products accumulate in FP64 either way
+    const float *Q_vf, *R_vf, *Rt_vf;
     // Jacobi preconditioner M = diag(Q) + 1/tau (NULL: none)
     const double *m_diag, *m_inv;
     const double *tol_scale; // device scalar sqrt(sum |M| / n)
@@ -110,19 +113,67 @@ __device__ __forceinline__ void bb_block_partial(double v, double *part)
     __syncthreads();
 }
 
+// Dense R (every row over columns 0..r_width-1): warp w of block b takes
+// rows 4w .. 4w+3, 4(w + WARPS) .., and sums each row's b-th chunk with
+// the row's own accumulator, so one load of v serves four rows and four
+// loads of R are in flight per lane; each row's lane partials and warp sum
+// run in the order of the one-row loop.
+template <typename T>
+__device__ __forceinline__ void bb_rx_partials_dense(const BBData &D, const T *R, const double *v)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nb = gridDim.x;
+    const long long w = D.r_width;
+    const int cb = (int)(w * blockIdx.x / nb), ce = (int)(w * (blockIdx.x + 1) / nb);
+    for (int r0 = 4 * wid; r0 < D.k; r0 += 4 * WARPS) {
+        const int nr = min(4, D.k - r0);
+        const T *row[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            row[q] = R + (long long)D.R_rp[r0 + (q < nr ? q : 0)];
+        double s[4] = {0.0, 0.0, 0.0, 0.0};
+        if (nr == 4) {
+            for (int c = cb + lane; c < ce; c += 32) {
+                const double vc = v[c];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    s[q] += (double)row[q][c] * vc;
+            }
+        } else {
+            for (int c = cb + lane; c < ce; c += 32) {
+                const double vc = v[c];
+                for (int q = 0; q < nr; ++q)
+                    s[q] += (double)row[q][c] * vc;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double t = warp_sum(s[q]);
+            if (q < nr && lane == 0)
+                D.rx_part[(size_t)blockIdx.x * D.k + r0 + q] = t;
+        }
+    }
+}
+
 // Low-rank part, step 1: partials of R v.  Block b owns the b-th chunk of
 // every row of R; warp w of the block folds rows w, w + WARPS, ...
 __device__ void bb_rx_partials(const BBData &D, const double *v)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nb = gridDim.x;
+    if (D.r_width) {
+        if (D.R_vf)
+            bb_rx_partials_dense(D, D.R_vf, v);
+        else
+            bb_rx_partials_dense(D, D.R_v, v);
+        return;
+    }
     for (int r = wid; r < D.k; r += WARPS) {
         int b0 = D.R_rp[r], e0 = D.R_rp[r + 1];
         long long len = e0 - b0;
         int cb = b0 + (int)(len * blockIdx.x / nb), ce = b0 + (int)(len * (blockIdx.x + 1) / nb);
         double s = 0.0;
-        if (D.r_width) // column of entry e is e - b0
+        if (D.R_vf)
             for (int e = cb + lane; e < ce; e += 32)
-                s += D.R_v[e] * v[e - b0];
+                s += (double)D.R_vf[e] * v[D.R_ci[e]];
         else
             for (int e = cb + lane; e < ce; e += 32)
                 s += D.R_v[e] * v[D.R_ci[e]];
@@ -182,16 +233,43 @@ __device__ __forceinline__ double bb_rt_part(const BBData &D, const double *drx,
 {
     double s = 0.0;
     if (D.r_width) { // column j of the row-major R, rows in increasing order (the order of R^T row j)
-        if (j < D.r_width) {
-            const double *col = D.R_v + j;
-            for (int r = sub; r < D.k; r += G)
-                s += col[(size_t)r * D.r_width] * drx[r];
+        if (j < D.r_width) { // unrolled so that many loads of the column are in flight
+            if (D.R_vf) {
+                const float *col = D.R_vf + j;
+#pragma unroll 16
+                for (int r = sub; r < D.k; r += G)
+                    s += (double)col[(size_t)r * D.r_width] * drx[r];
+            } else {
+                const double *col = D.R_v + j;
+#pragma unroll 16
+                for (int r = sub; r < D.k; r += G)
+                    s += col[(size_t)r * D.r_width] * drx[r];
+            }
         }
     } else {
         int b = D.Rt_rp[j], e = D.Rt_rp[j + 1];
-        for (int t = b + sub; t < e; t += G)
-            s += D.Rt_v[t] * drx[D.Rt_ci[t]];
+        if (D.Rt_vf)
+            for (int t = b + sub; t < e; t += G)
+                s += (double)D.Rt_vf[t] * drx[D.Rt_ci[t]];
+        else
+            for (int t = b + sub; t < e; t += G)
+                s += D.Rt_v[t] * drx[D.Rt_ci[t]];
     }
+    return s;
+}
+
+// This lane's share (entries sub, sub + G, ...) of Q row j . v
+template <int G>
+__device__ __forceinline__ double bb_qsp_part(const BBData &D, const double *v, int j, int sub)
+{
+    const int b = D.Q_rp[j], e = D.Q_rp[j + 1];
+    double s = 0.0;
+    if (D.Q_vf)
+        for (int t = b + sub; t < e; t += G)
+            s += (double)D.Q_vf[t] * v[D.Q_ci[t]];
+    else
+        for (int t = b + sub; t < e; t += G)
+            s += D.Q_v[t] * v[D.Q_ci[t]];
     return s;
 }
 
@@ -202,11 +280,8 @@ __device__ __forceinline__ double bb_q_row(const BBData &D, const double *v, con
                                            bool ok)
 {
     double s = 0.0;
-    if (ok && D.sparse) {
-        int b = D.Q_rp[j], e = D.Q_rp[j + 1];
-        for (int t = b + sub; t < e; t += G)
-            s += D.Q_v[t] * v[D.Q_ci[t]];
-    }
+    if (ok && D.sparse)
+        s = bb_qsp_part<G>(D, v, j, sub);
     if (ok && D.k > 0) {
         s += bb_rt_part<G>(D, drx, j, sub);
     }
@@ -245,11 +320,8 @@ __device__ __forceinline__ double bb_cone_block(const BBData &D, const double *d
             bool ok = slot < L;
             int j = st + (ok ? slot : 0);
             double s = 0.0;
-            if (ok && D.sparse) {
-                int b = D.Q_rp[j], e = D.Q_rp[j + 1];
-                for (int t = b + sub; t < e; t += G)
-                    s += D.Q_v[t] * D.x[D.Q_ci[t]];
-            }
+            if (ok && D.sparse)
+                s = bb_qsp_part<G>(D, D.x, j, sub);
             if (ok && D.k > 0)
                 s += bb_rt_part<G>(D, drx, j, sub);
             s = group_sum<G>(s);
@@ -327,8 +399,7 @@ __device__ __noinline__ double bb_psd_long_block(const BBData &D, const double *
         if (init) {
             double q = 0.0; // (Q x)_j, one lane per slot
             if (D.sparse)
-                for (int t = D.Q_rp[j]; t < D.Q_rp[j + 1]; ++t)
-                    q += D.Q_v[t] * D.x[D.Q_ci[t]];
+                q = bb_qsp_part<1>(D, D.x, j, 0);
             if (D.k > 0)
                 q += bb_rt_part<1>(D, drx, j, 0);
             g = q + D.c[j] - D.aty[j];
@@ -382,11 +453,8 @@ __device__ double bb_var_phase(const BBData &D, const double *drx, bool init, do
                 // Q x for the gradient at the prox centre
                 if (D.sparse || D.k > 0) {
                     double s = 0.0;
-                    if (ok && D.sparse) {
-                        int b = D.Q_rp[j], e = D.Q_rp[j + 1];
-                        for (int t = b + sub; t < e; t += G)
-                            s += D.Q_v[t] * D.x[D.Q_ci[t]];
-                    }
+                    if (ok && D.sparse)
+                        s = bb_qsp_part<G>(D, D.x, j, sub);
                     if (ok && D.k > 0)
                         s += bb_rt_part<G>(D, drx, j, sub);
                     q = group_sum<G>(s);

@@ -171,8 +171,20 @@ __device__ __forceinline__ double warp_range_dot(const int *__restrict__ ci, con
         a2 += (double)__ldg(val + k + 64) * (double)__ldg(x + __ldg(ci + k + 64));
         a3 += (double)__ldg(val + k + 96) * (double)__ldg(x + __ldg(ci + k + 96));
     }
-    for (; k < e; k += 32)
-        a0 += (double)__ldg(val + k) * (double)__ldg(x + __ldg(ci + k));
+    // at most three strides remain (k + 96 >= e): their loads are issued
+    // together, then added to a0 in stride order
+    const bool p0 = k < e, p1 = k + 32 < e, p2 = k + 64 < e;
+    const int c0 = p0 ? __ldg(ci + k) : 0, c1 = p1 ? __ldg(ci + k + 32) : 0, c2 = p2 ? __ldg(ci + k + 64) : 0;
+    const double v0 = p0 ? (double)__ldg(val + k) : 0.0, v1 = p1 ? (double)__ldg(val + k + 32) : 0.0,
+                 v2 = p2 ? (double)__ldg(val + k + 64) : 0.0;
+    const double x0 = p0 ? (double)__ldg(x + c0) : 0.0, x1 = p1 ? (double)__ldg(x + c1) : 0.0,
+                 x2 = p2 ? (double)__ldg(x + c2) : 0.0;
+    if (p0)
+        a0 += v0 * x0;
+    if (p1)
+        a0 += v1 * x1;
+    if (p2)
+        a0 += v2 * x2;
     return warp_sum((a0 + a1) + (a2 + a3));
 }
 

@@ -269,6 +269,7 @@ struct DevCsr {
     int *rp = nullptr, *ci = nullptr;
     double *v = nullptr;
     LongRows lr{}; // rows of more than LONG_ROW entries, cut into segments (n = 0: none)
+    long long long_nnz = 0; // entries in those rows
 };
 
 // The long rows of M and their segments.  A count on the device decides
@@ -291,9 +292,11 @@ void build_long_rows(DevCsr &M, Arena &ar, cudaStream_t s)
     CK(cudaStreamSynchronize(s));
     std::vector<int> rows, first{0};
     std::vector<int2> seg;
+    M.long_nnz = 0;
     for (int r = 0; r < M.rows; ++r) {
         if (rp[r + 1] - rp[r] <= LONG_ROW)
             continue;
+        M.long_nnz += rp[r + 1] - rp[r];
         rows.push_back(r);
         for (int b = rp[r]; b < rp[r + 1]; b += LONG_SEG)
             seg.push_back(make_int2(b, std::min(rp[r + 1], b + LONG_SEG)));
@@ -702,7 +705,7 @@ private:
     template <typename T>
     StepData<T> step_data();
     double step_bytes(size_t s, bool store_primal, bool store_dual) const;
-    double bb_inner_bytes() const;
+    double bb_inner_bytes(bool fp32) const;
     template <typename V, typename X>
     void long_pass(const DevCsr &M, const V *val, const X *x);
     void enqueue_residual(bool want_dist);
@@ -710,6 +713,8 @@ private:
     void enqueue_residual_t(bool want_dist);
     void enter_fp32();
     void leave_fp32();
+    void enter_bb_fp32();
+    void leave_bb_fp32();
     void read_residual();
     void enqueue_fpe(int slot);
     pdhcg_result_t *make_result();
@@ -739,6 +744,12 @@ private:
     double *bb_diag_h_ = nullptr, *bb_m_ = nullptr, *bb_minv_ = nullptr;
     int *bb_inner_ = nullptr;
     double bb_cached_inv_tau_ = -1.0, bb_min_tol_ = 1e-9;
+    // mixed precision on the inner-solve path: FP32 copies of Q's, R's and
+    // R^T's values while bb_fp32_ (iterates and accumulation stay FP64)
+    bool bb_fp32_ = false;
+    float *Qf_ = nullptr, *Rf_ = nullptr, *Rtf_ = nullptr;
+    float *Af_ = nullptr, *Atf_ = nullptr; // and of A's, A^T's values, read by the long-row passes
+    long long bb_inner_fp32_ = 0;          // inner iterations taken with the FP32 values
     BBData bb_data() const;
     void setup_bb();
     void enqueue_q_apply(const double *v, double *qx);
@@ -1152,6 +1163,9 @@ BBData Solve::bb_data() const
     D.dkind = dp_.dkind;
     D.Ddiag = dp_.Ddiag;
     D.Ddense = dp_.Ddense;
+    D.Q_vf = bb_fp32_ && Q_.nnz > 0 ? Qf_ : nullptr;
+    D.R_vf = bb_fp32_ && R_.nnz > 0 ? Rf_ : nullptr;
+    D.Rt_vf = bb_fp32_ && Rt_.nnz > 0 && !r_width_ ? Rtf_ : nullptr;
     D.m_diag = bb_m_;
     D.m_inv = bb_minv_;
     D.tol_scale = bb_tscale_;
@@ -1428,7 +1442,14 @@ template <typename T>
 void Solve::launch_dual(const StepData<T> &D, const StepParams &P)
 {
     cudaStream_t s = st_;
-    long_pass(A_, D.A_v, D.xr);
+    if constexpr (std::is_same<T, double>::value) {
+        if (bb_fp32_ && Af_)
+            long_pass(A_, (const float *)Af_, D.xr);
+        else
+            long_pass(A_, D.A_v, D.xr);
+    } else {
+        long_pass(A_, D.A_v, D.xr);
+    }
     if (D.n_aff > 0) { // affine cone blocks: one warp each
         dispatch_s(dp_.S_aff, [&](auto SC) {
             dual_cone_kernel<SC.value, T><<<grid_for(D.n_aff, WARPS), TPB, 0, s>>>(D, P);
@@ -1472,7 +1493,10 @@ void Solve::enqueue_step_bb(bool store_dual, bool want_fpe, double w)
         tau = std::fmax(tau, -1.01 * std::fmin(0.0, nonconvexity_));
         tau /= 100;
     }
-    long_pass(At_, At_.v, y_);
+    if (bb_fp32_ && Atf_)
+        long_pass(At_, (const float *)Atf_, y_);
+    else
+        long_pass(At_, At_.v, y_);
     spmv_kernel<<<grid_for(((long long)n_ + 31) / 32, WARPS), TPB, 0, s>>>(n_, At_.rp, At_.ci, At_.v, y_, bb_aty_,
                                                                           At_.lr);
     double inv_tau = 1.0 / tau;
@@ -1507,7 +1531,13 @@ void Solve::enqueue_step_bb(bool store_dual, bool want_fpe, double w)
     launch_dual<double>(SD, P);
     stats_.kernel_launches += 2;
     stats_.step_kernel_launches++;
-    step_bytes_sum_ += step_bytes(sizeof(double), true, store_dual);
+    if (bb_fp32_)
+        stats_.fp32_iterations++;
+    {
+        // entries of long rows read as FP32 values in the mixed bulk phase
+        const double f32 = bb_fp32_ ? (double)((Af_ ? A_.long_nnz : 0) + (Atf_ ? At_.long_nnz : 0)) : 0.0;
+        step_bytes_sum_ += step_bytes(sizeof(double), true, store_dual) - 4.0 * f32;
+    }
     if (opt_.time_steps)
         CK(cudaEventRecord(ev_pool_[ev_used_++], s));
 }
@@ -1610,13 +1640,14 @@ double Solve::step_bytes(size_t s, bool store_primal, bool store_dual) const
 // with x_p gathered once, and fifteen n-vectors of the gradient and
 // projection phases (grad phase: c, A^T y, x_p, x, grad, dir read, grad,
 // Q x written; var phase: grad, x_p, l, u, M^-1 read, x_p, dir written).
-double Solve::bb_inner_bytes() const
+double Solve::bb_inner_bytes(bool fp32) const
 {
     double n = n_;
-    double q = Q_.nnz > 0 ? Q_.nnz * 12.0 + (n + 1) * 4 + n * 8 : 0.0;
+    const double vb = fp32 ? 4.0 : 8.0; // bytes of a value of Q, R, R^T
+    double q = Q_.nnz > 0 ? Q_.nnz * (4.0 + vb) + (n + 1) * 4 + n * 8 : 0.0;
     double r = R_.nnz == 0 ? 0.0
-               : r_width_ ? 2.0 * R_.nnz * 8.0 + r_width_ * 8.0 // values only, x_p read contiguously
-                          : 2.0 * R_.nnz * 12.0 + (R_.rows + 1) * 4.0 + (n + 1) * 4 + n * 8;
+               : r_width_ ? 2.0 * R_.nnz * vb + r_width_ * 8.0 // values only, x_p read contiguously
+                          : 2.0 * R_.nnz * (4.0 + vb) + (R_.rows + 1) * 4.0 + (n + 1) * 4 + n * 8;
     return q + r + 15.0 * n * 8;
 }
 
@@ -1877,6 +1908,53 @@ void Solve::enter_fp32()
     fp32_ = true;
 }
 
+// the inner-solve path: FP32 copies of the quadratic term's values and of
+// the values of A's and A^T's long rows (the products keep FP64 iterates and
+// accumulation); leaving only switches the pointers back, since the
+// iterates never left FP64
+void Solve::enter_bb_fp32()
+{
+    cudaStream_t s = st_;
+    auto mk = [&](long long k) { return ar_.alloc<float>((size_t)std::max(k, 1LL)); };
+    auto cv = [&](const double *src, float *dst, long long k) {
+        if (k > 0 && src)
+            convert_kernel<double, float><<<grid_for(k, TPB), TPB, 0, s>>>(src, dst, k);
+    };
+    if (Q_.nnz > 0) {
+        Qf_ = mk(Q_.nnz);
+        cv(Q_.v, Qf_, Q_.nnz);
+    }
+    if (R_.nnz > 0) {
+        Rf_ = mk(R_.nnz);
+        cv(R_.v, Rf_, R_.nnz);
+    }
+    if (Rt_.nnz > 0 && !r_width_) {
+        Rtf_ = mk(Rt_.nnz);
+        cv(Rt_.v, Rtf_, Rt_.nnz);
+    }
+    // the long rows of A and A^T (segment passes ahead of the products) read
+    // FP32 values too; the products' other rows keep FP64 values
+    if (A_.lr.n > 0) {
+        Af_ = mk(A_.nnz);
+        cv(A_.v, Af_, A_.nnz);
+    }
+    if (At_.lr.n > 0) {
+        Atf_ = mk(At_.nnz);
+        cv(At_.v, Atf_, At_.nnz);
+    }
+    CK(cudaGetLastError());
+    bb_fp32_ = true;
+}
+
+void Solve::leave_bb_fp32()
+{
+    int inner = 0;
+    CK(cudaMemcpyAsync(&inner, bb_inner_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+    CK(cudaStreamSynchronize(st_));
+    bb_inner_fp32_ = inner_total_ + inner; // first passes counted here, further ones on the device
+    bb_fp32_ = false;
+}
+
 void Solve::leave_fp32()
 {
     cudaStream_t s = st_;
@@ -1993,7 +2071,7 @@ void Solve::loop()
                 reason_ = TERMINATION_REASON_TIME_LIMIT;
             if (reason_ != TERMINATION_REASON_UNSPECIFIED)
                 break;
-            if (fp32_) {
+            if (fp32_ || bb_fp32_) {
                 // FP32 bulk phase hands over to FP64 once the relative KKT error
                 // is below the polish threshold, or when it stops improving
                 double kkt = std::fmax(rel_p_, std::fmax(rel_d_, rel_gap_));
@@ -2003,8 +2081,12 @@ void Solve::loop()
                 } else {
                     ++fp32_stall_;
                 }
-                if (kkt < opt_.polish_threshold || fp32_stall_ >= 30)
-                    leave_fp32();
+                if (kkt < opt_.polish_threshold || fp32_stall_ >= 30) {
+                    if (fp32_)
+                        leave_fp32();
+                    else
+                        leave_bb_fp32();
+                }
             }
         }
         if (is_major_ || k_ == 0) {
@@ -2286,8 +2368,12 @@ pdhcg_result_t *Solve::run()
     bb_ = qtype_ != PDHCG_NON_Q && (qtype_ != PDHCG_DIAG_Q || dp_.var_psd);
     if (bb_)
         setup_bb();
-    if (opt_.precision == PDHCG_B200_MIXED && !bb_) // the inner BB solve runs in FP64 only
-        enter_fp32();
+    if (opt_.precision == PDHCG_B200_MIXED) {
+        if (bb_)
+            enter_bb_fp32();
+        else
+            enter_fp32();
+    }
     stats_.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_setup).count();
     loop();
     if (bb_) {
@@ -2303,8 +2389,10 @@ pdhcg_result_t *Solve::run()
     double nnz = (double)A_.nnz;
     stats_.spmv_bytes = 2.0 * nnz * (8 + 4) + 4.0 * ((double)n_ + m_ + 2) + 8.0 * ((double)n_ + m_);
     double bytes = step_bytes_sum_;
-    if (bb_) // the inner solve: one first pass per step plus every further inner iteration
-        bytes += (double)inner_total_ * bb_inner_bytes();
+    if (bb_) { // the inner solve: one first pass per step plus every further inner iteration
+        const long long in32 = std::min(bb_inner_fp32_, inner_total_);
+        bytes += (double)(inner_total_ - in32) * bb_inner_bytes(false) + (double)in32 * bb_inner_bytes(true);
+    }
     stats_.step_bytes = stats_.step_kernel_launches > 0 ? bytes / stats_.step_kernel_launches : 0.0;
     stats_.primal_weight = omega_;
     stats_.step_size = step_;

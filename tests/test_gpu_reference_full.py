@@ -73,6 +73,11 @@ def test_portfolio_full_size(lib, ref):
     g, r = _solve(lib, p, _eps(1e-6)), _solve(ref, p, _eps(1e-6))
     assert g["total_count"] == r["total_count"], (g["total_count"], r["total_count"])
     check_same_solution(g, r, 1e-6, sol_tol=1e-6)
+    # mixed: FP32 values of R and of A's long rows in the bulk phase, FP64 polish
+    mixed = _solve(lib, p, _eps(1e-6), native.default_options(precision=1))
+    assert abs(mixed["total_count"] - r["total_count"]) <= 0.1 * r["total_count"], (mixed["total_count"],
+                                                                                   r["total_count"])
+    check_same_solution(mixed, r, 1e-6, obj_tol=1e-7, sol_tol=1e-6, res_tol=0.5)
 
 
 def test_mpc_batch_sample_against_reference(lib, ref):

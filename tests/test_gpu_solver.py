@@ -144,11 +144,13 @@ def _solve_gpu_opts(lib, p, params, **opts):
     return d, native.last_stats()
 
 
-@pytest.mark.parametrize("name", ["diag_qp", "conic_qp", "soc_qp_small", "box_lp", "dense_rows_qp", "affine_qp"])
+@pytest.mark.parametrize("name", ["diag_qp", "conic_qp", "soc_qp_small", "box_lp", "dense_rows_qp", "affine_qp",
+                                  "sparse_qp_small", "portfolio_small", "psd_qp"])
 def test_mixed_precision_reaches_fp64_answer(lib, name):
     """FP32 bulk phase + FP64 polish: same status as plain FP64, objective
     within the termination tolerance of the FP64 answer, and the FP32 phase
-    actually ran (fp32_iterations > 0)."""
+    actually ran (fp32_iterations > 0).  The last three take the inner BB
+    solve, whose bulk phase reads FP32 values of Q, R and R^T."""
     make, prm = CASES[name]
     p = make()
     prm = {"termination_criteria.iteration_limit": 100000,
