@@ -132,6 +132,7 @@ __device__ __forceinline__ void bb_rx_partials_dense(const BBData &D, const T *R
             row[q] = R + (long long)D.R_rp[r0 + (q < nr ? q : 0)];
         double s[4] = {0.0, 0.0, 0.0, 0.0};
         if (nr == 4) {
+#pragma unroll 4
             for (int c = cb + lane; c < ce; c += 32) {
                 const double vc = v[c];
 #pragma unroll

@@ -165,6 +165,29 @@ __device__ __forceinline__ double warp_range_dot(const int *__restrict__ ci, con
 {
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
     int k = b + lane;
+    // two strides of 128 at a time: the eight index and value loads, then the
+    // eight gathers, are in flight together; each partial sum still adds its
+    // entries in stride order
+    for (; k + 224 < e; k += 256) {
+        int c[8];
+        double v[8], w[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            c[u] = __ldg(ci + k + 32 * u);
+            v[u] = (double)__ldg(val + k + 32 * u);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            w[u] = (double)__ldg(x + c[u]);
+        a0 += v[0] * w[0];
+        a1 += v[1] * w[1];
+        a2 += v[2] * w[2];
+        a3 += v[3] * w[3];
+        a0 += v[4] * w[4];
+        a1 += v[5] * w[5];
+        a2 += v[6] * w[6];
+        a3 += v[7] * w[7];
+    }
     for (; k + 96 < e; k += 128) {
         a0 += (double)__ldg(val + k) * (double)__ldg(x + __ldg(ci + k));
         a1 += (double)__ldg(val + k + 32) * (double)__ldg(x + __ldg(ci + k + 32));
@@ -195,11 +218,15 @@ __device__ __forceinline__ void long_partials(const LongRows &L, const int *__re
                                               const V *__restrict__ val, const X *__restrict__ x, int gw, int nw,
                                               int lane)
 {
+    // the next segment's bounds are loaded before this segment's sum, so a
+    // warp that walks many short segments does not wait for them each time
+    int2 r = gw < L.nseg ? L.seg[gw] : make_int2(0, 0);
     for (int sg = gw; sg < L.nseg; sg += nw) {
-        const int2 r = L.seg[sg];
+        const int2 rn = sg + nw < L.nseg ? L.seg[sg + nw] : make_int2(0, 0);
         const double a = warp_range_dot(ci, val, x, r.x, r.y, lane);
         if (lane == 0)
             L.part[sg] = a;
+        r = rn;
     }
 }
 

@@ -1657,7 +1657,10 @@ void Solve::long_pass(const DevCsr &M, const V *val, const X *x)
 {
     if (M.lr.n == 0)
         return;
-    long_partials_kernel<V, X><<<grid_for(M.lr.nseg, WARPS), TPB, 0, st_>>>(M.lr, M.ci, val, x);
+    // at most what is resident at once: warps walk their segments
+    // grid-stride, the next one's bounds in flight
+    const int grid = std::min(grid_for(M.lr.nseg, WARPS), resident_blocks((const void *)long_partials_kernel<V, X>));
+    long_partials_kernel<V, X><<<grid, TPB, 0, st_>>>(M.lr, M.ci, val, x);
     stats_.kernel_launches++;
 }
 
