@@ -20,6 +20,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <unordered_map>
 #include <vector>
@@ -65,6 +66,79 @@ double *pinned_scalars()
     return b.p;
 }
 
+// Host-to-device copy of a large host array through two page-locked chunks
+// kept for the process: the host threads copy chunk i into one buffer while
+// the DMA engine moves the previous chunk out of the other, so the copy runs
+// at page-locked speed instead of through the driver's pageable staging.
+// The source may be freed when this returns; the destination is written in
+// stream order on s.  A chunk's buffer is reused once its copy has ended
+// (its event), also across calls, which take turns on the buffers.
+constexpr size_t STAGE_CHUNK = 32u << 20;
+constexpr size_t STAGE_MIN = 16u << 20; // smaller copies go straight through
+
+void staged_upload(void *dst, const void *src, size_t bytes, cudaStream_t s)
+{
+    static std::mutex mu;
+    static char *buf[2] = {nullptr, nullptr};
+    static cudaEvent_t ev[2] = {nullptr, nullptr};
+    static bool pending[2] = {false, false};
+    static int ev_dev = -1;
+    static int b = 0;
+    std::lock_guard<std::mutex> lock(mu);
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (!buf[0]) {
+        void *p = nullptr;
+        if (cudaHostAlloc(&p, 2 * STAGE_CHUNK, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+            CK(cudaStreamSynchronize(s));
+            return;
+        }
+        buf[0] = (char *)p;
+        buf[1] = (char *)p + STAGE_CHUNK;
+    }
+    if (ev_dev != dev) { // events are recorded on this device's streams
+        for (int i = 0; i < 2; ++i) {
+            if (ev[i]) {
+                if (pending[i])
+                    cudaEventSynchronize(ev[i]);
+                cudaEventDestroy(ev[i]);
+                ev[i] = nullptr;
+            }
+            pending[i] = false;
+        }
+        CK(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+        ev_dev = dev;
+    }
+    const int nt = (int)std::min<unsigned>(8u, std::max(1u, std::thread::hardware_concurrency()));
+    const char *from = (const char *)src;
+    char *to = (char *)dst;
+    for (size_t off = 0; off < bytes; off += STAGE_CHUNK, b ^= 1) {
+        const size_t len = std::min(STAGE_CHUNK, bytes - off);
+        if (pending[b]) {
+            CK(cudaEventSynchronize(ev[b]));
+            pending[b] = false;
+        }
+        // the chunk's host copy, split over up to nt threads
+        const size_t part = (len + nt - 1) / nt;
+        char *chunk = buf[b];
+        std::vector<std::thread> th;
+        for (int t = 1; t < nt && (size_t)t * part < len; ++t)
+            th.emplace_back([=]() {
+                const size_t a = (size_t)t * part, e = std::min(len, a + part);
+                std::memcpy(chunk + a, from + off + a, e - a);
+            });
+        std::memcpy(chunk, from + off, std::min(len, part));
+        for (auto &x : th)
+            x.join();
+        CK(cudaMemcpyAsync(to + off, chunk, len, cudaMemcpyHostToDevice, s));
+        CK(cudaEventRecord(ev[b], s));
+        pending[b] = true;
+    }
+}
+
 // The device's default memory pool keeps what solves free (no release
 // threshold), so the allocations of the next solve are served from the pool
 // instead of cudaMalloc; set once per device.
@@ -106,7 +180,9 @@ struct Arena {
     T *upload(const T *h, size_t count, cudaStream_t s)
     {
         T *d = alloc<T>(count);
-        if (count)
+        if (count * sizeof(T) >= STAGE_MIN)
+            staged_upload(d, h, count * sizeof(T), s);
+        else if (count)
             CK(cudaMemcpyAsync(d, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
         return d;
     }
@@ -2636,9 +2712,11 @@ static pdhcg_result_t *solve_on_device(const qp_problem_t *prob, const pdhg_para
                 throw;
             }
             cudaStreamDestroy(us);
+            const double build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
             opt.solution_on_device = 0; // the temporary device problem dies with this call
             Solve s(*dp, true, prm, opt);
             r = s.run();
+            g_last_stats.upload_ms += build_ms; // the problem's copies to the device (ended by a synchronise)
         }
         g_last_stats.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         if (r && prm.verbose >= 1) {
