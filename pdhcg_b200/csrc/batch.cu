@@ -28,6 +28,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <optional>
 #include <thread>
@@ -1208,7 +1209,46 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
         double *huc = (double *)(H + L.uc);
         int *hS = (int *)(H + L.S);
         // pack: every instance copied by a pool of host threads into its slot
-        // of the staging buffer (A^T is built on the device)
+        // of the staging buffer (A^T is built on the device).  The instances
+        // form NG groups of consecutive slots; the thread that packs a
+        // group's last instance queues that group's host-to-device copies, so
+        // the copies of early groups overlap the packing of later ones.
+        const int NG = std::min(nb, 16);
+        std::vector<int> gstart(NG + 1);
+        for (int g = 0; g <= NG; ++g)
+            gstart[g] = (int)((long long)nb * g / NG);
+        std::unique_ptr<std::atomic<int>[]> left(new std::atomic<int>[NG]);
+        for (int g = 0; g < NG; ++g)
+            left[g] = gstart[g + 1] - gstart[g];
+        std::atomic<int> copy_err{0};
+        auto copy_group = [&](int g) {
+            if (cudaSetDevice(dev) != cudaSuccess) { // the pool's threads start on device 0
+                copy_err = 1;
+                return;
+            }
+            const BInst &f = inst[gstart[g]];
+            const bool last = g + 1 == NG;
+            const BInst *e = last ? nullptr : &inst[gstart[g + 1]];
+            // {region, element size, first element, end element}
+            const struct {
+                size_t base, es;
+                long long a, b;
+            } rg[] = {{L.S, 4, f.so_off, last ? tot_s : e->so_off},
+                      {L.A_rp, 4, f.rp_off, last ? tot_rp : e->rp_off},
+                      {L.A_ci, 4, f.k_off, last ? tot_k : e->k_off},
+                      {L.A_v, 8, f.k_off, last ? tot_k : e->k_off},
+                      {L.c, 8, f.x_off, last ? tot_x : e->x_off},
+                      {L.l, 8, f.x_off, last ? tot_x : e->x_off},
+                      {L.u, 8, f.x_off, last ? tot_x : e->x_off},
+                      {L.q, 8, f.x_off, last ? tot_x : e->x_off},
+                      {L.lc, 8, f.y_off, last ? tot_y : e->y_off},
+                      {L.uc, 8, f.y_off, last ? tot_y : e->y_off}};
+            for (const auto &r : rg) {
+                const size_t off = r.base + (size_t)r.a * r.es, len = (size_t)(r.b - r.a) * r.es;
+                if (len > 0 && cudaMemcpyAsync(G + off, H + off, len, cudaMemcpyHostToDevice, 0) != cudaSuccess)
+                    copy_err = 1;
+            }
+        };
         parallel_for(nb, [&](int bi) {
             const qp_problem_t *p = probs[batched[bi]];
             const BInst &b = inst[bi];
@@ -1229,7 +1269,15 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
             std::memcpy(hq + b.x_off, qd.data(), n * sizeof(double));
             std::memcpy(hlc + b.y_off, p->constraint_lower_bound, m * sizeof(double));
             std::memcpy(huc + b.y_off, p->constraint_upper_bound, m * sizeof(double));
+            const int g = (int)(std::upper_bound(gstart.begin(), gstart.end(), bi) - gstart.begin()) - 1;
+            if (left[g].fetch_sub(1) == 1)
+                copy_group(g);
         });
+        BCK(cudaSetDevice(dev));
+        if (copy_err) {
+            std::fprintf(stderr, "[pdhcg_b200_solve_batch] host-to-device copy failed.\n");
+            return -1;
+        }
         std::memcpy(H + L.v0, v0.data(), v0.size() * sizeof(double));
         std::memcpy(H + L.inst, inst.data(), inst.size() * sizeof(BInst));
         std::memcpy(H + L.order, order.data(), order.size() * sizeof(int));
@@ -1258,7 +1306,10 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
         int *d_next = (int *)(G + L.next);
         h2d = L.in_end;
         d2h = L.end - L.out;
-        BCK(cudaMemcpyAsync(G, H, h2d, cudaMemcpyHostToDevice, 0));
+        // the parts no group copied: the power-method start vector, then the
+        // instance table and the order
+        BCK(cudaMemcpyAsync(G + L.v0, H + L.v0, L.S - L.v0, cudaMemcpyHostToDevice, 0));
+        BCK(cudaMemcpyAsync(G + L.inst, H + L.inst, L.in_end - L.inst, cudaMemcpyHostToDevice, 0));
         BCK(cudaMemsetAsync(G + L.next, 0, L.out - L.next, 0));
         BCK(cudaMemsetAsync(G + L.out, 0, d2h, 0));
         cudaEvent_t e0, e1;
