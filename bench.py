@@ -431,7 +431,8 @@ def measure_batch(count: int, steps: int, warmup: int, rank: int = 0, world: int
                "sequential_plain_solves": {"value": seq, "unit": "instances/s", "sample": min(seq_sample, k),
                                            "call": "solve_qp_problem per instance, one GPU"},
                "speedup_vs_sequential": (count / wall) / seq,
-               "shape": int(opts.shape), "autotune_ms": list(shape_ms), "gpu_launches": launches[0],
+               "shape": int(opts.shape), "band_shapes": [int(b) - 1 for b in opts.band_shape],
+               "autotune_ms": list(shape_ms), "gpu_launches": launches[0],
                "partition": {"ranks": world, "instances_on_rank0": k, "nnz_on_rank0": nnz_mine,
                              "nnz_total": int(sum(weights))}}
     for b in built:

@@ -129,8 +129,11 @@ int cone_block_length(const cone_blocks_t *blocks, int block);
  * per instance).  results[i] receives a heap result of problem i (free each
  * with pdhcg_result_free); returns 0, or -1 on error. */
 typedef struct {
-    int shape;       /* launch shape (index into the shapes below), -1: by size */
-    int reserved[7];
+    int shape;         /* launch shape (index into the shapes below), -1: by size */
+    int band_shape[7]; /* per size band, 1 + the band's launch shape; 0: not set (shape, or by size).
+                          Band b holds the instances that need more than 1/2^(b+1) and at most 1/2^b
+                          of a CTA's shared memory (band 6: everything smaller); each band present
+                          in a batch is one launch. */
 } pdhcg_b200_batch_options_t;
 
 /* Launch shapes {threads per CTA, threads per instance}:
@@ -157,9 +160,11 @@ int pdhcg_b200_last_batch_stats(pdhcg_b200_batch_stats_t *out);
  * (sized for the largest batch so far) between calls; this frees both. */
 void pdhcg_b200_batch_release(void);
 
-/* Times every launch shape on the given instances (solving them each time)
- * and stores the fastest in opts->shape; shape_ms (may be NULL) receives
- * PDHCG_B200_BATCH_SHAPES wall times in milliseconds. */
+/* Times every launch shape on each size band's instances among the given
+ * ones (at most 256 per band, solving them each time), stores each band's
+ * fastest in opts->band_shape and the fastest over all bands in
+ * opts->shape; shape_ms (may be NULL) receives PDHCG_B200_BATCH_SHAPES wall
+ * times in milliseconds, summed over the bands. */
 int pdhcg_b200_batch_autotune(int count, const qp_problem_t *const *probs, const pdhg_parameters_t *params,
                               pdhcg_b200_batch_options_t *opts, double *shape_ms);
 

@@ -987,6 +987,69 @@ bool diag_q(const qp_problem_t *p, std::vector<double> &q)
     return true;
 }
 
+// Size band of an instance by its shared-memory need: band b holds the
+// needs in (CAP / 2^(b+1), CAP / 2^b], band BATCH_BANDS - 1 everything
+// smaller.  Instances of one band form one launch (a size class).
+constexpr int BATCH_BANDS = 7;
+int size_band(int smem)
+{
+    int b = 0;
+    while (b < BATCH_BANDS - 1 && (long long)smem * 2 <= (long long)(SMEM_CAP >> b))
+        ++b;
+    return b;
+}
+
+// The slice tables of p's A and A^T for the sliced layout: T holds, for
+// each 32 rows of A, the offset of its slice (32 x its longest row), then
+// the end, then the same for A^T.  False when A is not valid CSR.
+bool slice_tables(const qp_problem_t *p, std::vector<int> &T)
+{
+    const int n = p->num_variables, m = p->num_constraints;
+    const int *rp = p->constraint_matrix->row_ptr, *ci = p->constraint_matrix->col_ind;
+    bool ok = rp[0] == 0;
+    for (int r = 0; ok && r < m; ++r)
+        ok = rp[r] <= rp[r + 1];
+    const int nnz = ok ? rp[m] : 0;
+    for (int k = 0; ok && k < nnz; ++k)
+        ok = ci[k] >= 0 && ci[k] < n;
+    if (!ok)
+        return false;
+    const int sa = slices(m), sat = slices(n);
+    T.resize(sa + 1 + sat + 1);
+    int o = 0;
+    for (int s = 0; s < sa; ++s) {
+        int mx = 0;
+        for (int r = 32 * s; r < std::min(32 * s + 32, m); ++r)
+            mx = std::max(mx, rp[r + 1] - rp[r]);
+        T[s] = o;
+        o += 32 * mx;
+    }
+    T[sa] = o;
+    std::vector<int> cnt(n, 0);
+    for (int k = 0; k < nnz; ++k)
+        cnt[ci[k]]++;
+    int *Tt = T.data() + sa + 1;
+    o = 0;
+    for (int s = 0; s < sat; ++s) {
+        int mx = 0;
+        for (int j = 32 * s; j < std::min(32 * s + 32, n); ++j)
+            mx = std::max(mx, cnt[j]);
+        Tt[s] = o;
+        o += 32 * mx;
+    }
+    Tt[sat] = o;
+    return true;
+}
+
+// The batch kernel's problem class (LP or diagonal Q, no cones, rows and
+// columns below 65536, a constraint matrix)
+bool batchable(const qp_problem_t *p, std::vector<double> &qd)
+{
+    const int n = p->num_variables, m = p->num_constraints;
+    return n > 0 && m > 0 && n < 65536 && m < 65536 && p->cones.num_cones == 0 && p->affine_cones.num_cones == 0 &&
+           p->constraint_matrix && diag_q(p, qd);
+}
+
 // smallest-group shape that holds the class's largest instance
 int default_shape(int max_smem, int max_dim)
 {
@@ -1050,51 +1113,11 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
                 std::fprintf(stderr, "[pdhcg_b200_solve_batch] problem %d is NULL.\n", i);
                 return -1;
             }
-            const int n = p->num_variables, m = p->num_constraints;
-            cand[i] = n > 0 && m > 0 && n < 65536 && m < 65536 && p->cones.num_cones == 0 &&
-                      p->affine_cones.num_cones == 0 && p->constraint_matrix && diag_q(p, qd);
+            cand[i] = batchable(p, qd);
         }
         parallel_for(count, [&](int i) {
-            if (!cand[i])
-                return;
-            const qp_problem_t *p = probs[i];
-            const int n = p->num_variables, m = p->num_constraints;
-            const int *rp = p->constraint_matrix->row_ptr, *ci = p->constraint_matrix->col_ind;
-            bool ok = rp[0] == 0;
-            for (int r = 0; ok && r < m; ++r)
-                ok = rp[r] <= rp[r + 1];
-            const int nnz = ok ? rp[m] : 0;
-            for (int k = 0; ok && k < nnz; ++k)
-                ok = ci[k] >= 0 && ci[k] < n;
-            if (!ok) {
+            if (cand[i] && !slice_tables(probs[i], tab[i]))
                 valid[i] = 0;
-                return;
-            }
-            const int sa = slices(m), sat = slices(n);
-            std::vector<int> &T = tab[i];
-            T.resize(sa + 1 + sat + 1);
-            int o = 0;
-            for (int s = 0; s < sa; ++s) {
-                int mx = 0;
-                for (int r = 32 * s; r < std::min(32 * s + 32, m); ++r)
-                    mx = std::max(mx, rp[r + 1] - rp[r]);
-                T[s] = o;
-                o += 32 * mx;
-            }
-            T[sa] = o;
-            std::vector<int> cnt(n, 0);
-            for (int k = 0; k < nnz; ++k)
-                cnt[ci[k]]++;
-            int *Tt = T.data() + sa + 1;
-            o = 0;
-            for (int s = 0; s < sat; ++s) {
-                int mx = 0;
-                for (int j = 32 * s; j < std::min(32 * s + 32, n); ++j)
-                    mx = std::max(mx, cnt[j]);
-                Tt[s] = o;
-                o += 32 * mx;
-            }
-            Tt[sat] = o;
         });
         for (int i = 0; i < count; ++i)
             if (cand[i] && !valid[i]) {
@@ -1182,10 +1205,11 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
         for (int i = 0; i < nb; ++i)
             order[i] = i;
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return inst[a].smem > inst[b].smem; });
+        // size classes: the runs of one size band in that order
         std::vector<std::pair<int, int>> classes; // [begin, end) in order
         for (int b = 0; b < nb;) {
             int e = b + 1;
-            while (e < nb && inst[order[e]].smem * 2 > inst[order[b]].smem)
+            while (e < nb && size_band(inst[order[e]].smem) == size_band(inst[order[b]].smem))
                 ++e;
             classes.push_back({b, e});
             b = e;
@@ -1348,7 +1372,10 @@ extern "C" int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *prob
                 max_smem = std::max(max_smem, inst[order[i]].smem);
                 max_dim = std::max(max_dim, std::max(inst[order[i]].n, inst[order[i]].m));
             }
-            int sh = o.shape >= 0 && o.shape < NSHAPES ? o.shape : default_shape(max_smem, max_dim);
+            const int bs = o.band_shape[size_band(inst[order[b]].smem)] - 1;
+            int sh = bs >= 0 && bs < NSHAPES ? bs
+                     : o.shape >= 0 && o.shape < NSHAPES ? o.shape
+                                                         : default_shape(max_smem, max_dim);
             if (sh < 0 || (long long)max_smem * (SHAPES[sh].bt / SHAPES[sh].group) > SMEM_CAP)
                 sh = default_shape(max_smem, max_dim);
             BData Dc = D;
@@ -1491,27 +1518,61 @@ extern "C" int pdhcg_b200_batch_autotune(int count, const qp_problem_t *const *p
         std::fprintf(stderr, "[pdhcg_b200_batch_autotune] invalid arguments.\n");
         return -1;
     }
-    std::vector<pdhcg_result_t *> res(count);
-    double best = INFINITY;
-    int best_shape = -1;
-    for (int sh = 0; sh < NSHAPES; ++sh) {
-        pdhcg_b200_batch_options_t o = *opts;
-        o.shape = sh;
-        cudaDeviceSynchronize();
-        auto t0 = std::chrono::steady_clock::now();
-        int rc = pdhcg_b200_solve_batch(count, probs, params, &o, res.data());
-        double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-        for (auto *r : res)
-            if (r)
-                pdhcg_result_free(r);
-        if (rc != 0)
-            return rc;
-        if (shape_ms)
-            shape_ms[sh] = ms;
-        if (ms < best) {
-            best = ms;
-            best_shape = sh;
+    // the batched instances by size band (at most 256 of each band)
+    std::vector<std::vector<const qp_problem_t *>> band(BATCH_BANDS);
+    {
+        std::vector<double> qd;
+        std::vector<int> T;
+        for (int i = 0; i < count; ++i) {
+            const qp_problem_t *p = probs[i];
+            if (!p || !batchable(p, qd) || !slice_tables(p, T))
+                continue;
+            const int n = p->num_variables, m = p->num_constraints;
+            const Layout Lo(n, m, T[slices(m)], T.back());
+            if (Lo.total > SMEM_CAP)
+                continue;
+            auto &v = band[size_band(Lo.total)];
+            if (v.size() < 256)
+                v.push_back(p);
         }
+    }
+    // every shape on every band's sample; a band keeps its fastest shape,
+    // opts->shape the fastest over all bands together
+    double tot[NSHAPES] = {};
+    for (int b = 0; b < BATCH_BANDS; ++b) {
+        if (band[b].empty())
+            continue;
+        std::vector<pdhcg_result_t *> res(band[b].size());
+        double best = INFINITY;
+        int best_shape = -1;
+        for (int sh = 0; sh < NSHAPES; ++sh) {
+            pdhcg_b200_batch_options_t o = *opts;
+            o.shape = sh;
+            for (int k = 0; k < BATCH_BANDS; ++k)
+                o.band_shape[k] = 0;
+            cudaDeviceSynchronize();
+            auto t0 = std::chrono::steady_clock::now();
+            int rc = pdhcg_b200_solve_batch((int)band[b].size(), band[b].data(), params, &o, res.data());
+            double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            for (auto *r : res)
+                if (r)
+                    pdhcg_result_free(r);
+            if (rc != 0)
+                return rc;
+            tot[sh] += ms;
+            if (ms < best) {
+                best = ms;
+                best_shape = sh;
+            }
+        }
+        opts->band_shape[b] = best_shape + 1;
+    }
+    int best_shape = 0;
+    for (int sh = 0; sh < NSHAPES; ++sh) {
+        if (shape_ms)
+            shape_ms[sh] = tot[sh];
+        if (tot[sh] < tot[best_shape])
+            best_shape = sh;
     }
     opts->shape = best_shape;
     return 0;

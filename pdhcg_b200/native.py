@@ -36,7 +36,7 @@ class Stats(C.Structure):
 
 class BatchOptions(C.Structure):
     """pdhcg_b200_batch_options_t (include/pdhcg_b200.h)."""
-    _fields_ = [("shape", C.c_int), ("reserved", C.c_int * 7)]
+    _fields_ = [("shape", C.c_int), ("band_shape", C.c_int * 7)]
 
 
 BATCH_SHAPES = 5

@@ -60,6 +60,14 @@ def test_batch_autotune_picks_a_shape(lib):
     assert lib.pdhcg_b200_batch_autotune(len(built), arr, C.byref(prm), C.byref(opts), ms) == 0
     assert 0 <= opts.shape < native.BATCH_SHAPES
     assert all(v > 0 for v in ms)
+    # horizons 10..60 span several size bands, each tuned on its own
+    tuned = [b for b in opts.band_shape if b != 0]
+    assert len(tuned) >= 2 and all(1 <= b <= native.BATCH_SHAPES for b in tuned)
+    res = (C.POINTER(capi.PdhcgResult) * len(built))()
+    assert lib.pdhcg_b200_solve_batch(len(built), arr, C.byref(prm), C.byref(opts), res) == 0
+    for p, r in zip(probs, res):
+        assert capi.TERMINATION_REASONS[r.contents.termination_reason] == "OPTIMAL"
+        lib.pdhcg_result_free(r)
     for b in built:
         lib.qp_problem_free(b[0])
 
