@@ -137,8 +137,8 @@ typedef struct {
 } pdhcg_b200_batch_options_t;
 
 /* Launch shapes {threads per CTA, threads per instance}:
- * 0 {128, 32}, 1 {256, 64}, 2 {256, 128}, 3 {256, 256}, 4 {512, 512}. */
-#define PDHCG_B200_BATCH_SHAPES 5
+ * 0 {128, 32}, 1 {256, 64}, 2 {256, 128}, 3 {256, 256}, 4 {512, 512}, 5 {1024, 1024}. */
+#define PDHCG_B200_BATCH_SHAPES 6
 
 void pdhcg_b200_default_batch_options(pdhcg_b200_batch_options_t *opts);
 int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *probs, const pdhg_parameters_t *params,

@@ -932,7 +932,7 @@ struct ClassStreams {
 struct Shape {
     int bt, group;
 };
-const Shape SHAPES[] = {{128, 32}, {256, 64}, {256, 128}, {256, 256}, {512, 512}};
+const Shape SHAPES[] = {{128, 32}, {256, 64}, {256, 128}, {256, 256}, {512, 512}, {1024, 1024}};
 constexpr int NSHAPES = sizeof(SHAPES) / sizeof(SHAPES[0]);
 
 template <int BT, int GROUP>
@@ -963,7 +963,8 @@ cudaError_t launch(int shape, const BData &D, const BParams &P, int smem_group, 
     case 1: return launch_shape<256, 64>(D, P, smem_group, sms, s);
     case 2: return launch_shape<256, 128>(D, P, smem_group, sms, s);
     case 3: return launch_shape<256, 256>(D, P, smem_group, sms, s);
-    default: return launch_shape<512, 512>(D, P, smem_group, sms, s);
+    case 4: return launch_shape<512, 512>(D, P, smem_group, sms, s);
+    default: return launch_shape<1024, 1024>(D, P, smem_group, sms, s);
     }
 }
 
@@ -1550,15 +1551,20 @@ extern "C" int pdhcg_b200_batch_autotune(int count, const qp_problem_t *const *p
             o.shape = sh;
             for (int k = 0; k < BATCH_BANDS; ++k)
                 o.band_shape[k] = 0;
-            cudaDeviceSynchronize();
-            auto t0 = std::chrono::steady_clock::now();
-            int rc = pdhcg_b200_solve_batch((int)band[b].size(), band[b].data(), params, &o, res.data());
-            double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-            for (auto *r : res)
-                if (r)
-                    pdhcg_result_free(r);
-            if (rc != 0)
-                return rc;
+            // an untimed pass first (the kernel's first launch, the buffers'
+            // growth), then the timed one
+            double ms = 0.0;
+            for (int pass = 0; pass < 2; ++pass) {
+                cudaDeviceSynchronize();
+                auto t0 = std::chrono::steady_clock::now();
+                int rc = pdhcg_b200_solve_batch((int)band[b].size(), band[b].data(), params, &o, res.data());
+                ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+                for (auto *r : res)
+                    if (r)
+                        pdhcg_result_free(r);
+                if (rc != 0)
+                    return rc;
+            }
             tot[sh] += ms;
             if (ms < best) {
                 best = ms;
