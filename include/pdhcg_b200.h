@@ -137,8 +137,9 @@ typedef struct {
 } pdhcg_b200_batch_options_t;
 
 /* Launch shapes {threads per CTA, threads per instance}:
- * 0 {128, 32}, 1 {256, 64}, 2 {256, 128}, 3 {256, 256}, 4 {512, 512}, 5 {1024, 1024}. */
-#define PDHCG_B200_BATCH_SHAPES 6
+ * 0 {128, 32}, 1 {256, 64}, 2 {256, 128}, 3 {256, 256}, 4 {512, 512}, 5 {1024, 1024},
+ * 6 {128, 128}. */
+#define PDHCG_B200_BATCH_SHAPES 7
 
 void pdhcg_b200_default_batch_options(pdhcg_b200_batch_options_t *opts);
 int pdhcg_b200_solve_batch(int count, const qp_problem_t *const *probs, const pdhg_parameters_t *params,

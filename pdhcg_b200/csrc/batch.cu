@@ -932,7 +932,7 @@ struct ClassStreams {
 struct Shape {
     int bt, group;
 };
-const Shape SHAPES[] = {{128, 32}, {256, 64}, {256, 128}, {256, 256}, {512, 512}, {1024, 1024}};
+const Shape SHAPES[] = {{128, 32}, {256, 64}, {256, 128}, {256, 256}, {512, 512}, {1024, 1024}, {128, 128}};
 constexpr int NSHAPES = sizeof(SHAPES) / sizeof(SHAPES[0]);
 
 template <int BT, int GROUP>
@@ -964,7 +964,8 @@ cudaError_t launch(int shape, const BData &D, const BParams &P, int smem_group, 
     case 2: return launch_shape<256, 128>(D, P, smem_group, sms, s);
     case 3: return launch_shape<256, 256>(D, P, smem_group, sms, s);
     case 4: return launch_shape<512, 512>(D, P, smem_group, sms, s);
-    default: return launch_shape<1024, 1024>(D, P, smem_group, sms, s);
+    case 5: return launch_shape<1024, 1024>(D, P, smem_group, sms, s);
+    default: return launch_shape<128, 128>(D, P, smem_group, sms, s);
     }
 }
 
@@ -1062,7 +1063,7 @@ int default_shape(int max_smem, int max_dim)
         if ((long long)max_smem * (SHAPES[sh].bt / SHAPES[sh].group) <= cap)
             return sh;
     }
-    return (long long)max_smem <= cap ? NSHAPES - 1 : -1;
+    return (long long)max_smem <= cap ? 4 : -1; // {512, 512}: one instance per CTA
 }
 
 } // namespace

@@ -39,7 +39,7 @@ class BatchOptions(C.Structure):
     _fields_ = [("shape", C.c_int), ("band_shape", C.c_int * 7)]
 
 
-BATCH_SHAPES = 6
+BATCH_SHAPES = 7
 
 
 class BatchStats(C.Structure):

@@ -17,7 +17,7 @@ PRM = {"termination_criteria.eps_optimal_relative": EPS, "termination_criteria.e
        "termination_criteria.iteration_limit": 200000, "termination_criteria.time_sec_limit": 60.0}
 
 
-@pytest.mark.parametrize("shape", [-1, 0, 2, 4, 5])
+@pytest.mark.parametrize("shape", [-1, 0, 2, 4, 5, 6])
 def test_batch_matches_single_solves(lib, shape):
     probs = instances.mpc_batch(seed=5, count=24, tmin=10, tmax=100)
     got = native.solve_batch(probs, PRM, shape=shape)
