@@ -801,12 +801,19 @@ void parallel_for(int count, F &&f)
         return;
     }
     std::atomic<int> next{0};
+    auto work = [&]() {
+        for (int i; (i = next.fetch_add(1)) < count;)
+            f(i);
+    };
     std::vector<std::thread> pool;
-    for (int t = 0; t < nt; ++t)
-        pool.emplace_back([&]() {
-            for (int i; (i = next.fetch_add(1)) < count;)
-                f(i);
-        });
+    for (int t = 1; t < nt; ++t) {
+        try {
+            pool.emplace_back(work);
+        } catch (...) { // fewer threads: the ones there take the rest
+            break;
+        }
+    }
+    work(); // the calling thread takes part
     for (auto &th : pool)
         th.join();
 }

@@ -125,11 +125,14 @@ void staged_upload(void *dst, const void *src, size_t bytes, cudaStream_t s)
         const size_t part = (len + nt - 1) / nt;
         char *chunk = buf[b];
         std::vector<std::thread> th;
-        for (int t = 1; t < nt && (size_t)t * part < len; ++t)
-            th.emplace_back([=]() {
-                const size_t a = (size_t)t * part, e = std::min(len, a + part);
+        for (int t = 1; t < nt && (size_t)t * part < len; ++t) {
+            const size_t a = (size_t)t * part, e = std::min(len, a + part);
+            try {
+                th.emplace_back([=]() { std::memcpy(chunk + a, from + off + a, e - a); });
+            } catch (...) { // no thread to be had: this part here
                 std::memcpy(chunk + a, from + off + a, e - a);
-            });
+            }
+        }
         std::memcpy(chunk, from + off, std::min(len, part));
         for (auto &x : th)
             x.join();
