@@ -36,14 +36,15 @@ EPS = 1e-6
 METRIC = "time-to-1e-6 KKT (s) & SpMV GB/s: mixed/warm-start vs plain FP64, 1 B200"
 WORKLOAD = "soc_qp: n=1e6 (20000 SOC blocks x 50), m=5e5 eq rows, 10 nnz/row, diag Q, eps 1e-6"
 
+# DRAM read + write bytes of one step of the SOC-QP workload (both
+# kernels), from an ncu capture of the two step kernels on it
+STEP_TRAFFIC = {"f64": 202.5e6, "f32": 121.4e6}
+# random 4- / 8-byte gathers per second of one B200 through L1TEX, measured
+# by pdhcg_b200/csrc/probes/gather_ceiling.cu
+GATHER_RATE = 1.95e11
+
 # Single-instance workloads: the generator, whether the mixed form is timed
 # beside FP64, and what keeps the timed solves out of L2.
-# DRAM read + write bytes of one step of the SOC-QP workload (both
-# kernels), measured by ncu (profiles/step_kernels_soc_qp_n1e6.md)
-STEP_TRAFFIC = {"f64": 202.5e6, "f32": 121.4e6}
-# random 4- / 8-byte gathers per second of one B200 through L1TEX
-# (profiles/spmv_gather_ceiling_b200.md)
-GATHER_RATE = 1.95e11
 
 WORKLOADS = {
     "soc_qp": {"make": lambda scale, r: instances.soc_qp(seed=2 + r, scale=scale), "desc": WORKLOAD,
@@ -262,8 +263,8 @@ def run_ours(args):
     def roof(tstats):
         step_ms = tstats["step_kernel_ms"] / max(1, tstats["step_kernel_launches"])
         ach = tstats["step_bytes"] / (step_ms * 1e-3) / 1e9 if step_ms > 0 else None
-        # DRAM bytes (read + write) of one step's kernels, from the ncu capture of
-        # profiles/step_kernels_soc_qp_n1e6.md, weighted like the timed steps
+        # DRAM bytes (read + write) of one step's kernels, from the ncu
+        # capture of the step kernels, weighted like the timed steps
         traffic = None
         if args.workload == "soc_qp" and args.scale == 1.0 and tstats["step_kernel_launches"] > 0:
             f32 = tstats["fp32_iterations"] / tstats["step_kernel_launches"]
