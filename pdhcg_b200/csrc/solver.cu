@@ -12,6 +12,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cfloat>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <csignal>
@@ -140,6 +142,31 @@ void staged_upload(void *dst, const void *src, size_t bytes, cudaStream_t s)
         CK(cudaEventRecord(ev[b], s));
         pending[b] = true;
     }
+}
+
+// f(begin, end) over [0, n) in up to 8 chunks on host threads, the calling
+// thread taking the first (the problem checks of a device-problem build);
+// chunks run at once, so f writes nothing that another chunk writes
+template <typename F>
+void host_chunks(long long n, F &&f)
+{
+    const int nt = n < (1 << 16) ? 1 : (int)std::min<unsigned>(8u, std::max(1u, std::thread::hardware_concurrency()));
+    if (nt <= 1) {
+        f(0LL, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t) {
+        const long long a = n * t / nt, e = n * (t + 1) / nt;
+        try {
+            th.emplace_back([&f, a, e]() { f(a, e); });
+        } catch (...) { // no thread to be had: this chunk here
+            f(a, e);
+        }
+    }
+    f(0LL, n / nt);
+    for (auto &x : th)
+        x.join();
 }
 
 // The device's default memory pool keeps what solves free (no release
@@ -518,10 +545,23 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
         d.lc = ar.upload(p->constraint_lower_bound, d.m, s);
         d.uc = ar.upload(p->constraint_upper_bound, d.m, s);
         d.g = ar.upload(p->affine_cone_offset, d.m, s);
-        for (int i = 0; i < d.m; ++i) {
-            d.has_g |= p->affine_cone_offset[i] != 0.0;
-            d.eq_rows &= p->constraint_lower_bound[i] == p->constraint_upper_bound[i] &&
-                         std::isfinite(p->constraint_lower_bound[i]);
+        {
+            const double *gg = p->affine_cone_offset, *lo = p->constraint_lower_bound,
+                         *up = p->constraint_upper_bound;
+            std::atomic<int> any_g{0}, unequal{0};
+            host_chunks(d.m, [&](long long a, long long e) {
+                int hg = 0, eq = 1;
+                for (long long i = a; i < e; ++i) {
+                    hg |= gg[i] != 0.0;
+                    eq &= (lo[i] == up[i]) & (std::fabs(lo[i]) <= DBL_MAX); // equal and finite
+                }
+                if (hg)
+                    any_g = 1;
+                if (!eq)
+                    unequal = 1;
+            });
+            d.has_g = d.has_g || any_g;
+            d.eq_rows = d.eq_rows && !unequal;
         }
         if (p->dual_start)
             d.dstart = ar.upload(p->dual_start, d.m, s);
@@ -531,8 +571,18 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
     d.u = ar.upload(p->variable_upper_bound, d.n, s);
     if (p->primal_start)
         d.pstart = ar.upload(p->primal_start, d.n, s);
-    for (int i = 0; i < d.n; ++i)
-        d.box_free &= !std::isfinite(p->variable_lower_bound[i]) && !std::isfinite(p->variable_upper_bound[i]);
+    {
+        const double *lo = p->variable_lower_bound, *up = p->variable_upper_bound;
+        std::atomic<int> boxed{0};
+        host_chunks(d.n, [&](long long a, long long e) {
+            int fin = 0; // a finite bound
+            for (long long i = a; i < e; ++i)
+                fin |= (std::fabs(lo[i]) <= DBL_MAX) | (std::fabs(up[i]) <= DBL_MAX);
+            if (fin)
+                boxed = 1;
+        });
+        d.box_free = d.box_free && !boxed;
+    }
 
     int nnzq = (p->objective_sparse_matrix && p->objective_sparse_matrix->row_ptr)
                    ? p->objective_sparse_matrix_num_nonzeros
@@ -545,14 +595,18 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
     else if (nnzr > 0)
         d.qtype = nnzq > 0 ? PDHCG_LOW_RANK_PLUS_SPARSE_Q : PDHCG_LOW_RANK_Q;
     else {
-        d.qtype = PDHCG_DIAG_Q;
-        const CsrComponent *Q = p->objective_sparse_matrix;
-        for (int i = 0; i < d.n && d.qtype == PDHCG_DIAG_Q; ++i)
-            for (int k = Q->row_ptr[i]; k < Q->row_ptr[i + 1]; ++k)
-                if (Q->col_ind[k] != i) {
-                    d.qtype = PDHCG_SPARSE_Q;
-                    break;
-                }
+        // diagonal unless some entry lies off the diagonal
+        const int *qrp = p->objective_sparse_matrix->row_ptr, *qci = p->objective_sparse_matrix->col_ind;
+        std::atomic<int> off{0};
+        host_chunks(d.n, [&](long long a, long long e) {
+            int o = 0;
+            for (long long i = a; i < e; ++i)
+                for (int k = qrp[i]; k < qrp[i + 1]; ++k)
+                    o |= qci[k] != (int)i;
+            if (o)
+                off = 1;
+        });
+        d.qtype = off ? PDHCG_SPARSE_Q : PDHCG_DIAG_Q;
     }
     if (d.qtype != PDHCG_NON_Q && nnzq > 0) {
         const CsrComponent *Q = p->objective_sparse_matrix;
@@ -620,10 +674,14 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
         // (their length does not set the class)
         if (!(p->cones.type[b] == CONE_PSD && len > 32 * 8))
             maxlen = std::max(maxlen, len);
-        for (int i = 0; i < len; ++i) {
-            int j = p->cones.start_idx[b] + i;
-            in_cone[j] = 1;
-            d.cone_box |= std::isfinite(p->variable_lower_bound[j]) || std::isfinite(p->variable_upper_bound[j]);
+        {
+            const int st = p->cones.start_idx[b];
+            const double *lo = p->variable_lower_bound + st, *up = p->variable_upper_bound + st;
+            std::fill(in_cone.begin() + st, in_cone.begin() + st + len, (char)1);
+            int fin = 0;
+            for (int i = 0; i < len; ++i)
+                fin |= (std::fabs(lo[i]) <= DBL_MAX) | (std::fabs(up[i]) <= DBL_MAX);
+            d.cone_box = d.cone_box || fin;
         }
         d.psd_off.push_back(d.psd_total);
         if (p->cones.type[b] == CONE_PSD) {
@@ -637,9 +695,14 @@ std::unique_ptr<DeviceProblem> make_device_problem(const qp_problem_t *p, cudaSt
     }
     int nc = (int)d.cone_start.size();
     if (nc > 0) {
+        size_t nfree = 0;
         for (int i = 0; i < d.n; ++i)
-            if (!in_cone[i])
-                d.free_idx.push_back(i);
+            nfree += !in_cone[i];
+        d.free_idx.reserve(nfree);
+        if (nfree > 0)
+            for (int i = 0; i < d.n; ++i)
+                if (!in_cone[i])
+                    d.free_idx.push_back(i);
         d.S = slots_class(maxlen);
         d.cst = ar.upload(d.cone_start.data(), nc, s);
         d.clen = ar.upload(d.cone_len.data(), nc, s);
